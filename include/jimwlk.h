@@ -1,0 +1,230 @@
+/*
+ * jimwlk.h -- C ABI of libjimwlk, a B200 (sm_100a) JIMWLK Langevin engine.
+ *
+ * Two layers:
+ *
+ *  1. Call-for-call replacements of the reference solver's hot-path functions
+ *     (ElsevierSoftwareX/SOFTX-D-21-00092: field.h, mpi_fftw_class.h,
+ *     su3_matrix.h, config.h), operating on device-resident fields.  A port of
+ *     main_optimized.cpp's evolution loop replaces each reference call with
+ *     the jw_* call named beside it and gets the reference's results (FP64,
+ *     same operation order, noise from a seeded counter-based stream instead
+ *     of the reference's clock-seeded ranlux24).
+ *
+ *  2. The batched engine: many independent events of (possibly different)
+ *     lattice sizes resident on one GPU, advanced by fused kernels -- noise
+ *     generation, the V xi V^dagger rotation, both momentum-space convolutions
+ *     (FFT -> kernel multiply -> inverse FFT) and the SU(3) update -- in FP64
+ *     or mixed precision (FP32 transforms, FP64 exponentials and V), with the
+ *     dipole correlator accumulated on the device.
+ *
+ * Conventions
+ *  - Every function returns a jw_status (0 = JW_OK, negative = error).
+ *  - Host field arrays use the reference's layout (field.h:73, 170-173):
+ *    site-major, interleaved complex double, component k (row-major 3x3 index
+ *    3*row+col for t = 9; k = 0 for t = 1) of site (x, y) at complex offset
+ *    (x*Ny + y)*t + k.
+ *  - Work is ordered on the context's / engine's CUDA stream.  Functions that
+ *    copy to or from the host synchronise that stream; the others only
+ *    enqueue.  jw_context_sync / jw_engine_sync wait for completion and
+ *    return the first device-side error flagged since the previous sync
+ *    (JW_ENOCONV when the QL eigensolver did not converge at some site,
+ *    JW_ENAN for a non-finite result).
+ *  - A context or engine may be used from one host thread at a time.
+ *  - Lattice sides are powers of two from 8 to 2048 (Nx == Ny).
+ */
+#ifndef JIMWLK_H
+#define JIMWLK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int jw_status;
+#define JW_OK 0
+#define JW_EINVAL (-1)       /* bad argument (size, enum, null pointer, mismatched fields) */
+#define JW_ENOMEM (-2)       /* device or host allocation failed / footprint over budget */
+#define JW_ECUDA (-3)        /* a CUDA runtime call failed */
+#define JW_ENOCONV (-4)      /* eigensolver QL fallback did not converge at some site */
+#define JW_ENAN (-5)         /* non-finite value produced */
+#define JW_ETIMEOUT (-6)     /* a bounded wait ran out */
+#define JW_EUNSUPPORTED (-7) /* option the reference does not define (e.g. HATTA in momentum space) */
+#define JW_ENOTFOUND (-8)    /* unknown event / request id */
+#define JW_EBUSY (-9)        /* resource in use */
+
+const char* jw_status_string(jw_status s);
+
+/* ------------------------------------------------------------------ config */
+/* Enumerations with the reference's values (config.h:38-42). */
+#define JW_POSITION_EVOLUTION 0
+#define JW_MOMENTUM_EVOLUTION 1
+#define JW_SQRT_COUPLING_CONSTANT 0
+#define JW_NOISE_COUPLING_CONSTANT 1
+#define JW_HATTA_COUPLING_CONSTANT 2
+/* Fixed coupling (alpha_s folded into `step`): the reference's plain
+ * generate_gaussian (field.h:2116) with the NOISE_COUPLING_CONSTANT kernel
+ * factor 1 (field.h:2035-2036, 2049-2050).  main_optimized.cpp:243-247 pairs
+ * NOISE with the site-indexed noise factor instead, so this value exists only
+ * in this library. */
+#define JW_FIXED_COUPLING_CONSTANT 3
+#define JW_LINEAR_KERNEL 0
+#define JW_SIN_KERNEL 1
+
+/* class config (config.h:44-73); Nx, Ny are compile-time macros there
+ * (config.h:31-32) and run-time fields here. */
+typedef struct jw_config {
+    int Nx, Ny;
+    int stat;
+    double mu;
+    double mass;
+    int elementaryWilsonLines;
+    char file_name[64];
+    int langevin_steps;
+    int measurements;
+    double step;
+    int EvolutionChoice;
+    int CouplingChoice;
+    int KernelChoice;
+    uint64_t seed; /* noise stream key (the reference seeds from the clock) */
+} jw_config;
+
+/* Defaults of config.h:60-73 with Nx = Ny = 64, seed = 1. */
+jw_status jw_config_defaults(jw_config* cfg);
+/* config::read_config_from_file (config.h:76-136): same line grammar; mu,
+ * mass and step are parsed through float exactly as the reference does, so
+ * the doubles match it bit for bit.  Unknown choice strings keep the
+ * previous value, as in the reference. */
+jw_status jw_config_read(jw_config* cfg, const char* path);
+
+/* ------------------------------------------------------------------ context & fields */
+typedef struct jw_context jw_context;
+typedef struct jw_field jw_field;
+
+/* Replaces the set-up of main_optimized.cpp:68-92 (mpi_class, momenta,
+ * positions, fftw2D::init2D): binds device `device`, creates a stream and the
+ * FFT twiddle tables for cfg->Nx. */
+jw_status jw_context_create(const jw_config* cfg, int device, jw_context** out);
+jw_status jw_context_destroy(jw_context* ctx);
+jw_status jw_context_sync(jw_context* ctx);
+/* The context's cudaStream_t, as void*. */
+void* jw_context_stream(jw_context* ctx);
+
+/* lfield<double,t>(Nxl, Nyl) (field.h:152-283): t = 1 or 9, zero-filled. */
+jw_status jw_field_create(jw_context* ctx, int t, jw_field** out);
+jw_status jw_field_destroy(jw_field* f);
+/* Host <-> device in the reference layout (2*t*Nx*Ny doubles). */
+jw_status jw_field_set(jw_field* f, const double* host);
+jw_status jw_field_get(const jw_field* f, double* host);
+/* lfield::operator= (field.h:301-318). */
+jw_status jw_field_copy(jw_field* dst, const jw_field* src);
+/* lfield::setToUnit / setToZero (field.h:181-211). */
+jw_status jw_field_set_unit(jw_field* f);
+jw_status jw_field_set_zero(jw_field* f);
+
+/* ------------------------------------------------------------------ reference hot-path calls */
+/* fftw2D::execute2D(lfield*, dir) (mpi_fftw_class.h:191-315): in-place 2-D
+ * DFT of every component, dir = 1 X->K (exp(-i...)), dir = 0 K->X, then
+ * x 1/sqrt(Nx*Ny). */
+jw_status jw_execute2D(jw_context* ctx, jw_field* f, int dir);
+
+/* generate_gaussian (field.h:2116-2243) and, when with_coupling != 0,
+ * generate_gaussian_with_noise_coupling_constant (field.h:2245-2365): 16 unit
+ * normals per site from the stream of (ctx seed, step_index), embedded as
+ * sum_a n_a lambda_a into xi_x and sum_a m_a lambda_a into xi_y. */
+jw_status jw_generate_gaussian(jw_context* ctx, jw_field* xi_x, jw_field* xi_y, uint64_t step_index,
+                               int with_coupling);
+
+/* lfield::setMVModel (field.h:683-757): 8 normals per site from the MV stream
+ * of (ctx seed, slice) times sigma = g*mu/sqrt(Ny_slices), embedded. */
+jw_status jw_set_mv_model(jw_context* ctx, jw_field* f, int slice, double g, double mu, int ny_slices);
+/* lfield::solvePoisson (field.h:867-877): f(k) *= -g / (-phat2(k) + mass^2). */
+jw_status jw_solve_poisson(jw_context* ctx, jw_field* f, double mass, double g);
+/* lfield::operator*= (field.h:337-365): V(x) <- V(x) exp(+i f(x)). */
+jw_status jw_mul_exp(jw_context* ctx, jw_field* V, const jw_field* f);
+
+/* prepare_A_local(out, xi_x, xi_y, momenta, mpi, Coupling, Kernel) (field.h:1998-2075). */
+jw_status jw_prepare_A_local(jw_context* ctx, jw_field* out, const jw_field* xi_x, const jw_field* xi_y,
+                             int coupling, int kernel);
+/* uxiulocal (field.h:1892-1933): ux = V xi_x V^dagger, uy = V xi_y V^dagger. */
+jw_status jw_uxiulocal(jw_context* ctx, jw_field* ux, jw_field* uy, const jw_field* V, const jw_field* xi_x,
+                       const jw_field* xi_y);
+/* update_uf (field.h:1966-1996): V <- exp(+i sqrt(step) B) V exp(-i sqrt(step) A). */
+jw_status jw_update_uf(jw_context* ctx, jw_field* V, const jw_field* B, const jw_field* A, double step);
+
+/* lfield::trace (field.h:1375-1432): corr(k) = tr(Vk Vk^dagger)/(Nx Ny)^2, corr t = 1. */
+jw_status jw_trace(jw_context* ctx, const jw_field* Vk, jw_field* corr);
+/* gfield::average_and_symmetrize (field.h:1460-1492). */
+jw_status jw_average_and_symmetrize(jw_context* ctx, jw_field* corr);
+/* gfield::reduce(sum, err, mpi) (field.h:1521-1536): sum += corr, err += corr^2. */
+jw_status jw_reduce(jw_context* ctx, const jw_field* corr, jw_field* sum, jw_field* err);
+/* print(measurement, sum, err, momenta, x, mpi, fileroot) (field.h:2521-2547):
+ * appends to <fileroot>_<Nx>_<Ny>_mpi1_r0.dat. */
+jw_status jw_print(jw_context* ctx, int measurement, const jw_field* sum, const jw_field* err, double x,
+                   const char* fileroot);
+
+/* Whole-driver conveniences built from the calls above (main_optimized.cpp). */
+/* :88, 178-191 -- MV initial condition into V with the config's mu, mass,
+ * elementaryWilsonLines (g = 1, mu_MV = mu/Nx). */
+jw_status jw_initial_condition(jw_context* ctx, jw_field* V);
+/* :243-269, 304 -- n momentum-space Langevin steps with global step indices
+ * step0 .. step0+n-1 and the config's coupling, kernel and step. */
+jw_status jw_evolve_momentum(jw_context* ctx, jw_field* V, uint64_t step0, int n);
+
+/* ------------------------------------------------------------------ batched engine */
+#define JW_PRECISION_FP64 0  /* FP64 everywhere */
+#define JW_PRECISION_MIXED 1 /* FP32 noise/rotation/transforms, FP64 exponentials, V, reunitarisation, sums */
+
+typedef struct jw_engine_options {
+    int precision;        /* JW_PRECISION_* */
+    int reunitarize;      /* project V back onto SU(3) after every step (FP64) */
+    size_t max_bytes;     /* device-memory budget for events and workspaces; 0 = 90% of free */
+    int max_batch;        /* events advanced per launch group (0 = all) */
+} jw_engine_options;
+
+typedef struct jw_event_desc {
+    int N;                /* lattice side */
+    int ny_slices;        /* MV slices (elementaryWilsonLines) */
+    double mu;            /* config mu (mu_MV = mu/N, g = 1) */
+    double mass;          /* config mass (Poisson mass = mass * mu_MV) */
+    double step;          /* Langevin step (config step) */
+    int coupling;         /* JW_SQRT_COUPLING_CONSTANT or JW_NOISE_COUPLING_CONSTANT */
+    int kernel;           /* JW_SIN_KERNEL or JW_LINEAR_KERNEL */
+    uint64_t seed;        /* noise stream key of this event */
+} jw_event_desc;
+
+typedef struct jw_engine jw_engine;
+
+jw_status jw_engine_create(const jw_engine_options* opt, int device, jw_engine** out);
+jw_status jw_engine_destroy(jw_engine* e);
+jw_status jw_engine_sync(jw_engine* e);
+void* jw_engine_stream(jw_engine* e);
+/* Device bytes an event of this description holds while resident. */
+size_t jw_engine_event_bytes(const jw_engine* e, const jw_event_desc* d);
+/* Admit an event (allocates its V and accumulators; V = 1). */
+jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, int* event_id);
+jw_status jw_engine_remove_event(jw_engine* e, int event_id);
+/* MV initial condition for the listed events (main_optimized.cpp:178-191). */
+jw_status jw_engine_init_mv(jw_engine* e, const int* ids, int n);
+/* Host V in the reference layout. */
+jw_status jw_engine_set_V(jw_engine* e, int event_id, const double* host);
+jw_status jw_engine_get_V(jw_engine* e, int event_id, double* host);
+/* Advance the listed events by nsteps Langevin steps each (fused kernels). */
+jw_status jw_engine_step(jw_engine* e, const int* ids, int n, int nsteps);
+/* Dipole measurement of the listed events: C(k) of main_optimized.cpp:321-334
+ * accumulated (sum, sum of squares) into each event's FP64 accumulators. */
+jw_status jw_engine_measure(jw_engine* e, const int* ids, int n);
+/* Accumulated sum / err (N*N complex each, reference layout t = 1) and count. */
+jw_status jw_engine_get_correlator(jw_engine* e, int event_id, double* sum, double* err, int* nmeas);
+/* Reset an event's accumulators. */
+jw_status jw_engine_reset_correlator(jw_engine* e, int event_id);
+/* Steps taken so far by an event (its next noise index). */
+jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

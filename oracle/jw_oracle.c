@@ -626,19 +626,20 @@ void jwo_evolve_momentum(double* V, int N, int steps, uint64_t step0, double ste
     double* B = (double*)malloc(sizeof(double) * 18 * vol);
     double* ux = (double*)malloc(sizeof(double) * 18 * vol);
     double* uy = (double*)malloc(sizeof(double) * 18 * vol);
+    const int kc = (coupling == JWO_FIXED_COUPLING) ? JWO_NOISE_COUPLING : coupling;
     for (int s = 0; s < steps; ++s) {
         jwo_langevin_normals(seed, step0 + (uint64_t)s, N, z);
         jwo_generate_gaussian(z, xx, xy, N, coupling == JWO_NOISE_COUPLING);
         jwo_execute2D(xx, N, 9, 1);
         jwo_execute2D(xy, N, 9, 1);
-        jwo_prepare_A_local(A, xx, xy, N, coupling, kernel);
+        jwo_prepare_A_local(A, xx, xy, N, kc, kernel);
         jwo_execute2D(A, N, 9, 0);
         jwo_execute2D(xx, N, 9, 0);
         jwo_execute2D(xy, N, 9, 0);
         jwo_uxiulocal(ux, uy, V, xx, xy, N);
         jwo_execute2D(ux, N, 9, 1);
         jwo_execute2D(uy, N, 9, 1);
-        jwo_prepare_A_local(B, ux, uy, N, coupling, kernel);
+        jwo_prepare_A_local(B, ux, uy, N, kc, kernel);
         jwo_execute2D(B, N, 9, 0);
         jwo_update_uf(V, B, A, N, step);
     }

@@ -27,6 +27,8 @@ extern "C" {
 /* enum values identical to config.h:38-42 */
 enum { JWO_POSITION_EVOLUTION = 0, JWO_MOMENTUM_EVOLUTION = 1 };
 enum { JWO_SQRT_COUPLING = 0, JWO_NOISE_COUPLING = 1, JWO_HATTA_COUPLING = 2 };
+/* fixed coupling: plain generate_gaussian + the NOISE kernel factor 1 (see jwo_evolve_momentum) */
+enum { JWO_FIXED_COUPLING = 3 };
 enum { JWO_LINEAR_KERNEL = 0, JWO_SIN_KERNEL = 1 };
 
 /* ---- noise stream (the engine's definition; the reference's RNG is clock-seeded) ---- */
@@ -64,7 +66,9 @@ void jwo_reduce(const double* corr, double* sum, double* err, int N);
  * Poisson mass = mass_cfg * g^2 * mu_MV. */
 void jwo_initial_condition(double* V, int N, double mu_cfg, double mass_cfg, int nslices, uint64_t seed);
 /* main_optimized.cpp:243-269, 304: `steps` momentum-space steps starting at
- * global step index step0. */
+ * global step index step0.  coupling = SQRT or NOISE as in the reference (NOISE
+ * takes generate_gaussian_with_noise_coupling_constant); FIXED takes plain
+ * generate_gaussian with the NOISE kernel factor 1. */
 void jwo_evolve_momentum(double* V, int N, int steps, uint64_t step0, double step, int coupling,
                          int kernel, uint64_t seed);
 /* main_optimized.cpp:321-334: FFT(V), trace, symmetrise, reduce into sum/err. */

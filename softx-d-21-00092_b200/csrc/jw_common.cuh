@@ -1,0 +1,426 @@
+// jw_common.cuh -- device building blocks shared by every kernel of libjimwlk:
+// complex arithmetic on float2/double2, the counter-based noise stream, the
+// Gell-Mann embedding used by the reference, 3x3 products and the FP64
+// Hermitian exponential (eigen route).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace jw {
+
+// ------------------------------------------------------------------ complex
+template <typename T> struct cplx_t;
+template <> struct cplx_t<float> { using type = float2; };
+template <> struct cplx_t<double> { using type = double2; };
+template <typename T> using C2 = typename cplx_t<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ C2<T> mk(T r, T i) { C2<T> z; z.x = r; z.y = i; return z; }
+template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) { a.x += b.x; a.y += b.y; return a; }
+template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
+    V c; c.x = a.x * b.x - a.y * b.y; c.y = a.x * b.y + a.y * b.x; return c;
+}
+template <typename V> __host__ __device__ __forceinline__ V cconj(V a) { a.y = -a.y; return a; }
+template <typename V, typename S> __host__ __device__ __forceinline__ V cscale(V a, S s) { a.x *= s; a.y *= s; return a; }
+template <typename V> __host__ __device__ __forceinline__ auto cabs2(V a) -> decltype(a.x) { return a.x * a.x + a.y * a.y; }
+// a * conj(b)
+template <typename V> __host__ __device__ __forceinline__ V cmulc(V a, V b) {
+    V c; c.x = a.x * b.x + a.y * b.y; c.y = a.y * b.x - a.x * b.y; return c;
+}
+// multiply by (sign * i)
+template <typename V, typename S> __host__ __device__ __forceinline__ V cmul_si(V a, S sign) {
+    V c; c.x = -sign * a.y; c.y = sign * a.x; return c;
+}
+
+// ------------------------------------------------------------------ noise
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), the engine's noise
+// generator.  Counter layout of the stream (shared with the oracle):
+//   Langevin step s, site i, call c in 0..3: {i, lo32(s), 0x4A570000|c, hi32(s)}
+//   MV slice l,      site i, call c in 0..1: {i, l,       0x4D560000|c, 0}
+//   key = {lo32(seed), hi32(seed)}
+// Each call yields 4 words -> 2 Box-Muller pairs -> 4 unit normals; the 16
+// Langevin normals of a site are z[4c+j] and enter the reference's draw order
+// n_k = z[2k], m_k = z[2k+1] (field.h:2170-2173); the 8 MV normals are z[a].
+constexpr uint32_t kTagLangevin = 0x4A570000u;
+constexpr uint32_t kTagMV = 0x4D560000u;
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Box-Muller in FP64: u = (r + 1/2) 2^-32, z0 = sqrt(-2 ln u0) cos(2 pi u1),
+// z1 = sqrt(-2 ln u0) sin(2 pi u1).
+__device__ __forceinline__ void box_muller(uint32_t r0, uint32_t r1, double& z0, double& z1) {
+    const double u0 = ((double)r0 + 0.5) * 2.3283064365386963e-10;
+    const double u1 = ((double)r1 + 0.5) * 2.3283064365386963e-10;
+    const double rad = sqrt(-2.0 * log(u0));
+    double s, c;
+    sincos(6.283185307179586 * u1, &s, &c);
+    z0 = rad * c;
+    z1 = rad * s;
+}
+
+// Box-Muller in FP32 for the same words: ln u0 is taken as log(u0) below 1/2
+// and as log1p(-(1-u0)) above, with 1-u0 formed from ~r0, so that the result
+// carries full single-precision relative accuracy at both ends.
+__device__ __forceinline__ void box_muller(uint32_t r0, uint32_t r1, float& z0, float& z1) {
+    float lg;
+    if (r0 < 0x80000000u) {
+        lg = logf(((float)r0 + 0.5f) * 2.3283064365386963e-10f);
+    } else {
+        lg = log1pf(-(((float)(~r0) + 0.5f) * 2.3283064365386963e-10f));
+    }
+    const float rad = sqrtf(-2.0f * lg);
+    float s, c;
+    sincospif(2.0f * (((float)r1 + 0.5f) * 2.3283064365386963e-10f), &s, &c);
+    z0 = rad * c;
+    z1 = rad * s;
+}
+
+template <typename T>
+__device__ __forceinline__ void langevin_normals(uint64_t seed, uint64_t step, uint32_t site, T z[16]) {
+    const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+#pragma unroll
+    for (uint32_t c = 0; c < 4; ++c) {
+        uint4 r = philox4x32_10(make_uint4(site, (uint32_t)step, kTagLangevin | c, (uint32_t)(step >> 32)), key);
+        box_muller(r.x, r.y, z[4 * c + 0], z[4 * c + 1]);
+        box_muller(r.z, r.w, z[4 * c + 2], z[4 * c + 3]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void mv_normals(uint64_t seed, uint32_t slice, uint32_t site, T z[8]) {
+    const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+#pragma unroll
+    for (uint32_t c = 0; c < 2; ++c) {
+        uint4 r = philox4x32_10(make_uint4(site, slice, kTagMV | c, 0u), key);
+        box_muller(r.x, r.y, z[4 * c + 0], z[4 * c + 1]);
+        box_muller(r.z, r.w, z[4 * c + 2], z[4 * c + 3]);
+    }
+}
+
+// ------------------------------------------------------------------ Gell-Mann basis
+// The reference embeds 8 real numbers as sum_a n_a L_a with the matrices it
+// writes out in generate_gaussian / setMVModel (field.h:2176-2231, 716-746):
+//   L0: (0,1)=(1,0)=1          L1: (0,1)=+i, (1,0)=-i     L2: diag(1,-1,0)
+//   L3: (0,2)=(2,0)=1          L4: (0,2)=+i, (2,0)=-i     L5: (1,2)=(2,1)=1
+//   L6: (1,2)=+i, (2,1)=-i     L7: diag(1,1,-2)/sqrt(3)
+// (Gell-Mann lambdas, not lambda/2; L1, L4, L6 are the transposed lambda_2,5,7.)
+// tr(L_a L_b) = 2 delta_ab, so the coefficient of a Hermitian traceless H is
+// tr(L_a H)/2.
+template <typename T, typename V>
+__device__ __forceinline__ void embed_lambda(const T n[8], V m[9]) {
+    const T inv_s3 = (T)0.57735026918962573;  // 1/sqrt(3)
+    const T d8 = n[7] * inv_s3;
+    m[0] = mk<T>(n[2] + d8, 0);
+    m[1] = mk<T>(n[0], n[1]);
+    m[2] = mk<T>(n[3], n[4]);
+    m[3] = mk<T>(n[0], -n[1]);
+    m[4] = mk<T>(-n[2] + d8, 0);
+    m[5] = mk<T>(n[5], n[6]);
+    m[6] = mk<T>(n[3], -n[4]);
+    m[7] = mk<T>(n[5], -n[6]);
+    m[8] = mk<T>((T)-2 * d8, 0);
+}
+
+// The reference's exact sequence of accumulations for one site (used by the
+// call-for-call FP64 path so that xi matches generate_gaussian bit for bit).
+__device__ __forceinline__ void embed_lambda_ref(const double n[8], double2 m[9]) {
+    const double s3 = 1.7320508075688772;  // sqrt(3.0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m[k] = make_double2(0.0, 0.0);
+    m[1].x += n[0]; m[3].x += n[0];
+    m[1].y += n[1]; m[3].y -= n[1];
+    m[0].x += n[2]; m[4].x -= n[2];
+    m[2].x += n[3]; m[6].x += n[3];
+    m[2].y += n[4]; m[6].y -= n[4];
+    m[5].x += n[5]; m[7].x += n[5];
+    m[5].y += n[6]; m[7].y -= n[6];
+    m[0].x += n[7] / s3; m[4].x += n[7] / s3; m[8].x += -2.0 * n[7] / s3;
+}
+
+// Coefficients h_a = tr(L_a H)/2 of a Hermitian H (only the upper triangle
+// and the real diagonal are read).
+template <typename T, typename V>
+__device__ __forceinline__ void project_lambda(const V m[9], T h[8]) {
+    const T s3 = (T)1.7320508075688772;
+    h[0] = m[1].x;
+    h[1] = m[1].y;
+    h[2] = (T)0.5 * (m[0].x - m[4].x);
+    h[3] = m[2].x;
+    h[4] = m[2].y;
+    h[5] = m[5].x;
+    h[6] = m[5].y;
+    h[7] = (m[0].x + m[4].x - (T)2 * m[8].x) / ((T)2 * s3);
+}
+
+// ------------------------------------------------------------------ 3x3
+template <typename V>
+__device__ __forceinline__ void mul3(const V a[9], const V b[9], V c[9]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            V s = cmul(a[i * 3 + 0], b[0 * 3 + j]);
+            s = cadd(s, cmul(a[i * 3 + 1], b[1 * 3 + j]));
+            s = cadd(s, cmul(a[i * 3 + 2], b[2 * 3 + j]));
+            c[i * 3 + j] = s;
+        }
+}
+// c = a * b^dagger
+template <typename V>
+__device__ __forceinline__ void mul3_adj(const V a[9], const V b[9], V c[9]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            V s = cmulc(a[i * 3 + 0], b[j * 3 + 0]);
+            s = cadd(s, cmulc(a[i * 3 + 1], b[j * 3 + 1]));
+            s = cadd(s, cmulc(a[i * 3 + 2], b[j * 3 + 2]));
+            c[i * 3 + j] = s;
+        }
+}
+
+// ------------------------------------------------------------------ Hermitian eigen / exp (FP64)
+// The route su3_matrix::exponentiate takes (su3_matrix.h:173-253, 256-359):
+// Cardano eigenvalues, eigenvectors by cross products of the columns of
+// A - w I, and the QL fallback (Householder tridiagonalisation + implicit-shift
+// QL, at most 30 sweeps) when a cross product is too small.  This is the
+// published algorithm of J. Kopp, Int. J. Mod. Phys. C 19 (2008) 523
+// (arXiv:physics/0610206), restated here for double2 registers.  Only the
+// upper triangle and the real parts of the diagonal are read, except in the
+// Householder step, which reads the complex diagonal as the reference does.
+struct Mat3d { double2 a[3][3]; };
+
+__device__ __forceinline__ double d_sqr(double x) { return x * x; }
+
+__device__ __forceinline__ void eig_cardano(const double2 (&A)[3][3], double w[3]) {
+    const double2 de = cmul(A[0][1], A[1][2]);
+    const double dd = cabs2(A[0][1]), ee = cabs2(A[1][2]), ff = cabs2(A[0][2]);
+    const double a = A[0][0].x, b = A[1][1].x, c = A[2][2].x;
+    const double m = a + b + c;
+    const double c1 = (a * b + a * c + b * c) - (dd + ee + ff);
+    const double c0 = c * dd + a * ee + b * ff - a * b * c - 2.0 * (A[0][2].x * de.x + A[0][2].y * de.y);
+    const double p = d_sqr(m) - 3.0 * c1;
+    const double q = m * (p - 1.5 * c1) - 13.5 * c0;
+    const double sqrt_p = sqrt(fabs(p));
+    double phi = 27.0 * (0.25 * d_sqr(c1) * (p - c1) + c0 * (q + 6.75 * c0));
+    phi = (1.0 / 3.0) * atan2(sqrt(fabs(phi)), q);
+    double sn, cs;
+    sincos(phi, &sn, &cs);
+    const double cc = sqrt_p * cs;
+    const double s = 0.57735026918962573 * sqrt_p * sn;
+    w[1] = (1.0 / 3.0) * (m - cc);
+    w[2] = w[1] + s;
+    w[0] = w[1] + cc;
+    w[1] -= s;
+}
+
+__device__ inline void tridiag_householder(const double2 (&A)[3][3], double2 (&Q)[3][3], double d[3], double e[3]) {
+    double2 u[3], q[3], omega, f;
+    double K, h, g;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Q[i][j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    h = cabs2(A[0][1]) + cabs2(A[0][2]);
+    g = (A[0][1].x > 0) ? -sqrt(h) : sqrt(h);
+    e[0] = g;
+    f = cscale(A[0][1], g);
+    u[1] = make_double2(A[0][1].x - g, -A[0][1].y);
+    u[2] = cconj(A[0][2]);
+    omega = make_double2(h - f.x, -f.y);
+    if (omega.x > 0.0) {
+        // omega <- 0.5 (1 + conj(omega)/omega) / Re(omega)
+        const double den = cabs2(omega);
+        double2 r = cmul(cconj(omega), cconj(omega));  // conj(omega)^2 / |omega|^2 = conj(omega)/omega
+        r = cscale(r, 1.0 / den);
+        omega = cscale(make_double2(1.0 + r.x, r.y), 0.5 / omega.x);
+        K = 0.0;
+#pragma unroll
+        for (int i = 1; i < 3; ++i) {
+            f = cadd(cmul(cconj(A[1][i]), u[1]), cmul(A[i][2], u[2]));
+            q[i] = cmul(omega, f);
+            K += cmulc(f, u[i]).x;  // Re(conj(u) f)
+        }
+        K *= 0.5 * cabs2(omega);
+#pragma unroll
+        for (int i = 1; i < 3; ++i) q[i] = csub(q[i], cscale(u[i], K));
+        d[0] = A[0][0].x;
+        d[1] = A[1][1].x - 2.0 * cmulc(q[1], u[1]).x;
+        d[2] = A[2][2].x - 2.0 * cmulc(q[2], u[2]).x;
+#pragma unroll
+        for (int j = 1; j < 3; ++j) {
+            f = cmul(omega, cconj(u[j]));
+#pragma unroll
+            for (int i = 1; i < 3; ++i) Q[i][j] = csub(Q[i][j], cmul(f, u[i]));
+        }
+        f = csub(csub(A[1][2], cmulc(q[1], u[2])), cmulc(u[1], q[2]));
+    } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) d[i] = A[i][i].x;
+        f = A[1][2];
+    }
+    e[1] = sqrt(cabs2(f));
+    if (e[1] != 0.0) {
+        f = cscale(cconj(f), 1.0 / e[1]);
+#pragma unroll
+        for (int i = 1; i < 3; ++i) Q[i][2] = cmul(Q[i][2], f);
+    }
+}
+
+// Returns 0, or -1 when the QL sweeps did not converge within 30 iterations.
+__device__ inline int eig_ql(const double2 (&A)[3][3], double2 (&Q)[3][3], double w[3]) {
+    double e[3];
+    tridiag_householder(A, Q, w, e);
+    for (int l = 0; l < 2; ++l) {
+        int nIter = 0;
+        for (;;) {
+            int m;
+            for (m = l; m <= 1; ++m) {
+                const double g = fabs(w[m]) + fabs(w[m + 1]);
+                if (fabs(e[m]) + g == g) break;
+            }
+            if (m == l) break;
+            if (nIter++ >= 30) return -1;
+            double g = (w[l + 1] - w[l]) / (e[l] + e[l]);
+            double r = sqrt(d_sqr(g) + 1.0);
+            g = (g > 0) ? w[m] - w[l] + e[l] / (g + r) : w[m] - w[l] + e[l] / (g - r);
+            double s = 1.0, c = 1.0, p = 0.0;
+            for (int i = m - 1; i >= l; --i) {
+                const double f = s * e[i];
+                const double b = c * e[i];
+                if (fabs(f) > fabs(g)) {
+                    c = g / f;
+                    r = sqrt(d_sqr(c) + 1.0);
+                    e[i + 1] = f * r;
+                    s = 1.0 / r;
+                    c *= s;
+                } else {
+                    s = f / g;
+                    r = sqrt(d_sqr(s) + 1.0);
+                    e[i + 1] = g * r;
+                    c = 1.0 / r;
+                    s *= c;
+                }
+                g = w[i + 1] - p;
+                r = (w[i] - g) * s + 2.0 * c * b;
+                p = s * r;
+                w[i + 1] = g + p;
+                g = c * r - b;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const double2 t = Q[k][i + 1];
+                    Q[k][i + 1] = cadd(cscale(Q[k][i], s), cscale(t, c));
+                    Q[k][i] = csub(cscale(Q[k][i], c), cscale(t, s));
+                }
+            }
+            w[l] -= p;
+            e[l] = g;
+            e[m] = 0.0;
+        }
+    }
+    return 0;
+}
+
+// Hybrid solver.  Returns 0 (analytic or converged QL) or -1 (QL failed).
+__device__ __forceinline__ int eigh3(const double2 (&A)[3][3], double2 (&Q)[3][3], double w[3]) {
+    eig_cardano(A, w);
+    double t = fabs(w[0]), u;
+    if ((u = fabs(w[1])) > t) t = u;
+    if ((u = fabs(w[2])) > t) t = u;
+    u = (t < 1.0) ? t : d_sqr(t);
+    const double error = 256.0 * 2.220446049250313e-16 * d_sqr(u);
+    double2 q01 = csub(cmul(A[0][1], A[1][2]), cscale(A[0][2], A[1][1].x));
+    double2 q11 = csub(cmulc(A[0][2], A[0][1]), cscale(A[1][2], A[0][0].x));
+    const double q21 = cabs2(A[0][1]);
+    double2 v0 = cadd(q01, cscale(A[0][2], w[0]));
+    double2 v1 = cadd(q11, cscale(A[1][2], w[0]));
+    double v2 = (A[0][0].x - w[0]) * (A[1][1].x - w[0]) - q21;
+    double norm = cabs2(v0) + cabs2(v1) + d_sqr(v2);
+    if (norm <= error) return eig_ql(A, Q, w);
+    norm = sqrt(1.0 / norm);
+    Q[0][0] = cscale(v0, norm);
+    Q[1][0] = cscale(v1, norm);
+    Q[2][0] = make_double2(v2 * norm, 0.0);
+    v0 = cadd(q01, cscale(A[0][2], w[1]));
+    v1 = cadd(q11, cscale(A[1][2], w[1]));
+    v2 = (A[0][0].x - w[1]) * (A[1][1].x - w[1]) - q21;
+    norm = cabs2(v0) + cabs2(v1) + d_sqr(v2);
+    if (norm <= error) return eig_ql(A, Q, w);
+    norm = sqrt(1.0 / norm);
+    Q[0][1] = cscale(v0, norm);
+    Q[1][1] = cscale(v1, norm);
+    Q[2][1] = make_double2(v2 * norm, 0.0);
+    Q[0][2] = cconj(csub(cmul(Q[1][0], Q[2][1]), cmul(Q[2][0], Q[1][1])));
+    Q[1][2] = cconj(csub(cmul(Q[2][0], Q[0][1]), cmul(Q[0][0], Q[2][1])));
+    Q[2][2] = cconj(csub(cmul(Q[0][0], Q[1][1]), cmul(Q[1][0], Q[0][1])));
+    return 0;
+}
+
+// m <- Q diag(exp(i sign w)) Q^dagger for the Hermitian matrix held in m.
+// Returns the eigensolver status.
+__device__ __forceinline__ int expi_herm(double2 m[9], double sign) {
+    double2 A[3][3], Q[3][3];
+    double w[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) A[i][j] = m[i * 3 + j];
+    const int status = eigh3(A, Q, w);
+    double2 ph[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double s, c;
+        sincos(sign * w[k], &s, &c);
+        ph[k] = make_double2(c, s);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double2 acc = cmulc(cmul(Q[i][0], ph[0]), Q[j][0]);
+            acc = cadd(acc, cmulc(cmul(Q[i][1], ph[1]), Q[j][1]));
+            acc = cadd(acc, cmulc(cmul(Q[i][2], ph[2]), Q[j][2]));
+            m[i * 3 + j] = acc;
+        }
+    return status;
+}
+
+// Reunitarisation: Gram-Schmidt on rows 0 and 1, row 2 = conj(row0 x row1),
+// which is the nearest-in-practice SU(3) projection for a matrix that is
+// unitary up to rounding.
+__device__ __forceinline__ void reunitarize(double2 m[9]) {
+    double n0 = rsqrt(cabs2(m[0]) + cabs2(m[1]) + cabs2(m[2]));
+    m[0] = cscale(m[0], n0); m[1] = cscale(m[1], n0); m[2] = cscale(m[2], n0);
+    // <r0, r1> = sum conj(r0) r1
+    double2 d = cadd(cadd(cmulc(m[3], m[0]), cmulc(m[4], m[1])), cmulc(m[5], m[2]));
+    m[3] = csub(m[3], cmul(d, m[0]));
+    m[4] = csub(m[4], cmul(d, m[1]));
+    m[5] = csub(m[5], cmul(d, m[2]));
+    double n1 = rsqrt(cabs2(m[3]) + cabs2(m[4]) + cabs2(m[5]));
+    m[3] = cscale(m[3], n1); m[4] = cscale(m[4], n1); m[5] = cscale(m[5], n1);
+    m[6] = cconj(csub(cmul(m[1], m[5]), cmul(m[2], m[4])));
+    m[7] = cconj(csub(cmul(m[2], m[3]), cmul(m[0], m[5])));
+    m[8] = cconj(csub(cmul(m[0], m[4]), cmul(m[1], m[3])));
+}
+
+// ------------------------------------------------------------------ lattice momenta
+// momenta::set (momenta.h:90-124): phat2 = 4 sin^2(pi kx/N) + 4 sin^2(pi ky/N),
+// pbar_i = sin(2 pi k_i / N), with the unwrapped index k in 0..N-1.
+__device__ __forceinline__ double phat2_d(int kx, int ky, int N) {
+    const double sx = sin(3.141592653589793 * kx / (1.0 * N));
+    const double sy = sin(3.141592653589793 * ky / (1.0 * N));
+    return 4.0 * sx * sx + 4.0 * sy * sy;
+}
+
+}  // namespace jw

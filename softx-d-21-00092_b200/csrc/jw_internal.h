@@ -1,0 +1,77 @@
+// jw_internal.h -- host-side internals shared by the libjimwlk translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "../../include/jimwlk.h"
+#include "jw_common.cuh"
+
+#define JW_EXPORT extern "C" __attribute__((visibility("default")))
+
+// Device-side error flags (bit mask in a device int, cleared by the syncs).
+#define JW_FLAG_NOCONV 1
+#define JW_FLAG_NAN 2
+
+#define JW_CUDA(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            fprintf(stderr, "libjimwlk: %s failed at %s:%d: %s\n", #call, __FILE__, __LINE__, \
+                    cudaGetErrorString(e_));                                                  \
+            return JW_ECUDA;                                                                  \
+        }                                                                                     \
+    } while (0)
+
+#define JW_CHECK(cond)                 \
+    do {                               \
+        if (!(cond)) return JW_EINVAL; \
+    } while (0)
+
+namespace jw {
+
+// FP64-accurate twiddle tables exp(+2 pi i m / N), m < N, for one N.
+struct Twiddles {
+    int N = 0;
+    double2* d64 = nullptr;
+    float2* d32 = nullptr;
+};
+cudaError_t twiddles_create(int N, Twiddles* tw);
+void twiddles_destroy(Twiddles* tw);
+
+bool supported_n(int N);
+
+// Converts a device error-flag word to a status (and clears nothing).
+inline jw_status flags_to_status(int flags) {
+    if (flags & JW_FLAG_NOCONV) return JW_ENOCONV;
+    if (flags & JW_FLAG_NAN) return JW_ENAN;
+    return JW_OK;
+}
+
+}  // namespace jw
+
+struct jw_context {
+    jw_config cfg;
+    int device = 0;
+    int N = 0;
+    cudaStream_t stream = nullptr;
+    jw::Twiddles tw;
+    int* d_flags = nullptr;       // device error flags
+    double2* d_tmp = nullptr;     // one plane of scratch (average_and_symmetrize)
+};
+
+struct jw_field {
+    jw_context* ctx = nullptr;
+    int t = 0;                    // 1 or 9
+    double2* d = nullptr;         // t planes of N*N, plane k at d + k*N*N (row-major x, y)
+};
+
+// FFT launchers over contiguous planes of N*N complex (rows then columns,
+// in place, scaled by `scale` after the column pass).
+namespace jw {
+template <typename T>
+cudaError_t fft2d_planes(C2<T>* planes, int nplanes, int N, int dir, T scale, const Twiddles& tw,
+                         cudaStream_t s);
+}

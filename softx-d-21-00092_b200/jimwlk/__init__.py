@@ -1,0 +1,241 @@
+"""Python binding of libjimwlk (include/jimwlk.h) over ctypes.
+
+The product is the CUDA library ``lib/libjimwlk.so`` built from ``csrc/``;
+this module only marshals arguments.  It has no CPU fallback: if the library
+is missing, importing raises ``JimwlkError``.
+
+Host field arrays are numpy complex128 arrays of shape (N, N, t) in the
+reference solver's site-major layout (t = 9: row-major 3x3; t = 1: scalar).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libjimwlk.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ENOCONV, ENAN, ETIMEOUT, EUNSUPPORTED, ENOTFOUND, EBUSY = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
+POSITION_EVOLUTION, MOMENTUM_EVOLUTION = 0, 1
+SQRT_COUPLING_CONSTANT, NOISE_COUPLING_CONSTANT, HATTA_COUPLING_CONSTANT, FIXED_COUPLING_CONSTANT = 0, 1, 2, 3
+LINEAR_KERNEL, SIN_KERNEL = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class JimwlkError(RuntimeError):
+    def __init__(self, status: int, where: str = ""):
+        self.status = status
+        msg = _lib.jw_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{where}: {msg} ({status})" if where else f"{msg} ({status})")
+
+
+class jw_config(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("stat", ctypes.c_int), ("mu", ctypes.c_double),
+                ("mass", ctypes.c_double), ("elementaryWilsonLines", ctypes.c_int), ("file_name", ctypes.c_char * 64),
+                ("langevin_steps", ctypes.c_int), ("measurements", ctypes.c_int), ("step", ctypes.c_double),
+                ("EvolutionChoice", ctypes.c_int), ("CouplingChoice", ctypes.c_int), ("KernelChoice", ctypes.c_int),
+                ("seed", ctypes.c_uint64)]
+
+
+class jw_engine_options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("reunitarize", ctypes.c_int), ("max_bytes", ctypes.c_size_t),
+                ("max_batch", ctypes.c_int)]
+
+
+class jw_event_desc(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("ny_slices", ctypes.c_int), ("mu", ctypes.c_double), ("mass", ctypes.c_double),
+                ("step", ctypes.c_double), ("coupling", ctypes.c_int), ("kernel", ctypes.c_int),
+                ("seed", ctypes.c_uint64)]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libjimwlk is not built ({LIB_PATH}); run `make -C softx-d-21-00092_b200` "
+                          "or __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "jw_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "jw_config_defaults": ([ctypes.POINTER(jw_config)], ctypes.c_int),
+        "jw_config_read": ([ctypes.POINTER(jw_config), ctypes.c_char_p], ctypes.c_int),
+        "jw_context_create": ([ctypes.POINTER(jw_config), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+        "jw_context_destroy": ([_vp], ctypes.c_int),
+        "jw_context_sync": ([_vp], ctypes.c_int),
+        "jw_context_stream": ([_vp], _vp),
+        "jw_field_create": ([_vp, ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+        "jw_field_destroy": ([_vp], ctypes.c_int),
+        "jw_field_set": ([_vp, _dp], ctypes.c_int),
+        "jw_field_get": ([_vp, _dp], ctypes.c_int),
+        "jw_field_copy": ([_vp, _vp], ctypes.c_int),
+        "jw_field_set_unit": ([_vp], ctypes.c_int),
+        "jw_field_set_zero": ([_vp], ctypes.c_int),
+        "jw_execute2D": ([_vp, _vp, ctypes.c_int], ctypes.c_int),
+        "jw_generate_gaussian": ([_vp, _vp, _vp, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
+        "jw_set_mv_model": ([_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int], ctypes.c_int),
+        "jw_solve_poisson": ([_vp, _vp, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "jw_mul_exp": ([_vp, _vp, _vp], ctypes.c_int),
+        "jw_prepare_A_local": ([_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "jw_uxiulocal": ([_vp, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+        "jw_update_uf": ([_vp, _vp, _vp, _vp, ctypes.c_double], ctypes.c_int),
+        "jw_trace": ([_vp, _vp, _vp], ctypes.c_int),
+        "jw_average_and_symmetrize": ([_vp, _vp], ctypes.c_int),
+        "jw_reduce": ([_vp, _vp, _vp, _vp], ctypes.c_int),
+        "jw_print": ([_vp, ctypes.c_int, _vp, _vp, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
+        "jw_initial_condition": ([_vp, _vp], ctypes.c_int),
+        "jw_evolve_momentum": ([_vp, _vp, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    return L
+
+
+_lib = None
+_lib = _load()
+
+
+def lib():
+    return _lib
+
+
+def _ck(status: int, where: str) -> None:
+    if status != OK:
+        raise JimwlkError(status, where)
+
+
+def config_defaults(**kw) -> jw_config:
+    c = jw_config()
+    _ck(_lib.jw_config_defaults(ctypes.byref(c)), "jw_config_defaults")
+    for k, v in kw.items():
+        if k == "file_name":
+            v = v.encode() if isinstance(v, str) else v
+        setattr(c, k, v)
+    return c
+
+
+def config_read(path: str, base: jw_config | None = None) -> jw_config:
+    c = base if base is not None else config_defaults()
+    _ck(_lib.jw_config_read(ctypes.byref(c), path.encode()), "jw_config_read")
+    return c
+
+
+class Context:
+    """A device context for one lattice size (jw_context)."""
+
+    def __init__(self, cfg: jw_config, device: int = 0):
+        self._h = _vp()
+        _ck(_lib.jw_context_create(ctypes.byref(cfg), device, ctypes.byref(self._h)), "jw_context_create")
+        self.cfg = cfg
+        self.N = cfg.Nx
+
+    def close(self):
+        if self._h:
+            _lib.jw_context_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self) -> int:
+        return _lib.jw_context_sync(self._h)
+
+    def field(self, t: int = 9) -> "Field":
+        return Field(self, t)
+
+    # reference hot-path calls
+    def execute2D(self, f, direction):
+        _ck(_lib.jw_execute2D(self._h, f._h, direction), "jw_execute2D")
+
+    def generate_gaussian(self, xi_x, xi_y, step_index: int, with_coupling: bool):
+        _ck(_lib.jw_generate_gaussian(self._h, xi_x._h, xi_y._h, step_index, int(with_coupling)),
+            "jw_generate_gaussian")
+
+    def set_mv_model(self, f, slice_: int, g: float, mu: float, ny_slices: int):
+        _ck(_lib.jw_set_mv_model(self._h, f._h, slice_, g, mu, ny_slices), "jw_set_mv_model")
+
+    def solve_poisson(self, f, mass: float, g: float):
+        _ck(_lib.jw_solve_poisson(self._h, f._h, mass, g), "jw_solve_poisson")
+
+    def mul_exp(self, V, f):
+        _ck(_lib.jw_mul_exp(self._h, V._h, f._h), "jw_mul_exp")
+
+    def prepare_A_local(self, out, xi_x, xi_y, coupling: int, kernel: int):
+        _ck(_lib.jw_prepare_A_local(self._h, out._h, xi_x._h, xi_y._h, coupling, kernel), "jw_prepare_A_local")
+
+    def uxiulocal(self, ux, uy, V, xi_x, xi_y):
+        _ck(_lib.jw_uxiulocal(self._h, ux._h, uy._h, V._h, xi_x._h, xi_y._h), "jw_uxiulocal")
+
+    def update_uf(self, V, B, A, step: float):
+        _ck(_lib.jw_update_uf(self._h, V._h, B._h, A._h, step), "jw_update_uf")
+
+    def trace(self, Vk, corr):
+        _ck(_lib.jw_trace(self._h, Vk._h, corr._h), "jw_trace")
+
+    def average_and_symmetrize(self, corr):
+        _ck(_lib.jw_average_and_symmetrize(self._h, corr._h), "jw_average_and_symmetrize")
+
+    def reduce(self, corr, sum_, err):
+        _ck(_lib.jw_reduce(self._h, corr._h, sum_._h, err._h), "jw_reduce")
+
+    def print(self, measurement: int, sum_, err, x: float, fileroot: str):
+        _ck(_lib.jw_print(self._h, measurement, sum_._h, err._h, x, fileroot.encode()), "jw_print")
+
+    def initial_condition(self, V):
+        _ck(_lib.jw_initial_condition(self._h, V._h), "jw_initial_condition")
+
+    def evolve_momentum(self, V, step0: int, n: int):
+        _ck(_lib.jw_evolve_momentum(self._h, V._h, step0, n), "jw_evolve_momentum")
+
+
+class Field:
+    """A device field lfield<double,t> (jw_field)."""
+
+    def __init__(self, ctx: Context, t: int = 9):
+        self.ctx = ctx
+        self.t = t
+        self._h = _vp()
+        _ck(_lib.jw_field_create(ctx._h, t, ctypes.byref(self._h)), "jw_field_create")
+
+    def close(self):
+        if self._h:
+            _lib.jw_field_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set(self, a: np.ndarray) -> "Field":
+        N = self.ctx.N
+        a = np.ascontiguousarray(a, np.complex128)
+        if a.shape != (N, N, self.t):
+            raise ValueError(f"expected shape {(N, N, self.t)}, got {a.shape}")
+        _ck(_lib.jw_field_set(self._h, a.ctypes.data_as(_dp)), "jw_field_set")
+        return self
+
+    def get(self) -> np.ndarray:
+        N = self.ctx.N
+        a = np.empty((N, N, self.t), np.complex128)
+        _ck(_lib.jw_field_get(self._h, a.ctypes.data_as(_dp)), "jw_field_get")
+        return a
+
+    def copy_from(self, other: "Field"):
+        _ck(_lib.jw_field_copy(self._h, other._h), "jw_field_copy")
+
+    def set_unit(self):
+        _ck(_lib.jw_field_set_unit(self._h), "jw_field_set_unit")
+
+    def set_zero(self):
+        _ck(_lib.jw_field_set_zero(self._h), "jw_field_set_zero")

@@ -1,0 +1,124 @@
+"""Generates the golden vectors in tests/golden/ from the reference's own code.
+
+Run in a container that has the reference tree (for oracle/_ref/libref_<N>.so,
+built by `make -C oracle ref`):
+
+    python tests/golden/make_golden.py
+
+Every output array below is produced by the reference's functions (field.h,
+su3_matrix.h, zheevh3, mpi_fftw_class.h with the project FFT shim) fed with the
+engine's Philox noise stream (the oracle's host copy of it, oracle/jw_oracle.c),
+so that the GPU tests can check the CUDA library against the reference on a
+machine without the reference tree.  The script also checks the oracle against
+the same outputs and refuses to write fixtures if they disagree.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+from jwref import Oracle, Reference, config_text, f32  # noqa: E402
+
+FIXED = 3  # fixed coupling: plain generate_gaussian + NOISE kernel factor 1
+
+
+def fixture_functions(o: Oracle, N: int, seed: int) -> dict:
+    """One application of each hot-path function at lattice N."""
+    cfg = dict(mu=0.5 * N, mass=0.04, wilson_lines=6, step=0.0004, coupling="NOISE_COUPLING_CONSTANT")
+    r = Reference(N, config_text(**cfg))
+    c = r.config()
+    rng = np.random.default_rng(seed)
+    out = {"N": N, "seed": seed, "mu": c["mu"], "mass": c["mass"], "step": c["step"], "slices": 6}
+    f = rng.standard_normal((N, N, 9)) + 1j * rng.standard_normal((N, N, 9))
+    out["fft_in"] = f
+    out["fft_fwd"] = r.execute2D(f, 1)
+    out["fft_bwd"] = r.execute2D(f, 0)
+    z = o.langevin_normals(seed, 0, N)
+    out["xi_x"], out["xi_y"] = r.generate_gaussian(z, False)
+    out["xi_x_nc"], out["xi_y_nc"] = r.generate_gaussian(z, True)
+    X = r.execute2D(out["xi_x"], 1)
+    Y = r.execute2D(out["xi_y"], 1)
+    out["xi_x_k"], out["xi_y_k"] = X, Y
+    for cp, cname in ((0, "sqrt"), (1, "noise")):
+        for k, kname in ((0, "linear"), (1, "sin")):
+            out[f"A_{cname}_{kname}"] = r.prepare_A_local(X, Y, cp, k)
+    V = r.initial_condition(np.concatenate([o.mv_normals(seed, s, N).ravel() for s in range(6)]))
+    out["V_mv"] = V
+    ux, uy = r.uxiulocal(V, out["xi_x"], out["xi_y"])
+    out["ux"], out["uy"] = ux, uy
+    A = r.execute2D(out["A_noise_sin"], 0)
+    B = r.execute2D(r.prepare_A_local(r.execute2D(ux, 1), r.execute2D(uy, 1), 1, 1), 0)
+    out["A_x"], out["B_x"] = A, B
+    out["V_upd"] = r.update_uf(V, B, A, c["step"])
+    corr, s, e = r.measure(V)
+    out["corr"], out["sum"], out["err"] = corr, s, e
+    return out
+
+
+def fixture_evolution(o: Oracle, N: int, seed: int, coupling: str, steps: int, step: float, slices: int,
+                      mu: float, mass: float, kernel: str = "SIN_KERNEL") -> dict:
+    """MV initial condition then `steps` Langevin steps and one measurement."""
+    cfg_coupling = "NOISE_COUPLING_CONSTANT" if coupling == "FIXED" else coupling
+    r = Reference(N, config_text(mu=mu, mass=mass, wilson_lines=slices, step=step, coupling=cfg_coupling,
+                                 kernel=kernel))
+    c = r.config()
+    V0 = r.initial_condition(np.concatenate([o.mv_normals(seed, s, N).ravel() for s in range(slices)]))
+    zs = np.concatenate([o.langevin_normals(seed, s, N).ravel() for s in range(steps)])
+    if coupling == "FIXED":
+        V1 = r.evolve_momentum_fixed(V0, zs, steps)
+    else:
+        V1 = r.evolve_momentum(V0, zs, steps)
+    corr, s, e = r.measure(V1)
+    return {"N": N, "seed": seed, "mu": c["mu"], "mass": c["mass"], "step": c["step"], "slices": slices,
+            "steps": steps, "coupling": coupling, "kernel": kernel, "V_mv": V0, "V_final": V1, "corr": corr,
+            "sum": s, "err": e}
+
+
+def check_oracle(o: Oracle, fx: dict) -> float:
+    N, seed = fx["N"], fx["seed"]
+    V0 = o.initial_condition(N, fx["mu"], fx["mass"], fx["slices"], seed)
+    cp = {"FIXED": FIXED, "NOISE_COUPLING_CONSTANT": 1, "SQRT_COUPLING_CONSTANT": 0}[fx["coupling"]]
+    kn = 1 if fx["kernel"] == "SIN_KERNEL" else 0
+    V1 = o.evolve_momentum(V0, fx["steps"], 0, fx["step"], cp, kn, seed)
+    corr, _, _ = o.measure(V1)
+    return max(np.abs(V0 - fx["V_mv"]).max(), np.abs(V1 - fx["V_final"]).max(),
+               np.abs(corr - fx["corr"]).max() / np.abs(fx["corr"]).max())
+
+
+def main() -> None:
+    o = Oracle()
+    fns = fixture_functions(o, 16, 101)
+    np.savez_compressed(os.path.join(HERE, "functions_N16.npz"), **{k: np.asarray(v) for k, v in fns.items()})
+    runs = {
+        # reference default main path: MOMENTUM + NOISE coupling (site-indexed noise factor), SIN kernel
+        "evolve_noise_N16": dict(N=16, seed=7, coupling="NOISE_COUPLING_CONSTANT", steps=20, step=f32(0.0004),
+                                 slices=10, mu=8.0, mass=f32(0.04)),
+        # running coupling in momentum space
+        "evolve_sqrt_N16": dict(N=16, seed=8, coupling="SQRT_COUPLING_CONSTANT", steps=20, step=f32(0.0004),
+                                slices=10, mu=8.0, mass=f32(0.04)),
+        # linear kernel (Nyquist rows make A non-Hermitian; exercised on purpose)
+        "evolve_linear_N16": dict(N=16, seed=9, coupling="SQRT_COUPLING_CONSTANT", steps=10, step=f32(0.0004),
+                                  slices=10, mu=8.0, mass=f32(0.04), kernel="LINEAR_KERNEL"),
+        # first workload: 64^2, g^2 mu a = 0.5, m a = 0.02, 50 slices, 100 fixed-coupling steps,
+        # step = alpha_s * ds / pi^2 with alpha_s = 0.15, ds = 1e-4
+        "c1_N64": dict(N=64, seed=1, coupling="FIXED", steps=100, step=0.15 * 1e-4 / np.pi ** 2, slices=50,
+                       mu=32.0, mass=f32(0.04)),
+        # the reference's default step at 32^2 for a visible evolution
+        "evolve_fixed_N32": dict(N=32, seed=3, coupling="FIXED", steps=50, step=f32(0.0004), slices=20, mu=16.0,
+                                 mass=f32(0.04)),
+    }
+    for name, kw in runs.items():
+        fx = fixture_evolution(o, **kw)
+        d = check_oracle(o, fx)
+        print(f"{name}: oracle vs reference max deviation {d:.3e}")
+        if d > 1e-12:
+            raise SystemExit(f"oracle disagrees with the reference on {name}")
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fx.items()})
+
+
+if __name__ == "__main__":
+    main()

@@ -213,6 +213,7 @@ class Reference:
         L.ref_su3_exponentiate.restype = ctypes.c_int
         L.ref_initial_condition.argtypes = [_dp]
         L.ref_evolve_momentum.argtypes = [_dp, ctypes.c_int]
+        L.ref_evolve_momentum_fixed.argtypes = [_dp, ctypes.c_int]
         L.ref_measure.argtypes = [_dp, _dp, _dp, _dp]
         L.ref_print.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_char_p]
         path = b""
@@ -304,6 +305,12 @@ class Reference:
         self.inject(z_all)
         V = np.ascontiguousarray(V, np.complex128).copy()
         self.L.ref_evolve_momentum(_ptr(V.view(np.float64)), steps)
+        return V
+
+    def evolve_momentum_fixed(self, V, z_all: np.ndarray, steps: int) -> np.ndarray:
+        self.inject(z_all)
+        V = np.ascontiguousarray(V, np.complex128).copy()
+        self.L.ref_evolve_momentum_fixed(_ptr(V.view(np.float64)), steps)
         return V
 
     def measure(self, V, sum_=None, err=None):
