@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Throughput of the JIMWLK Langevin evolution on B200.
+
+Workload (one "step" = one Langevin step of the whole batch): 64 independent
+events on 512 x 512 lattices, MV initial condition with g^2 mu a = 0.5,
+m a = 0.02 and 50 slices, fixed coupling alpha_s = 0.15 and ds = 1e-4
+(step = alpha_s ds / pi^2), SIN kernel, advanced by the batched engine in mixed
+precision (FP32 noise, rotation and transforms; FP64 exponentials, V and
+dipole sums).  Seeded synthetic inputs; no dataset is involved.  The
+per-event fields (V 144 B/site, workspaces 192 B/site) total ~5.6 GB, far above
+the 126 MB L2, so no flush is needed between steps.
+
+Arms
+  default            the engine through the C ABI (softx-d-21-00092_b200/lib/libjimwlk.so)
+  --impl reference   the reference's own main_optimized (oracle/_ref, OpenMP on all
+                     host cores, single-rank MPI and FFTW shims) on one 512^2 event
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torchrun, one rank per GPU, each rank advancing its own 64 events (weak
+scaling; the events are independent, so the only collective is the max of the
+ranks' timings).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "softx-d-21-00092_b200")
+REF_MAIN = os.path.join(REPO, "oracle", "_ref", "main_optimized_omp_512")
+
+EVENTS = 64
+N = 512
+NY_SLICES = 50
+MU = 0.5 * N          # g^2 mu a = 0.5 with g = 1 -> config mu = 0.5 N
+MASS = 0.04           # m a = 0.02 = mass * mu_MV
+ALPHA_S, DS = 0.15, 1e-4
+STEP = ALPHA_S * DS / math.pi ** 2
+METRIC = "lattice site-steps/s"
+# algorithmic HBM bytes per site of each fused kernel (mixed precision):
+#   pass 1: read V (9 complex FP64 = 144 B) + write 16 FP32 complex planes (128 B)
+#   pass 2: read 16 planes (128 B) + write 8 planes (64 B)
+#   pass 3: read 8 planes (64 B) + read and write V (288 B)
+PASS_BYTES = {"step_pass1": 272, "step_pass2": 192, "step_pass3": 352}
+PASS_NAMES = ["step_pass1", "step_pass2", "step_pass3"]
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of each fused kernel from the committed ncu summary
+    (profiles/step_kernels_512x64.md, a line `traffic <kernel> <bytes_per_site>`)."""
+    p = os.path.join(REPO, "profiles", "step_kernels_512x64.md")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            m = re.match(r"\s*traffic\s+(\S+)\s+([0-9.]+)", line)
+            if m:
+                out[m.group(1)] = float(m.group(2))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.send_signal(signal.SIGTERM)
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].isdigit():
+                    rows.append(f)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def parse_evolution_times(text: str):
+    return [float(x) for x in re.findall(r"Evolution time:\s*([0-9.eE+-]+)", text)]
+
+
+def run_reference_main(steps: int, warmup: int, nthreads: int | None = None):
+    """The reference's main_optimized on one 512^2 event: returns seconds per
+    Langevin step (mean over the last `steps` of warmup + steps)."""
+    if not os.path.exists(REF_MAIN):
+        return None, "reference binary oracle/_ref/main_optimized_omp_512 not built"
+    with tempfile.TemporaryDirectory() as d:
+        cfg = os.path.join(d, "config")
+        with open(cfg, "w") as fh:
+            # 1 MV slice: the initial condition is outside the per-step timing;
+            # SQRT coupling takes the reference's parallel generate_gaussian.
+            fh.write(f"stat = 1\nmu = {MU}\nmass = {MASS}\nelementaryWilsonLines = 1\nfile_name = bench\n"
+                     f"langevin_steps = {warmup + steps}\nmeasurements = 1\nstep = {STEP}\n"
+                     "EvolutionChoice = MOMENTUM_EVOLUTION\nCouplingChoice = SQRT_COUPLING_CONSTANT\n"
+                     "KernelChoice = SIN_KERNEL\n")
+        env = dict(os.environ)
+        env["OMP_NUM_THREADS"] = str(nthreads or os.cpu_count())
+        r = subprocess.run([REF_MAIN, "1", "1", cfg], cwd=d, capture_output=True, text=True, env=env,
+                           timeout=3600)
+        t = parse_evolution_times(r.stdout)
+        if len(t) < warmup + steps:
+            return None, f"reference run produced {len(t)} step timings (rc={r.returncode})"
+        return statistics.mean(t[warmup:]), None
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cores = os.cpu_count()
+    steps = max(1, min(args.steps, 10))
+    warm = max(1, min(args.warmup, 3))
+    t, why = run_reference_main(steps, warm)
+    if t is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    value = N * N / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": 0,
+        "steps": steps, "warmup": warm, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{EVENTS} events x {N}^2 Langevin evolution (reference: one event at a time)",
+                   "N": N, "events": EVENTS, "step": STEP, "kernel": "SIN", "coupling": "running (SQRT)"},
+        "cpu_baseline": {"value": value, "unit": "site-steps/s", "cores": cores, "kind": "reference",
+                         "sample": f"1 event {N}^2, {steps} Langevin steps after {warm} warm-up; main_optimized "
+                                   f"with OpenMP ({cores} threads, {cpu_model()}), FFTW replaced by the project "
+                                   "FFT shim"},
+        "e2e": {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main_arm(args):
+    rank, world, local = dist_env()
+    sys.path.insert(0, PKG)
+    import torch
+    import jimwlk as jw
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier_max(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local)
+    ids = [eng.add_event(N, ny_slices=NY_SLICES, mu=MU, mass=MASS, step=STEP, coupling=jw.FIXED_COUPLING_CONSTANT,
+                         seed=1_000_003 * (rank + 1) + i) for i in range(EVENTS)]
+    eng.init_mv(ids)
+    eng.step(ids, args.warmup)
+    if eng.sync() != jw.OK:
+        raise RuntimeError("device error during warm-up")
+    sites = EVENTS * N * N
+
+    # ---- timed region: K steps, a CUDA event around every fused kernel
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        pass_ms, total_ms = eng.step_timed(ids, args.steps)
+    torch.cuda.synchronize()
+    status = eng.sync()
+    if status != jw.OK:
+        raise RuntimeError(f"device status {status} in the timed region")
+    total_ms = barrier_max(total_ms)
+    clocks = clk.summary()
+    value = world * sites * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers: per step one
+    # jw_engine_step call (slot list H2D) and one ensemble dipole measurement
+    # read back to host memory (D2H), as main_optimized does with measurements
+    # == langevin_steps.
+    k_e2e = max(3, min(args.steps, 10))
+    sum_h = np.empty((N, N), np.complex128)
+    err_h = np.empty((N, N), np.complex128)
+    eng.measure_ensemble(ids, sum_h, err_h)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(k_e2e):
+        eng.step(ids, 1)
+        eng.measure_ensemble(ids, sum_h, err_h)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = barrier_max(e0.elapsed_time(e1))
+    e2e_value = world * sites * k_e2e / (e2e_ms / 1e3)
+    h2d = 2 * 4 * EVENTS               # slot lists of the step and the measurement
+    d2h = 4 * N * N * 8                # sum, err and their compensation planes
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = measured_peaks()
+    dom = int(np.argmax(pass_ms))
+    name = PASS_NAMES[dom]
+    alg_bytes = PASS_BYTES[name] * sites
+    achieved = alg_bytes / (pass_ms[dom] / 1e3) / 1e9
+    traffic = profiled_traffic().get(name)
+    roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic * sites if traffic else None,
+            "algorithmic_bytes": alg_bytes,
+            "pass_ms": {n: m for n, m in zip(PASS_NAMES, pass_ms)},
+            "pass_frac": {n: PASS_BYTES[n] * sites / (m / 1e3) / 1e9 / peak for n, m in zip(PASS_NAMES, pass_ms)}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 transforms / f64 exponentials and V", "data": "synthetic",
+        "config": {"workload": f"{EVENTS} events x {N}^2, mixed precision, batched (per GPU)", "events": EVENTS,
+                   "N": N, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "alpha_s": ALPHA_S, "ds": DS,
+                   "step": STEP, "kernel": "SIN", "coupling": "fixed", "l2": "inputs ~5.6 GB per GPU > L2",
+                   "parallelism": f"events sharded, {world} rank(s)"},
+        "e2e": {"value": e2e_value, "unit": "site-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": k_e2e, "what": "jw_engine_step + jw_engine_measure_ensemble per step, host arrays"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks,
+        "roofline": roof,
+    }
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        # plain FP64 form: the call-for-call layer (reference structure), one event at a time
+        cfg = jw.config_defaults(Nx=N, Ny=N, seed=7, mu=MU, mass=MASS, elementaryWilsonLines=1, step=STEP,
+                                 CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
+        ctx = jw.Context(cfg)
+        V = ctx.field()
+        ctx.initial_condition(V)
+        ctx.evolve_momentum(V, 0, 2)
+        ctx.sync()
+        s0 = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kp = 5
+        a0.record(s0)
+        ctx.evolve_momentum(V, 2, kp)
+        a1.record(s0)
+        a1.synchronize()
+        plain = N * N * kp / (a0.elapsed_time(a1) / 1e3)
+        line["fp64_plain"] = {"value": plain, "unit": "site-steps/s",
+                              "what": "jw_evolve_momentum, reference call structure, FP64, one 512^2 event",
+                              "mixed_batched_over_plain": value / plain}
+        ctx.close()
+        # CPU baseline: the reference's own main on a bounded sample
+        t, why = run_reference_main(2, 1)
+        if t is not None:
+            line["cpu_baseline"] = {"value": N * N / t, "unit": "site-steps/s", "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"1 event {N}^2, 2 Langevin steps after 1 warm-up; main_optimized "
+                                              f"with OpenMP ({os.cpu_count()} threads, {cpu_model()}), FFT shim"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": "site-steps/s", "cores": 0, "kind": "reference",
+                                    "sample": why}
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64-plain and CPU-baseline legs")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "engine":
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        main_arm(args)
+
+
+if __name__ == "__main__":
+    main()

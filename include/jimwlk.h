@@ -222,6 +222,16 @@ jw_status jw_engine_get_correlator(jw_engine* e, int event_id, double* sum, doub
 jw_status jw_engine_reset_correlator(jw_engine* e, int event_id);
 /* Steps taken so far by an event (its next noise index). */
 jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
+/* One ensemble measurement over the listed events (one lattice size): the
+ * symmetrised correlators of main_optimized.cpp:321-334 summed over the events
+ * as gfield::reduce sums them over stats (field.h:1521-1536), written to host
+ * arrays sum and err (N*N complex each, reference layout t = 1).  The events'
+ * own accumulators are not touched. */
+jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double* sum, double* err);
+/* nsteps Langevin steps of the listed events (one lattice size, one launch
+ * group) with a CUDA event around each of the three fused kernels; returns
+ * the mean milliseconds per kernel (pass_ms[3]) and the total. */
+jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms, double* total_ms);
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Device-side error flags (bit mask in a device int, cleared by the syncs).
+#define JW_FLAG_NOCONV 1
+#define JW_FLAG_NAN 2
+
 namespace jw {
 
 // ------------------------------------------------------------------ complex

@@ -1,0 +1,834 @@
+// jw_engine.cu -- the batched engine: resident events grouped by lattice
+// size, fused Langevin steps (jw_engine_kernels.cuh) launched per group over
+// all requested events at once, CUDA-graph replay of a step, device-side
+// dipole accumulation, and the jw_engine_* C ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "jw_engine_kernels.cuh"
+#include "jw_internal.h"
+
+using namespace jw;
+
+namespace {
+
+constexpr int kCouplings = 4;  // indexed by JW_*_COUPLING_CONSTANT
+
+struct Group {
+    int N = 0;
+    Twiddles tw;
+    EventDev* d_ev = nullptr;        // device descriptors, one per slot
+    std::vector<int> owner;          // event id per slot, -1 if free
+    int* d_slots = nullptr;          // slot lists of the current call
+    int slots_cap = 0;
+    unsigned char* ws = nullptr;     // workspace, ws_events events
+    int ws_events = 0;
+    double* k64[kCouplings] = {};    // kernel tables per coupling ([2][N*N])
+    float* k32[kCouplings] = {};
+    double* nf64 = nullptr;          // noise factor (NOISE coupling)
+    float* nf32 = nullptr;
+};
+
+struct Event {
+    int id = -1;
+    int N = 0;
+    int slot = -1;
+    jw_event_desc desc{};
+    double2* V = nullptr;
+    double* acc = nullptr;
+};
+
+template <typename T> size_t step_ws_bytes(int N) { return sizeof(C2<T>) * 24 * (size_t)N * N; }
+size_t meas_ws_bytes(int N) { return (sizeof(double2) * 9 + sizeof(double)) * (size_t)N * N; }
+size_t mv_ws_bytes(int N) { return sizeof(double2) * 4 * (size_t)N * N; }
+
+bool engine_supported(int precision, int N) {
+    if (!supported_n(N)) return false;
+    if (precision == JW_PRECISION_FP64 && N > 1024) return false;  // pass 3 row of 8 FP64 planes > 128 KB
+    return true;
+}
+
+// prepare_A_local's kernel (field.h:1998-2075) for the SIN kernel, imaginary
+// parts of K_x and K_y divided by N^2 (the two unitary transforms).
+void kernel_table(int N, int coupling, std::vector<double>& t) {
+    const long vol = (long)N * N;
+    t.assign(2 * vol, 0.0);
+    const double inv = 1.0 / ((double)N * (double)N);
+    for (int ix = 0; ix < N; ++ix)
+        for (int iy = 0; iy < N; ++iy) {
+            const long i = (long)ix * N + iy;
+            int xx = ix, yy = iy;
+            if (xx >= N / 2) xx -= N;
+            if (yy >= N / 2) yy -= N;
+            const double px = 2.0 * M_PI * xx / (1.0 * N), py = 2.0 * M_PI * yy / (1.0 * N);
+            if (!(std::fabs(px * px + py * py) > 10e-9)) continue;
+            const double sx = std::sin(M_PI * ix / (1.0 * N)), sy = std::sin(M_PI * iy / (1.0 * N));
+            const double ph2 = 4.0 * std::pow(sx, 2.0) + 4.0 * std::pow(sy, 2.0);
+            double cc = 1.0;
+            if (coupling == JW_SQRT_COUPLING_CONSTANT)
+                cc = 4.0 * M_PI / ((11.0 - 2.0 * 3.0 / 3.0) *
+                                   std::log(std::pow(std::pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2) +
+                                                         std::pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2),
+                                                     0.2)));
+            t[i] = -2.0 * M_PI * std::sqrt(cc) * std::sin(2.0 * M_PI * ix / (1.0 * N)) / ph2 * inv;
+            t[vol + i] = -2.0 * M_PI * std::sqrt(cc) * std::sin(2.0 * M_PI * iy / (1.0 * N)) / ph2 * inv;
+        }
+}
+
+// generate_gaussian_with_noise_coupling_constant's factor at the momentum
+// index equal to the site index (field.h:2267-2273).
+void noise_factor_table(int N, std::vector<double>& t) {
+    t.resize((size_t)N * N);
+    const double tmp = std::pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    const double tmp2 = 4.0 * M_PI / (11.0 - 2.0 * 3.0 / 3.0);
+    for (int ix = 0; ix < N; ++ix)
+        for (int iy = 0; iy < N; ++iy) {
+            const double sx = std::sin(M_PI * ix / (1.0 * N)), sy = std::sin(M_PI * iy / (1.0 * N));
+            const double ph2 = 4.0 * std::pow(sx, 2.0) + 4.0 * std::pow(sy, 2.0);
+            t[(size_t)ix * N + iy] =
+                std::sqrt(tmp2 / std::log(std::pow(tmp + std::pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2), 0.2)));
+        }
+}
+
+template <typename T>
+cudaError_t upload_table(const std::vector<double>& h, T** d) {
+    std::vector<T> c(h.begin(), h.end());
+    cudaError_t e = cudaMalloc(d, sizeof(T) * c.size());
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*d, c.data(), sizeof(T) * c.size(), cudaMemcpyHostToDevice);
+}
+
+__global__ void k_set_unit_planes(double2* V, long vol) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) V[k * vol + i] = make_double2((k == 0 || k == 4 || k == 8) ? 1.0 : 0.0, 0.0);
+}
+
+// reference layout (site-major, 9 interleaved) <-> planes
+__global__ void k_aos_to_planes(const double2* __restrict__ aos, double2* __restrict__ V, long vol) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * vol) return;
+    const long site = i / 9;
+    const int k = (int)(i % 9);
+    V[k * vol + site] = aos[i];
+}
+__global__ void k_planes_to_aos(const double2* __restrict__ V, double2* __restrict__ aos, long vol) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * vol) return;
+    const long site = i / 9;
+    const int k = (int)(i % 9);
+    aos[i] = V[k * vol + site];
+}
+
+}  // namespace
+
+struct jw_engine {
+    jw_engine_options opt{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int* d_flags = nullptr;
+    std::map<int, std::unique_ptr<Group>> groups;  // by N
+    std::map<int, Event> events;                   // by id
+    int next_id = 1;
+    size_t bytes_in_use = 0;
+    size_t budget = 0;
+    double2* d_stage = nullptr;  // host-layout staging for set/get V
+    size_t stage_bytes = 0;
+    double2* h_pinned = nullptr;  // pinned host staging
+    size_t pinned_bytes = 0;
+};
+
+namespace {
+
+template <typename T> int elem_size() { return (int)sizeof(C2<T>); }
+
+size_t ws_per_event(const jw_engine* e, int N) {
+    const size_t s = e->opt.precision == JW_PRECISION_MIXED ? step_ws_bytes<float>(N) : step_ws_bytes<double>(N);
+    return std::max(std::max(s, meas_ws_bytes(N)), mv_ws_bytes(N));
+}
+
+jw_status ensure_workspace(jw_engine* e, Group& g, int nev) {
+    if (g.ws_events >= nev) return JW_OK;
+    const size_t per = ws_per_event(e, g.N);
+    const size_t old = per * (size_t)g.ws_events;
+    const size_t need = per * (size_t)nev;
+    if (e->bytes_in_use - old + need > e->budget) return JW_ENOMEM;
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    if (g.ws) cudaFree(g.ws);
+    g.ws = nullptr;
+    g.ws_events = 0;
+    e->bytes_in_use -= old;
+    if (cudaMalloc(&g.ws, need) != cudaSuccess) return JW_ENOMEM;
+    g.ws_events = nev;
+    e->bytes_in_use += need;
+    return JW_OK;
+}
+
+jw_status ensure_slots(Group& g, int n) {
+    if (g.slots_cap >= n) return JW_OK;
+    if (g.d_slots) cudaFree(g.d_slots);
+    g.d_slots = nullptr;
+    if (cudaMalloc(&g.d_slots, sizeof(int) * n) != cudaSuccess) return JW_ENOMEM;
+    g.slots_cap = n;
+    return JW_OK;
+}
+
+jw_status group_get(jw_engine* e, int N, Group** out) {
+    auto it = e->groups.find(N);
+    if (it != e->groups.end()) {
+        *out = it->second.get();
+        return JW_OK;
+    }
+    auto g = std::make_unique<Group>();
+    g->N = N;
+    JW_CUDA(twiddles_create(N, &g->tw));
+    std::vector<double> t;
+    for (int c : {JW_SQRT_COUPLING_CONSTANT, JW_NOISE_COUPLING_CONSTANT, JW_FIXED_COUPLING_CONSTANT}) {
+        kernel_table(N, c, t);
+        JW_CUDA(upload_table(t, &g->k64[c]));
+        JW_CUDA(upload_table(t, &g->k32[c]));
+    }
+    noise_factor_table(N, t);
+    JW_CUDA(upload_table(t, &g->nf64));
+    JW_CUDA(upload_table(t, &g->nf32));
+    *out = g.get();
+    e->groups[N] = std::move(g);
+    return JW_OK;
+}
+
+jw_status grow_slots(Group& g, cudaStream_t s) {
+    const int old = (int)g.owner.size();
+    const int cap = std::max(4, 2 * old);
+    EventDev* d = nullptr;
+    if (cudaMalloc(&d, sizeof(EventDev) * cap) != cudaSuccess) return JW_ENOMEM;
+    JW_CUDA(cudaMemsetAsync(d, 0, sizeof(EventDev) * cap, s));
+    if (g.d_ev) {
+        JW_CUDA(cudaMemcpyAsync(d, g.d_ev, sizeof(EventDev) * old, cudaMemcpyDeviceToDevice, s));
+        JW_CUDA(cudaStreamSynchronize(s));
+        cudaFree(g.d_ev);
+    }
+    g.d_ev = d;
+    g.owner.resize(cap, -1);
+    return JW_OK;
+}
+
+void group_destroy(Group& g) {
+    twiddles_destroy(&g.tw);
+    if (g.d_ev) cudaFree(g.d_ev);
+    if (g.d_slots) cudaFree(g.d_slots);
+    if (g.ws) cudaFree(g.ws);
+    for (int c = 0; c < kCouplings; ++c) {
+        if (g.k64[c]) cudaFree(g.k64[c]);
+        if (g.k32[c]) cudaFree(g.k32[c]);
+    }
+    if (g.nf64) cudaFree(g.nf64);
+    if (g.nf32) cudaFree(g.nf32);
+}
+
+// --------------------------------------------------------------- launches
+template <typename T, int N>
+cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
+    using V2 = C2<T>;
+    const long vol = (long)N * N;
+    V2* P = reinterpret_cast<V2*>(ws);
+    V2* Q = P + (size_t)16 * vol * nb;
+    const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
+    constexpr int SEQ = p1_seq<T, N>();
+    constexpr int RT = row_threads<N>();
+    constexpr int C = p2_cols<T, N>();
+    const size_t sm1 = sizeof(V2) * padded_len(SEQ * N);
+    const size_t sm2 = sizeof(V2) * 2 * padded_len(N * C);
+    const size_t sm3 = sizeof(V2) * padded_len(8 * N);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_step_pass1<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_step_pass2<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        cudaFuncSetAttribute(k_step_pass3<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
+        configured = true;
+    }
+    k_step_pass1<T, N><<<dim3(N, 16 / SEQ, nb), RT, sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
+    k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);
+    k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, d_slots, Q, tw, e->d_flags);
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_mv_slice(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws, int slice) {
+    double2* P = reinterpret_cast<double2*>(ws);
+    constexpr int RT = row_threads<N>();
+    constexpr int C = p2_cols<double, N>();
+    const size_t sm1 = sizeof(double2) * padded_len(4 * N);
+    const size_t sm2 = sizeof(double2) * padded_len(N * C);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_mv_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_mv_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        cudaFuncSetAttribute(k_mv_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        configured = true;
+    }
+    k_mv_pass1<N><<<dim3(N, nb), RT, sm1, e->stream>>>(g.d_ev, d_slots, slice, P, g.tw.d64);
+    k_mv_pass2<N><<<dim3(N / C, 4, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, g.tw.d64);
+    k_mv_pass3<N><<<dim3(N, nb), RT, sm1, e->stream>>>(g.d_ev, d_slots, P, g.tw.d64, e->d_flags);
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_measure(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
+    const long vol = (long)N * N;
+    double2* M = reinterpret_cast<double2*>(ws);
+    double* corr = reinterpret_cast<double*>(M + (size_t)9 * vol * nb);
+    constexpr int RT = row_threads<N>();
+    constexpr int C = p2_cols<double, N>();
+    constexpr int ROWS = meas_rows_per_cta<N>();
+    const size_t sm1 = sizeof(double2) * padded_len(ROWS * N);
+    const size_t sm2 = sizeof(double2) * padded_len(N * C);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_meas_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_meas_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        configured = true;
+    }
+    (void)RT;
+    k_meas_rows<N><<<dim3((unsigned)((9L * N + ROWS - 1) / ROWS), nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, M,
+                                                                                           g.tw.d64);
+    k_meas_cols<N><<<dim3(N / C, nb), C * (N / 8), sm2, e->stream>>>(d_slots, M, corr, g.tw.d64);
+    k_meas_reduce<N><<<dim3((unsigned)((vol + 255) / 256), nb), 256, 0, e->stream>>>(g.d_ev, d_slots, corr);
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws,
+                                   double* ens) {
+    const long vol = (long)N * N;
+    double2* M = reinterpret_cast<double2*>(ws);
+    double* corr = reinterpret_cast<double*>(M + (size_t)9 * vol * nb);
+    constexpr int C = p2_cols<double, N>();
+    constexpr int ROWS = meas_rows_per_cta<N>();
+    const size_t sm1 = sizeof(double2) * padded_len(ROWS * N);
+    const size_t sm2 = sizeof(double2) * padded_len(N * C);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_meas_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_meas_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        configured = true;
+    }
+    k_meas_rows<N><<<dim3((unsigned)((9L * N + ROWS - 1) / ROWS), nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, M,
+                                                                                           g.tw.d64);
+    k_meas_cols<N><<<dim3(N / C, nb), C * (N / 8), sm2, e->stream>>>(d_slots, M, corr, g.tw.d64);
+    k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, nb, ens);
+    return cudaGetLastError();
+}
+
+#define JW_DISPATCH_N(N, CALL)                   \
+    switch (N) {                                 \
+        case 8: { constexpr int NN = 8; return CALL; }       \
+        case 16: { constexpr int NN = 16; return CALL; }     \
+        case 32: { constexpr int NN = 32; return CALL; }     \
+        case 64: { constexpr int NN = 64; return CALL; }     \
+        case 128: { constexpr int NN = 128; return CALL; }   \
+        case 256: { constexpr int NN = 256; return CALL; }   \
+        case 512: { constexpr int NN = 512; return CALL; }   \
+        case 1024: { constexpr int NN = 1024; return CALL; } \
+        case 2048: { constexpr int NN = 2048; return CALL; } \
+        default: return cudaErrorInvalidValue;   \
+    }
+
+cudaError_t dispatch_step(jw_engine* e, Group& g, const int* d_slots, int nb) {
+    if (e->opt.precision == JW_PRECISION_MIXED) {
+        JW_DISPATCH_N(g.N, (launch_step<float, NN>(e, g, d_slots, nb, g.ws)))
+    }
+    switch (g.N) {
+        case 8: return launch_step<double, 8>(e, g, d_slots, nb, g.ws);
+        case 16: return launch_step<double, 16>(e, g, d_slots, nb, g.ws);
+        case 32: return launch_step<double, 32>(e, g, d_slots, nb, g.ws);
+        case 64: return launch_step<double, 64>(e, g, d_slots, nb, g.ws);
+        case 128: return launch_step<double, 128>(e, g, d_slots, nb, g.ws);
+        case 256: return launch_step<double, 256>(e, g, d_slots, nb, g.ws);
+        case 512: return launch_step<double, 512>(e, g, d_slots, nb, g.ws);
+        case 1024: return launch_step<double, 1024>(e, g, d_slots, nb, g.ws);
+        default: return cudaErrorInvalidValue;
+    }
+}
+cudaError_t dispatch_mv(jw_engine* e, Group& g, const int* d_slots, int nb, int slice) {
+    JW_DISPATCH_N(g.N, (launch_mv_slice<NN>(e, g, d_slots, nb, g.ws, slice)))
+}
+cudaError_t dispatch_measure(jw_engine* e, Group& g, const int* d_slots, int nb) {
+    JW_DISPATCH_N(g.N, (launch_measure<NN>(e, g, d_slots, nb, g.ws)))
+}
+
+cudaError_t dispatch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
+    JW_DISPATCH_N(g.N, (launch_measure_ensemble<NN>(e, g, d_slots, nb, g.ws, ens)))
+}
+
+template <typename T, int N>
+cudaError_t launch_step_timed(jw_engine* e, Group& g, int nb, cudaEvent_t* t) {
+    using V2 = C2<T>;
+    const long vol = (long)N * N;
+    V2* P = reinterpret_cast<V2*>(g.ws);
+    V2* Q = P + (size_t)16 * vol * nb;
+    const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
+    constexpr int SEQ = p1_seq<T, N>();
+    constexpr int RT = row_threads<N>();
+    constexpr int C = p2_cols<T, N>();
+    const size_t sm1 = sizeof(V2) * padded_len(SEQ * N);
+    const size_t sm2 = sizeof(V2) * 2 * padded_len(N * C);
+    const size_t sm3 = sizeof(V2) * padded_len(8 * N);
+    k_step_pass1<T, N><<<dim3(N, 16 / SEQ, nb), RT, sm1, e->stream>>>(g.d_ev, g.d_slots, P, tw);
+    cudaEventRecord(t[1], e->stream);
+    k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, g.d_slots, P, Q, tw);
+    cudaEventRecord(t[2], e->stream);
+    k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, g.d_slots, Q, tw, e->d_flags);
+    cudaEventRecord(t[3], e->stream);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t dispatch_pass_timed(jw_engine* e, Group& g, int nb, cudaEvent_t* t) {
+    if (sizeof(T) == 8 && g.N > 1024) return cudaErrorInvalidValue;
+    switch (g.N) {
+        case 8: return launch_step_timed<T, 8>(e, g, nb, t);
+        case 16: return launch_step_timed<T, 16>(e, g, nb, t);
+        case 32: return launch_step_timed<T, 32>(e, g, nb, t);
+        case 64: return launch_step_timed<T, 64>(e, g, nb, t);
+        case 128: return launch_step_timed<T, 128>(e, g, nb, t);
+        case 256: return launch_step_timed<T, 256>(e, g, nb, t);
+        case 512: return launch_step_timed<T, 512>(e, g, nb, t);
+        case 1024: return launch_step_timed<T, 1024>(e, g, nb, t);
+        case 2048: return launch_step_timed<T, (sizeof(T) == 8 ? 1024 : 2048)>(e, g, nb, t);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Resolve ids into per-group slot lists.
+jw_status collect(jw_engine* e, const int* ids, int n, std::map<int, std::vector<int>>& by_n) {
+    if (n < 0 || (n > 0 && !ids)) return JW_EINVAL;
+    for (int k = 0; k < n; ++k) {
+        auto it = e->events.find(ids[k]);
+        if (it == e->events.end()) return JW_ENOTFOUND;
+        auto& v = by_n[it->second.N];
+        if (std::find(v.begin(), v.end(), it->second.slot) != v.end()) return JW_EINVAL;  // duplicate
+        v.push_back(it->second.slot);
+    }
+    return JW_OK;
+}
+
+int chunk_size(const jw_engine* e, int count) {
+    int c = count;
+    if (e->opt.max_batch > 0) c = std::min(c, e->opt.max_batch);
+    return std::max(c, 1);
+}
+
+jw_status upload_slots(jw_engine* e, Group& g, const std::vector<int>& slots) {
+    jw_status s = ensure_slots(g, (int)slots.size());
+    if (s) return s;
+    JW_CUDA(cudaMemcpyAsync(g.d_slots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    return JW_OK;
+}
+
+jw_status ensure_stage(jw_engine* e, size_t bytes) {
+    if (e->stage_bytes < bytes) {
+        if (e->d_stage) cudaFree(e->d_stage);
+        e->d_stage = nullptr;
+        e->stage_bytes = 0;
+        if (cudaMalloc(&e->d_stage, bytes) != cudaSuccess) return JW_ENOMEM;
+        e->stage_bytes = bytes;
+    }
+    if (e->pinned_bytes < bytes) {
+        if (e->h_pinned) cudaFreeHost(e->h_pinned);
+        e->h_pinned = nullptr;
+        e->pinned_bytes = 0;
+        if (cudaMallocHost(&e->h_pinned, bytes) != cudaSuccess) return JW_ENOMEM;
+        e->pinned_bytes = bytes;
+    }
+    return JW_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+JW_EXPORT jw_status jw_engine_create(const jw_engine_options* opt, int device, jw_engine** out) {
+    JW_CHECK(opt && out);
+    *out = nullptr;
+    JW_CHECK(opt->precision == JW_PRECISION_FP64 || opt->precision == JW_PRECISION_MIXED);
+    JW_CUDA(cudaSetDevice(device));
+    auto* e = new jw_engine();
+    e->opt = *opt;
+    e->device = device;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&e->d_flags, sizeof(int)) != cudaSuccess || cudaMemset(e->d_flags, 0, sizeof(int)) != cudaSuccess) {
+        jw_engine_destroy(e);
+        return JW_ECUDA;
+    }
+    e->budget = opt->max_bytes ? opt->max_bytes : (size_t)(0.9 * (double)free_b);
+    *out = e;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_destroy(jw_engine* e) {
+    if (!e) return JW_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (auto& kv : e->events) {
+        cudaFree(kv.second.V);
+        cudaFree(kv.second.acc);
+    }
+    for (auto& kv : e->groups) group_destroy(*kv.second);
+    if (e->d_flags) cudaFree(e->d_flags);
+    if (e->d_stage) cudaFree(e->d_stage);
+    if (e->h_pinned) cudaFreeHost(e->h_pinned);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_sync(jw_engine* e) {
+    JW_CHECK(e);
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    int flags = 0;
+    JW_CUDA(cudaMemcpy(&flags, e->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags) JW_CUDA(cudaMemset(e->d_flags, 0, sizeof(int)));
+    return flags_to_status(flags);
+}
+
+JW_EXPORT void* jw_engine_stream(jw_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+JW_EXPORT size_t jw_engine_event_bytes(const jw_engine* e, const jw_event_desc* d) {
+    if (!e || !d || !supported_n(d->N)) return 0;
+    const size_t vol = (size_t)d->N * d->N;
+    return vol * (sizeof(double2) * 9 + sizeof(double) * 4) + ws_per_event(e, d->N);
+}
+
+JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, int* event_id) {
+    JW_CHECK(e && d && event_id);
+    *event_id = -1;
+    if (!engine_supported(e->opt.precision, d->N)) return JW_EUNSUPPORTED;
+    if (d->kernel != JW_SIN_KERNEL) return JW_EUNSUPPORTED;
+    if (d->coupling != JW_SQRT_COUPLING_CONSTANT && d->coupling != JW_NOISE_COUPLING_CONSTANT &&
+        d->coupling != JW_FIXED_COUPLING_CONSTANT)
+        return JW_EUNSUPPORTED;
+    JW_CHECK(d->ny_slices >= 0 && d->step >= 0.0 && std::isfinite(d->mu) && std::isfinite(d->mass) &&
+             std::isfinite(d->step));
+    const size_t vol = (size_t)d->N * d->N;
+    const size_t own = vol * (sizeof(double2) * 9 + sizeof(double) * 4);
+    if (e->bytes_in_use + own + ws_per_event(e, d->N) > e->budget) return JW_ENOMEM;
+    Group* g = nullptr;
+    jw_status s = group_get(e, d->N, &g);
+    if (s) return s;
+    int slot = -1;
+    for (int k = 0; k < (int)g->owner.size(); ++k)
+        if (g->owner[k] < 0) {
+            slot = k;
+            break;
+        }
+    if (slot < 0) {
+        slot = (int)g->owner.size();
+        if ((s = grow_slots(*g, e->stream))) return s;
+    }
+    Event ev;
+    ev.id = e->next_id++;
+    ev.N = d->N;
+    ev.slot = slot;
+    ev.desc = *d;
+    if (cudaMalloc(&ev.V, sizeof(double2) * 9 * vol) != cudaSuccess) return JW_ENOMEM;
+    if (cudaMalloc(&ev.acc, sizeof(double) * 4 * vol) != cudaSuccess) {
+        cudaFree(ev.V);
+        return JW_ENOMEM;
+    }
+    e->bytes_in_use += own;
+    k_set_unit_planes<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ev.V, (long)vol);
+    JW_CUDA(cudaMemsetAsync(ev.acc, 0, sizeof(double) * 4 * vol, e->stream));
+    EventDev h{};
+    h.V = ev.V;
+    h.acc = ev.acc;
+    const int cp = d->coupling;
+    h.k64 = g->k64[cp];
+    h.k32 = g->k32[cp];
+    h.nf64 = cp == JW_NOISE_COUPLING_CONSTANT ? g->nf64 : nullptr;
+    h.nf32 = cp == JW_NOISE_COUPLING_CONSTANT ? g->nf32 : nullptr;
+    h.seed = d->seed;
+    h.step = 0;
+    h.sqrt_eps = std::sqrt(d->step);
+    const double gg = 1.0, mu = d->mu / d->N;
+    h.mv_sigma = d->ny_slices > 0 ? gg * mu / std::sqrt((double)d->ny_slices) : 0.0;
+    const double m = d->mass * std::pow(gg, 2.0) * mu;
+    h.mv_mass2 = m * m;
+    h.mv_g = gg;
+    h.N = d->N;
+    h.reunit = e->opt.reunitarize ? 1 : 0;
+    h.nmeas = 0;
+    JW_CUDA(cudaMemcpyAsync(g->d_ev + slot, &h, sizeof(EventDev), cudaMemcpyHostToDevice, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    g->owner[slot] = ev.id;
+    e->events[ev.id] = ev;
+    *event_id = ev.id;
+    return ensure_workspace(e, *g, 1);
+}
+
+JW_EXPORT jw_status jw_engine_remove_event(jw_engine* e, int id) {
+    JW_CHECK(e);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    Event& ev = it->second;
+    Group& g = *e->groups[ev.N];
+    g.owner[ev.slot] = -1;
+    cudaFree(ev.V);
+    cudaFree(ev.acc);
+    const size_t vol = (size_t)ev.N * ev.N;
+    e->bytes_in_use -= vol * (sizeof(double2) * 9 + sizeof(double) * 4);
+    e->events.erase(it);
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_set_V(jw_engine* e, int id, const double* host) {
+    JW_CHECK(e && host);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const long vol = (long)it->second.N * it->second.N;
+    const size_t bytes = sizeof(double2) * 9 * vol;
+    jw_status s = ensure_stage(e, bytes);
+    if (s) return s;
+    std::memcpy(e->h_pinned, host, bytes);
+    JW_CUDA(cudaMemcpyAsync(e->d_stage, e->h_pinned, bytes, cudaMemcpyHostToDevice, e->stream));
+    k_aos_to_planes<<<(unsigned)((9 * vol + 255) / 256), 256, 0, e->stream>>>(e->d_stage, it->second.V, vol);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_get_V(jw_engine* e, int id, double* host) {
+    JW_CHECK(e && host);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const long vol = (long)it->second.N * it->second.N;
+    const size_t bytes = sizeof(double2) * 9 * vol;
+    jw_status s = ensure_stage(e, bytes);
+    if (s) return s;
+    k_planes_to_aos<<<(unsigned)((9 * vol + 255) / 256), 256, 0, e->stream>>>(it->second.V, e->d_stage, vol);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(cudaMemcpyAsync(e->h_pinned, e->d_stage, bytes, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    std::memcpy(host, e->h_pinned, bytes);
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_init_mv(jw_engine* e, const int* ids, int n) {
+    JW_CHECK(e);
+    std::map<int, std::vector<int>> by_n;
+    jw_status s = collect(e, ids, n, by_n);
+    if (s) return s;
+    for (auto& kv : by_n) {
+        Group& g = *e->groups[kv.first];
+        // events of one group and one slice count run together
+        std::map<int, std::vector<int>> by_ny;
+        for (int slot : kv.second) by_ny[e->events[g.owner[slot]].desc.ny_slices].push_back(slot);
+        for (auto& nv : by_ny) {
+            const std::vector<int>& slots = nv.second;
+            const int cs = chunk_size(e, (int)slots.size());
+            if ((s = ensure_workspace(e, g, cs))) return s;
+            if ((s = upload_slots(e, g, slots))) return s;
+            for (size_t c0 = 0; c0 < slots.size(); c0 += cs) {
+                const int nb = (int)std::min<size_t>(cs, slots.size() - c0);
+                for (int slot : std::vector<int>(slots.begin() + c0, slots.begin() + c0 + nb))
+                    k_set_unit_planes<<<(unsigned)(((long)g.N * g.N + 255) / 256), 256, 0, e->stream>>>(
+                        e->events[g.owner[slot]].V, (long)g.N * g.N);
+                for (int sl = 0; sl < nv.first; ++sl) JW_CUDA(dispatch_mv(e, g, g.d_slots + c0, nb, sl));
+            }
+        }
+    }
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_step(jw_engine* e, const int* ids, int n, int nsteps) {
+    JW_CHECK(e && nsteps >= 0);
+    std::map<int, std::vector<int>> by_n;
+    jw_status s = collect(e, ids, n, by_n);
+    if (s || nsteps == 0) return s;
+    // per group: workspace for one chunk, slot list on the device
+    struct Work { Group* g; int nb; int off; };
+    std::vector<Work> work;
+    for (auto& kv : by_n) {
+        Group& g = *e->groups[kv.first];
+        const int cs = chunk_size(e, (int)kv.second.size());
+        if ((s = ensure_workspace(e, g, cs))) return s;
+        if ((s = upload_slots(e, g, kv.second))) return s;
+        for (int c0 = 0; c0 < (int)kv.second.size(); c0 += cs)
+            work.push_back({&g, std::min(cs, (int)kv.second.size() - c0), c0});
+    }
+    // one step of every chunk, captured once as a graph and replayed
+    auto record = [&]() -> cudaError_t {
+        for (const Work& w : work) {
+            cudaError_t ce = dispatch_step(e, *w.g, w.g->d_slots + w.off, w.nb);
+            if (ce != cudaSuccess) return ce;
+        }
+        return cudaSuccess;
+    };
+    if (nsteps == 1) {
+        JW_CUDA(record());
+        return JW_OK;
+    }
+    // groups that share one workspace run chunk after chunk inside the step,
+    // which stream order keeps correct within the graph as well
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    JW_CUDA(record());  // first step also sets kernel attributes outside capture
+    JW_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = record();
+    cudaError_t ce2 = cudaStreamEndCapture(e->stream, &graph);
+    if (ce != cudaSuccess || ce2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return JW_ECUDA;
+    }
+    JW_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    for (int k = 1; k < nsteps; ++k) {
+        ce = cudaGraphLaunch(exec, e->stream);
+        if (ce != cudaSuccess) break;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    JW_CUDA(ce);
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_measure(jw_engine* e, const int* ids, int n) {
+    JW_CHECK(e);
+    std::map<int, std::vector<int>> by_n;
+    jw_status s = collect(e, ids, n, by_n);
+    if (s) return s;
+    for (auto& kv : by_n) {
+        Group& g = *e->groups[kv.first];
+        const int cs = chunk_size(e, (int)kv.second.size());
+        if ((s = ensure_workspace(e, g, cs))) return s;
+        if ((s = upload_slots(e, g, kv.second))) return s;
+        for (int c0 = 0; c0 < (int)kv.second.size(); c0 += cs)
+            JW_CUDA(dispatch_measure(e, g, g.d_slots + c0, std::min(cs, (int)kv.second.size() - c0)));
+    }
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_get_correlator(jw_engine* e, int id, double* sum, double* err, int* nmeas) {
+    JW_CHECK(e);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const Event& ev = it->second;
+    const long vol = (long)ev.N * ev.N;
+    std::vector<double> h(4 * vol);
+    JW_CUDA(cudaMemcpyAsync(h.data(), ev.acc, sizeof(double) * 4 * vol, cudaMemcpyDeviceToHost, e->stream));
+    EventDev d{};
+    JW_CUDA(cudaMemcpyAsync(&d, e->groups[ev.N]->d_ev + ev.slot, sizeof(EventDev), cudaMemcpyDeviceToHost,
+                            e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    for (long i = 0; i < vol; ++i) {
+        if (sum) { sum[2 * i] = h[i] + h[vol + i]; sum[2 * i + 1] = 0.0; }
+        if (err) { err[2 * i] = h[2 * vol + i] + h[3 * vol + i]; err[2 * i + 1] = 0.0; }
+    }
+    if (nmeas) *nmeas = d.nmeas;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_reset_correlator(jw_engine* e, int id) {
+    JW_CHECK(e);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const Event& ev = it->second;
+    JW_CUDA(cudaMemsetAsync(ev.acc, 0, sizeof(double) * 4 * (size_t)ev.N * ev.N, e->stream));
+    const int zero = 0;
+    JW_CUDA(cudaMemcpyAsync(&e->groups[ev.N]->d_ev[ev.slot].nmeas, &zero, sizeof(int), cudaMemcpyHostToDevice,
+                            e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_event_steps(jw_engine* e, int id, uint64_t* steps) {
+    JW_CHECK(e && steps);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    EventDev d{};
+    JW_CUDA(cudaMemcpyAsync(&d, e->groups[it->second.N]->d_ev + it->second.slot, sizeof(EventDev),
+                            cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    *steps = d.step;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double* sum, double* err) {
+    JW_CHECK(e && sum && err && n > 0);
+    std::map<int, std::vector<int>> by_n;
+    jw_status s = collect(e, ids, n, by_n);
+    if (s) return s;
+    if (by_n.size() != 1) return JW_EINVAL;  // one lattice size per ensemble
+    Group& g = *e->groups[by_n.begin()->first];
+    const std::vector<int>& slots = by_n.begin()->second;
+    const long vol = (long)g.N * g.N;
+    const int cs = chunk_size(e, (int)slots.size());
+    if ((s = ensure_workspace(e, g, cs))) return s;
+    if ((s = upload_slots(e, g, slots))) return s;
+    if ((s = ensure_stage(e, sizeof(double) * 4 * vol))) return s;
+    double* ens = reinterpret_cast<double*>(e->d_stage);
+    JW_CUDA(cudaMemsetAsync(ens, 0, sizeof(double) * 4 * vol, e->stream));
+    for (int c0 = 0; c0 < (int)slots.size(); c0 += cs)
+        JW_CUDA(dispatch_measure_ensemble(e, g, g.d_slots + c0, std::min(cs, (int)slots.size() - c0), ens));
+    double* h = reinterpret_cast<double*>(e->h_pinned);
+    JW_CUDA(cudaMemcpyAsync(h, ens, sizeof(double) * 4 * vol, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    for (long i = 0; i < vol; ++i) {
+        sum[2 * i] = h[i] + h[vol + i];
+        sum[2 * i + 1] = 0.0;
+        err[2 * i] = h[2 * vol + i] + h[3 * vol + i];
+        err[2 * i + 1] = 0.0;
+    }
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms,
+                                         double* total_ms) {
+    JW_CHECK(e && nsteps > 0 && pass_ms && total_ms);
+    std::map<int, std::vector<int>> by_n;
+    jw_status s = collect(e, ids, n, by_n);
+    if (s) return s;
+    if (by_n.size() != 1) return JW_EINVAL;  // timing is reported for one lattice size
+    Group& g = *e->groups[by_n.begin()->first];
+    const std::vector<int>& slots = by_n.begin()->second;
+    const int nb = (int)slots.size();
+    if (chunk_size(e, nb) != nb) return JW_EINVAL;
+    if ((s = ensure_workspace(e, g, nb))) return s;
+    if ((s = upload_slots(e, g, slots))) return s;
+    JW_CUDA(dispatch_step(e, g, g.d_slots, nb));  // kernel attributes, outside the timing
+    std::vector<cudaEvent_t> ev(4 * nsteps);
+    for (auto& x : ev) JW_CUDA(cudaEventCreate(&x));
+    const bool mixed = e->opt.precision == JW_PRECISION_MIXED;
+    cudaError_t ce = cudaSuccess;
+    for (int k = 0; k < nsteps && ce == cudaSuccess; ++k) {
+        cudaEvent_t* t = &ev[4 * k];
+        ce = cudaEventRecord(t[0], e->stream);
+        if (ce == cudaSuccess) ce = mixed ? dispatch_pass_timed<float>(e, g, nb, t) : dispatch_pass_timed<double>(e, g, nb, t);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    double tot = 0, p[3] = {0, 0, 0};
+    for (int k = 0; k < nsteps && ce == cudaSuccess; ++k) {
+        float a;
+        for (int q = 0; q < 3; ++q) {
+            cudaEventElapsedTime(&a, ev[4 * k + q], ev[4 * k + q + 1]);
+            p[q] += a;
+        }
+    }
+    if (ce == cudaSuccess) {
+        float a;
+        cudaEventElapsedTime(&a, ev[0], ev[4 * (nsteps - 1) + 3]);
+        tot = a;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    JW_CUDA(ce);
+    for (int q = 0; q < 3; ++q) pass_ms[q] = p[q] / nsteps;
+    *total_ms = tot;
+    return JW_OK;
+}

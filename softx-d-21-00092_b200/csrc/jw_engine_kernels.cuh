@@ -1,0 +1,474 @@
+// jw_engine_kernels.cuh -- the fused kernels of the batched engine.
+//
+// One Langevin step (main_optimized.cpp:243-304) of every event in a batch is
+// three launches over the events' planes:
+//
+//  pass 1 (row)    per row x: 16 Philox normals per site (field.h:2116-2243 /
+//                  2245-2365), V xi V^dagger (field.h:1892-1933) projected on
+//                  the 8 Gell-Mann coefficients, packed as 16 complex sequences
+//                     s = 0..3   n_{2s} + i n_{2s+1}       (xi_x)
+//                     s = 4..7   m_{2s'} + i m_{2s'+1}     (xi_y)
+//                     s = 8..11  bx_{2s'} + i bx_{2s'+1}   (V xi_x V^dagger)
+//                     s = 12..15 by_{2s'} + i by_{2s'+1}   (V xi_y V^dagger)
+//                  and row-transformed (forward) into P[16][N][N].
+//  pass 2 (column) per output plane j and column tile: column transform of the
+//                  x- and y-packs, W = K_x Zx + K_y Zy (prepare_A_local,
+//                  field.h:1998-2075, with the 1/N^2 of the two unitary
+//                  transforms folded into K), inverse column transform into
+//                  Q[8][N][N]: j = 0..3 give A, 4..7 give B.
+//  pass 3 (row)    inverse row transform of Q's row x, which yields
+//                  A_{2s} + i A_{2s+1} (the kernel is Hermitian-symmetric for
+//                  the SIN kernel, so both coefficients are real), then per
+//                  site the FP64 update V <- exp(+i sqrt(eps) B) V exp(-i sqrt(eps) A)
+//                  (update_uf, field.h:1966-1996) through the eigen-route
+//                  exponential, optional reunitarisation, and the event's step
+//                  counter advances.
+//
+// Because x_a -> sum_a x_a L_a is linear and the transforms are linear,
+// transforming the 8 real coefficients instead of the 9 complex matrix
+// entries gives the reference's A and B up to rounding; the 72 plane
+// transforms of a reference step become 24 (16 forward, 8 inverse).
+//
+// The MV initial condition (main_optimized.cpp:178-191) uses the same three
+// passes with 4 planes per slice and the Poisson kernel, in FP64.  The dipole
+// measurement (main_optimized.cpp:321-334) transforms V's 9 planes in FP64 and
+// accumulates |V~|^2 per momentum in the column pass.
+#pragma once
+
+#include "jw_fft.cuh"
+
+namespace jw {
+
+struct EventDev {
+    double2* V;                 // 9 planes of N*N
+    double* acc;                // 4 planes of N*N: sum, sum compensation, err, err compensation
+    const double* k64;          // kernel tables: [2][N*N] imag(K_x), imag(K_y), scaled by 1/N^2
+    const float* k32;
+    const double* nf64;         // per-site noise factor (NOISE coupling) or null
+    const float* nf32;
+    unsigned long long seed;
+    unsigned long long step;    // next Langevin step index (advanced by pass 3)
+    double sqrt_eps;            // sqrt(step)
+    double mv_sigma;            // g mu / sqrt(ny_slices)
+    double mv_mass2;            // (mass * g^2 * mu)^2
+    double mv_g;
+    int N;
+    int reunit;
+    int nmeas;
+    int pad_;
+};
+
+// sequences of the row pass kept per CTA (shared memory <= 128 KB)
+template <typename T, int N> constexpr int p1_seq() {
+    constexpr int cap = 131072 / (N * (int)sizeof(C2<T>));
+    return cap >= 16 ? 16 : (cap >= 8 ? 8 : 4);
+}
+template <int N> constexpr int row_threads() { return (N / 8) > 256 ? (N / 8) : 256; }
+// column tile width: 64-byte row segments, capped so the tile holds <= 64 KB
+template <typename T, int N> constexpr int p2_cols() {
+    constexpr int want = 64 / (int)sizeof(C2<T>);
+    constexpr int cap = 65536 / (N * (int)sizeof(C2<T>));
+    constexpr int c = want < cap ? want : (cap > 0 ? cap : 1);
+    return c < N ? c : N;
+}
+
+// Transform NSEQ contiguous padded sequences in rounds of blockDim/(N/8).
+template <typename T, int N, int NSEQ>
+__device__ __forceinline__ void fft_rows_smem(C2<T>* sm, T sign, const C2<T>* __restrict__ tw) {
+    constexpr int TPS = N / 8;
+    const int spr = blockDim.x / TPS;
+    const int r = threadIdx.x / TPS;
+    for (int s0 = 0; s0 < NSEQ; s0 += spr) {
+        const int s = s0 + r;
+        fft_smem<T, N>(sm, RowIdx{s * N}, threadIdx.x % TPS, r < spr && s < NSEQ, sign, tw);
+    }
+}
+
+template <typename T> __device__ __forceinline__ const T* ktab(const EventDev& e);
+template <> __device__ __forceinline__ const double* ktab<double>(const EventDev& e) { return e.k64; }
+template <> __device__ __forceinline__ const float* ktab<float>(const EventDev& e) { return e.k32; }
+template <typename T> __device__ __forceinline__ const T* nftab(const EventDev& e);
+template <> __device__ __forceinline__ const double* nftab<double>(const EventDev& e) { return e.nf64; }
+template <> __device__ __forceinline__ const float* nftab<float>(const EventDev& e) { return e.nf32; }
+
+// ------------------------------------------------------------------ pass 1
+template <typename T, int N>
+__global__ void __launch_bounds__(row_threads<N>()) k_step_pass1(const EventDev* __restrict__ ev,
+                                                                  const int* __restrict__ slots,
+                                                                  C2<T>* __restrict__ P,
+                                                                  const C2<T>* __restrict__ tw) {
+    using V2 = C2<T>;
+    constexpr int SEQ = p1_seq<T, N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V2* sm = reinterpret_cast<V2*>(smem_raw);
+    const int x = blockIdx.x, g = blockIdx.y, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const int s_lo = g * SEQ, s_hi = s_lo + SEQ;
+    const bool need_rot = s_hi > 8;
+    const T* nf = nftab<T>(e);
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        T z[16];
+        langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
+        const T f = nf ? nf[site] : (T)1;
+        T n[8], m[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            n[k] = z[2 * k] * f;
+            m[k] = z[2 * k + 1] * f;
+        }
+        T vals[16 * 2];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            vals[2 * s] = n[2 * s]; vals[2 * s + 1] = n[2 * s + 1];
+            vals[8 + 2 * s] = m[2 * s]; vals[8 + 2 * s + 1] = m[2 * s + 1];
+        }
+        if (need_rot) {
+            V2 v[9], xi[9], t[9], r[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const double2 d = e.V[k * vol + site];
+                v[k] = mk<T>((T)d.x, (T)d.y);
+            }
+            T h[8];
+            embed_lambda<T>(n, xi);
+            mul3(v, xi, t);
+            mul3_adj(t, v, r);
+            project_lambda<T>(r, h);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) vals[16 + k] = h[k];
+            embed_lambda<T>(m, xi);
+            mul3(v, xi, t);
+            mul3_adj(t, v, r);
+            project_lambda<T>(r, h);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) vals[24 + k] = h[k];
+        }
+#pragma unroll
+        for (int s = 0; s < 16; ++s)
+            if (s >= s_lo && s < s_hi) sm[pad((s - s_lo) * N + y)] = mk<T>(vals[2 * s], vals[2 * s + 1]);
+    }
+    __syncthreads();
+    fft_rows_smem<T, N, SEQ>(sm, (T)-1, tw);
+    V2* out = P + ((long)b * 16 + s_lo) * vol + (long)x * N;
+    for (int i = threadIdx.x; i < SEQ * N; i += blockDim.x) {
+        const int s = i / N, y = i % N;
+        out[s * vol + y] = sm[pad(i)];
+    }
+}
+
+// ------------------------------------------------------------------ pass 2
+template <typename T, int N>
+__global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8)) k_step_pass2(const EventDev* __restrict__ ev,
+                                                                           const int* __restrict__ slots,
+                                                                           const C2<T>* __restrict__ P,
+                                                                           C2<T>* __restrict__ Q,
+                                                                           const C2<T>* __restrict__ tw) {
+    using V2 = C2<T>;
+    constexpr int C = p2_cols<T, N>();
+    constexpr int TILE = padded_len(N * C);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V2* t0 = reinterpret_cast<V2*>(smem_raw);
+    V2* t1 = t0 + TILE;
+    const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const int p0 = j < 4 ? j : 8 + (j - 4), p1 = p0 + 4;
+    const V2* in0 = P + ((long)b * 16 + p0) * vol + c0;
+    const V2* in1 = P + ((long)b * 16 + p1) * vol + c0;
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
+        const long off = (long)(i / C) * N + (i % C);
+        t0[pad(i)] = in0[off];
+        t1[pad(i)] = in1[off];
+    }
+    __syncthreads();
+    const int c = threadIdx.x % C, t = threadIdx.x / C;
+    fft_smem<T, N>(t0, ColIdx<C>{c}, t, true, (T)-1, tw);
+    fft_smem<T, N>(t1, ColIdx<C>{c}, t, true, (T)-1, tw);
+    const T* kt = ktab<T>(e);
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
+        const long k = (long)(i / C) * N + c0 + (i % C);
+        const T kx = kt[k], ky = kt[vol + k];
+        const V2 a = t0[pad(i)], bb = t1[pad(i)];
+        // (i kx) a + (i ky) b
+        t0[pad(i)] = mk<T>(-kx * a.y - ky * bb.y, kx * a.x + ky * bb.x);
+    }
+    __syncthreads();
+    fft_smem<T, N>(t0, ColIdx<C>{c}, t, true, (T)1, tw);
+    V2* out = Q + ((long)b * 8 + j) * vol + c0;
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) out[(long)(i / C) * N + (i % C)] = t0[pad(i)];
+}
+
+// ------------------------------------------------------------------ pass 3
+template <typename T, int N>
+__global__ void __launch_bounds__(row_threads<N>()) k_step_pass3(EventDev* __restrict__ ev,
+                                                                  const int* __restrict__ slots,
+                                                                  const C2<T>* __restrict__ Q,
+                                                                  const C2<T>* __restrict__ tw,
+                                                                  int* __restrict__ flags) {
+    using V2 = C2<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V2* sm = reinterpret_cast<V2*>(smem_raw);
+    const int x = blockIdx.x, b = blockIdx.y;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const V2* in = Q + (long)b * 8 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 8 * N; i += blockDim.x) sm[pad(i)] = in[(long)(i / N) * vol + (i % N)];
+    __syncthreads();
+    fft_rows_smem<T, N, 8>(sm, (T)1, tw);
+    const double se = e.sqrt_eps;
+    int fl = 0;
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        double a[8], bq[8];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const V2 u = sm[pad(s * N + y)], w = sm[pad((4 + s) * N + y)];
+            a[2 * s] = (double)u.x; a[2 * s + 1] = (double)u.y;
+            bq[2 * s] = (double)w.x; bq[2 * s + 1] = (double)w.y;
+        }
+        double2 mA[9], mB[9], v[9], tmp[9];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            a[k] *= se;
+            bq[k] *= -se;
+        }
+        embed_lambda<double>(a, mA);
+        embed_lambda<double>(bq, mB);
+        int st = expi_herm(mB, -1.0);
+        st |= expi_herm(mA, -1.0);
+        const long site = (long)x * N + y;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
+        mul3(mB, v, tmp);
+        mul3(tmp, mA, v);
+        if (e.reunit) reunitarize(v);
+        if (st) fl |= JW_FLAG_NOCONV;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+            e.V[k * vol + site] = v[k];
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+    if (x == 0 && threadIdx.x == 0) e.step += 1;
+}
+
+// ------------------------------------------------------------------ MV initial condition (FP64)
+// slice pass 1: rho_a = sigma z_a packed as 4 sequences rho_{2s} + i rho_{2s+1}, row transform.
+template <int N>
+__global__ void __launch_bounds__(row_threads<N>()) k_mv_pass1(const EventDev* __restrict__ ev,
+                                                                const int* __restrict__ slots, int slice,
+                                                                double2* __restrict__ P,
+                                                                const double2* __restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int x = blockIdx.x, b = blockIdx.y;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        double z[8];
+        mv_normals<double>(e.seed, (uint32_t)slice, (uint32_t)((long)x * N + y), z);
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            sm[pad(s * N + y)] = make_double2(z[2 * s] * e.mv_sigma + 0.0, z[2 * s + 1] * e.mv_sigma + 0.0);
+    }
+    __syncthreads();
+    fft_rows_smem<double, N, 4>(sm, -1.0, tw);
+    double2* out = P + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x) out[(long)(i / N) * vol + (i % N)] = sm[pad(i)];
+}
+
+// slice pass 2: column transform, x -g/(-phat2 + m^2)/N^2 (solvePoisson, field.h:867-877), inverse.
+template <int N>
+__global__ void __launch_bounds__(p2_cols<double, N>() * (N / 8)) k_mv_pass2(const EventDev* __restrict__ ev,
+                                                                              const int* __restrict__ slots,
+                                                                              double2* __restrict__ P,
+                                                                              const double2* __restrict__ tw) {
+    constexpr int C = p2_cols<double, N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* t0 = reinterpret_cast<double2*>(smem_raw);
+    const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    double2* io = P + ((long)b * 4 + j) * vol + c0;
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) t0[pad(i)] = io[(long)(i / C) * N + (i % C)];
+    __syncthreads();
+    const int c = threadIdx.x % C, t = threadIdx.x / C;
+    fft_smem<double, N>(t0, ColIdx<C>{c}, t, true, -1.0, tw);
+    const double inv = 1.0 / ((double)N * (double)N);
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
+        const int kx = i / C, ky = c0 + i % C;
+        const double fac = -1.0 * e.mv_g / (-phat2_d(kx, ky, N) + e.mv_mass2) * inv;
+        t0[pad(i)] = cscale(t0[pad(i)], fac);
+    }
+    __syncthreads();
+    fft_smem<double, N>(t0, ColIdx<C>{c}, t, true, 1.0, tw);
+    for (int i = threadIdx.x; i < N * C; i += blockDim.x) io[(long)(i / C) * N + (i % C)] = t0[pad(i)];
+}
+
+// slice pass 3: inverse row transform, f = sum_a f_a L_a, V <- V exp(+i f) (field.h:337-365).
+template <int N>
+__global__ void __launch_bounds__(row_threads<N>()) k_mv_pass3(EventDev* __restrict__ ev,
+                                                                const int* __restrict__ slots,
+                                                                const double2* __restrict__ P,
+                                                                const double2* __restrict__ tw,
+                                                                int* __restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int x = blockIdx.x, b = blockIdx.y;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const double2* in = P + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x) sm[pad(i)] = in[(long)(i / N) * vol + (i % N)];
+    __syncthreads();
+    fft_rows_smem<double, N, 4>(sm, 1.0, tw);
+    int fl = 0;
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        double f[8];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double2 u = sm[pad(s * N + y)];
+            f[2 * s] = u.x;
+            f[2 * s + 1] = u.y;
+        }
+        double2 m[9], v[9], r[9];
+        embed_lambda<double>(f, m);
+        const int st = expi_herm(m, 1.0);
+        const long site = (long)x * N + y;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
+        mul3(v, m, r);
+        if (st) fl |= JW_FLAG_NOCONV;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            if (!isfinite(r[k].x) || !isfinite(r[k].y)) fl |= JW_FLAG_NAN;
+            e.V[k * vol + site] = r[k];
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+}
+
+// ------------------------------------------------------------------ measurement (FP64)
+// rows of V's 9 planes, forward, out of place into M: the 9*N rows of an
+// event are contiguous, ROWS of them per CTA
+template <int N> constexpr int meas_rows_per_cta() { return (2048 / N) > 0 ? (2048 / N) : 1; }
+
+template <int N>
+__global__ void __launch_bounds__(256) k_meas_rows(const EventDev* __restrict__ ev, const int* __restrict__ slots,
+                                                   double2* __restrict__ M, const double2* __restrict__ tw) {
+    constexpr int ROWS = meas_rows_per_cta<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int b = blockIdx.y;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const long row0 = (long)blockIdx.x * ROWS;
+    const int nr = (int)min((long)ROWS, 9L * N - row0);
+    const double2* in = e.V + row0 * N;
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) sm[pad(i)] = in[i];
+    __syncthreads();
+    constexpr int TPS = N / 8;
+    const int r = threadIdx.x / TPS;
+    fft_smem<double, N>(sm, RowIdx{r * N}, threadIdx.x % TPS, r < nr, -1.0, tw);
+    double2* out = M + (long)b * 9 * vol + row0 * N;
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) out[i] = sm[pad(i)];
+}
+
+// columns: sum over the 9 components of |X|^2 / N^6  (trace, field.h:1375-1432)
+template <int N>
+__global__ void __launch_bounds__(p2_cols<double, N>() * (N / 8)) k_meas_cols(const int* __restrict__ slots,
+                                                                               const double2* __restrict__ M,
+                                                                               double* __restrict__ corr,
+                                                                               const double2* __restrict__ tw) {
+    constexpr int C = p2_cols<double, N>();
+    constexpr int PER = 8;  // tile elements per thread: N*C / (C*N/8)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* t0 = reinterpret_cast<double2*>(smem_raw);
+    const int c0 = blockIdx.x * C, b = blockIdx.y;
+    const long vol = (long)N * N;
+    double acc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) acc[q] = 0.0;
+    const int c = threadIdx.x % C, t = threadIdx.x / C;
+    for (int comp = 0; comp < 9; ++comp) {
+        const double2* in = M + ((long)b * 9 + comp) * vol + c0;
+        for (int i = threadIdx.x; i < N * C; i += blockDim.x) t0[pad(i)] = in[(long)(i / C) * N + (i % C)];
+        __syncthreads();
+        fft_smem<double, N>(t0, ColIdx<C>{c}, t, true, -1.0, tw);
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const double2 v = t0[pad(threadIdx.x + q * blockDim.x)];
+            acc[q] += v.x * v.x + v.y * v.y;
+        }
+        __syncthreads();
+    }
+    const double n2 = (double)N * (double)N;
+    const double inv = 1.0 / (n2 * n2 * n2);
+    double* out = corr + (long)b * vol + c0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int i = threadIdx.x + q * blockDim.x;
+        out[(long)(i / C) * N + (i % C)] = acc[q] * inv;
+    }
+    (void)slots;
+}
+
+// average_and_symmetrize (field.h:1460-1492) + reduce (field.h:1521-1536) with
+// compensated (Neumaier) FP64 accumulation of sum and sum of squares.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
+    const double t = s + v;
+    c += (fabs(s) >= fabs(v)) ? (s - t) + v : (v - t) + s;
+    s = t;
+}
+
+template <int N>
+__global__ void k_meas_reduce(EventDev* __restrict__ ev, const int* __restrict__ slots,
+                              const double* __restrict__ corr) {
+    const long vol = (long)N * N;
+    const int b = blockIdx.y;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    EventDev& e = ev[slots[b]];
+    if (i < vol) {
+        const double* cb = corr + (long)b * vol;
+        const int x = (int)(i / N), y = (int)(i % N);
+        const int a = (N - x) % N, bb = (N - y) % N;
+        auto tsym = [&](int p, int q) { return 0.5 * (cb[(long)p * N + q] + cb[(long)q * N + p]); };
+        const double s = 0.25 * (((tsym(x, y) + tsym(a, y)) + tsym(x, bb)) + tsym(a, bb));
+        double* acc = e.acc;
+        double s0 = acc[i], s1 = acc[vol + i], e0 = acc[2 * vol + i], e1 = acc[3 * vol + i];
+        neumaier_add(s0, s1, s);
+        neumaier_add(e0, e1, s * s);
+        acc[i] = s0;
+        acc[vol + i] = s1;
+        acc[2 * vol + i] = e0;
+        acc[3 * vol + i] = e1;
+    }
+    if (i == 0) e.nmeas += 1;
+}
+
+// Ensemble measurement: symmetrise the correlators of the nb events of a
+// batch and add their sum and sum of squares (over events) into ens[4][N*N]
+// (sum, compensation, err, compensation) -- gfield::reduce over stats.
+template <int N>
+__global__ void k_meas_reduce_ensemble(const double* __restrict__ corr, int nb, double* __restrict__ ens) {
+    const long vol = (long)N * N;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    const int x = (int)(i / N), y = (int)(i % N);
+    const int a = (N - x) % N, bb = (N - y) % N;
+    double s0 = ens[i], s1 = ens[vol + i], e0 = ens[2 * vol + i], e1 = ens[3 * vol + i];
+    for (int b = 0; b < nb; ++b) {
+        const double* cb = corr + (long)b * vol;
+        auto tsym = [&](int p, int q) { return 0.5 * (cb[(long)p * N + q] + cb[(long)q * N + p]); };
+        const double s = 0.25 * (((tsym(x, y) + tsym(a, y)) + tsym(x, bb)) + tsym(a, bb));
+        neumaier_add(s0, s1, s);
+        neumaier_add(e0, e1, s * s);
+    }
+    ens[i] = s0;
+    ens[vol + i] = s1;
+    ens[2 * vol + i] = e0;
+    ens[3 * vol + i] = e1;
+}
+
+}  // namespace jw

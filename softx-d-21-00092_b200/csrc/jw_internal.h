@@ -11,9 +11,6 @@
 
 #define JW_EXPORT extern "C" __attribute__((visibility("default")))
 
-// Device-side error flags (bit mask in a device int, cleared by the syncs).
-#define JW_FLAG_NOCONV 1
-#define JW_FLAG_NAN 2
 
 #define JW_CUDA(call)                                                                         \
     do {                                                                                      \

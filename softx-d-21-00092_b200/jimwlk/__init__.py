@@ -89,6 +89,24 @@ def _load():
         "jw_print": ([_vp, ctypes.c_int, _vp, _vp, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
         "jw_initial_condition": ([_vp, _vp], ctypes.c_int),
         "jw_evolve_momentum": ([_vp, _vp, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
+        "jw_engine_create": ([ctypes.POINTER(jw_engine_options), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+        "jw_engine_destroy": ([_vp], ctypes.c_int),
+        "jw_engine_sync": ([_vp], ctypes.c_int),
+        "jw_engine_stream": ([_vp], _vp),
+        "jw_engine_event_bytes": ([_vp, ctypes.POINTER(jw_event_desc)], ctypes.c_size_t),
+        "jw_engine_add_event": ([_vp, ctypes.POINTER(jw_event_desc), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "jw_engine_remove_event": ([_vp, ctypes.c_int], ctypes.c_int),
+        "jw_engine_init_mv": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+        "jw_engine_set_V": ([_vp, ctypes.c_int, _dp], ctypes.c_int),
+        "jw_engine_get_V": ([_vp, ctypes.c_int, _dp], ctypes.c_int),
+        "jw_engine_step": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "jw_engine_measure": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+        "jw_engine_get_correlator": ([_vp, ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "jw_engine_reset_correlator": ([_vp, ctypes.c_int], ctypes.c_int),
+        "jw_engine_event_steps": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "jw_engine_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp], ctypes.c_int),
+        "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
+                                 ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -239,3 +257,125 @@ class Field:
 
     def set_zero(self):
         _ck(_lib.jw_field_set_zero(self._h), "jw_field_set_zero")
+
+
+def _ids(ids):
+    ids = list(ids)
+    arr = (ctypes.c_int * max(len(ids), 1))(*ids)
+    return arr, len(ids)
+
+
+class Engine:
+    """The batched engine (jw_engine): resident events advanced by fused kernels."""
+
+    def __init__(self, precision: int = PRECISION_MIXED, reunitarize: bool = False, max_bytes: int = 0,
+                 max_batch: int = 0, device: int = 0):
+        self.opt = jw_engine_options(precision, int(reunitarize), max_bytes, max_batch)
+        self._h = _vp()
+        _ck(_lib.jw_engine_create(ctypes.byref(self.opt), device, ctypes.byref(self._h)), "jw_engine_create")
+        self.N = {}
+
+    def close(self):
+        if self._h:
+            _lib.jw_engine_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return _lib.jw_engine_stream(self._h) or 0
+
+    def sync(self) -> int:
+        return _lib.jw_engine_sync(self._h)
+
+    def event_bytes(self, **desc) -> int:
+        d = jw_event_desc(**desc)
+        return _lib.jw_engine_event_bytes(self._h, ctypes.byref(d))
+
+    def add_event(self, N: int, ny_slices: int = 50, mu: float | None = None, mass: float = 0.04,
+                  step: float = 0.0004, coupling: int = FIXED_COUPLING_CONSTANT, kernel: int = SIN_KERNEL,
+                  seed: int = 1) -> int:
+        d = jw_event_desc(N, ny_slices, 0.5 * N if mu is None else mu, mass, step, coupling, kernel, seed)
+        eid = ctypes.c_int(-1)
+        _ck(_lib.jw_engine_add_event(self._h, ctypes.byref(d), ctypes.byref(eid)), "jw_engine_add_event")
+        self.N[eid.value] = N
+        return eid.value
+
+    def try_add_event(self, **kw):
+        """add_event returning (status, id) instead of raising."""
+        N = kw["N"]
+        d = jw_event_desc(N, kw.get("ny_slices", 50), kw.get("mu", 0.5 * N), kw.get("mass", 0.04),
+                          kw.get("step", 0.0004), kw.get("coupling", FIXED_COUPLING_CONSTANT),
+                          kw.get("kernel", SIN_KERNEL), kw.get("seed", 1))
+        eid = ctypes.c_int(-1)
+        st = _lib.jw_engine_add_event(self._h, ctypes.byref(d), ctypes.byref(eid))
+        if st == OK:
+            self.N[eid.value] = N
+        return st, eid.value
+
+    def remove_event(self, eid: int):
+        _ck(_lib.jw_engine_remove_event(self._h, eid), "jw_engine_remove_event")
+        self.N.pop(eid, None)
+
+    def init_mv(self, ids):
+        arr, n = _ids(ids)
+        _ck(_lib.jw_engine_init_mv(self._h, arr, n), "jw_engine_init_mv")
+
+    def step(self, ids, nsteps: int = 1):
+        arr, n = _ids(ids)
+        _ck(_lib.jw_engine_step(self._h, arr, n, nsteps), "jw_engine_step")
+
+    def measure(self, ids):
+        arr, n = _ids(ids)
+        _ck(_lib.jw_engine_measure(self._h, arr, n), "jw_engine_measure")
+
+    def set_V(self, eid: int, V: np.ndarray):
+        N = self.N[eid]
+        V = np.ascontiguousarray(V, np.complex128)
+        assert V.shape == (N, N, 9)
+        _ck(_lib.jw_engine_set_V(self._h, eid, V.ctypes.data_as(_dp)), "jw_engine_set_V")
+
+    def get_V(self, eid: int) -> np.ndarray:
+        N = self.N[eid]
+        V = np.empty((N, N, 9), np.complex128)
+        _ck(_lib.jw_engine_get_V(self._h, eid, V.ctypes.data_as(_dp)), "jw_engine_get_V")
+        return V
+
+    def correlator(self, eid: int):
+        N = self.N[eid]
+        s = np.empty((N, N), np.complex128)
+        e = np.empty((N, N), np.complex128)
+        n = ctypes.c_int(0)
+        _ck(_lib.jw_engine_get_correlator(self._h, eid, s.ctypes.data_as(_dp), e.ctypes.data_as(_dp),
+                                          ctypes.byref(n)), "jw_engine_get_correlator")
+        return s, e, n.value
+
+    def reset_correlator(self, eid: int):
+        _ck(_lib.jw_engine_reset_correlator(self._h, eid), "jw_engine_reset_correlator")
+
+    def steps_taken(self, eid: int) -> int:
+        v = ctypes.c_uint64(0)
+        _ck(_lib.jw_engine_event_steps(self._h, eid, ctypes.byref(v)), "jw_engine_event_steps")
+        return v.value
+
+    def measure_ensemble(self, ids, sum_out: np.ndarray | None = None, err_out: np.ndarray | None = None):
+        ids = list(ids)
+        N = self.N[ids[0]]
+        s = np.empty((N, N), np.complex128) if sum_out is None else sum_out
+        e = np.empty((N, N), np.complex128) if err_out is None else err_out
+        arr, n = _ids(ids)
+        _ck(_lib.jw_engine_measure_ensemble(self._h, arr, n, s.ctypes.data_as(_dp), e.ctypes.data_as(_dp)),
+            "jw_engine_measure_ensemble")
+        return s, e
+
+    def step_timed(self, ids, nsteps: int):
+        arr, n = _ids(ids)
+        p = (ctypes.c_double * 3)()
+        tot = ctypes.c_double(0)
+        _ck(_lib.jw_engine_step_timed(self._h, arr, n, nsteps, p, ctypes.byref(tot)), "jw_engine_step_timed")
+        return list(p), tot.value
