@@ -221,14 +221,15 @@ def main_arm(args):
             import torch.distributed as dist
             dist.barrier()
 
-    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local)
+    events = args.events
+    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch)
     ids = [eng.add_event(N, ny_slices=NY_SLICES, mu=MU, mass=MASS, step=STEP, coupling=jw.FIXED_COUPLING_CONSTANT,
-                         seed=1_000_003 * (rank + 1) + i) for i in range(EVENTS)]
+                         seed=1_000_003 * (rank + 1) + i) for i in range(events)]
     eng.init_mv(ids)
     eng.step(ids, args.warmup)
     if eng.sync() != jw.OK:
         raise RuntimeError("device error during warm-up")
-    sites = EVENTS * N * N
+    sites = events * N * N
 
     # ---- timed region: K steps, a CUDA event around every fused kernel
     barrier()
@@ -263,7 +264,7 @@ def main_arm(args):
     e1.synchronize()
     e2e_ms = barrier_max(e0.elapsed_time(e1))
     e2e_value = world * sites * k_e2e / (e2e_ms / 1e3)
-    h2d = 2 * 4 * EVENTS               # slot lists of the step and the measurement
+    h2d = 2 * 4 * events               # slot lists of the step and the measurement
     d2h = 4 * N * N * 8                # sum, err and their compensation planes
 
     # ---- roofline of the dominant kernel
@@ -283,7 +284,8 @@ def main_arm(args):
         "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 transforms / f64 exponentials and V", "data": "synthetic",
-        "config": {"workload": f"{EVENTS} events x {N}^2, mixed precision, batched (per GPU)", "events": EVENTS,
+        "config": {"workload": f"{events} events x {N}^2, mixed precision, batched (per GPU)", "events": events,
+                   "max_batch": args.max_batch,
                    "N": N, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "alpha_s": ALPHA_S, "ds": DS,
                    "step": STEP, "kernel": "SIN", "coupling": "fixed", "l2": "inputs ~5.6 GB per GPU > L2",
                    "parallelism": f"events sharded, {world} rank(s)"},
@@ -341,6 +343,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64-plain and CPU-baseline legs")
+    ap.add_argument("--events", type=int, default=EVENTS, help="events per GPU (profiling runs use fewer)")
+    ap.add_argument("--max-batch", type=int, default=0, help="events per launch group (0 = engine default)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "engine":
         args.warmup = 3

@@ -228,9 +228,10 @@ jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
  * arrays sum and err (N*N complex each, reference layout t = 1).  The events'
  * own accumulators are not touched. */
 jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double* sum, double* err);
-/* nsteps Langevin steps of the listed events (one lattice size, one launch
- * group) with a CUDA event around each of the three fused kernels; returns
- * the mean milliseconds per kernel (pass_ms[3]) and the total. */
+/* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
+ * event around each fused kernel launch; returns the milliseconds per step
+ * spent in each of the three kernels (summed over launch groups, pass_ms[3])
+ * and the total time from the first launch to the last. */
 jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms, double* total_ms);
 
 #ifdef __cplusplus

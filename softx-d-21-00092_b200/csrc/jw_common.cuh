@@ -400,6 +400,81 @@ __device__ __forceinline__ int expi_herm(double2 m[9], double sign) {
     return status;
 }
 
+// exp(i Q) of a traceless Hermitian 3x3 by the Cayley-Hamilton theorem:
+// exp(iQ) = f0 + f1 Q + f2 Q^2 with the coefficients of C. Morningstar and
+// M. Peardon, Phys. Rev. D 69 (2004) 054501, eqs. (23)-(33):
+//   c0 = det Q, c1 = tr(Q^2)/2, c0max = 2 (c1/3)^(3/2), theta = acos(c0/c0max),
+//   u = sqrt(c1/3) cos(theta/3), w = sqrt(c1) sin(theta/3), xi0(w) = sin(w)/w,
+//   h0 = (u^2 - w^2) e^{2iu} + e^{-iu} [8u^2 cos w + 2iu (3u^2 + w^2) xi0],
+//   h1 = 2u e^{2iu} - e^{-iu} [2u cos w - i (3u^2 - w^2) xi0],
+//   h2 = e^{2iu} - e^{-iu} [cos w + 3iu xi0],       f_j = h_j / (9u^2 - w^2),
+// evaluated for |c0| (f_j(-c0) = (-1)^j conj f_j(c0)) so that 9u^2 - w^2 >= 2 c1.
+// For c1 < 1e-4 (|Q| below ~1e-2) the series of exp(iQ) reduced with
+// Q^3 = c1 Q + c0 is used instead (truncation ~|Q|^7/7! < 1e-17).
+// Only the upper triangle and the real diagonal of m are read.
+__device__ __forceinline__ void expi_ch(double2 m[9], double sign) {
+    const double a = sign * m[0].x, b = sign * m[4].x, c = sign * m[8].x;
+    const double2 d = cscale(m[1], sign), f = cscale(m[2], sign), e = cscale(m[5], sign);
+    const double dd = cabs2(d), ee = cabs2(e), ff = cabs2(f);
+    // Q^2 (Hermitian): diagonal and upper triangle
+    const double q00 = a * a + dd + ff, q11 = dd + b * b + ee, q22 = ff + ee + c * c;
+    const double2 q01 = cadd(cscale(d, a + b), cmulc(f, e));           // a d + d b + f conj(e)
+    const double2 q02 = cadd(cscale(f, a + c), cmul(d, e));            // a f + d e + f c
+    const double2 q12 = cadd(cmul(cconj(d), f), cscale(e, b + c));     // conj(d) f + b e + e c
+    const double c1 = 0.5 * (q00 + q11 + q22);
+    const double2 def = cmulc(cmul(d, e), f);                          // d e conj(f)
+    const double c0 = a * b * c - a * ee - b * ff - c * dd + 2.0 * def.x;
+    double2 f0, f1, f2;
+    if (c1 < 1e-4) {
+        // f0 = 1 - i c0/6 + i c1 c0/120 - c0^2/720,  f1 = i(1 - c1/6 + c1^2/120) + c0/24 - c0 c1/360,
+        // f2 = -1/2 + c1/24 - c1^2/720 + i c0/120
+        f0 = make_double2(1.0 - c0 * c0 / 720.0, -c0 / 6.0 + c1 * c0 / 120.0);
+        f1 = make_double2(c0 / 24.0 - c0 * c1 / 360.0, 1.0 - c1 / 6.0 + c1 * c1 / 120.0);
+        f2 = make_double2(-0.5 + c1 / 24.0 - c1 * c1 / 720.0, c0 / 120.0);
+    } else {
+        const bool neg = c0 < 0.0;
+        const double c0a = fabs(c0);
+        const double s13 = sqrt(c1 / 3.0);
+        const double c0max = 2.0 * s13 * s13 * s13;
+        const double r = fmin(c0a / c0max, 1.0);
+        const double theta = acos(r);
+        double st, ct;
+        sincos(theta / 3.0, &st, &ct);
+        const double u = s13 * ct, w = sqrt(c1) * st;
+        const double u2 = u * u, w2 = w * w;
+        double su, cu, sw, cw;
+        sincos(u, &su, &cu);
+        sincos(w, &sw, &cw);
+        const double xi0 = (fabs(w) < 0.05) ? 1.0 - w2 / 6.0 * (1.0 - w2 / 20.0 * (1.0 - w2 / 42.0)) : sw / w;
+        // e^{2iu} = (cos 2u, sin 2u) from the half angle; e^{-iu} = (cos u, -sin u)
+        const double2 e2 = make_double2(1.0 - 2.0 * su * su, 2.0 * su * cu);
+        const double2 em = make_double2(cu, -su);
+        const double2 h0 = cadd(cscale(e2, u2 - w2), cmul(em, make_double2(8.0 * u2 * cw, 2.0 * u * (3.0 * u2 + w2) * xi0)));
+        const double2 h1 = csub(cscale(e2, 2.0 * u), cmul(em, make_double2(2.0 * u * cw, -(3.0 * u2 - w2) * xi0)));
+        const double2 h2 = csub(e2, cmul(em, make_double2(cw, 3.0 * u * xi0)));
+        const double inv = 1.0 / (9.0 * u2 - w2);
+        f0 = cscale(h0, inv);
+        f1 = cscale(h1, inv);
+        f2 = cscale(h2, inv);
+        if (neg) {
+            f0 = cconj(f0);
+            f1 = make_double2(-f1.x, f1.y);
+            f2 = cconj(f2);
+        }
+    }
+    // exp(iQ) = f0 I + f1 Q + f2 Q^2, Q and Q^2 Hermitian
+    const double2 Qm[9] = {make_double2(a, 0.0), d, f, cconj(d), make_double2(b, 0.0), e, cconj(f), cconj(e),
+                           make_double2(c, 0.0)};
+    const double2 Q2[9] = {make_double2(q00, 0.0), q01, q02, cconj(q01), make_double2(q11, 0.0), q12,
+                           cconj(q02), cconj(q12), make_double2(q22, 0.0)};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        double2 v = cadd(cmul(f1, Qm[k]), cmul(f2, Q2[k]));
+        if (k == 0 || k == 4 || k == 8) v = cadd(v, f0);
+        m[k] = v;
+    }
+}
+
 // Reunitarisation: Gram-Schmidt on rows 0 and 1, row 2 = conj(row0 x row1),
 // which is the nearest-in-practice SU(3) projection for a matrix that is
 // unitary up to rounding.

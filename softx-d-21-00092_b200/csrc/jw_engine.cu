@@ -238,12 +238,11 @@ cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsi
     V2* P = reinterpret_cast<V2*>(ws);
     V2* Q = P + (size_t)16 * vol * nb;
     const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
-    constexpr int SEQ = p1_seq<T, N>();
     constexpr int RT = row_threads<N>();
     constexpr int C = p2_cols<T, N>();
-    const size_t sm1 = sizeof(V2) * padded_len(SEQ * N);
-    const size_t sm2 = sizeof(V2) * 2 * padded_len(N * C);
-    const size_t sm3 = sizeof(V2) * padded_len(8 * N);
+    const size_t sm1 = p1_smem<T, N>(1);
+    const size_t sm2 = p2_smem<T, N>();
+    const size_t sm3 = p3_smem<T, N>();
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_step_pass1<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
@@ -251,7 +250,7 @@ cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsi
         cudaFuncSetAttribute(k_step_pass3<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
         configured = true;
     }
-    k_step_pass1<T, N><<<dim3(N, 16 / SEQ, nb), RT, sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
+    k_step_pass1<T, N><<<dim3(N, 2, nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
     k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);
     k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, d_slots, Q, tw, e->d_flags);
     return cudaGetLastError();
@@ -366,40 +365,42 @@ cudaError_t dispatch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots
 }
 
 template <typename T, int N>
-cudaError_t launch_step_timed(jw_engine* e, Group& g, int nb, cudaEvent_t* t) {
+cudaError_t launch_step_timed(jw_engine* e, Group& g, const int* d_slots, int nb, cudaEvent_t* t) {
     using V2 = C2<T>;
     const long vol = (long)N * N;
     V2* P = reinterpret_cast<V2*>(g.ws);
     V2* Q = P + (size_t)16 * vol * nb;
     const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
-    constexpr int SEQ = p1_seq<T, N>();
     constexpr int RT = row_threads<N>();
     constexpr int C = p2_cols<T, N>();
-    const size_t sm1 = sizeof(V2) * padded_len(SEQ * N);
-    const size_t sm2 = sizeof(V2) * 2 * padded_len(N * C);
-    const size_t sm3 = sizeof(V2) * padded_len(8 * N);
-    k_step_pass1<T, N><<<dim3(N, 16 / SEQ, nb), RT, sm1, e->stream>>>(g.d_ev, g.d_slots, P, tw);
+    const size_t sm1 = p1_smem<T, N>(1);
+    const size_t sm2 = p2_smem<T, N>();
+    const size_t sm3 = p3_smem<T, N>();
+    cudaEventRecord(t[0], e->stream);
+    k_step_pass1<T, N><<<dim3(N, 2, nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
     cudaEventRecord(t[1], e->stream);
-    k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, g.d_slots, P, Q, tw);
     cudaEventRecord(t[2], e->stream);
-    k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, g.d_slots, Q, tw, e->d_flags);
+    k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);
     cudaEventRecord(t[3], e->stream);
+    cudaEventRecord(t[4], e->stream);
+    k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, d_slots, Q, tw, e->d_flags);
+    cudaEventRecord(t[5], e->stream);
     return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t dispatch_pass_timed(jw_engine* e, Group& g, int nb, cudaEvent_t* t) {
+cudaError_t dispatch_pass_timed(jw_engine* e, Group& g, const int* d_slots, int nb, cudaEvent_t* t) {
     if (sizeof(T) == 8 && g.N > 1024) return cudaErrorInvalidValue;
     switch (g.N) {
-        case 8: return launch_step_timed<T, 8>(e, g, nb, t);
-        case 16: return launch_step_timed<T, 16>(e, g, nb, t);
-        case 32: return launch_step_timed<T, 32>(e, g, nb, t);
-        case 64: return launch_step_timed<T, 64>(e, g, nb, t);
-        case 128: return launch_step_timed<T, 128>(e, g, nb, t);
-        case 256: return launch_step_timed<T, 256>(e, g, nb, t);
-        case 512: return launch_step_timed<T, 512>(e, g, nb, t);
-        case 1024: return launch_step_timed<T, 1024>(e, g, nb, t);
-        case 2048: return launch_step_timed<T, (sizeof(T) == 8 ? 1024 : 2048)>(e, g, nb, t);
+        case 8: return launch_step_timed<T, 8>(e, g, d_slots, nb, t);
+        case 16: return launch_step_timed<T, 16>(e, g, d_slots, nb, t);
+        case 32: return launch_step_timed<T, 32>(e, g, d_slots, nb, t);
+        case 64: return launch_step_timed<T, 64>(e, g, d_slots, nb, t);
+        case 128: return launch_step_timed<T, 128>(e, g, d_slots, nb, t);
+        case 256: return launch_step_timed<T, 256>(e, g, d_slots, nb, t);
+        case 512: return launch_step_timed<T, 512>(e, g, d_slots, nb, t);
+        case 1024: return launch_step_timed<T, 1024>(e, g, d_slots, nb, t);
+        case 2048: return launch_step_timed<T, (sizeof(T) == 8 ? 1024 : 2048)>(e, g, d_slots, nb, t);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -799,36 +800,38 @@ JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, in
     Group& g = *e->groups[by_n.begin()->first];
     const std::vector<int>& slots = by_n.begin()->second;
     const int nb = (int)slots.size();
-    if (chunk_size(e, nb) != nb) return JW_EINVAL;
-    if ((s = ensure_workspace(e, g, nb))) return s;
+    const int cs = chunk_size(e, nb);
+    const int nch = (nb + cs - 1) / cs;
+    if ((s = ensure_workspace(e, g, cs))) return s;
     if ((s = upload_slots(e, g, slots))) return s;
-    JW_CUDA(dispatch_step(e, g, g.d_slots, nb));  // kernel attributes, outside the timing
-    std::vector<cudaEvent_t> ev(4 * nsteps);
+    JW_CUDA(dispatch_step(e, g, g.d_slots, std::min(cs, nb)));  // kernel attributes, outside the timing
+    const int per_step = 6 * nch;
+    std::vector<cudaEvent_t> ev((size_t)per_step * nsteps);
     for (auto& x : ev) JW_CUDA(cudaEventCreate(&x));
     const bool mixed = e->opt.precision == JW_PRECISION_MIXED;
     cudaError_t ce = cudaSuccess;
-    for (int k = 0; k < nsteps && ce == cudaSuccess; ++k) {
-        cudaEvent_t* t = &ev[4 * k];
-        ce = cudaEventRecord(t[0], e->stream);
-        if (ce == cudaSuccess) ce = mixed ? dispatch_pass_timed<float>(e, g, nb, t) : dispatch_pass_timed<double>(e, g, nb, t);
-    }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-    double tot = 0, p[3] = {0, 0, 0};
-    for (int k = 0; k < nsteps && ce == cudaSuccess; ++k) {
-        float a;
-        for (int q = 0; q < 3; ++q) {
-            cudaEventElapsedTime(&a, ev[4 * k + q], ev[4 * k + q + 1]);
-            p[q] += a;
+    for (int k = 0; k < nsteps && ce == cudaSuccess; ++k)
+        for (int c = 0; c < nch && ce == cudaSuccess; ++c) {
+            cudaEvent_t* t = &ev[(size_t)k * per_step + 6 * c];
+            const int nbc = std::min(cs, nb - c * cs);
+            ce = mixed ? dispatch_pass_timed<float>(e, g, g.d_slots + c * cs, nbc, t)
+                       : dispatch_pass_timed<double>(e, g, g.d_slots + c * cs, nbc, t);
         }
-    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    double p[3] = {0, 0, 0}, tot = 0;
     if (ce == cudaSuccess) {
         float a;
-        cudaEventElapsedTime(&a, ev[0], ev[4 * (nsteps - 1) + 3]);
+        for (size_t b = 0; b < ev.size(); b += 6)
+            for (int q = 0; q < 3; ++q) {
+                cudaEventElapsedTime(&a, ev[b + 2 * q], ev[b + 2 * q + 1]);
+                p[q] += a;
+            }
+        cudaEventElapsedTime(&a, ev.front(), ev.back());
         tot = a;
     }
     for (auto& x : ev) cudaEventDestroy(x);
     JW_CUDA(ce);
-    for (int q = 0; q < 3; ++q) pass_ms[q] = p[q] / nsteps;
+    for (int q = 0; q < 3; ++q) pass_ms[q] = p[q] / nsteps;  // per step, summed over launch groups
     *total_ms = tot;
     return JW_OK;
 }

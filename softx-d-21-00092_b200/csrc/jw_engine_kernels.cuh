@@ -58,18 +58,47 @@ struct EventDev {
     int pad_;
 };
 
-// sequences of the row pass kept per CTA (shared memory <= 128 KB)
-template <typename T, int N> constexpr int p1_seq() {
-    constexpr int cap = 131072 / (N * (int)sizeof(C2<T>));
-    return cap >= 16 ? 16 : (cap >= 8 ? 8 : 4);
-}
 template <int N> constexpr int row_threads() { return (N / 8) > 256 ? (N / 8) : 256; }
+// V is staged through shared memory in chunks of at most 512 sites (72 KB)
+template <int N> constexpr int v_chunk() { return N < 512 ? N : 512; }
 // column tile width: 64-byte row segments, capped so the tile holds <= 64 KB
 template <typename T, int N> constexpr int p2_cols() {
     constexpr int want = 64 / (int)sizeof(C2<T>);
     constexpr int cap = 65536 / (N * (int)sizeof(C2<T>));
     constexpr int c = want < cap ? want : (cap > 0 ? cap : 1);
     return c < N ? c : N;
+}
+template <typename T, int N> constexpr size_t p2_smem() {
+    return sizeof(C2<T>) * 2 * padded_len(N * p2_cols<T, N>()) + sizeof(T) * 2 * N * p2_cols<T, N>();
+}
+template <typename T, int N> constexpr size_t p1_smem(int group) {
+    return sizeof(C2<T>) * padded_len(8 * N) + (group ? sizeof(double2) * 9 * v_chunk<N>() : 0);
+}
+template <typename T, int N> constexpr size_t p3_smem() {
+    return sizeof(C2<T>) * padded_len(8 * N) + sizeof(double2) * 9 * v_chunk<N>();
+}
+
+// ---- asynchronous global -> shared copies (cp.async, sm_80+)
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (B == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+// V sites [c0, c0 + VC) of row x into smV[k][VC] (16-byte copies)
+template <int N>
+__device__ __forceinline__ void stage_v(double2* smV, const double2* __restrict__ V, long vol, int x, int c0) {
+    constexpr int VC = v_chunk<N>();
+    for (int i = threadIdx.x; i < 9 * VC; i += blockDim.x) {
+        const int k = i / VC, yy = i - k * VC;
+        cp_async<16>(&smV[i], &V[k * vol + (long)x * N + c0 + yy]);
+    }
 }
 
 // Transform NSEQ contiguous padded sequences in rounds of blockDim/(N/8).
@@ -92,75 +121,88 @@ template <> __device__ __forceinline__ const double* nftab<double>(const EventDe
 template <> __device__ __forceinline__ const float* nftab<float>(const EventDev& e) { return e.nf32; }
 
 // ------------------------------------------------------------------ pass 1
+// blockIdx.y = 0: sequences 0..7 (the noise itself); 1: sequences 8..15
+// (V xi V^dagger), whose CTA stages V through shared memory (cp.async) in
+// chunks of v_chunk sites.
 template <typename T, int N>
-__global__ void __launch_bounds__(row_threads<N>()) k_step_pass1(const EventDev* __restrict__ ev,
-                                                                  const int* __restrict__ slots,
-                                                                  C2<T>* __restrict__ P,
-                                                                  const C2<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(256) k_step_pass1(const EventDev* __restrict__ ev, const int* __restrict__ slots,
+                                                    C2<T>* __restrict__ P, const C2<T>* __restrict__ tw) {
     using V2 = C2<T>;
-    constexpr int SEQ = p1_seq<T, N>();
+    constexpr int VC = v_chunk<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V2* sm = reinterpret_cast<V2*>(smem_raw);
+    double2* smV = reinterpret_cast<double2*>(smem_raw + sizeof(V2) * padded_len(8 * N));
     const int x = blockIdx.x, g = blockIdx.y, b = blockIdx.z;
     const EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
-    const int s_lo = g * SEQ, s_hi = s_lo + SEQ;
-    const bool need_rot = s_hi > 8;
     const T* nf = nftab<T>(e);
-    for (int y = threadIdx.x; y < N; y += blockDim.x) {
-        const long site = (long)x * N + y;
-        T z[16];
-        langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
-        const T f = nf ? nf[site] : (T)1;
-        T n[8], m[8];
+    if (g == 0) {
+        for (int y = threadIdx.x; y < N; y += blockDim.x) {
+            const long site = (long)x * N + y;
+            T z[16];
+            langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
+            const T f = nf ? nf[site] : (T)1;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            n[k] = z[2 * k] * f;
-            m[k] = z[2 * k + 1] * f;
-        }
-        T vals[16 * 2];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            vals[2 * s] = n[2 * s]; vals[2 * s + 1] = n[2 * s + 1];
-            vals[8 + 2 * s] = m[2 * s]; vals[8 + 2 * s + 1] = m[2 * s + 1];
-        }
-        if (need_rot) {
-            V2 v[9], xi[9], t[9], r[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                const double2 d = e.V[k * vol + site];
-                v[k] = mk<T>((T)d.x, (T)d.y);
+            for (int s = 0; s < 4; ++s) {
+                sm[pad(s * N + y)] = mk<T>(z[4 * s] * f, z[4 * s + 2] * f);            // n_{2s} + i n_{2s+1}
+                sm[pad((4 + s) * N + y)] = mk<T>(z[4 * s + 1] * f, z[4 * s + 3] * f);  // m_{2s} + i m_{2s+1}
             }
-            T h[8];
-            embed_lambda<T>(n, xi);
-            mul3(v, xi, t);
-            mul3_adj(t, v, r);
-            project_lambda<T>(r, h);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) vals[16 + k] = h[k];
-            embed_lambda<T>(m, xi);
-            mul3(v, xi, t);
-            mul3_adj(t, v, r);
-            project_lambda<T>(r, h);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) vals[24 + k] = h[k];
         }
+    } else {
+        stage_v<N>(smV, e.V, vol, x, 0);
+        cp_async_commit();
+        for (int c0 = 0; c0 < N; c0 += VC) {
+            if (c0 > 0) {
+                __syncthreads();
+                stage_v<N>(smV, e.V, vol, x, c0);
+                cp_async_commit();
+            }
+            cp_async_wait<0>();
+            __syncthreads();
+            for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
+                const long site = (long)x * N + y;
+                T z[16];
+                langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
+                const T f = nf ? nf[site] : (T)1;
+                T n[8], m[8], h[8];
 #pragma unroll
-        for (int s = 0; s < 16; ++s)
-            if (s >= s_lo && s < s_hi) sm[pad((s - s_lo) * N + y)] = mk<T>(vals[2 * s], vals[2 * s + 1]);
+                for (int k = 0; k < 8; ++k) {
+                    n[k] = z[2 * k] * f;
+                    m[k] = z[2 * k + 1] * f;
+                }
+                V2 v[9], xi[9], t[9], r[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    const double2 dv = smV[k * VC + (y - c0)];
+                    v[k] = mk<T>((T)dv.x, (T)dv.y);
+                }
+                embed_lambda<T>(n, xi);
+                mul3(v, xi, t);
+                mul3_adj(t, v, r);
+                project_lambda<T>(r, h);
+#pragma unroll
+                for (int s = 0; s < 4; ++s) sm[pad(s * N + y)] = mk<T>(h[2 * s], h[2 * s + 1]);
+                embed_lambda<T>(m, xi);
+                mul3(v, xi, t);
+                mul3_adj(t, v, r);
+                project_lambda<T>(r, h);
+#pragma unroll
+                for (int s = 0; s < 4; ++s) sm[pad((4 + s) * N + y)] = mk<T>(h[2 * s], h[2 * s + 1]);
+            }
+        }
     }
     __syncthreads();
-    fft_rows_smem<T, N, SEQ>(sm, (T)-1, tw);
-    V2* out = P + ((long)b * 16 + s_lo) * vol + (long)x * N;
-    for (int i = threadIdx.x; i < SEQ * N; i += blockDim.x) {
-        const int s = i / N, y = i % N;
+    fft_rows_smem<T, N, 8>(sm, (T)-1, tw);
+    V2* out = P + ((long)b * 16 + 8 * g) * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 8 * N; i += blockDim.x) {
+        const int s = i / N, y = i - s * N;
         out[s * vol + y] = sm[pad(i)];
     }
 }
 
 // ------------------------------------------------------------------ pass 2
 template <typename T, int N>
-__global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8)) k_step_pass2(const EventDev* __restrict__ ev,
+__global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8), p2_cols<T, N>() * (N / 8) <= 512 ? 2 : 1) k_step_pass2(const EventDev* __restrict__ ev,
                                                                            const int* __restrict__ slots,
                                                                            const C2<T>* __restrict__ P,
                                                                            C2<T>* __restrict__ Q,
@@ -168,6 +210,8 @@ __global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8)) k_step_pass2(const 
     using V2 = C2<T>;
     constexpr int C = p2_cols<T, N>();
     constexpr int TILE = padded_len(N * C);
+    constexpr int TH = C * (N / 8);
+    constexpr int PER = (N * C) / TH;  // = 8
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V2* t0 = reinterpret_cast<V2*>(smem_raw);
     V2* t1 = t0 + TILE;
@@ -175,79 +219,105 @@ __global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8)) k_step_pass2(const 
     const EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     const int p0 = j < 4 ? j : 8 + (j - 4), p1 = p0 + 4;
-    const V2* in0 = P + ((long)b * 16 + p0) * vol + c0;
-    const V2* in1 = P + ((long)b * 16 + p1) * vol + c0;
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
-        const long off = (long)(i / C) * N + (i % C);
-        t0[pad(i)] = in0[off];
-        t1[pad(i)] = in1[off];
+    // thread -> (row r0 + q N/8, column cc) of the tile for q < PER
+    const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
+    constexpr int RSTEP = TH / C;  // = N / 8
+    const V2* in0 = P + ((long)b * 16 + p0) * vol + c0 + (long)r0 * N + cc;
+    const V2* in1 = P + ((long)b * 16 + p1) * vol + c0 + (long)r0 * N + cc;
+    // kernel table tile (imag K_x, imag K_y) beside the data tiles
+    T* kxs = reinterpret_cast<T*>(t1 + TILE);
+    T* kys = kxs + N * C;
+    const T* kt = ktab<T>(e) + c0 + (long)r0 * N + cc;
+#pragma unroll 1
+    for (int q = 0; q < PER; ++q) {
+        const int i = threadIdx.x + q * TH;
+        const int goff = q * RSTEP * N;
+        cp_async<(int)sizeof(V2)>(&t0[pad(i)], in0 + goff);
+        cp_async<(int)sizeof(V2)>(&t1[pad(i)], in1 + goff);
+        cp_async<(int)sizeof(T)>(&kxs[i], kt + goff);
+        cp_async<(int)sizeof(T)>(&kys[i], kt + vol + goff);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     const int c = threadIdx.x % C, t = threadIdx.x / C;
     fft_smem<T, N>(t0, ColIdx<C>{c}, t, true, (T)-1, tw);
     fft_smem<T, N>(t1, ColIdx<C>{c}, t, true, (T)-1, tw);
-    const T* kt = ktab<T>(e);
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
-        const long k = (long)(i / C) * N + c0 + (i % C);
-        const T kx = kt[k], ky = kt[vol + k];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int i = threadIdx.x + q * TH;
         const V2 a = t0[pad(i)], bb = t1[pad(i)];
+        const T kx = kxs[i], ky = kys[i];
         // (i kx) a + (i ky) b
         t0[pad(i)] = mk<T>(-kx * a.y - ky * bb.y, kx * a.x + ky * bb.x);
     }
     __syncthreads();
     fft_smem<T, N>(t0, ColIdx<C>{c}, t, true, (T)1, tw);
-    V2* out = Q + ((long)b * 8 + j) * vol + c0;
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) out[(long)(i / C) * N + (i % C)] = t0[pad(i)];
+    V2* out = Q + ((long)b * 8 + j) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll 2
+    for (int q = 0; q < PER; ++q) out[q * RSTEP * N] = t0[pad(threadIdx.x + q * TH)];
 }
 
 // ------------------------------------------------------------------ pass 3
 template <typename T, int N>
-__global__ void __launch_bounds__(row_threads<N>()) k_step_pass3(EventDev* __restrict__ ev,
-                                                                  const int* __restrict__ slots,
-                                                                  const C2<T>* __restrict__ Q,
-                                                                  const C2<T>* __restrict__ tw,
-                                                                  int* __restrict__ flags) {
+__global__ void __launch_bounds__(row_threads<N>(), 2) k_step_pass3(EventDev* __restrict__ ev,
+                                                                     const int* __restrict__ slots,
+                                                                     const C2<T>* __restrict__ Q,
+                                                                     const C2<T>* __restrict__ tw,
+                                                                     int* __restrict__ flags) {
     using V2 = C2<T>;
+    constexpr int VC = v_chunk<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V2* sm = reinterpret_cast<V2*>(smem_raw);
+    double2* smV = reinterpret_cast<double2*>(smem_raw + sizeof(V2) * padded_len(8 * N));
     const int x = blockIdx.x, b = blockIdx.y;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     const V2* in = Q + (long)b * 8 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 8 * N; i += blockDim.x) sm[pad(i)] = in[(long)(i / N) * vol + (i % N)];
+    for (int i = threadIdx.x; i < 8 * N; i += blockDim.x)
+        cp_async<(int)sizeof(V2)>(&sm[pad(i)], &in[(long)(i / N) * vol + (i % N)]);
+    cp_async_commit();
+    stage_v<N>(smV, e.V, vol, x, 0);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
     fft_rows_smem<T, N, 8>(sm, (T)1, tw);
     const double se = e.sqrt_eps;
     int fl = 0;
-    for (int y = threadIdx.x; y < N; y += blockDim.x) {
-        double a[8], bq[8];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const V2 u = sm[pad(s * N + y)], w = sm[pad((4 + s) * N + y)];
-            a[2 * s] = (double)u.x; a[2 * s + 1] = (double)u.y;
-            bq[2 * s] = (double)w.x; bq[2 * s + 1] = (double)w.y;
+    for (int c0 = 0; c0 < N; c0 += VC) {
+        if (c0 > 0) {
+            __syncthreads();
+            stage_v<N>(smV, e.V, vol, x, c0);
+            cp_async_commit();
         }
-        double2 mA[9], mB[9], v[9], tmp[9];
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
+            double a[8], bq[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            a[k] *= se;
-            bq[k] *= -se;
-        }
-        embed_lambda<double>(a, mA);
-        embed_lambda<double>(bq, mB);
-        int st = expi_herm(mB, -1.0);
-        st |= expi_herm(mA, -1.0);
-        const long site = (long)x * N + y;
+            for (int s = 0; s < 4; ++s) {
+                const V2 u = sm[pad(s * N + y)], w = sm[pad((4 + s) * N + y)];
+                a[2 * s] = (double)u.x * se;
+                a[2 * s + 1] = (double)u.y * se;
+                bq[2 * s] = (double)w.x * -se;
+                bq[2 * s + 1] = (double)w.y * -se;
+            }
+            double2 mA[9], mB[9], v[9], tmp[9];
+            embed_lambda<double>(a, mA);
+            embed_lambda<double>(bq, mB);
+            expi_ch(mB, -1.0);  // exp(+i sqrt(eps) B)
+            expi_ch(mA, -1.0);  // exp(-i sqrt(eps) A)
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
-        mul3(mB, v, tmp);
-        mul3(tmp, mA, v);
-        if (e.reunit) reunitarize(v);
-        if (st) fl |= JW_FLAG_NOCONV;
+            for (int k = 0; k < 9; ++k) v[k] = smV[k * VC + (y - c0)];
+            mul3(mB, v, tmp);
+            mul3(tmp, mA, v);
+            if (e.reunit) reunitarize(v);
+            const long site = (long)x * N + y;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
-            e.V[k * vol + site] = v[k];
+            for (int k = 0; k < 9; ++k) {
+                if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+                e.V[k * vol + site] = v[k];
+            }
         }
     }
     if (fl) atomicOr(flags, fl);
@@ -334,7 +404,8 @@ __global__ void __launch_bounds__(row_threads<N>()) k_mv_pass3(EventDev* __restr
         }
         double2 m[9], v[9], r[9];
         embed_lambda<double>(f, m);
-        const int st = expi_herm(m, 1.0);
+        expi_ch(m, 1.0);
+        const int st = 0;
         const long site = (long)x * N + y;
 #pragma unroll
         for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
