@@ -409,8 +409,9 @@ __device__ __forceinline__ int expi_herm(double2 m[9], double sign) {
 //   h1 = 2u e^{2iu} - e^{-iu} [2u cos w - i (3u^2 - w^2) xi0],
 //   h2 = e^{2iu} - e^{-iu} [cos w + 3iu xi0],       f_j = h_j / (9u^2 - w^2),
 // evaluated for |c0| (f_j(-c0) = (-1)^j conj f_j(c0)) so that 9u^2 - w^2 >= 2 c1.
-// For c1 < 1e-4 (|Q| below ~1e-2) the series of exp(iQ) reduced with
-// Q^3 = c1 Q + c0 is used instead (truncation ~|Q|^7/7! < 1e-17).
+// For c1 <= 0.05 (|Q| below ~0.3: every Langevin update at the usual step
+// sizes) the Taylor series of exp(iQ), reduced with Q^3 = c1 Q + c0, is used
+// instead; it needs no transcendental functions.
 // Only the upper triangle and the real diagonal of m are read.
 __device__ __forceinline__ void expi_ch(double2 m[9], double sign) {
     const double a = sign * m[0].x, b = sign * m[4].x, c = sign * m[8].x;
@@ -425,12 +426,25 @@ __device__ __forceinline__ void expi_ch(double2 m[9], double sign) {
     const double2 def = cmulc(cmul(d, e), f);                          // d e conj(f)
     const double c0 = a * b * c - a * ee - b * ff - c * dd + 2.0 * def.x;
     double2 f0, f1, f2;
-    if (c1 < 1e-4) {
-        // f0 = 1 - i c0/6 + i c1 c0/120 - c0^2/720,  f1 = i(1 - c1/6 + c1^2/120) + c0/24 - c0 c1/360,
-        // f2 = -1/2 + c1/24 - c1^2/720 + i c0/120
-        f0 = make_double2(1.0 - c0 * c0 / 720.0, -c0 / 6.0 + c1 * c0 / 120.0);
-        f1 = make_double2(c0 / 24.0 - c0 * c1 / 360.0, 1.0 - c1 / 6.0 + c1 * c1 / 120.0);
-        f2 = make_double2(-0.5 + c1 / 24.0 - c1 * c1 / 720.0, c0 / 120.0);
+    if (c1 <= 0.05) {
+        // sum_n (i^n / n!) Q^n with Q^n = a_n + b_n Q + c_n Q^2 and, from
+        // Q^3 = c1 Q + c0: (a, b, c)_{n+1} = (c0 c_n, a_n + c1 c_n, b_n).
+        // |Q| <= sqrt(2 c1) <= 0.32, so 16 terms leave < 1e-21.
+        double an = 1.0, bn = 0.0, cn = 0.0, fac = 1.0;
+        double r0 = 0.0, i0 = 0.0, r1 = 0.0, i1 = 0.0, r2 = 0.0, i2 = 0.0;
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            // i^n: n mod 4 = 0 -> +1, 1 -> +i, 2 -> -1, 3 -> -i
+            const double sg = (n & 2) ? -fac : fac;
+            if (n & 1) { i0 += sg * an; i1 += sg * bn; i2 += sg * cn; }
+            else { r0 += sg * an; r1 += sg * bn; r2 += sg * cn; }
+            const double a2 = c0 * cn, b2 = an + c1 * cn;
+            cn = bn; an = a2; bn = b2;
+            fac /= (double)(n + 1);
+        }
+        f0 = make_double2(r0, i0);
+        f1 = make_double2(r1, i1);
+        f2 = make_double2(r2, i2);
     } else {
         const bool neg = c0 < 0.0;
         const double c0a = fabs(c0);

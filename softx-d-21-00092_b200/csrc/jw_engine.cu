@@ -240,7 +240,7 @@ cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsi
     const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
     constexpr int RT = row_threads<N>();
     constexpr int C = p2_cols<T, N>();
-    const size_t sm1 = p1_smem<T, N>(1);
+    const size_t sm1 = p1_smem_bytes<T, N>();
     const size_t sm2 = p2_smem<T, N>();
     const size_t sm3 = p3_smem<T, N>();
     static bool configured = false;
@@ -250,7 +250,7 @@ cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsi
         cudaFuncSetAttribute(k_step_pass3<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
         configured = true;
     }
-    k_step_pass1<T, N><<<dim3(N, 2, nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
+    k_step_pass1<T, N><<<dim3(N, p1_groups<T, N>(), nb), p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
     k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);
     k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, d_slots, Q, tw, e->d_flags);
     return cudaGetLastError();
@@ -373,11 +373,11 @@ cudaError_t launch_step_timed(jw_engine* e, Group& g, const int* d_slots, int nb
     const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
     constexpr int RT = row_threads<N>();
     constexpr int C = p2_cols<T, N>();
-    const size_t sm1 = p1_smem<T, N>(1);
+    const size_t sm1 = p1_smem_bytes<T, N>();
     const size_t sm2 = p2_smem<T, N>();
     const size_t sm3 = p3_smem<T, N>();
     cudaEventRecord(t[0], e->stream);
-    k_step_pass1<T, N><<<dim3(N, 2, nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
+    k_step_pass1<T, N><<<dim3(N, p1_groups<T, N>(), nb), p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
     cudaEventRecord(t[1], e->stream);
     cudaEventRecord(t[2], e->stream);
     k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);

@@ -71,9 +71,6 @@ template <typename T, int N> constexpr int p2_cols() {
 template <typename T, int N> constexpr size_t p2_smem() {
     return sizeof(C2<T>) * 2 * padded_len(N * p2_cols<T, N>()) + sizeof(T) * 2 * N * p2_cols<T, N>();
 }
-template <typename T, int N> constexpr size_t p1_smem(int group) {
-    return sizeof(C2<T>) * padded_len(8 * N) + (group ? sizeof(double2) * 9 * v_chunk<N>() : 0);
-}
 template <typename T, int N> constexpr size_t p3_smem() {
     return sizeof(C2<T>) * padded_len(8 * N) + sizeof(double2) * 9 * v_chunk<N>();
 }
@@ -121,80 +118,105 @@ template <> __device__ __forceinline__ const double* nftab<double>(const EventDe
 template <> __device__ __forceinline__ const float* nftab<float>(const EventDev& e) { return e.nf32; }
 
 // ------------------------------------------------------------------ pass 1
-// blockIdx.y = 0: sequences 0..7 (the noise itself); 1: sequences 8..15
-// (V xi V^dagger), whose CTA stages V through shared memory (cp.async) in
-// chunks of v_chunk sites.
+// One CTA per row when its 16 sequences and a V chunk fit in shared memory
+// (p1_groups == 1): V is staged with cp.async while the CTA draws the noise.
+// Otherwise (p1_groups == 2) blockIdx.y = 0 builds sequences 0..7 (the noise)
+// and blockIdx.y = 1 sequences 8..15 (V xi V^dagger), each drawing the noise.
+template <typename T, int N> constexpr int p1_groups() {
+    return (16 * N * (int)sizeof(C2<T>) + 9 * v_chunk<N>() * 16) <= 140 * 1024 ? 1 : 2;
+}
+template <int N> constexpr int p1_threads() { return N >= 512 ? 512 : 256; }
+template <typename T, int N> constexpr size_t p1_smem_bytes() {
+    return sizeof(C2<T>) * padded_len(16 / p1_groups<T, N>() * N) + sizeof(double2) * 9 * v_chunk<N>();
+}
+
 template <typename T, int N>
-__global__ void __launch_bounds__(256) k_step_pass1(const EventDev* __restrict__ ev, const int* __restrict__ slots,
-                                                    C2<T>* __restrict__ P, const C2<T>* __restrict__ tw) {
+__device__ __forceinline__ void p1_noise(const EventDev& e, const T* __restrict__ nf, int x, int y, T z[16]) {
+    const long site = (long)x * N + y;
+    langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
+    const T f = nf ? nf[site] : (T)1;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) z[k] *= f;
+}
+
+// V xi V^dagger coefficients for xi = sum n_a L_a
+template <typename T>
+__device__ __forceinline__ void p1_rotate(const C2<T> v[9], const T n[8], T h[8]) {
+    C2<T> xi[9], t[9], r[9];
+    embed_lambda<T>(n, xi);
+    mul3(v, xi, t);
+    mul3_adj(t, v, r);
+    project_lambda<T>(r, h);
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(p1_threads<N>()) k_step_pass1(const EventDev* __restrict__ ev,
+                                                                 const int* __restrict__ slots,
+                                                                 C2<T>* __restrict__ P,
+                                                                 const C2<T>* __restrict__ tw) {
     using V2 = C2<T>;
     constexpr int VC = v_chunk<N>();
+    constexpr int G = p1_groups<T, N>();
+    constexpr int NSEQ = 16 / G;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V2* sm = reinterpret_cast<V2*>(smem_raw);
-    double2* smV = reinterpret_cast<double2*>(smem_raw + sizeof(V2) * padded_len(8 * N));
+    double2* smV = reinterpret_cast<double2*>(smem_raw + sizeof(V2) * padded_len(NSEQ * N));
     const int x = blockIdx.x, g = blockIdx.y, b = blockIdx.z;
     const EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     const T* nf = nftab<T>(e);
-    if (g == 0) {
-        for (int y = threadIdx.x; y < N; y += blockDim.x) {
-            const long site = (long)x * N + y;
-            T z[16];
-            langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
-            const T f = nf ? nf[site] : (T)1;
+    const bool want_noise = (G == 1) || g == 0;
+    const bool want_rot = (G == 1) || g == 1;
+    const int rot_base = (G == 1) ? 8 : 0;  // local sequence index of the first rotated pack
+    // one site per thread per chunk: VC <= blockDim.x
+    for (int c0 = 0; c0 < N; c0 += VC) {
+        if (want_rot) {
+            if (c0 > 0) __syncthreads();
+            stage_v<N>(smV, e.V, vol, x, c0);
+            cp_async_commit();
+        }
+        const bool have = threadIdx.x < VC;
+        const int y = c0 + threadIdx.x;
+        T z[16];
+        if (have) {
+            p1_noise<T, N>(e, nf, x, y, z);
+            if (want_noise) {
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                sm[pad(s * N + y)] = mk<T>(z[4 * s] * f, z[4 * s + 2] * f);            // n_{2s} + i n_{2s+1}
-                sm[pad((4 + s) * N + y)] = mk<T>(z[4 * s + 1] * f, z[4 * s + 3] * f);  // m_{2s} + i m_{2s+1}
+                for (int s = 0; s < 4; ++s) {
+                    sm[pad(s * N + y)] = mk<T>(z[4 * s], z[4 * s + 2]);            // n_{2s} + i n_{2s+1}
+                    sm[pad((4 + s) * N + y)] = mk<T>(z[4 * s + 1], z[4 * s + 3]);  // m_{2s} + i m_{2s+1}
+                }
             }
         }
-    } else {
-        stage_v<N>(smV, e.V, vol, x, 0);
-        cp_async_commit();
-        for (int c0 = 0; c0 < N; c0 += VC) {
-            if (c0 > 0) {
-                __syncthreads();
-                stage_v<N>(smV, e.V, vol, x, c0);
-                cp_async_commit();
-            }
+        if (want_rot) {
             cp_async_wait<0>();
             __syncthreads();
-            for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
-                const long site = (long)x * N + y;
-                T z[16];
-                langevin_normals<T>(e.seed, e.step, (uint32_t)site, z);
-                const T f = nf ? nf[site] : (T)1;
+            if (have) {
                 T n[8], m[8], h[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    n[k] = z[2 * k] * f;
-                    m[k] = z[2 * k + 1] * f;
+                    n[k] = z[2 * k];
+                    m[k] = z[2 * k + 1];
                 }
-                V2 v[9], xi[9], t[9], r[9];
+                V2 v[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) {
-                    const double2 dv = smV[k * VC + (y - c0)];
+                    const double2 dv = smV[k * VC + threadIdx.x];
                     v[k] = mk<T>((T)dv.x, (T)dv.y);
                 }
-                embed_lambda<T>(n, xi);
-                mul3(v, xi, t);
-                mul3_adj(t, v, r);
-                project_lambda<T>(r, h);
+                p1_rotate<T>(v, n, h);
 #pragma unroll
-                for (int s = 0; s < 4; ++s) sm[pad(s * N + y)] = mk<T>(h[2 * s], h[2 * s + 1]);
-                embed_lambda<T>(m, xi);
-                mul3(v, xi, t);
-                mul3_adj(t, v, r);
-                project_lambda<T>(r, h);
+                for (int s = 0; s < 4; ++s) sm[pad((rot_base + s) * N + y)] = mk<T>(h[2 * s], h[2 * s + 1]);
+                p1_rotate<T>(v, m, h);
 #pragma unroll
-                for (int s = 0; s < 4; ++s) sm[pad((4 + s) * N + y)] = mk<T>(h[2 * s], h[2 * s + 1]);
+                for (int s = 0; s < 4; ++s) sm[pad((rot_base + 4 + s) * N + y)] = mk<T>(h[2 * s], h[2 * s + 1]);
             }
         }
     }
     __syncthreads();
-    fft_rows_smem<T, N, 8>(sm, (T)-1, tw);
-    V2* out = P + ((long)b * 16 + 8 * g) * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 8 * N; i += blockDim.x) {
+    fft_rows_smem<T, N, NSEQ>(sm, (T)-1, tw);
+    V2* out = P + ((long)b * 16 + NSEQ * g) * vol + (long)x * N;
+    for (int i = threadIdx.x; i < NSEQ * N; i += blockDim.x) {
         const int s = i / N, y = i - s * N;
         out[s * vol + y] = sm[pad(i)];
     }
