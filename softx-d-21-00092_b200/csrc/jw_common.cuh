@@ -90,6 +90,31 @@ __device__ __forceinline__ void box_muller(uint32_t r0, uint32_t r1, float& z0, 
     z1 = rad * s;
 }
 
+// Box-Muller in FP32 with the hardware approximations: ln u0 from __logf
+// (absolute error <= 2^-21.4 near 1, relative ~2^-21 elsewhere) and
+// sin/cos of 2 pi u1 - pi from __sincosf (absolute error <= 2^-21.4 on
+// [-pi, pi]).  Each normal differs from the FP64 stream by at most ~3e-6
+// absolute; used by the mixed-precision engine.
+__device__ __forceinline__ void box_muller_fast(uint32_t r0, uint32_t r1, float& z0, float& z1) {
+    const float u0 = __uint2float_rn(r0) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
+    const float u1 = __uint2float_rn(r1) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
+    const float rad = sqrtf(-2.0f * __logf(u0));
+    float s, c;
+    __sincosf(6.28318530717958648f * u1 - 3.14159265358979324f, &s, &c);
+    z0 = -rad * c;  // cos(2 pi u1) = -cos(2 pi u1 - pi)
+    z1 = -rad * s;
+}
+
+__device__ __forceinline__ void langevin_normals_fast(uint64_t seed, uint64_t step, uint32_t site, float z[16]) {
+    const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+#pragma unroll
+    for (uint32_t c = 0; c < 4; ++c) {
+        uint4 r = philox4x32_10(make_uint4(site, (uint32_t)step, kTagLangevin | c, (uint32_t)(step >> 32)), key);
+        box_muller_fast(r.x, r.y, z[4 * c + 0], z[4 * c + 1]);
+        box_muller_fast(r.z, r.w, z[4 * c + 2], z[4 * c + 3]);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void langevin_normals(uint64_t seed, uint64_t step, uint32_t site, T z[16]) {
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "jw_engine_kernels.cuh"
+#include "jw_mixed_kernels.cuh"
 #include "jw_internal.h"
 
 using namespace jw;
@@ -231,8 +232,34 @@ void group_destroy(Group& g) {
 }
 
 // --------------------------------------------------------------- launches
+template <int N>
+cudaError_t launch_mix_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws, cudaEvent_t* t) {
+    const long vol = (long)N * N;
+    float4* P = reinterpret_cast<float4*>(ws);
+    float4* Q = P + (size_t)8 * vol * nb;
+    const size_t sm1 = mx_p1_smem<N>(), sm2 = mx_p2_smem<N>(), sm3 = mx_p3_smem<N>();
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
+        configured = true;
+    }
+    if (t) cudaEventRecord(t[0], e->stream);
+    k_mix_pass1<N><<<dim3(N, mx_groups<N>(), nb), mx_p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P,
+                                                                                        g.tw.d32);
+    if (t) { cudaEventRecord(t[1], e->stream); cudaEventRecord(t[2], e->stream); }
+    k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), sm2, e->stream>>>(g.d_ev, d_slots, P, Q,
+                                                                                          g.tw.d32);
+    if (t) { cudaEventRecord(t[3], e->stream); cudaEventRecord(t[4], e->stream); }
+    k_mix_pass3<N><<<dim3(N, nb), row_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32, e->d_flags);
+    if (t) cudaEventRecord(t[5], e->stream);
+    return cudaGetLastError();
+}
+
 template <typename T, int N>
 cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
+    if constexpr (sizeof(T) == 4) return launch_mix_step<N>(e, g, d_slots, nb, ws, nullptr);
     using V2 = C2<T>;
     const long vol = (long)N * N;
     V2* P = reinterpret_cast<V2*>(ws);
@@ -366,6 +393,7 @@ cudaError_t dispatch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots
 
 template <typename T, int N>
 cudaError_t launch_step_timed(jw_engine* e, Group& g, const int* d_slots, int nb, cudaEvent_t* t) {
+    if constexpr (sizeof(T) == 4) return launch_mix_step<N>(e, g, d_slots, nb, g.ws, t);
     using V2 = C2<T>;
     const long vol = (long)N * N;
     V2* P = reinterpret_cast<V2*>(g.ws);

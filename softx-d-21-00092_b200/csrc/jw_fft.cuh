@@ -151,3 +151,140 @@ struct ColIdx {
 };
 
 }  // namespace jw
+
+// ============================================================================
+// 16-byte-element core: each shared-memory element carries VL complex values
+// (VL = 2 for FP32 as float4, VL = 1 for FP64 as double2) that are transformed
+// as independent sequences with the same twiddles, so one 128-bit access and
+// one twiddle set serve both.  Same Stockham schedule as fft_smem.  Twiddles
+// per radix-8 butterfly: w, w^2, w^4 from the table, w^3 = w w^2, w^5 = w^4 w,
+// w^6 = w^4 w^2, w^7 = w^4 w^3.
+namespace jw {
+
+template <typename T> struct Elem16;
+template <> struct Elem16<float> { using E = float4; static constexpr int VL = 2; };
+template <> struct Elem16<double> { using E = double2; static constexpr int VL = 1; };
+
+__device__ __forceinline__ void unpack16(const float4& e, float2* v) {
+    v[0] = make_float2(e.x, e.y);
+    v[1] = make_float2(e.z, e.w);
+}
+__device__ __forceinline__ float4 pack16(const float2* v) { return make_float4(v[0].x, v[0].y, v[1].x, v[1].y); }
+__device__ __forceinline__ void unpack16(const double2& e, double2* v) { v[0] = e; }
+__device__ __forceinline__ double2 pack16(const double2* v) { return v[0]; }
+
+// padded row index for 16-byte elements: one spare element every 8
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 3); }
+__host__ __device__ constexpr int padded_len16(int n) { return n + (n >> 3); }
+
+struct RowIdx16 {
+    int base;
+    __device__ __forceinline__ int operator()(int e) const { return pad16(base + e); }
+};
+// column c of a [N][C] tile of 16-byte elements; with C * 16 = 128 bytes a
+// quarter warp covers one tile row, so no padding is needed
+template <int C>
+struct ColIdx16 {
+    int c;
+    __device__ __forceinline__ int operator()(int e) const { return e * C + c; }
+};
+
+template <typename V, typename T>
+__device__ __forceinline__ V tw_load(const V* __restrict__ tw, int m, T sign) {
+    V w = __ldg(&tw[m]);
+    w.y *= sign;
+    return w;
+}
+
+template <typename T, int N, int Ns, int R, typename IdxF>
+__device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
+                                                bool active, T sign, const C2<T>* __restrict__ tw) {
+    using V = C2<T>;
+    using E = typename Elem16<T>::E;
+    constexpr int VL = Elem16<T>::VL;
+    constexpr int B = 8 / R;
+    constexpr int NB = N / R;
+    constexpr int TPS = N / 8;
+    constexpr int TWS = N / (Ns * R);
+    V v[VL][8];
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int b = t + q * TPS;
+            const int k = b & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                V u[VL];
+                unpack16(sm[idx(b + r * NB)], u);
+#pragma unroll
+                for (int l = 0; l < VL; ++l) v[l][q * R + r] = u[l];
+            }
+            if (Ns > 1) {
+                V w[8];
+                w[1] = tw_load(tw, k * TWS, sign);
+                if constexpr (R >= 4) w[2] = tw_load(tw, 2 * k * TWS, sign);
+                if constexpr (R == 4) w[3] = cmul(w[1], w[2]);
+                if constexpr (R == 8) {
+                    w[4] = tw_load(tw, 4 * k * TWS, sign);
+                    w[3] = cmul(w[1], w[2]);
+                    w[5] = cmul(w[4], w[1]);
+                    w[6] = cmul(w[4], w[2]);
+                    w[7] = cmul(w[4], w[3]);
+                }
+#pragma unroll
+                for (int r = 1; r < R; ++r)
+#pragma unroll
+                    for (int l = 0; l < VL; ++l) v[l][q * R + r] = cmul(v[l][q * R + r], w[r]);
+            }
+#pragma unroll
+            for (int l = 0; l < VL; ++l) {
+                if constexpr (R == 8) {
+                    bfly8<V, T>(v[l], sign);
+                } else if constexpr (R == 4) {
+                    bfly4<V, T>(v[l][q * 4 + 0], v[l][q * 4 + 1], v[l][q * 4 + 2], v[l][q * 4 + 3], sign);
+                } else {
+                    bfly2<V, T>(v[l][q * 2 + 0], v[l][q * 2 + 1]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int b = t + q * TPS;
+            const int k = b & (Ns - 1);
+            const int base = (b / Ns) * Ns * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                V u[VL];
+#pragma unroll
+                for (int l = 0; l < VL; ++l) u[l] = v[l][q * R + r];
+                sm[idx(base + r * Ns)] = pack16(u);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int N, int Ns, typename IdxF>
+__device__ __forceinline__ void fft16_passes(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
+                                             const C2<T>* __restrict__ tw) {
+    if constexpr (Ns < N) {
+        constexpr int rem = N / Ns;
+        constexpr int R = rem >= 8 ? 8 : rem;
+        stockham_pass16<T, N, Ns, R>(sm, idx, t, active, sign, tw);
+        fft16_passes<T, N, Ns * R>(sm, idx, t, active, sign, tw);
+    }
+}
+
+// Transform the VL sequences held in the elements sm[idx(e)], e < N, with
+// thread t < N/8; all threads of the CTA must call it.
+template <typename T, int N, typename IdxF>
+__device__ __forceinline__ void fft16(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
+                                      const C2<T>* __restrict__ tw) {
+    static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two N >= 8");
+    fft16_passes<T, N, 1>(sm, idx, t, active, sign, tw);
+}
+
+}  // namespace jw

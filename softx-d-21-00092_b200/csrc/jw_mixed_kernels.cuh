@@ -1,0 +1,297 @@
+// jw_mixed_kernels.cuh -- the mixed-precision (FP32 transform) Langevin step
+// on "pair planes": each 16-byte element holds two complex FP32 values that
+// travel together through the whole step, so every shared-memory access and
+// every HBM access moves both at once and one twiddle set serves both.
+//
+//   pass 1 (row)    P[j]   = (X_j, Y_j)    j = 0..3, X_j = n_{2j} + i n_{2j+1}, Y_j = m_{2j} + i m_{2j+1}
+//                   P[4+j] = (BX_j, BY_j)  the same packs of V xi_x V^dagger and V xi_y V^dagger
+//                   16 row transforms of length N (8 pair rows), forward.
+//   pass 2 (column) per j: column transforms of P[j] and P[4+j], then
+//                   W_A = K_x X + K_y Y, W_B = K_x BX + K_y BY (prepare_A_local,
+//                   field.h:1998-2075, 1/N^2 folded into K) and the inverse column
+//                   transform of (W_A, W_B) into Q[j].
+//   pass 3 (row)    inverse row transform of Q[j] = (A_{2j} + i A_{2j+1}, B_{2j} + i B_{2j+1}),
+//                   then the FP64 update of V (update_uf, field.h:1966-1996).
+//
+// HBM per site: pass 1 reads V (144 B) and writes P (128 B); pass 2 reads P
+// (128 B) and writes Q (64 B); pass 3 reads Q (64 B) and V and writes V (288 B).
+#pragma once
+
+#include "jw_engine_kernels.cuh"
+
+namespace jw {
+
+// pass 1 stages V in chunks of 256 sites (36 KB) so that two CTAs fit per SM at N = 512
+template <int N> constexpr int mx_vc() { return N < 256 ? N : 256; }
+template <int N> constexpr int mx_groups() {
+    return (16 * padded_len16(8 * N) + 16 * 9 * mx_vc<N>()) > 220 * 1024 ? 2 : 1;
+}
+template <int N> constexpr int mx_p1_threads() { return 256; }
+template <int N> constexpr size_t mx_p1_smem() {
+    return 16 * (size_t)padded_len16(8 / mx_groups<N>() * N) + 16 * 9 * (size_t)mx_vc<N>();
+}
+// pass 2 tile width: 4 columns (64-byte rows, padded) while two tiles fit in 80 KB
+template <int N> constexpr int mx_cols() {
+    constexpr int cap = 32768 / (N * 16);
+    constexpr int c = cap >= 4 ? 4 : (cap >= 1 ? cap : 1);
+    return c < N ? c : N;
+}
+template <int N> constexpr int mx_p2_threads() { return mx_cols<N>() * (N / 8); }
+// column tiles narrower than 128 bytes are padded by one row every 8 rows
+template <int C> struct ColIdx16P {
+    int c;
+    __device__ __forceinline__ int operator()(int e) const {
+        return (C >= 8) ? e * C + c : e * C + c + (e >> 3) * C;
+    }
+};
+template <int N> constexpr int mx_tile_len() {
+    return mx_cols<N>() >= 8 ? N * mx_cols<N>() : N * mx_cols<N>() + (N / 8) * mx_cols<N>();
+}
+template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile_len<N>(); }
+template <int N> constexpr size_t mx_p3_smem() {
+    return 16 * (size_t)padded_len16(4 * N) + 16 * 9 * (size_t)v_chunk<N>();
+}
+
+// V sites [c0, c0 + VC) of row x into smV[k][VC] (16-byte copies)
+template <int N, int VC>
+__device__ __forceinline__ void stage_v_chunk(double2* smV, const double2* __restrict__ V, long vol, int x, int c0) {
+    for (int i = threadIdx.x; i < 9 * VC; i += blockDim.x) {
+        const int k = i / VC, yy = i - k * VC;
+        cp_async<16>(&smV[i], &V[k * vol + (long)x * N + c0 + yy]);
+    }
+}
+
+// Gell-Mann coefficients of R = V xi V^dagger, xi = sum_a n_a L_a: only the
+// upper triangle and the real diagonal of R are formed (R is Hermitian).
+__device__ __forceinline__ void rotate_herm(const float2 v[9], const float n[8], float h[8]) {
+    float2 xi[9], t[9];
+    embed_lambda<float>(n, xi);
+    mul3(v, xi, t);  // t = V xi
+    // R_ij = sum_k t_ik conj(V_jk)
+    auto rij = [&](int i, int j) {
+        float2 s = cmulc(t[i * 3 + 0], v[j * 3 + 0]);
+        s = cadd(s, cmulc(t[i * 3 + 1], v[j * 3 + 1]));
+        return cadd(s, cmulc(t[i * 3 + 2], v[j * 3 + 2]));
+    };
+    auto rii = [&](int i) {
+        return t[i * 3 + 0].x * v[i * 3 + 0].x + t[i * 3 + 0].y * v[i * 3 + 0].y + t[i * 3 + 1].x * v[i * 3 + 1].x +
+               t[i * 3 + 1].y * v[i * 3 + 1].y + t[i * 3 + 2].x * v[i * 3 + 2].x + t[i * 3 + 2].y * v[i * 3 + 2].y;
+    };
+    const float2 r01 = rij(0, 1), r02 = rij(0, 2), r12 = rij(1, 2);
+    const float r00 = rii(0), r11 = rii(1), r22 = rii(2);
+    h[0] = r01.x;
+    h[1] = r01.y;
+    h[2] = 0.5f * (r00 - r11);
+    h[3] = r02.x;
+    h[4] = r02.y;
+    h[5] = r12.x;
+    h[6] = r12.y;
+    h[7] = (r00 + r11 - 2.0f * r22) / (2.0f * 1.7320508075688772f);
+}
+
+// Transform NP contiguous padded pair rows (16-byte elements) in rounds.
+template <int N, int NP>
+__device__ __forceinline__ void fft16_rows(float4* sm, float sign, const float2* __restrict__ tw) {
+    constexpr int TPS = N / 8;
+    const int spr = blockDim.x / TPS;
+    const int r = threadIdx.x / TPS;
+    for (int p0 = 0; p0 < NP; p0 += spr) {
+        const int p = p0 + r;
+        fft16<float, N>(sm, RowIdx16{p * N}, threadIdx.x % TPS, r < spr && p < NP, sign, tw);
+    }
+}
+
+// ------------------------------------------------------------------ pass 1
+template <int N>
+__global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev* __restrict__ ev,
+                                                                   const int* __restrict__ slots,
+                                                                   float4* __restrict__ P,
+                                                                   const float2* __restrict__ tw) {
+    constexpr int VC = mx_vc<N>();
+    constexpr int G = mx_groups<N>();
+    constexpr int NP = 8 / G;  // pair rows per CTA
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* sm = reinterpret_cast<float4*>(smem_raw);
+    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(NP * N));
+    const int x = blockIdx.x, g = blockIdx.y, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const float* nf = e.nf32;
+    const bool want_noise = (G == 1) || g == 0;
+    const bool want_rot = (G == 1) || g == 1;
+    const int rot_base = (G == 1) ? 4 : 0;
+    for (int c0 = 0; c0 < N; c0 += VC) {
+        if (want_rot) {
+            if (c0 > 0) __syncthreads();
+            stage_v_chunk<N, VC>(smV, e.V, vol, x, c0);
+            cp_async_commit();
+        }
+        const bool have = threadIdx.x < VC;
+        const int y = c0 + threadIdx.x;
+        float z[16];
+        if (have) {
+            const long site = (long)x * N + y;
+            langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+            const float f = nf ? nf[site] : 1.0f;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+            if (want_noise) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+                    sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+            }
+        }
+        if (want_rot) {
+            cp_async_wait<0>();
+            __syncthreads();
+            if (have) {
+                float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    n[k] = z[2 * k];
+                    m[k] = z[2 * k + 1];
+                }
+                float2 v[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    const double2 dv = smV[k * VC + threadIdx.x];
+                    v[k] = make_float2((float)dv.x, (float)dv.y);
+                }
+                rotate_herm(v, n, hx);
+                rotate_herm(v, m, hy);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+                    sm[pad16((rot_base + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+            }
+        }
+    }
+    __syncthreads();
+    fft16_rows<N, NP>(sm, -1.0f, tw);
+    float4* out = P + ((long)b * 8 + NP * g) * vol + (long)x * N;
+    for (int i = threadIdx.x; i < NP * N; i += blockDim.x) {
+        const int p = i / N, y = i - p * N;
+        out[p * vol + y] = sm[pad16(i)];
+    }
+}
+
+// ------------------------------------------------------------------ pass 2
+template <int N>
+__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 3 : 1) k_mix_pass2(const EventDev* __restrict__ ev,
+                                                                   const int* __restrict__ slots,
+                                                                   const float4* __restrict__ P,
+                                                                   float4* __restrict__ Q,
+                                                                   const float2* __restrict__ tw) {
+    constexpr int C = mx_cols<N>();
+    constexpr int TH = mx_p2_threads<N>();
+    constexpr int PER = N * C / TH;  // = 8
+    constexpr int TL = mx_tile_len<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* ta = reinterpret_cast<float4*>(smem_raw);
+    float4* tb = ta + TL;
+    const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
+    constexpr int RSTEP = TH / C;  // = N / 8
+    const ColIdx16P<C> cidx{cc};
+    const float4* ina = P + ((long)b * 8 + j) * vol + c0 + (long)r0 * N + cc;
+    const float4* inb = P + ((long)b * 8 + 4 + j) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll 1
+    for (int q = 0; q < PER; ++q) {
+        const int row = r0 + q * RSTEP;
+        cp_async<16>(&ta[cidx(row)], ina + (long)q * RSTEP * N);
+        cp_async<16>(&tb[cidx(row)], inb + (long)q * RSTEP * N);
+    }
+    cp_async_commit();
+    const float* kt = e.k32 + c0 + (long)r0 * N + cc;
+    float kx[PER], ky[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        kx[q] = __ldg(kt + (long)q * RSTEP * N);
+        ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    fft16<float, N>(ta, cidx, r0, true, -1.0f, tw);
+    fft16<float, N>(tb, cidx, r0, true, -1.0f, tw);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int i = cidx(r0 + q * RSTEP);
+        const float4 a = ta[i], bb = tb[i];
+        // (i kx) X + (i ky) Y  and  (i kx) BX + (i ky) BY
+        ta[i] = make_float4(-kx[q] * a.y - ky[q] * a.w, kx[q] * a.x + ky[q] * a.z,
+                            -kx[q] * bb.y - ky[q] * bb.w, kx[q] * bb.x + ky[q] * bb.z);
+    }
+    __syncthreads();
+    fft16<float, N>(ta, cidx, r0, true, 1.0f, tw);
+    float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll 2
+    for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = ta[cidx(r0 + q * RSTEP)];
+}
+
+// ------------------------------------------------------------------ pass 3
+template <int N>
+__global__ void __launch_bounds__(row_threads<N>(), 2) k_mix_pass3(EventDev* __restrict__ ev,
+                                                                    const int* __restrict__ slots,
+                                                                    const float4* __restrict__ Q,
+                                                                    const float2* __restrict__ tw,
+                                                                    int* __restrict__ flags) {
+    constexpr int VC = v_chunk<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* sm = reinterpret_cast<float4*>(smem_raw);
+    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(4 * N));
+    const int x = blockIdx.x, b = blockIdx.y;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const float4* in = Q + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
+        cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    cp_async_commit();
+    stage_v<N>(smV, e.V, vol, x, 0);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    fft16_rows<N, 4>(sm, 1.0f, tw);
+    const double se = e.sqrt_eps;
+    int fl = 0;
+    for (int c0 = 0; c0 < N; c0 += VC) {
+        if (c0 > 0) {
+            __syncthreads();
+            stage_v<N>(smV, e.V, vol, x, c0);
+            cp_async_commit();
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
+            double a[8], bq[8];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float4 u = sm[pad16(j * N + y)];
+                a[2 * j] = (double)u.x * se;
+                a[2 * j + 1] = (double)u.y * se;
+                bq[2 * j] = (double)u.z * -se;
+                bq[2 * j + 1] = (double)u.w * -se;
+            }
+            double2 mA[9], mB[9], v[9], tmp[9];
+            embed_lambda<double>(a, mA);
+            embed_lambda<double>(bq, mB);
+            expi_ch(mB, -1.0);  // exp(+i sqrt(eps) B)
+            expi_ch(mA, -1.0);  // exp(-i sqrt(eps) A)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) v[k] = smV[k * VC + (y - c0)];
+            mul3(mB, v, tmp);
+            mul3(tmp, mA, v);
+            if (e.reunit) reunitarize(v);
+            const long site = (long)x * N + y;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+                e.V[k * vol + site] = v[k];
+            }
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+    if (x == 0 && threadIdx.x == 0) e.step += 1;
+}
+
+}  // namespace jw
