@@ -158,6 +158,21 @@ jw_status jw_update_uf(jw_context* ctx, jw_field* V, const jw_field* B, const jw
 jw_status jw_trace(jw_context* ctx, const jw_field* Vk, jw_field* corr);
 /* gfield::average_and_symmetrize (field.h:1460-1492). */
 jw_status jw_average_and_symmetrize(jw_context* ctx, jw_field* corr);
+/* No counterpart in the reference.  jw_average_and_symmetrize for callers
+ * that cannot allocate device memory: jw_context_create allocates (a stream,
+ * tables and the scratch plane this operation needs), which a program that
+ * hands all device memory to its own pool allocator, or a time-critical loop
+ * that cannot afford cudaMalloc/cudaFree, must avoid.  corr is the caller's
+ * device array of N*N complex doubles (element (kx, ky) at complex offset
+ * kx*N + ky), symmetrised in place on `stream` (a cudaStream_t, 0 = the
+ * default stream).  The scratch plane is a fixed array inside the library,
+ * 512*512 complex doubles (4 MiB) on every GPU that loads it, held until the
+ * process exits; N > 512 returns JW_EINVAL.  All calls share that array and
+ * each call overwrites what it reads, so calls that overlap on the GPU race
+ * and must be ordered by the caller.  The first call on a device looks up the
+ * array's device address with that device current; make it before any
+ * stream capture begins.  Allocates nothing. */
+jw_status jw_average_and_symmetrize_noalloc(double* corr, int N, void* stream);
 /* gfield::reduce(sum, err, mpi) (field.h:1521-1536): sum += corr, err += corr^2. */
 jw_status jw_reduce(jw_context* ctx, const jw_field* corr, jw_field* sum, jw_field* err);
 /* print(measurement, sum, err, momenta, x, mpi, fileroot) (field.h:2521-2547):
