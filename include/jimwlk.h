@@ -237,6 +237,16 @@ jw_status jw_engine_get_correlator(jw_engine* e, int event_id, double* sum, doub
 jw_status jw_engine_reset_correlator(jw_engine* e, int event_id);
 /* Steps taken so far by an event (its next noise index). */
 jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
+/* Dipole in position space from the event's accumulated correlator (mean over
+ * its measurements; the reference stops at C(k), field.h:2521-2547):
+ * S(r) = (N^2/3) sum_k C(k) exp(+2 pi i k.r/N), optionally all N*N values
+ * (S_xy, row-major displacement), the angular average over bins
+ * b = floor(|r| + 1/2) <= N/2 (S_bins, r_bins = mean |r|, counts; nbins_cap >=
+ * N/2 + 1), and Q_s = sqrt(2)/r_s with S(r_s) = exp(-1/2) (linear
+ * interpolation between bins; 0 if S never falls below exp(-1/2)).  Any output
+ * pointer may be null. */
+jw_status jw_engine_dipole(jw_engine* e, int event_id, double* S_xy, double* S_bins, double* r_bins, int* counts,
+                           int nbins_cap, int* nbins, double* Qs);
 /* One ensemble measurement over the listed events (one lattice size): the
  * symmetrised correlators of main_optimized.cpp:321-334 summed over the events
  * as gfield::reduce sums them over stats (field.h:1521-1536), written to host
@@ -248,6 +258,67 @@ jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double
  * spent in each of the three kernels (summed over launch groups, pass_ms[3])
  * and the total time from the first launch to the last. */
 jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms, double* total_ms);
+
+/* ------------------------------------------------------------------ serving */
+/* Continuous-batching evolution server over the engine.  A request is one
+ * event: MV initial condition, `steps` Langevin steps, a final dipole
+ * measurement returned as the angle-averaged S(r) and Q_s (jw_engine_dipole).
+ * A worker thread owns the device: it admits queued requests first-fit by
+ * device footprint (max_bytes), advances every resident event together each
+ * tick (one launch group per lattice size, up to max_steps_per_tick steps),
+ * and retires finished events, freeing memory for the queue.  Requests that
+ * arrive while others run join at the next tick; an event's result does not
+ * depend on what else is resident.  The functions are thread-safe. */
+typedef struct jw_server_options {
+    int precision;              /* JW_PRECISION_* */
+    int reunitarize;
+    size_t max_bytes;           /* device budget for resident events (0 = 90% of free) */
+    int max_steps_per_tick;     /* steps per tick per launch group */
+    int max_active;             /* resident events (0 = no limit beyond memory) */
+    int fake_device;            /* 1: host-only stand-in backend (no GPU; scheduler tests) */
+    double fake_ns_per_site_step;
+} jw_server_options;
+
+typedef struct jw_request_desc {
+    int N;                      /* lattice side, power of two 8..2048 */
+    int ny_slices;              /* MV slices */
+    double mu;                  /* config mu (mu_MV = mu/N) */
+    double mass;                /* config mass */
+    double step;                /* Langevin step */
+    int coupling;               /* SQRT, NOISE or FIXED */
+    int kernel;                 /* SIN */
+    uint64_t seed;
+    int steps;                  /* Langevin steps */
+} jw_request_desc;
+
+typedef struct jw_request_result {
+    int status;                 /* JW_OK or the error that ended the request */
+    int N, steps;
+    double t_submit, t_admit, t_done;  /* seconds on the server's monotonic clock */
+    double Qs;
+    int nbins;                  /* N/2 + 1 */
+} jw_request_result;
+
+typedef struct jw_server_stats {
+    int64_t submitted, completed, failed, queued;
+    double site_steps;          /* Langevin site-steps executed */
+    int max_active;             /* most events resident at once */
+    double now;                 /* server clock, seconds */
+} jw_server_stats;
+
+typedef struct jw_server jw_server;
+jw_status jw_server_create(const jw_server_options* opt, int device, jw_server** out);
+/* Stops the worker; requests still queued or running are dropped. */
+jw_status jw_server_destroy(jw_server* s);
+/* JW_EUNSUPPORTED / JW_EINVAL for parameters the engine cannot run, JW_ENOMEM
+ * for a request larger than the whole budget; otherwise queued. */
+jw_status jw_server_submit(jw_server* s, const jw_request_desc* d, int64_t* request_id);
+/* Waits up to timeout_s for the request; JW_ETIMEOUT if it has not finished.
+ * On return the request is forgotten by the server.  S_bins/r_bins (may be
+ * null) receive nbins values when nbins_cap >= N/2 + 1. */
+jw_status jw_server_wait(jw_server* s, int64_t request_id, double timeout_s, jw_request_result* res,
+                         double* S_bins, double* r_bins, int nbins_cap);
+jw_status jw_server_get_stats(jw_server* s, jw_server_stats* st);
 
 #ifdef __cplusplus
 }

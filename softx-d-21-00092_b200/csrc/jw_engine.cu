@@ -103,6 +103,13 @@ cudaError_t upload_table(const std::vector<double>& h, T** d) {
     return cudaMemcpy(*d, c.data(), sizeof(T) * c.size(), cudaMemcpyHostToDevice);
 }
 
+// mean symmetrised correlator times N^2/3 as a complex plane (dipole S(r) input)
+__global__ void k_dipole_prep(const double* __restrict__ acc, double2* __restrict__ out, long vol, double scale) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    out[i] = make_double2((acc[i] + acc[vol + i]) * scale, 0.0);
+}
+
 __global__ void k_set_unit_planes(double2* V, long vol) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= vol) return;
@@ -861,5 +868,77 @@ JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, in
     JW_CUDA(ce);
     for (int q = 0; q < 3; ++q) pass_ms[q] = p[q] / nsteps;  // per step, summed over launch groups
     *total_ms = tot;
+    return JW_OK;
+}
+
+// Dipole in position space from an event's accumulated correlator (the mean
+// over its measurements): S(r) = (N^2/3) sum_k C(k) exp(+2 pi i k.r/N) (the
+// Wiener-Khinchin form of (1/3N^2) sum_x tr V(x) V^dagger(x+r)), then the
+// angular average over bins b = floor(|r| + 1/2), |r| the minimum-image length,
+// b <= N/2, and Q_s = sqrt(2)/r_s with S(r_s) = exp(-1/2) interpolated linearly
+// between the first pair of bins that brackets it (0 if none).
+JW_EXPORT jw_status jw_engine_dipole(jw_engine* e, int id, double* S_xy, double* S_bins, double* r_bins,
+                                     int* counts, int nbins_cap, int* nbins, double* Qs) {
+    JW_CHECK(e);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const Event& ev = it->second;
+    const int N = ev.N;
+    const long vol = (long)N * N;
+    const int nb = N / 2 + 1;
+    if (S_bins && nbins_cap < nb) return JW_EINVAL;
+    Group& g = *e->groups[N];
+    jw_status s = ensure_workspace(e, g, 1);
+    if (s) return s;
+    EventDev d{};
+    JW_CUDA(cudaMemcpyAsync(&d, g.d_ev + ev.slot, sizeof(EventDev), cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    if (d.nmeas <= 0) return JW_EINVAL;
+    double2* plane = reinterpret_cast<double2*>(g.ws);
+    const double scale = (double)N * (double)N / 3.0 / d.nmeas;
+    k_dipole_prep<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ev.acc, plane, vol, scale);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(fft2d_planes<double>(plane, 1, N, 0, 1.0, g.tw, e->stream));
+    std::vector<double2> h(vol);
+    JW_CUDA(cudaMemcpyAsync(h.data(), plane, sizeof(double2) * vol, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    if (S_xy)
+        for (long i = 0; i < vol; ++i) S_xy[i] = h[i].x;
+    std::vector<double> sb(nb, 0.0), rb(nb, 0.0);
+    std::vector<int> cb(nb, 0);
+    for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+            const int dx = x > N / 2 ? x - N : x, dy = y > N / 2 ? y - N : y;
+            const double r = std::sqrt((double)(dx * dx + dy * dy));
+            const int b = (int)std::floor(r + 0.5);
+            if (b >= nb) continue;
+            sb[b] += h[(long)x * N + y].x;
+            rb[b] += r;
+            cb[b] += 1;
+        }
+    for (int b = 0; b < nb; ++b)
+        if (cb[b]) {
+            sb[b] /= cb[b];
+            rb[b] /= cb[b];
+        }
+    if (S_bins)
+        for (int b = 0; b < nb; ++b) {
+            S_bins[b] = sb[b];
+            if (r_bins) r_bins[b] = rb[b];
+            if (counts) counts[b] = cb[b];
+        }
+    if (nbins) *nbins = nb;
+    if (Qs) {
+        const double target = std::exp(-0.5);
+        double q = 0.0;
+        for (int b = 0; b + 1 < nb; ++b)
+            if (sb[b] >= target && sb[b + 1] < target) {
+                const double t = (sb[b] - target) / (sb[b] - sb[b + 1]);
+                const double rs = rb[b] + t * (rb[b + 1] - rb[b]);
+                q = rs > 0.0 ? std::sqrt(2.0) / rs : 0.0;
+                break;
+            }
+        *Qs = q;
+    }
     return JW_OK;
 }

@@ -51,6 +51,30 @@ class jw_event_desc(ctypes.Structure):
                 ("seed", ctypes.c_uint64)]
 
 
+class jw_server_options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("reunitarize", ctypes.c_int), ("max_bytes", ctypes.c_size_t),
+                ("max_steps_per_tick", ctypes.c_int), ("max_active", ctypes.c_int), ("fake_device", ctypes.c_int),
+                ("fake_ns_per_site_step", ctypes.c_double)]
+
+
+class jw_request_desc(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("ny_slices", ctypes.c_int), ("mu", ctypes.c_double), ("mass", ctypes.c_double),
+                ("step", ctypes.c_double), ("coupling", ctypes.c_int), ("kernel", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("steps", ctypes.c_int)]
+
+
+class jw_request_result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("N", ctypes.c_int), ("steps", ctypes.c_int), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double), ("Qs", ctypes.c_double),
+                ("nbins", ctypes.c_int)]
+
+
+class jw_server_stats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("queued", ctypes.c_int64), ("site_steps", ctypes.c_double), ("max_active", ctypes.c_int),
+                ("now", ctypes.c_double)]
+
+
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
 
@@ -104,6 +128,14 @@ def _load():
         "jw_engine_get_correlator": ([_vp, ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "jw_engine_reset_correlator": ([_vp, ctypes.c_int], ctypes.c_int),
         "jw_engine_event_steps": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "jw_server_create": ([ctypes.POINTER(jw_server_options), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+        "jw_server_destroy": ([_vp], ctypes.c_int),
+        "jw_server_submit": ([_vp, ctypes.POINTER(jw_request_desc), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "jw_server_wait": ([_vp, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(jw_request_result), _dp, _dp,
+                            ctypes.c_int], ctypes.c_int),
+        "jw_server_get_stats": ([_vp, ctypes.POINTER(jw_server_stats)], ctypes.c_int),
+        "jw_engine_dipole": ([_vp, ctypes.c_int, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                              ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
         "jw_engine_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp], ctypes.c_int),
         "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
                                  ctypes.c_int),
@@ -379,3 +411,76 @@ class Engine:
         tot = ctypes.c_double(0)
         _ck(_lib.jw_engine_step_timed(self._h, arr, n, nsteps, p, ctypes.byref(tot)), "jw_engine_step_timed")
         return list(p), tot.value
+
+    def dipole(self, eid: int, with_xy: bool = False):
+        """(S_bins, r_bins, counts, Q_s[, S_xy]) from the event's accumulated correlator."""
+        N = self.N[eid]
+        nb = N // 2 + 1
+        sb, rb = np.empty(nb), np.empty(nb)
+        cb = np.empty(nb, np.int32)
+        q = ctypes.c_double(0)
+        n = ctypes.c_int(0)
+        sxy = np.empty((N, N)) if with_xy else None
+        _ck(_lib.jw_engine_dipole(self._h, eid, sxy.ctypes.data_as(_dp) if with_xy else None, sb.ctypes.data_as(_dp),
+                                  rb.ctypes.data_as(_dp), cb.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), nb,
+                                  ctypes.byref(n), ctypes.byref(q)), "jw_engine_dipole")
+        out = (sb, rb, cb, q.value)
+        return out + (sxy,) if with_xy else out
+
+
+class Server:
+    """Continuous-batching evolution server (jw_server_*)."""
+
+    def __init__(self, precision: int = PRECISION_MIXED, max_bytes: int = 0, max_steps_per_tick: int = 8,
+                 max_active: int = 0, reunitarize: bool = False, fake_device: bool = False,
+                 fake_ns_per_site_step: float = 0.0, device: int = 0):
+        o = jw_server_options(precision, int(reunitarize), max_bytes, max_steps_per_tick, max_active,
+                              int(fake_device), fake_ns_per_site_step)
+        self._h = _vp()
+        _ck(_lib.jw_server_create(ctypes.byref(o), device, ctypes.byref(self._h)), "jw_server_create")
+
+    def close(self):
+        if self._h:
+            _lib.jw_server_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, N: int, steps: int, ny_slices: int = 50, mu: float | None = None, mass: float = 0.04,
+               step: float = 0.0004, coupling: int = FIXED_COUPLING_CONSTANT, kernel: int = SIN_KERNEL,
+               seed: int = 1) -> int:
+        d = jw_request_desc(N, ny_slices, 0.5 * N if mu is None else mu, mass, step, coupling, kernel, seed, steps)
+        rid = ctypes.c_int64(-1)
+        _ck(_lib.jw_server_submit(self._h, ctypes.byref(d), ctypes.byref(rid)), "jw_server_submit")
+        return rid.value
+
+    def try_submit(self, **kw):
+        N = kw["N"]
+        d = jw_request_desc(N, kw.get("ny_slices", 50), kw.get("mu", 0.5 * N), kw.get("mass", 0.04),
+                            kw.get("step", 0.0004), kw.get("coupling", FIXED_COUPLING_CONSTANT),
+                            kw.get("kernel", SIN_KERNEL), kw.get("seed", 1), kw.get("steps", 1))
+        rid = ctypes.c_int64(-1)
+        st = _lib.jw_server_submit(self._h, ctypes.byref(d), ctypes.byref(rid))
+        return st, rid.value
+
+    def wait(self, rid: int, timeout: float = 600.0):
+        """(status, result struct, S_bins, r_bins); raises on JW_ETIMEOUT / unknown id."""
+        res = jw_request_result()
+        cap = 2048 // 2 + 1
+        sb, rb = np.zeros(cap), np.zeros(cap)
+        _ck(_lib.jw_server_wait(self._h, rid, timeout, ctypes.byref(res), sb.ctypes.data_as(_dp),
+                                rb.ctypes.data_as(_dp), cap), "jw_server_wait")
+        return res.status, res, sb[:res.nbins].copy(), rb[:res.nbins].copy()
+
+    def try_wait(self, rid: int, timeout: float):
+        res = jw_request_result()
+        return _lib.jw_server_wait(self._h, rid, timeout, ctypes.byref(res), None, None, 0), res
+
+    def stats(self) -> jw_server_stats:
+        st = jw_server_stats()
+        _ck(_lib.jw_server_get_stats(self._h, ctypes.byref(st)), "jw_server_get_stats")
+        return st
