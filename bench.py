@@ -159,6 +159,80 @@ def run_reference_main(steps: int, warmup: int, nthreads: int | None = None):
         return statistics.mean(t[warmup:]), None
 
 
+def quantize_n(n: float) -> int:
+    """Lattice sides are powers of two: the nearest one in log2."""
+    return int(2 ** int(round(math.log2(n))))
+
+
+def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int):
+    """Continuous batching under Poisson arrivals: requests (N log-uniform on
+    [64, 2048] rounded to a power of two, Ny in {50, 100}, steps uniform on
+    [10, 2000], g^2 mu a uniform on [0.3, 0.8], per-request seed) submitted at
+    their arrival times; latency = finished - arrived."""
+    import threading
+
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    reqs = []
+    for i in range(n_requests):
+        N = quantize_n(math.exp(rng.uniform(math.log(64), math.log(2048))))
+        reqs.append(dict(N=N, ny_slices=int(rng.choice([50, 100])), steps=int(rng.integers(10, 2001)),
+                         mu=float(rng.uniform(0.3, 0.8)) * N, seed=10_000 + i))
+    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=16, device=device)
+    rids = [None] * n_requests
+
+    def feeder():
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            rids[i] = srv.submit(r["N"], r["steps"], ny_slices=r["ny_slices"], mu=r["mu"], mass=MASS, step=STEP,
+                                 coupling=jw.FIXED_COUPLING_CONSTANT, seed=r["seed"])
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    lat, t_first, t_last, ok = [], None, 0.0, 0
+    for rid in rids:
+        st, res, _, _ = srv.wait(rid, timeout=3600)
+        ok += st == jw.OK
+        lat.append(res.t_done - res.t_submit)
+        t_first = res.t_submit if t_first is None else min(t_first, res.t_submit)
+        t_last = max(t_last, res.t_done)
+    stats = srv.stats()
+    srv.close()
+    site_steps = sum(r["N"] ** 2 * r["steps"] for r in reqs)
+    return {"requests": n_requests, "ok": ok, "rate_req_per_s": rate,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "site_steps_per_s": site_steps / (t_last - t_first), "wall_s": t_last - t_first,
+            "max_resident": stats.max_active,
+            "offered_site_steps_per_s": site_steps / arrivals[-1],
+            "what": "Poisson arrivals, N log-uniform 64..2048 rounded to powers of two, steps U[10,2000], "
+                    "Ny in {50,100}, mixed precision, continuous batching"}
+
+
+def uneven_leg(jw, device: int, seed: int):
+    """48 events N in {128,256,512,1024} (16/16/12/4), Ny = 50, steps U[200,2000],
+    fixed and running coupling mixed, all submitted at once to the server."""
+    rng = np.random.default_rng(seed)
+    sizes = [128] * 16 + [256] * 16 + [512] * 12 + [1024] * 4
+    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=32, device=device)
+    reqs = [dict(N=n, steps=int(rng.integers(200, 2001)), coupling=[jw.FIXED_COUPLING_CONSTANT,
+                                                                    jw.SQRT_COUPLING_CONSTANT][i % 2])
+            for i, n in enumerate(sizes)]
+    t0 = time.perf_counter()
+    rids = [srv.submit(r["N"], r["steps"], ny_slices=50, step=STEP, coupling=r["coupling"], seed=500 + i)
+            for i, r in enumerate(reqs)]
+    ok = sum(srv.wait(rid, timeout=3600)[0] == jw.OK for rid in rids)
+    wall = time.perf_counter() - t0
+    srv.close()
+    ss = sum(r["N"] ** 2 * r["steps"] for r in reqs)
+    return {"events": len(reqs), "ok": ok, "site_steps": ss, "wall_s": wall, "site_steps_per_s": ss / wall,
+            "what": "48 events N in {128,256,512,1024} (16/16/12/4), steps U[200,2000], mixed couplings, "
+                    "one server, MV initial conditions included"}
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -222,14 +296,15 @@ def main_arm(args):
             dist.barrier()
 
     events = args.events
+    n_side = args.n
     eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch)
-    ids = [eng.add_event(N, ny_slices=NY_SLICES, mu=MU, mass=MASS, step=STEP, coupling=jw.FIXED_COUPLING_CONSTANT,
-                         seed=1_000_003 * (rank + 1) + i) for i in range(events)]
+    ids = [eng.add_event(n_side, ny_slices=NY_SLICES, mu=0.5 * n_side, mass=MASS, step=STEP,
+                         coupling=jw.FIXED_COUPLING_CONSTANT, seed=1_000_003 * (rank + 1) + i) for i in range(events)]
     eng.init_mv(ids)
     eng.step(ids, args.warmup)
     if eng.sync() != jw.OK:
         raise RuntimeError("device error during warm-up")
-    sites = events * N * N
+    sites = events * n_side * n_side
 
     # ---- timed region: K steps, a CUDA event around every fused kernel
     barrier()
@@ -249,8 +324,8 @@ def main_arm(args):
     # read back to host memory (D2H), as main_optimized does with measurements
     # == langevin_steps.
     k_e2e = max(3, min(args.steps, 10))
-    sum_h = np.empty((N, N), np.complex128)
-    err_h = np.empty((N, N), np.complex128)
+    sum_h = np.empty((n_side, n_side), np.complex128)
+    err_h = np.empty((n_side, n_side), np.complex128)
     eng.measure_ensemble(ids, sum_h, err_h)
     stream = torch.cuda.ExternalStream(eng.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -265,7 +340,7 @@ def main_arm(args):
     e2e_ms = barrier_max(e0.elapsed_time(e1))
     e2e_value = world * sites * k_e2e / (e2e_ms / 1e3)
     h2d = 2 * 4 * events               # slot lists of the step and the measurement
-    d2h = 4 * N * N * 8                # sum, err and their compensation planes
+    d2h = 4 * n_side * n_side * 8      # sum, err and their compensation planes
 
     # ---- roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -284,9 +359,9 @@ def main_arm(args):
         "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 transforms / f64 exponentials and V", "data": "synthetic",
-        "config": {"workload": f"{events} events x {N}^2, mixed precision, batched (per GPU)", "events": events,
+        "config": {"workload": f"{events} events x {n_side}^2, mixed precision, batched (per GPU)", "events": events,
                    "max_batch": args.max_batch,
-                   "N": N, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "alpha_s": ALPHA_S, "ds": DS,
+                   "N": n_side, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "alpha_s": ALPHA_S, "ds": DS,
                    "step": STEP, "kernel": "SIN", "coupling": "fixed", "l2": "inputs ~5.6 GB per GPU > L2",
                    "parallelism": f"events sharded, {world} rank(s)"},
         "e2e": {"value": e2e_value, "unit": "site-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -296,7 +371,7 @@ def main_arm(args):
         "roofline": roof,
     }
 
-    if rank == 0 and world == 1 and not args.no_extras:
+    if rank == 0 and world == 1 and not args.no_extras and n_side == N:
         # plain FP64 form: the call-for-call layer (reference structure), one event at a time
         cfg = jw.config_defaults(Nx=N, Ny=N, seed=7, mu=MU, mass=MASS, elementaryWilsonLines=1, step=STEP,
                                  CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
@@ -317,6 +392,9 @@ def main_arm(args):
                               "what": "jw_evolve_momentum, reference call structure, FP64, one 512^2 event",
                               "mixed_batched_over_plain": value / plain}
         ctx.close()
+        line["serve"] = serve_leg(jw, local, args.serve_requests, 200.0, 2026)
+        line["serve"]["vs_fp64_plain"] = line["serve"]["site_steps_per_s"] / plain
+        line["uneven"] = uneven_leg(jw, local, 48)
         # CPU baseline: the reference's own main on a bounded sample
         t, why = run_reference_main(2, 1)
         if t is not None:
@@ -345,6 +423,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64-plain and CPU-baseline legs")
     ap.add_argument("--events", type=int, default=EVENTS, help="events per GPU (profiling runs use fewer)")
     ap.add_argument("--max-batch", type=int, default=0, help="events per launch group (0 = engine default)")
+    ap.add_argument("--serve-requests", type=int, default=100, help="requests in the serving window")
+    ap.add_argument("--n", type=int, default=N, help="lattice side (profiling runs; the workload is 512)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "engine":
         args.warmup = 3

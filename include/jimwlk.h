@@ -107,6 +107,8 @@ typedef struct jw_field jw_field;
  * positions, fftw2D::init2D): binds device `device`, creates a stream and the
  * FFT twiddle tables for cfg->Nx. */
 jw_status jw_context_create(const jw_config* cfg, int device, jw_context** out);
+/* Also releases every field still open in the context; those handles are
+ * invalid afterwards. */
 jw_status jw_context_destroy(jw_context* ctx);
 jw_status jw_context_sync(jw_context* ctx);
 /* The context's cudaStream_t, as void*. */

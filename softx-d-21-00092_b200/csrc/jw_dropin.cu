@@ -6,6 +6,7 @@
 // on contiguous planes and each per-site kernel reads every component with
 // coalesced 16-byte accesses.  jw_field_set / jw_field_get convert from / to
 // the reference's site-major layout (field.h:170-173).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -299,6 +300,11 @@ JW_EXPORT jw_status jw_context_destroy(jw_context* c) {
     if (!c) return JW_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (jw_field* f : c->fields) {
+        cudaFree(f->d);
+        delete f;
+    }
+    c->fields.clear();
     twiddles_destroy(&c->tw);
     if (c->d_flags) cudaFree(c->d_flags);
     if (c->d_tmp) cudaFree(c->d_tmp);
@@ -330,14 +336,17 @@ JW_EXPORT jw_status jw_field_create(jw_context* c, int t, jw_field** out) {
         return JW_ENOMEM;
     }
     JW_CUDA(cudaMemsetAsync(f->d, 0, bytes, c->stream));
+    c->fields.push_back(f);
     *out = f;
     return JW_OK;
 }
 
 JW_EXPORT jw_status jw_field_destroy(jw_field* f) {
     if (!f) return JW_OK;
-    cudaStreamSynchronize(f->ctx->stream);
+    jw_context* c = f->ctx;
+    cudaStreamSynchronize(c->stream);
     cudaFree(f->d);
+    c->fields.erase(std::remove(c->fields.begin(), c->fields.end(), f), c->fields.end());
     delete f;
     return JW_OK;
 }

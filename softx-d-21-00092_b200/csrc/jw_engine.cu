@@ -604,9 +604,20 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     JW_CUDA(cudaMemcpyAsync(g->d_ev + slot, &h, sizeof(EventDev), cudaMemcpyHostToDevice, e->stream));
     JW_CUDA(cudaStreamSynchronize(e->stream));
     g->owner[slot] = ev.id;
+    // workspace for every resident event of this size stepping in one launch group
+    int resident = 0;
+    for (int o : g->owner) resident += o >= 0;
+    s = ensure_workspace(e, *g, chunk_size(e, resident));
+    if (s) {
+        g->owner[slot] = -1;
+        cudaFree(ev.V);
+        cudaFree(ev.acc);
+        e->bytes_in_use -= own;
+        return s;
+    }
     e->events[ev.id] = ev;
     *event_id = ev.id;
-    return ensure_workspace(e, *g, 1);
+    return JW_OK;
 }
 
 JW_EXPORT jw_status jw_engine_remove_event(jw_engine* e, int id) {

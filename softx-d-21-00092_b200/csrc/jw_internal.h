@@ -57,6 +57,7 @@ struct jw_context {
     jw::Twiddles tw;
     int* d_flags = nullptr;       // device error flags
     double2* d_tmp = nullptr;     // one plane of scratch (average_and_symmetrize)
+    std::vector<jw_field*> fields;  // live fields, released by jw_context_destroy
 };
 
 struct jw_field {

@@ -184,9 +184,15 @@ class Context:
         _ck(_lib.jw_context_create(ctypes.byref(cfg), device, ctypes.byref(self._h)), "jw_context_create")
         self.cfg = cfg
         self.N = cfg.Nx
+        import weakref
+        self._fields = weakref.WeakSet()
 
     def close(self):
         if self._h:
+            # the context releases its fields; detach the Python handles first
+            for f in list(self._fields):
+                f._h = _vp()
+            self._fields.clear()
             _lib.jw_context_destroy(self._h)
             self._h = _vp()
 
@@ -255,11 +261,12 @@ class Field:
         self.t = t
         self._h = _vp()
         _ck(_lib.jw_field_create(ctx._h, t, ctypes.byref(self._h)), "jw_field_create")
+        ctx._fields.add(self)
 
     def close(self):
-        if self._h:
+        if self._h and self.ctx._h:
             _lib.jw_field_destroy(self._h)
-            self._h = _vp()
+        self._h = _vp()
 
     def __del__(self):
         try:
