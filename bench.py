@@ -52,8 +52,8 @@ METRIC = "lattice site-steps/s"
 #   pass 1: read V (9 complex FP64 = 144 B) + write 16 FP32 complex planes (128 B)
 #   pass 2: read 16 planes (128 B) + write 8 planes (64 B)
 #   pass 3: read 8 planes (64 B) + read and write V (288 B)
-PASS_BYTES = {"step_pass1": 272, "step_pass2": 192, "step_pass3": 352}
-PASS_NAMES = ["step_pass1", "step_pass2", "step_pass3"]
+PASS_BYTES = {"k_mix_pass1<512>": 272, "k_mix_pass2<512>": 192, "k_mix_pass3<512>": 352}
+PASS_NAMES = ["k_mix_pass1<512>", "k_mix_pass2<512>", "k_mix_pass3<512>"]
 
 
 def dist_env():
