@@ -657,6 +657,160 @@ void jwo_measure(const double* V, int N, double* corr, double* sum, double* err)
     free(c);
 }
 
+/* ======================= position-space evolution ======================= */
+
+void jwo_position_kernel(int dxi, int dyi, int N, int rr, int coupling, int kernel, double* kx, double* ky) {
+    double dx, dy, rrr;
+    if (kernel == JWO_SIN_KERNEL) {
+        /* positions::set (positions.h:130-141) at ii = dxi*N + dyi */
+        dx = 0.5 * N * sin(2.0 * M_PI * dxi / (1.0 * N)) / M_PI;
+        dy = 0.5 * N * sin(2.0 * M_PI * dyi / (1.0 * N)) / M_PI;
+        double sx = N * sin(M_PI * dxi / (1.0 * N)) / M_PI, sy = N * sin(M_PI * dyi / (1.0 * N)) / M_PI;
+        rrr = pow(sx, 2.0) + pow(sy, 2.0);
+    } else {
+        dx = dxi;
+        if (dx >= N / 2) dx = dx - N;
+        if (dx < -N / 2) dx = dx + N;
+        dy = dyi;
+        if (dy >= N / 2) dy = dy - N;
+        if (dy < -N / 2) dy = dy + N;
+        rrr = 1.0 * (dx * dx + dy * dy);
+    }
+    double rrrmin = rrr;
+    if (coupling == JWO_HATTA_COUPLING) rrrmin = (rrr <= rr) ? rrr : rr;
+    const double lambda = pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    double sc = 1.0;
+    if (coupling == JWO_SQRT_COUPLING || coupling == JWO_HATTA_COUPLING)
+        sc = sqrt(4.0 * M_PI / ((11.0 - 2.0 * 3.0 / 3.0) *
+                                log(pow(lambda + 1.26 / pow(6.0 * 6.0 * rrrmin / N / N, 1.0 / 0.2), 0.2))));
+    *kx = 0.0;
+    *ky = 0.0;
+    if (rrr > 10e-9) {
+        *kx = sc * dx / rrr;
+        *ky = sc * dy / rrr;
+    }
+}
+
+/* prepare_A_and_B_local (field.h:2368-2519): for output site x the sum over
+ * all y in (xx, yy) order, re and im accumulated separately. */
+void jwo_prepare_A_and_B(double* A, double* B, const double* xi_x, const double* xi_y, const double* V, int N,
+                         int rr, int coupling, int kernel) {
+    for (int xg = 0; xg < N; ++xg)
+        for (int yg = 0; yg < N; ++yg) {
+            double sAr[9] = {0}, sAi[9] = {0}, sBr[9] = {0}, sBi[9] = {0};
+            for (int xx = 0; xx < N; ++xx)
+                for (int yy = 0; yy < N; ++yy) {
+                    long i = (long)xx * N + yy;
+                    int dxi = xg >= xx ? xg - xx : xg - xx + N;
+                    int dyi = yg >= yy ? yg - yy : yg - yy + N;
+                    double kx, ky;
+                    jwo_position_kernel(dxi, dyi, N, rr, coupling, kernel, &kx, &ky);
+                    cplx Ak = CMPLX(kx, 0.0), Bk = CMPLX(ky, 0.0);
+                    cplx E[9], G[9], H[9], T[9], K[9];
+                    for (int k = 0; k < 9; ++k) {
+                        E[k] = Ak * ld(xi_x, i * 9 + k) + Bk * ld(xi_y, i * 9 + k);
+                        G[k] = ld(V, i * 9 + k);
+                    }
+                    dagger3(G, H);
+                    mul3(G, E, T);
+                    mul3(T, H, K);
+                    for (int k = 0; k < 9; ++k) {
+                        sAr[k] += creal(E[k]); sAi[k] += cimag(E[k]);
+                        sBr[k] += creal(K[k]); sBi[k] += cimag(K[k]);
+                    }
+                }
+            long o = (long)xg * N + yg;
+            for (int k = 0; k < 9; ++k) {
+                st(A, o * 9 + k, CMPLX(sAr[k], sAi[k]));
+                st(B, o * 9 + k, CMPLX(sBr[k], sBi[k]));
+            }
+        }
+}
+
+/* lfield::setCorrelationsForCouplingConstant (field.h:1633-1651), then the
+ * backward unitary transform (main_optimized.cpp:149). */
+void jwo_correlations(int N, double* corr) {
+    const double w = pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    const double f = 4.0 * M_PI / (11.0 - 2.0 * 3.0 / 3.0);
+    for (int xx = 0; xx < N; ++xx)
+        for (int yy = 0; yy < N; ++yy) {
+            long i = (long)xx * N + yy;
+            double sc = f / log(pow(w + pow((phat2_of(xx, yy, N) * N * N) / 6.0 / 6.0, 1.0 / 0.2), 0.2));
+            st(corr, i, CMPLX(sc / sqrt((double)(N * N)), 0.0));
+        }
+    jwo_execute2D(corr, N, 1, 0);
+}
+
+/* gmatrix::decompose (matrix.h:151-200): row-oriented complex-symmetric
+ * Cholesky, L_ii = sqrt(corr[0] - sum_k L_ik^2), L_ij = (corr[|dx| N + |dy|] -
+ * sum_k L_ik L_jk) / L_jj.  pow(z, 2) with an int exponent is z*z (then times
+ * 1) in libstdc++; complex sqrt and division as C99 csqrt and __divdc3. */
+void jwo_cholesky(const double* corr, int N, double* L) {
+    const long n = (long)N * N;
+    memset(L, 0, sizeof(double) * 2 * (size_t)n * n);
+    for (long i = 0; i < n; ++i)
+        for (long j = 0; j <= i; ++j) {
+            if (j == i) {
+                cplx sum = 0;
+                for (long k = 0; k < i; ++k) {
+                    cplx z = ld(L, i * n + k);
+                    sum += CMPLX(1.0, 0.0) * (z * z);
+                }
+                st(L, i * n + i, csqrt(ld(corr, 0) - sum));
+            } else {
+                cplx sum = 0;
+                for (long k = 0; k < j; ++k) sum += ld(L, i * n + k) * ld(L, j * n + k);
+                long xi = i / N, yi = i - xi * N, xj = j / N, yj = j - xj * N;
+                long ii = labs(xi - xj) * N + labs(yi - yj);
+                st(L, i * n + j, (ld(corr, ii) - sum) / ld(L, j * n + j));
+            }
+        }
+}
+
+/* gfield::multiplyByCholesky (field.h:1653-1689): per component, over all j. */
+void jwo_multiply_by_cholesky(const double* L, double* xi, int N) {
+    const long n = (long)N * N;
+    double* tmp = (double*)malloc(sizeof(double) * 2 * (size_t)n);
+    for (int tt = 0; tt < 9; ++tt) {
+        for (long a = 0; a < n; ++a) {
+            cplx s = 0;
+            for (long b = 0; b < n; ++b) s += ld(L, a * n + b) * ld(xi, b * 9 + tt);
+            st(tmp, a, s);
+        }
+        for (long a = 0; a < n; ++a) st(xi, a * 9 + tt, ld(tmp, a));
+    }
+    free(tmp);
+}
+
+void jwo_evolve_position(double* V, int N, int steps, uint64_t step0, double step, int coupling, int kernel,
+                         int rr, const double* L, uint64_t seed) {
+    const long vol = (long)N * N;
+    double* z = (double*)malloc(sizeof(double) * 16 * vol);
+    double* xx = (double*)malloc(sizeof(double) * 18 * vol);
+    double* xy = (double*)malloc(sizeof(double) * 18 * vol);
+    double* A = (double*)malloc(sizeof(double) * 18 * vol);
+    double* B = (double*)malloc(sizeof(double) * 18 * vol);
+    for (int s = 0; s < steps; ++s) {
+        jwo_langevin_normals(seed, step0 + (uint64_t)s, N, z);
+        jwo_generate_gaussian(z, xx, xy, N, 0);
+        if (coupling == JWO_NOISE_COUPLING && L) {
+            jwo_multiply_by_cholesky(L, xx, N);
+            jwo_multiply_by_cholesky(L, xy, N);
+        }
+        jwo_prepare_A_and_B(A, B, xx, xy, V, N, rr, coupling, kernel);
+        jwo_update_uf(V, B, A, N, step);
+    }
+    free(z); free(xx); free(xy); free(A); free(B);
+}
+
+void jwo_reduce_hatta(const double* corr, double* sum, double* err, int N, int xr, int yr) {
+    long i = (long)xr * N + yr;
+    cplx c = ld(corr, i);
+    st(sum, i, ld(sum, i) + c);
+    cplx sq = (cimag(c) == 0.0 && creal(c) > 0.0) ? CMPLX(pow(creal(c), 2.0), 0.0) : c * c;
+    st(err, i, ld(err, i) + sq);
+}
+
 /* ======================= position-space dipole ======================= */
 
 void jwo_dipole_position(const double* corr_sym, int N, double* S_xy) {

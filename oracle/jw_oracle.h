@@ -74,6 +74,31 @@ void jwo_evolve_momentum(double* V, int N, int steps, uint64_t step0, double ste
 /* main_optimized.cpp:321-334: FFT(V), trace, symmetrise, reduce into sum/err. */
 void jwo_measure(const double* V, int N, double* corr, double* sum, double* err);
 
+/* ---- position-space evolution (field.h:2368-2519, positions.h:105-150) ----
+ * A(x) = sum_y k(x-y) xi(y), B(x) = sum_y k(x-y) V(y) xi(y) V(y)^dagger, the
+ * direct O(V^2) sum in the reference's order.  rr = rr_hatta (main_optimized.cpp:229);
+ * for coupling HATTA the reference leaves the coupling uninitialised, and the
+ * oracle evaluates the running (SQRT) coupling at min(r^2, rr), its evident intent. */
+void jwo_prepare_A_and_B(double* A, double* B, const double* xi_x, const double* xi_y, const double* V, int N,
+                         int rr, int coupling, int kernel);
+/* The position-space kernel value at displacement (dx, dy) in 0..N-1 (the
+ * reference's k_x, k_y before multiplying xi; 0 at the origin). */
+void jwo_position_kernel(int dx, int dy, int N, int rr, int coupling, int kernel, double* kx, double* ky);
+/* Correlated noise (main_optimized.cpp:145-157): corr(x) =
+ * IFFT_unitary(sqrt_alpha(phat2)/N) (field.h:1633-1651); the complex-symmetric
+ * Cholesky factor L (L L^T = Sigma, Sigma_ij = corr(|dx|, |dy|), NON-periodic,
+ * gmatrix::decompose matrix.h:151-200), lower triangle, row-major V x V
+ * complex; multiplyByCholesky (field.h:1653-1689) xi' = L xi per component. */
+void jwo_correlations(int N, double* corr);
+void jwo_cholesky(const double* corr, int N, double* L);
+void jwo_multiply_by_cholesky(const double* L, double* xi, int N);
+/* POSITION branch of main_optimized.cpp:243-304: plain generate_gaussian,
+ * Cholesky (coupling NOISE, L given), prepare_A_and_B, update_uf. */
+void jwo_evolve_position(double* V, int N, int steps, uint64_t step0, double step, int coupling, int kernel,
+                         int rr, const double* L, uint64_t seed);
+/* gfield::reduce_hatta (field.h:1538-1567): only element (xr, yr). */
+void jwo_reduce_hatta(const double* corr, double* sum, double* err, int N, int xr, int yr);
+
 /* ---- dipole in position space (defined by this project; the reference stops at C(k)) ----
  * S(r) = (N^2/3) * sum_k C_sym(k) exp(+2 pi i k.r / N), real part, for every
  * displacement r on the lattice (S_xy[(dx*N+dy)], dx, dy in 0..N-1); then the

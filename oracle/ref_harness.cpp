@@ -301,6 +301,113 @@ void ref_evolve_momentum_fixed(double* V_io, int steps) {
     store(uftmp, V_io);
 }
 
+/* prepare_A_and_B_local (field.h:2368-2519) for every site, as the POSITION
+ * branch of main_optimized.cpp:284-300 drives it (global xi and V gathered). */
+void ref_prepare_A_and_B(double* A_out, double* B_out, const double* xi_x, const double* xi_y, const double* V,
+                         int rr, int coupling, int kernel) {
+    ensure_init(nullptr);
+    config* cnfg = ctx().cnfg;
+    gfield<double, 9> gx(Nx, Ny), gy(Nx, Ny), gv(Nx, Ny);
+    memcpy((void*)gx.u, xi_x, sizeof(double) * 18 * Nx * Ny);
+    memcpy((void*)gy.u, xi_y, sizeof(double) * 18 * Nx * Ny);
+    memcpy((void*)gv.u, V, sizeof(double) * 18 * Nx * Ny);
+    lfield<double, 9> A(cnfg->Nxl, cnfg->Nyl), B(cnfg->Nxl, cnfg->Nyl);
+    A.setToZero();
+    B.setToZero();
+    for (int x = 0; x < cnfg->Nxl; x++)
+        for (int y = 0; y < cnfg->Nyl; y++)
+            prepare_A_and_B_local(x, y, x, y, &gx, &gy, &A, &B, &gv, ctx().pos, rr, (Coupling)coupling, (Kernel)kernel);
+    store(A, A_out);
+    store(B, B_out);
+}
+
+/* The correlated-noise set-up of main_optimized.cpp:145-157:
+ * setCorrelationsForCouplingConstant, execute2D(-), allgather, decompose.
+ * The factor is kept for ref_multiply_by_cholesky and copied to L_out
+ * (V*V complex, row-major) when L_out is not null.  The matrix is zeroed
+ * after allocation: the reference mallocs it uninitialised and reads the
+ * whole of it in multiplyByCholesky (field.h:1653-1689); at the sizes it runs
+ * (V*V*16 bytes, far above malloc's mmap threshold) those pages are zero. */
+static gmatrix<double>* g_chol = nullptr;
+void ref_cholesky_setup(double* L_out, double* corr_out) {
+    ensure_init(nullptr);
+    config* cnfg = ctx().cnfg;
+    lfield<double, 1> corr(cnfg->Nxl, cnfg->Nyl);
+    gfield<double, 1> corr_global(Nx, Ny);
+    corr.setCorrelationsForCouplingConstant(ctx().mom);
+    ctx().fft->execute2D(&corr, 0);
+    corr_global.allgather(&corr, ctx().mpi);
+    if (corr_out) memcpy(corr_out, (const void*)corr_global.u, sizeof(double) * 2 * Nx * Ny);
+    if (g_chol) delete g_chol;
+    g_chol = new gmatrix<double>(Nx * Ny, Nx * Ny);
+    memset((void*)g_chol->u, 0, sizeof(double) * 2 * (size_t)Nx * Ny * Nx * Ny);
+    g_chol->decompose(&corr_global);
+    if (L_out) memcpy(L_out, (const void*)g_chol->u, sizeof(double) * 2 * (size_t)Nx * Ny * Nx * Ny);
+}
+
+/* gfield::multiplyByCholesky (field.h:1653-1689) with the set-up factor. */
+void ref_multiply_by_cholesky(double* xi_io) {
+    ensure_init(nullptr);
+    gfield<double, 9> g(Nx, Ny);
+    memcpy((void*)g.u, xi_io, sizeof(double) * 18 * Nx * Ny);
+    g.multiplyByCholesky(g_chol);
+    memcpy(xi_io, (const void*)g.u, sizeof(double) * 18 * Nx * Ny);
+}
+
+/* `steps` position-space steps of main_optimized.cpp:243-304 (POSITION
+ * branch): generate_gaussian, allgather, multiplyByCholesky when the coupling
+ * is NOISE (needs ref_cholesky_setup first), prepare_A_and_B_local at every
+ * site with rr_hatta = rr, update_uf. */
+void ref_evolve_position(double* V_io, int steps, int rr) {
+    ensure_init(nullptr);
+    config* cnfg = ctx().cnfg;
+    lfield<double, 9> uftmp(cnfg->Nxl, cnfg->Nyl);
+    lfield<double, 9> xi_local_x(cnfg->Nxl, cnfg->Nyl), xi_local_y(cnfg->Nxl, cnfg->Nyl);
+    gfield<double, 9> xi_global_x(Nx, Ny), xi_global_y(Nx, Ny), uf_global(Nx, Ny);
+    lfield<double, 9> A_local(cnfg->Nxl, cnfg->Nyl), B_local(cnfg->Nxl, cnfg->Nyl);
+    load(uftmp, V_io);
+    for (int langevin = 0; langevin < steps; langevin++) {
+        generate_gaussian(&xi_local_x, &xi_local_y, ctx().mpi, cnfg);
+        xi_global_x.allgather(&xi_local_x, ctx().mpi);
+        xi_global_y.allgather(&xi_local_y, ctx().mpi);
+        if (cnfg->CouplingChoice == NOISE_COUPLING_CONSTANT) {
+            xi_global_x.multiplyByCholesky(g_chol);
+            xi_global_y.multiplyByCholesky(g_chol);
+        }
+        uf_global.allgather(&uftmp, ctx().mpi);
+        A_local.setToZero();
+        B_local.setToZero();
+        for (int x = 0; x < cnfg->Nxl; x++)
+            for (int y = 0; y < cnfg->Nyl; y++)
+                prepare_A_and_B_local(x, y, x + ctx().mpi->getPosX() * cnfg->Nxl, y + ctx().mpi->getPosY() * cnfg->Nyl,
+                                      &xi_global_x, &xi_global_y, &A_local, &B_local, &uf_global, ctx().pos, rr,
+                                      cnfg->CouplingChoice, cnfg->KernelChoice);
+        update_uf(&uftmp, &B_local, &A_local, cnfg->step);
+    }
+    store(uftmp, V_io);
+}
+
+/* gfield::reduce_hatta (field.h:1538-1567) after average_and_symmetrize of a
+ * measurement of V (main_optimized.cpp:321-332). */
+void ref_measure_hatta(const double* V, double* sum_io, double* err_io, int xr, int yr) {
+    ensure_init(nullptr);
+    config* cnfg = ctx().cnfg;
+    lfield<double, 9> uf_copy(cnfg->Nxl, cnfg->Nyl);
+    lfield<double, 1> corr(cnfg->Nxl, cnfg->Nyl);
+    gfield<double, 1> corr_global(Nx, Ny);
+    lfield<double, 1> sum(cnfg->Nxl, cnfg->Nyl), err(cnfg->Nxl, cnfg->Nyl);
+    load(uf_copy, V);
+    load(sum, sum_io);
+    load(err, err_io);
+    ctx().fft->execute2D(&uf_copy, 1);
+    uf_copy.trace(&corr);
+    corr_global.allgather(&corr, ctx().mpi);
+    corr_global.average_and_symmetrize();
+    corr_global.reduce_hatta(&sum, &err, ctx().mpi, xr, yr);
+    store(sum, sum_io);
+    store(err, err_io);
+}
+
 /* One dipole measurement, main_optimized.cpp:321-334:
  * uf_copy = V; execute2D(+); trace; allgather; average_and_symmetrize;
  * reduce into sum/err (N*N complex each, accumulated in place).

@@ -78,6 +78,46 @@ def fixture_evolution(o: Oracle, N: int, seed: int, coupling: str, steps: int, s
             "sum": s, "err": e}
 
 
+def fixture_position(o: Oracle, N: int, seed: int, coupling: str, kernel: str, steps: int, slices: int) -> dict:
+    """Position-space evolution (main_optimized.cpp:271-304): MV initial
+    condition, `steps` steps with prepare_A_and_B_local and, for NOISE
+    coupling, Cholesky-correlated noise (main_optimized.cpp:145-157)."""
+    r = Reference(N, config_text(mu=0.5 * N, mass=0.04, wilson_lines=slices, step=0.0004,
+                                 evolution="POSITION_EVOLUTION", coupling=coupling, kernel=kernel))
+    c = r.config()
+    V0 = r.initial_condition(np.concatenate([o.mv_normals(seed, s, N).ravel() for s in range(slices)]))
+    out = {"N": N, "seed": seed, "mu": c["mu"], "mass": c["mass"], "step": c["step"], "slices": slices,
+           "steps": steps, "coupling": coupling, "kernel": kernel, "V_mv": V0}
+    z0 = o.langevin_normals(seed, 0, N)
+    xx, xy = o.generate_gaussian(z0, False)
+    cp = 1 if coupling == "NOISE_COUPLING_CONSTANT" else 0
+    kn = 1 if kernel == "SIN_KERNEL" else 0
+    if cp == 1:
+        L, corr = r.cholesky_setup()
+        out["chol_corr"] = corr
+        if N <= 8:
+            out["chol_L"] = L
+        out["xi_x_corr"] = r.multiply_by_cholesky(xx)
+        xx_c, xy_c = out["xi_x_corr"], r.multiply_by_cholesky(xy)
+    else:
+        xx_c, xy_c = xx, xy
+    out["A_pos"], out["B_pos"] = r.prepare_A_and_B(xx_c, xy_c, V0, 0, cp, kn)
+    zs = np.concatenate([o.langevin_normals(seed, s, N).ravel() for s in range(steps)])
+    V1 = r.evolve_position(V0, zs, steps)
+    out["V_final"] = V1
+    out["corr"], out["sum"], out["err"] = r.measure(V1)
+    return out
+
+
+def check_oracle_position(o: Oracle, fx: dict) -> float:
+    N, seed = int(fx["N"]), int(fx["seed"])
+    cp = 1 if str(fx["coupling"]) == "NOISE_COUPLING_CONSTANT" else 0
+    kn = 1 if str(fx["kernel"]) == "SIN_KERNEL" else 0
+    L = o.cholesky(o.correlations(N)) if cp == 1 else None
+    V1 = o.evolve_position(fx["V_mv"], int(fx["steps"]), 0, float(fx["step"]), cp, kn, 0, L, seed)
+    return float(np.abs(V1 - fx["V_final"]).max())
+
+
 def check_oracle(o: Oracle, fx: dict) -> float:
     N, seed = fx["N"], fx["seed"]
     V0 = o.initial_condition(N, fx["mu"], fx["mass"], fx["slices"], seed)
@@ -114,6 +154,23 @@ def main() -> None:
     for name, kw in runs.items():
         fx = fixture_evolution(o, **kw)
         d = check_oracle(o, fx)
+        print(f"{name}: oracle vs reference max deviation {d:.3e}")
+        if d > 1e-12:
+            raise SystemExit(f"oracle disagrees with the reference on {name}")
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fx.items()})
+    pos = {
+        "position_sqrt_sin_N16": dict(N=16, seed=21, coupling="SQRT_COUPLING_CONSTANT", kernel="SIN_KERNEL", steps=4,
+                                      slices=6),
+        "position_sqrt_linear_N8": dict(N=8, seed=22, coupling="SQRT_COUPLING_CONSTANT", kernel="LINEAR_KERNEL",
+                                        steps=4, slices=6),
+        "position_cholesky_N8": dict(N=8, seed=23, coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL", steps=4,
+                                     slices=6),
+        "position_cholesky_N16": dict(N=16, seed=24, coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL",
+                                      steps=3, slices=6),
+    }
+    for name, kw in pos.items():
+        fx = fixture_position(o, **kw)
+        d = check_oracle_position(o, fx)
         print(f"{name}: oracle vs reference max deviation {d:.3e}")
         if d > 1e-12:
             raise SystemExit(f"oracle disagrees with the reference on {name}")

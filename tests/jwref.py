@@ -68,6 +68,15 @@ class Oracle:
         L.jwo_evolve_momentum.argtypes = [_dp, ctypes.c_int, ctypes.c_int, u64, ctypes.c_double, ctypes.c_int,
                                           ctypes.c_int, u64]
         L.jwo_measure.argtypes = [_dp, ctypes.c_int, _dp, _dp, _dp]
+        L.jwo_prepare_A_and_B.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int]
+        L.jwo_position_kernel.argtypes = [ctypes.c_int] * 6 + [_dp, _dp]
+        L.jwo_correlations.argtypes = [ctypes.c_int, _dp]
+        L.jwo_cholesky.argtypes = [_dp, ctypes.c_int, _dp]
+        L.jwo_multiply_by_cholesky.argtypes = [_dp, _dp, ctypes.c_int]
+        L.jwo_evolve_position.argtypes = [_dp, ctypes.c_int, ctypes.c_int, u64, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, _dp, u64]
+        L.jwo_reduce_hatta.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.jwo_dipole_position.argtypes = [_dp, ctypes.c_int, _dp]
         L.jwo_dipole_radial.argtypes = [_dp, ctypes.c_int, _dp, _dp, _ip]
         L.jwo_dipole_radial.restype = ctypes.c_int
@@ -171,6 +180,40 @@ class Oracle:
                            _ptr(sum_.view(np.float64)), _ptr(err.view(np.float64)))
         return corr, sum_, err
 
+    def prepare_A_and_B(self, xi_x, xi_y, V, rr: int, coupling: int, kernel: int):
+        N = V.shape[0]
+        A = np.empty((N, N, 9), np.complex128)
+        B = np.empty((N, N, 9), np.complex128)
+        self.L.jwo_prepare_A_and_B(_ptr(A.view(np.float64)), _ptr(B.view(np.float64)),
+                                   _ptr(np.ascontiguousarray(xi_x).view(np.float64)),
+                                   _ptr(np.ascontiguousarray(xi_y).view(np.float64)),
+                                   _ptr(np.ascontiguousarray(V).view(np.float64)), N, rr, coupling, kernel)
+        return A, B
+
+    def correlations(self, N: int) -> np.ndarray:
+        c = np.empty((N, N), np.complex128)
+        self.L.jwo_correlations(N, _ptr(c.view(np.float64)))
+        return c
+
+    def cholesky(self, corr: np.ndarray) -> np.ndarray:
+        N = corr.shape[0]
+        L = np.empty((N * N, N * N), np.complex128)
+        self.L.jwo_cholesky(_ptr(np.ascontiguousarray(corr).view(np.float64)), N, _ptr(L.view(np.float64)))
+        return L
+
+    def multiply_by_cholesky(self, L, xi):
+        xi = np.ascontiguousarray(xi, np.complex128).copy()
+        self.L.jwo_multiply_by_cholesky(_ptr(np.ascontiguousarray(L).view(np.float64)), _ptr(xi.view(np.float64)),
+                                        xi.shape[0])
+        return xi
+
+    def evolve_position(self, V, steps, step0, step, coupling, kernel, rr, L, seed):
+        V = np.ascontiguousarray(V, np.complex128).copy()
+        Lp = _ptr(np.ascontiguousarray(L).view(np.float64)) if L is not None else None
+        self.L.jwo_evolve_position(_ptr(V.view(np.float64)), V.shape[0], steps, step0, step, coupling, kernel, rr,
+                                   Lp, seed)
+        return V
+
     def dipole(self, corr_sym: np.ndarray):
         N = corr_sym.shape[0]
         Sxy = np.empty((N, N), np.float64)
@@ -216,6 +259,11 @@ class Reference:
         L.ref_evolve_momentum_fixed.argtypes = [_dp, ctypes.c_int]
         L.ref_measure.argtypes = [_dp, _dp, _dp, _dp]
         L.ref_print.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_char_p]
+        L.ref_prepare_A_and_B.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.ref_cholesky_setup.argtypes = [_dp, _dp]
+        L.ref_multiply_by_cholesky.argtypes = [_dp]
+        L.ref_evolve_position.argtypes = [_dp, ctypes.c_int, ctypes.c_int]
+        L.ref_measure_hatta.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
         path = b""
         if config_text is not None:
             cfg = os.path.join(self._tmp, "config")
@@ -311,6 +359,34 @@ class Reference:
         self.inject(z_all)
         V = np.ascontiguousarray(V, np.complex128).copy()
         self.L.ref_evolve_momentum_fixed(_ptr(V.view(np.float64)), steps)
+        return V
+
+    def prepare_A_and_B(self, xi_x, xi_y, V, rr, coupling, kernel):
+        N = self.N
+        A = np.empty((N, N, 9), np.complex128)
+        B = np.empty((N, N, 9), np.complex128)
+        self.L.ref_prepare_A_and_B(_ptr(A.view(np.float64)), _ptr(B.view(np.float64)),
+                                   _ptr(np.ascontiguousarray(xi_x).view(np.float64)),
+                                   _ptr(np.ascontiguousarray(xi_y).view(np.float64)),
+                                   _ptr(np.ascontiguousarray(V).view(np.float64)), rr, coupling, kernel)
+        return A, B
+
+    def cholesky_setup(self):
+        N = self.N
+        L = np.empty((N * N, N * N), np.complex128)
+        c = np.empty((N, N), np.complex128)
+        self.L.ref_cholesky_setup(_ptr(L.view(np.float64)), _ptr(c.view(np.float64)))
+        return L, c
+
+    def multiply_by_cholesky(self, xi):
+        xi = np.ascontiguousarray(xi, np.complex128).copy()
+        self.L.ref_multiply_by_cholesky(_ptr(xi.view(np.float64)))
+        return xi
+
+    def evolve_position(self, V, z_all, steps, rr=0):
+        self.inject(z_all)
+        V = np.ascontiguousarray(V, np.complex128).copy()
+        self.L.ref_evolve_position(_ptr(V.view(np.float64)), steps, rr)
         return V
 
     def measure(self, V, sum_=None, err=None):

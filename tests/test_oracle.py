@@ -48,6 +48,51 @@ def test_oracle_matches_golden_functions(oracle, gold):
     assert np.abs(V - fx["V_upd"]).max() <= 1e-14
 
 
+@pytest.mark.parametrize("name", ["position_sqrt_sin_N16", "position_sqrt_linear_N8", "position_cholesky_N8",
+                                  "position_cholesky_N16"])
+def test_oracle_matches_golden_position(oracle, gold, name):
+    """Position-space evolution (main_optimized.cpp:271-304) with Cholesky-
+    correlated noise for NOISE coupling (main_optimized.cpp:145-157)."""
+    fx = gold(name)
+    N, seed = int(fx["N"]), int(fx["seed"])
+    cp = COUPLING[str(fx["coupling"])]
+    kn = 1 if str(fx["kernel"]) == "SIN_KERNEL" else 0
+    L = None
+    z0 = oracle.langevin_normals(seed, 0, N)
+    xx, xy = oracle.generate_gaussian(z0, False)
+    if cp == 1:
+        corr = oracle.correlations(N)
+        assert np.abs(corr - fx["chol_corr"]).max() <= 1e-15
+        L = oracle.cholesky(corr)
+        if "chol_L" in fx:
+            assert np.abs(L - fx["chol_L"]).max() <= 1e-13
+        xx = oracle.multiply_by_cholesky(L, xx)
+        assert np.abs(xx - fx["xi_x_corr"]).max() <= 1e-13
+        xy = oracle.multiply_by_cholesky(L, xy)
+    A, B = oracle.prepare_A_and_B(xx, xy, fx["V_mv"], 0, cp, kn)
+    assert np.abs(A - fx["A_pos"]).max() <= 1e-13 * np.abs(fx["A_pos"]).max()
+    assert np.abs(B - fx["B_pos"]).max() <= 1e-13 * np.abs(fx["B_pos"]).max()
+    V1 = oracle.evolve_position(fx["V_mv"], int(fx["steps"]), 0, float(fx["step"]), cp, kn, 0, L, seed)
+    assert np.abs(V1 - fx["V_final"]).max() <= 1e-13
+    c, _, _ = oracle.measure(V1)
+    assert np.abs(c - fx["corr"]).max() <= 1e-13 * np.abs(fx["corr"]).max()
+
+
+def test_cholesky_reconstructs_correlation(oracle):
+    """L L^T equals the site-site correlation matrix (main_optimized.cpp:145-157
+    factorises it so that L xi has that covariance)."""
+    N = 8
+    corr = oracle.correlations(N)
+    L = oracle.cholesky(corr)
+    V = N * N
+    S = np.empty((V, V), np.complex128)
+    for i in range(V):
+        for j in range(V):
+            S[i, j] = corr[abs(i // N - j // N), abs(i % N - j % N)]
+    assert np.abs(np.triu(L, 1)).max() == 0.0
+    assert np.abs(L @ L.T - S).max() <= 1e-12 * np.abs(S).max()
+
+
 @pytest.mark.skipif(not reference_available(8), reason="reference harness not built (needs the reference tree)")
 def test_oracle_bitwise_vs_reference_N8(oracle):
     N, seed = 8, 5
