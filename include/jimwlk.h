@@ -190,6 +190,56 @@ jw_status jw_initial_condition(jw_context* ctx, jw_field* V);
  * step0 .. step0+n-1 and the config's coupling, kernel and step. */
 jw_status jw_evolve_momentum(jw_context* ctx, jw_field* V, uint64_t step0, int n);
 
+/* ------------------------------------------------------------------ position-space evolution */
+/* The loop of main_optimized.cpp:290-301 over every site, i.e.
+ * prepare_A_and_B_local(x, y, x_global, y_global, xi_x, xi_y, A, B, uf,
+ * positions, rr, Coupling, Kernel) (field.h:2368-2519) for all (x, y):
+ *   A(x) = sum_y [k_x(x-y) xi_x(y) + k_y(x-y) xi_y(y)]
+ *   B(x) = sum_y V(y) [k_x(x-y) xi_x(y) + k_y(x-y) xi_y(y)] V(y)^dagger
+ * with the real kernel k_i(d) = c(d) d_i / r2(d) of positions::set
+ * (positions.h:105-150) for the SIN kernel or the wrapped distance for the
+ * LINEAR kernel, zero where r2 <= 1e-8.  c = 1 for NOISE and FIXED coupling,
+ * sqrt(4 pi / (9 log((lambda + 1.26 / (36 r2 / N^2)^5)^0.2))) for SQRT and,
+ * at min(r2, rr), for HATTA (the reference leaves c uninitialised there;
+ * this is the formula its comments describe).  Computed as circular
+ * convolutions through the transform (exact up to rounding).  The inputs are
+ * not modified. */
+jw_status jw_prepare_A_and_B(jw_context* ctx, jw_field* A, jw_field* B, const jw_field* xi_x,
+                             const jw_field* xi_y, const jw_field* V, int rr, int coupling, int kernel);
+
+/* lfield::setCorrelationsForCouplingConstant(momenta) (field.h:1633-1651):
+ * corr(k) = 4 pi / (9 log((lambda + (phat2(k) N^2 / 36)^5)^0.2)) / N, t = 1.
+ * main_optimized.cpp:147-149 follows it with jw_execute2D(corr, 0). */
+jw_status jw_set_correlations_for_coupling_constant(jw_context* ctx, jw_field* corr);
+
+/* gmatrix<double> holding the Cholesky factor (matrix.h:151-200). */
+typedef struct jw_cholesky jw_cholesky;
+/* gmatrix::decompose(corr) (matrix.h:151-200): the complex-symmetric
+ * Cholesky factor L (L L^T = S, no conjugation) of the site-site matrix
+ * S(i, j) = corr(|x_i - x_j|, |y_i - y_j|) (non-periodic distances), with
+ * (Nx Ny)^2 complex doubles on the device (68.7 GB at 256^2).  JW_ENOMEM when
+ * the device cannot hold it. */
+jw_status jw_cholesky_decompose(jw_context* ctx, const jw_field* corr, jw_cholesky** out);
+jw_status jw_cholesky_destroy(jw_cholesky* L);
+/* L to the host in the reference layout: row-major, element (i, j) at
+ * complex offset i * Nx*Ny + j, zero above the diagonal. */
+jw_status jw_cholesky_get(const jw_cholesky* L, double* host);
+/* gfield::multiplyByCholesky(gmatrix) (field.h:1653-1689): xi <- L xi for
+ * each of the t components. */
+jw_status jw_multiply_by_cholesky(jw_context* ctx, jw_field* xi, const jw_cholesky* L);
+
+/* gfield::reduce_hatta(sum, err, mpi, xr, yr) (field.h:1538-1564): adds
+ * corr(xr, yr) to sum(xr, yr) and its square to err(xr, yr). */
+jw_status jw_reduce_hatta(jw_context* ctx, const jw_field* corr, jw_field* sum, jw_field* err, int xr, int yr);
+
+/* :232-304 for EvolutionChoice == POSITION_EVOLUTION -- n position-space
+ * steps (step indices step0 .. step0+n-1) with the config's coupling, kernel
+ * and step: plain generate_gaussian noise, for NOISE coupling multiplied by
+ * the Cholesky factor L (required then, ignored otherwise), then
+ * jw_prepare_A_and_B with `rr` and jw_update_uf.  FIXED coupling is the
+ * NOISE kernel factor 1 without the Cholesky factor. */
+jw_status jw_evolve_position(jw_context* ctx, jw_field* V, uint64_t step0, int n, int rr, const jw_cholesky* L);
+
 /* ------------------------------------------------------------------ batched engine */
 #define JW_PRECISION_FP64 0  /* FP64 everywhere */
 #define JW_PRECISION_MIXED 1 /* FP32 noise/rotation/transforms, FP64 exponentials, V, reunitarisation, sums */

@@ -305,6 +305,7 @@ JW_EXPORT jw_status jw_context_destroy(jw_context* c) {
         delete f;
     }
     c->fields.clear();
+    position_release(c);
     twiddles_destroy(&c->tw);
     if (c->d_flags) cudaFree(c->d_flags);
     if (c->d_tmp) cudaFree(c->d_tmp);

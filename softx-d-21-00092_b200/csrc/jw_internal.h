@@ -58,7 +58,18 @@ struct jw_context {
     int* d_flags = nullptr;       // device error flags
     double2* d_tmp = nullptr;     // one plane of scratch (average_and_symmetrize)
     std::vector<jw_field*> fields;  // live fields, released by jw_context_destroy
+    // position-space evolution (jw_position.cu), allocated on first use
+    double2* d_pos_tab = nullptr;   // 2 planes: raw forward DFT of k_x(d), k_y(d)
+    int pos_key[3] = {-1, -1, -1};  // (rr, coupling, kernel) of d_pos_tab
+    double2* d_pos_scratch = nullptr;  // 18 planes
+    void* cublas = nullptr;         // cublasHandle_t (Cholesky decomposition)
+    std::vector<jw_cholesky*> choleskies;  // live factors, released by jw_context_destroy
 };
+
+namespace jw {
+// Frees what jw_position.cu attached to the context.
+void position_release(jw_context* c);
+}
 
 struct jw_field {
     jw_context* ctx = nullptr;

@@ -1,0 +1,644 @@
+// jw_position.cu -- position-space evolution (main_optimized.cpp:271-304):
+// prepare_A_and_B_local for every site as two circular convolutions through
+// the transform, the coupling-constant correlation and its complex-symmetric
+// Cholesky factor (gmatrix::decompose), the factor applied to the noise
+// (gfield::multiplyByCholesky) and reduce_hatta.
+//
+// prepare_A_and_B_local (field.h:2368-2519) sums, for each output site x,
+// k(x - y) xi(y) and k(x - y) V(y) xi(y) V(y)^dagger over all sites y: O(V^2)
+// per step.  Both sums are circular convolutions with a real kernel, so with
+// K = DFT(k) (raw, computed once per (rr, coupling, kernel)) they are
+//   A = U^-1 [K_x U(xi_x) + K_y U(xi_y)],  B = the same with V xi V^dagger,
+// U the unitary transform of execute2D: O(V log V) per step.
+//
+// The Cholesky factor L of the V x V site-site correlation (68.7 GB of
+// complex doubles at 256^2) is stored row-major lower, the reference's own
+// layout, which column-major BLAS sees as the upper factor U = L^T of
+// S = U^T U.  The decomposition is right-looking and blocked: a one-CTA
+// kernel factors each 128 x 128 diagonal block, and cuBLAS ZTRSM / ZSYRK (the
+// complex-symmetric, non-conjugating rank-k update) handle the panel and the
+// trailing matrix.  Applying L streams its lower triangle once per call
+// through a register-blocked FP64 kernel (k_chol_apply): each CTA owns 128
+// rows and one 4096-column chunk, stages 128 x 16 tiles of L with cp.async,
+// and multiplies them with up to 18 real right-hand sides.  For the Langevin
+// noise the right-hand sides are the 16 unit normals of each site (the
+// Gell-Mann embedding is linear and is applied after L), so the kernel reads
+// 16 B of L per 32 FP64 FMAs and is bound by HBM.  Partial products of the
+// chunks are summed in a fixed order, so results are deterministic.
+#include <cublas_v2.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "jw_internal.h"
+
+using namespace jw;
+
+struct jw_cholesky {
+    jw_context* ctx = nullptr;
+    long n = 0;                  // N*N
+    double2* d_L = nullptr;      // n*n complex, row-major lower, zero above the diagonal
+    int2* d_units = nullptr;     // apply work list: (row strip, column chunk)
+    int n_units = 0;
+    int n_chunks = 0;
+    double* d_X = nullptr;       // n x kMaxR real right-hand sides, site-major
+    double2* d_P = nullptr;      // n_chunks x n x kMaxR partial products
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+inline unsigned blocks_for(long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+// Cholesky apply tiling: 128 rows per CTA (one per thread), 16 columns per
+// staged tile, 4096 columns per chunk; at most 18 real right-hand sides.
+constexpr int kTR = 128, kKT = 16, kTC = 4096, kMaxR = 18;
+constexpr int kRowBytes = kKT * 16 + 16;  // padded shared row: conflict-free 16-byte loads across rows
+template <int R> constexpr int apply_stage_bytes() { return kTR * kRowBytes + kKT * R * 8; }
+constexpr int kDiagBlock = 128;
+
+__device__ __forceinline__ void cpa16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+// ---- position kernel (positions.h:105-150, field.h:2402-2462), host FP64
+// with the reference's own expressions so that the tabulated values are the
+// reference's bit for bit.
+void position_kernel_host(int dxi, int dyi, int N, int rr, int coupling, int kernel, double* kx, double* ky) {
+    double dx, dy, rrr;
+    if (kernel == JW_SIN_KERNEL) {
+        dx = 0.5 * N * std::sin(2.0 * M_PI * dxi / (1.0 * N)) / M_PI;
+        dy = 0.5 * N * std::sin(2.0 * M_PI * dyi / (1.0 * N)) / M_PI;
+        const double sx = N * std::sin(M_PI * dxi / (1.0 * N)) / M_PI;
+        const double sy = N * std::sin(M_PI * dyi / (1.0 * N)) / M_PI;
+        rrr = std::pow(sx, 2.0) + std::pow(sy, 2.0);
+    } else {
+        dx = dxi;
+        if (dx >= N / 2) dx = dx - N;
+        if (dx < -N / 2) dx = dx + N;
+        dy = dyi;
+        if (dy >= N / 2) dy = dy - N;
+        if (dy < -N / 2) dy = dy + N;
+        rrr = 1.0 * (dx * dx + dy * dy);
+    }
+    double rrrmin = rrr;
+    if (coupling == JW_HATTA_COUPLING_CONSTANT) rrrmin = (rrr <= rr) ? rrr : rr;
+    const double lambda = std::pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    double sc = 1.0;
+    if (coupling == JW_SQRT_COUPLING_CONSTANT || coupling == JW_HATTA_COUPLING_CONSTANT)
+        sc = std::sqrt(4.0 * M_PI /
+                       ((11.0 - 2.0 * 3.0 / 3.0) *
+                        std::log(std::pow(lambda + 1.26 / std::pow(6.0 * 6.0 * rrrmin / N / N, 1.0 / 0.2), 0.2))));
+    *kx = 0.0;
+    *ky = 0.0;
+    if (rrr > 10e-9) {
+        *kx = sc * dx / rrr;
+        *ky = sc * dy / rrr;
+    }
+}
+
+// out_k = K_x X_k + K_y Y_k for the 9 components (k-space product of the convolution).
+__global__ void k_pos_combine(double2* __restrict__ out, const double2* __restrict__ X, const double2* __restrict__ Y,
+                              const double2* __restrict__ tab, long vol) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    const double2 kx = tab[i], ky = tab[vol + i];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[k * vol + i] = cadd(cmul(kx, X[k * vol + i]), cmul(ky, Y[k * vol + i]));
+}
+
+// V xi_x V^dagger, V xi_y V^dagger (the B-side integrand, field.h:2479-2497).
+__global__ void k_pos_rotate(double2* __restrict__ ox, double2* __restrict__ oy, const double2* __restrict__ V,
+                             const double2* __restrict__ xx, const double2* __restrict__ xy, long vol) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    double2 a[9], b[9], t[9], e[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = V[k * vol + i];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = xx[k * vol + i];
+    mul3(a, b, t);
+    mul3_adj(t, a, e);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ox[k * vol + i] = e[k];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = xy[k * vol + i];
+    mul3(a, b, t);
+    mul3_adj(t, a, e);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) oy[k * vol + i] = e[k];
+}
+
+// ---- gfield::reduce_hatta (field.h:1538-1564)
+__global__ void k_reduce_hatta(const double2* __restrict__ c, double2* __restrict__ sum, double2* __restrict__ err,
+                               long i) {
+    const double2 v = c[i];
+    sum[i] = cadd(sum[i], v);
+    double2 sq;
+    if (v.y == 0.0 && v.x > 0.0) sq = make_double2(v.x * v.x, 0.0);
+    else sq = cmul(v, v);
+    err[i] = cadd(err[i], sq);
+}
+
+// ---- complex square root and division for the diagonal blocks (principal
+// branch; Smith's scaled division, CACM 5(8):435, 1962).
+__device__ __forceinline__ double2 csqrt_p(double2 z) {
+    if (z.x == 0.0 && z.y == 0.0) return make_double2(0.0, z.y);
+    const double t = sqrt(0.5 * (hypot(z.x, z.y) + fabs(z.x)));
+    if (z.x >= 0.0) return make_double2(t, z.y / (2.0 * t));
+    return make_double2(fabs(z.y) / (2.0 * t), copysign(t, z.y));
+}
+__device__ __forceinline__ double2 cdiv_smith(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x, den = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+    }
+    const double r = b.x / b.y, den = b.x * r + b.y;
+    return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+}
+
+// S(i, j) = corr(|x_i - x_j|, |y_i - y_j|) on and below the diagonal, zero
+// above (matrix.h:190-196: non-periodic distances).
+__global__ void k_chol_fill(double2* __restrict__ M, const double2* __restrict__ corr, int N, long n) {
+    const long total = n * n;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const long i = idx / n, j = idx - i * n;
+        double2 v = make_double2(0.0, 0.0);
+        if (j <= i) {
+            const int xi = (int)(i / N), yi = (int)(i % N), xj = (int)(j / N), yj = (int)(j % N);
+            v = corr[(long)abs(xi - xj) * N + abs(yi - yj)];
+        }
+        M[idx] = v;
+    }
+}
+
+// Unblocked right-looking complex-symmetric Cholesky of one b x b diagonal
+// block (row-major lower, leading dimension ld) whose trailing updates from
+// the columns to its left are already applied: L_jj = sqrt(a_jj),
+// L_ij = a_ij / L_jj, a_il -= L_ij L_lj.  One CTA; the block stays in L2.
+__global__ void __launch_bounds__(1024) k_chol_diag(double2* __restrict__ a, long ld, int b) {
+    for (int j = 0; j < b; ++j) {
+        if (threadIdx.x == 0) a[(long)j * ld + j] = csqrt_p(a[(long)j * ld + j]);
+        __syncthreads();
+        const double2 d = a[(long)j * ld + j];
+        for (int i = j + 1 + threadIdx.x; i < b; i += blockDim.x) a[(long)i * ld + j] = cdiv_smith(a[(long)i * ld + j], d);
+        __syncthreads();
+        const int m = b - j - 1;
+        for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+            const int i = j + 1 + q / m, l = j + 1 + q % m;
+            if (l <= i) a[(long)i * ld + l] = csub(a[(long)i * ld + l], cmul(a[(long)i * ld + j], a[(long)l * ld + j]));
+        }
+        __syncthreads();
+    }
+}
+
+// P[chunk][row][c] = sum over the chunk's columns k of L(row, k) X(k, c):
+// complex L times R real right-hand sides.  One CTA per (row strip, chunk)
+// unit, grid-strided; one output row per thread; tiles of 128 rows x 16
+// columns of L double-buffered in shared memory with cp.async.
+template <int R>
+__global__ void __launch_bounds__(kTR) k_chol_apply(const double2* __restrict__ L, const double* __restrict__ X,
+                                                    double2* __restrict__ P, const int2* __restrict__ units,
+                                                    int n_units, long n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int SB = apply_stage_bytes<R>();
+    const int tid = threadIdx.x;
+    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+        const int2 w = units[u];
+        const long row0 = (long)w.x * kTR;
+        const long k0 = (long)w.y * kTC;
+        const long kend = min(k0 + kTC, min(n, row0 + kTR));  // columns past the strip's last row are zero
+        const int nt = (int)((kend - k0) / kKT);               // n, kTR and kTC are multiples of kKT
+        auto stage = [&](int t, int s) {
+            unsigned char* sl = smem + s * SB;
+            double* sx = reinterpret_cast<double*>(sl + kTR * kRowBytes);
+            const long kb = k0 + (long)t * kKT;
+#pragma unroll
+            for (int j = 0; j < kKT; ++j) {
+                const int c = tid + j * kTR;
+                const int r = c / kKT, e = c % kKT;
+                if (row0 + r < n) cpa16(sl + r * kRowBytes + e * 16, L + (row0 + r) * n + kb + e);
+            }
+            for (int c = tid; c < kKT * R / 2; c += kTR) cpa16(sx + 2 * c, X + kb * R + 2 * c);
+            cpa_commit();
+        };
+        double ar[R], ai[R];
+#pragma unroll
+        for (int c = 0; c < R; ++c) ar[c] = ai[c] = 0.0;
+        stage(0, 0);
+        for (int t = 0; t < nt; ++t) {
+            if (t + 1 < nt) {
+                stage(t + 1, (t + 1) & 1);
+                cpa_wait<1>();
+            } else {
+                cpa_wait<0>();
+            }
+            __syncthreads();
+            const unsigned char* sl = smem + (t & 1) * SB;
+            const double* sx = reinterpret_cast<const double*>(sl + kTR * kRowBytes);
+            const double2* lr = reinterpret_cast<const double2*>(sl + tid * kRowBytes);
+#pragma unroll
+            for (int kk = 0; kk < kKT; ++kk) {
+                const double2 l = lr[kk];
+                const double2* xr = reinterpret_cast<const double2*>(sx + kk * R);
+#pragma unroll
+                for (int c = 0; c < R / 2; ++c) {
+                    const double2 x = xr[c];
+                    ar[2 * c] = fma(l.x, x.x, ar[2 * c]);
+                    ai[2 * c] = fma(l.y, x.x, ai[2 * c]);
+                    ar[2 * c + 1] = fma(l.x, x.y, ar[2 * c + 1]);
+                    ai[2 * c + 1] = fma(l.y, x.y, ai[2 * c + 1]);
+                }
+            }
+            __syncthreads();
+        }
+        const long row = row0 + tid;
+        if (row < n) {
+            double2* p = P + ((long)w.y * n + row) * R;
+#pragma unroll
+            for (int c = 0; c < R; ++c) p[c] = make_double2(ar[c], ai[c]);
+        }
+    }
+}
+
+// Number of column chunks that hold entries of `row` (those up to the end of its strip).
+__device__ __forceinline__ int chunks_of_row(long row, long n) {
+    const long last = min(n, (row / kTR + 1) * kTR) - 1;
+    return (int)(last / kTC) + 1;
+}
+
+// Real right-hand sides of a field: X(i, k) = Re xi_k(i), X(i, t + k) = Im xi_k(i).
+__global__ void k_chol_gather_field(const double2* __restrict__ xi, double* __restrict__ X, long n, int t) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = 0; k < t; ++k) {
+        const double2 v = xi[k * n + i];
+        X[i * 2 * t + k] = v.x;
+        X[i * 2 * t + t + k] = v.y;
+    }
+}
+
+// xi_k = Y_k + i Y_{t+k}, Y = sum of the chunk partials in chunk order.
+template <int R>
+__global__ void k_chol_finish_field(const double2* __restrict__ P, double2* __restrict__ xi, long n) {
+    constexpr int t = R / 2;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double2 y[R];
+#pragma unroll
+    for (int c = 0; c < R; ++c) y[c] = make_double2(0.0, 0.0);
+    const int nc = chunks_of_row(i, n);
+    for (int ch = 0; ch < nc; ++ch) {
+        const double2* p = P + ((long)ch * n + i) * R;
+#pragma unroll
+        for (int c = 0; c < R; ++c) y[c] = cadd(y[c], p[c]);
+    }
+#pragma unroll
+    for (int k = 0; k < t; ++k) xi[k * n + i] = make_double2(y[k].x - y[t + k].y, y[k].y + y[t + k].x);
+}
+
+// The 16 unit normals of each site in the reference's draw order
+// (field.h:2170-2173): X(i, a) = n_a (xi_x), X(i, 8 + a) = m_a (xi_y).
+__global__ void k_chol_noise_X(double* __restrict__ X, long n, uint64_t seed, uint64_t step) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double z[16];
+    langevin_normals<double>(seed, step, (uint32_t)i, z);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        X[i * 16 + a] = z[2 * a];
+        X[i * 16 + 8 + a] = z[2 * a + 1];
+    }
+}
+
+// xi_x = sum_a (L n_a) lambda_a, xi_y = sum_a (L m_a) lambda_a: the
+// correlated noise L (sum_a n_a lambda_a) of gfield::multiplyByCholesky,
+// with the (linear) embedding applied after L.
+__global__ void k_chol_finish_noise(const double2* __restrict__ P, double2* __restrict__ xx, double2* __restrict__ xy,
+                                    long n) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double2 y[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) y[c] = make_double2(0.0, 0.0);
+    const int nc = chunks_of_row(i, n);
+    for (int ch = 0; ch < nc; ++ch) {
+        const double2* p = P + ((long)ch * n + i) * 16;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) y[c] = cadd(y[c], p[c]);
+    }
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        double re[8], im[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            re[a] = y[8 * f + a].x;
+            im[a] = y[8 * f + a].y;
+        }
+        double2 mr[9], mi[9];
+        embed_lambda_ref(re, mr);
+        embed_lambda_ref(im, mi);
+        double2* o = f == 0 ? xx : xy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o[k * n + i] = make_double2(mr[k].x - mi[k].y, mr[k].y + mi[k].x);
+    }
+}
+
+bool same_ctx(const jw_field* a, const jw_field* b) { return a && b && a->ctx == b->ctx; }
+
+jw_status ensure_scratch(jw_context* c) {
+    if (c->d_pos_scratch) return JW_OK;
+    if (cudaMalloc(&c->d_pos_scratch, sizeof(double2) * 18 * (size_t)c->N * c->N) != cudaSuccess) {
+        c->d_pos_scratch = nullptr;
+        return JW_ENOMEM;
+    }
+    return JW_OK;
+}
+
+// The raw forward DFT of k_x(d), k_y(d) for (rr, coupling, kernel).
+jw_status ensure_table(jw_context* c, int rr, int coupling, int kernel) {
+    if (c->d_pos_tab && c->pos_key[0] == rr && c->pos_key[1] == coupling && c->pos_key[2] == kernel) return JW_OK;
+    const int N = c->N;
+    const long vol = (long)N * N;
+    if (!c->d_pos_tab && cudaMalloc(&c->d_pos_tab, sizeof(double2) * 2 * vol) != cudaSuccess) {
+        c->d_pos_tab = nullptr;
+        return JW_ENOMEM;
+    }
+    std::vector<double2> h(2 * vol);
+    for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+            double kx, ky;
+            position_kernel_host(x, y, N, rr, coupling, kernel, &kx, &ky);
+            h[(long)x * N + y] = make_double2(kx, 0.0);
+            h[vol + (long)x * N + y] = make_double2(ky, 0.0);
+        }
+    // the previous table may still be read by work queued on the stream
+    JW_CUDA(cudaStreamSynchronize(c->stream));
+    c->pos_key[0] = c->pos_key[1] = c->pos_key[2] = -1;
+    JW_CUDA(cudaMemcpy(c->d_pos_tab, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice));
+    JW_CUDA(fft2d_planes<double>(c->d_pos_tab, 2, N, 1, 1.0, c->tw, c->stream));
+    c->pos_key[0] = rr;
+    c->pos_key[1] = coupling;
+    c->pos_key[2] = kernel;
+    return JW_OK;
+}
+
+bool valid_coupling(int cp) {
+    return cp == JW_SQRT_COUPLING_CONSTANT || cp == JW_NOISE_COUPLING_CONSTANT || cp == JW_HATTA_COUPLING_CONSTANT ||
+           cp == JW_FIXED_COUPLING_CONSTANT;
+}
+
+int apply_grid(const void* fn, int smem, int units) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kTR, smem);
+    return std::max(1, std::min(units, sms * std::max(per, 1)));
+}
+
+template <int R>
+jw_status launch_apply(const jw_cholesky* L, cudaStream_t s) {
+    constexpr int smem = 2 * apply_stage_bytes<R>();
+    JW_CUDA(cudaFuncSetAttribute(k_chol_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int grid = apply_grid((const void*)k_chol_apply<R>, smem, L->n_units);
+    k_chol_apply<R><<<grid, kTR, smem, s>>>(L->d_L, L->d_X, L->d_P, L->d_units, L->n_units, L->n);
+    JW_CUDA(cudaGetLastError());
+    return JW_OK;
+}
+
+void cholesky_free(jw_cholesky* L) {
+    if (L->d_L) cudaFree(L->d_L);
+    if (L->d_units) cudaFree(L->d_units);
+    if (L->d_X) cudaFree(L->d_X);
+    if (L->d_P) cudaFree(L->d_P);
+    delete L;
+}
+
+// Correlated Langevin noise of one step into xi_x, xi_y.
+jw_status cholesky_noise(jw_context* c, const jw_cholesky* L, jw_field* xx, jw_field* xy, uint64_t step) {
+    const long n = L->n;
+    k_chol_noise_X<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_X, n, c->cfg.seed, step);
+    JW_CUDA(cudaGetLastError());
+    jw_status s = launch_apply<16>(L, c->stream);
+    if (s) return s;
+    k_chol_finish_noise<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xx->d, xy->d, n);
+    JW_CUDA(cudaGetLastError());
+    return JW_OK;
+}
+
+}  // namespace
+
+namespace jw {
+void position_release(jw_context* c) {
+    for (jw_cholesky* L : c->choleskies) cholesky_free(L);
+    c->choleskies.clear();
+    if (c->d_pos_tab) cudaFree(c->d_pos_tab);
+    if (c->d_pos_scratch) cudaFree(c->d_pos_scratch);
+    if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
+    c->d_pos_tab = nullptr;
+    c->d_pos_scratch = nullptr;
+    c->cublas = nullptr;
+}
+}  // namespace jw
+
+// =================================================================== C ABI
+
+JW_EXPORT jw_status jw_prepare_A_and_B(jw_context* c, jw_field* A, jw_field* B, const jw_field* xi_x,
+                                       const jw_field* xi_y, const jw_field* V, int rr, int coupling, int kernel) {
+    JW_CHECK(c && same_ctx(A, B) && same_ctx(B, xi_x) && same_ctx(xi_x, xi_y) && same_ctx(xi_y, V) && A->ctx == c);
+    JW_CHECK(A->t == 9 && B->t == 9 && xi_x->t == 9 && xi_y->t == 9 && V->t == 9);
+    JW_CHECK(A != B && A != xi_x && A != xi_y && A != V && B != xi_x && B != xi_y && B != V);
+    JW_CHECK(valid_coupling(coupling) && (kernel == JW_LINEAR_KERNEL || kernel == JW_SIN_KERNEL) && rr >= 0);
+    jw_status s = ensure_scratch(c);
+    if (!s) s = ensure_table(c, rr, coupling, kernel);
+    if (s) return s;
+    const int N = c->N;
+    const long vol = (long)N * N;
+    const double scale = 1.0 / std::sqrt((double)vol);
+    double2* S1 = c->d_pos_scratch;
+    double2* S2 = c->d_pos_scratch + 9 * vol;
+    JW_CUDA(cudaMemcpyAsync(S1, xi_x->d, sizeof(double2) * 9 * vol, cudaMemcpyDeviceToDevice, c->stream));
+    JW_CUDA(cudaMemcpyAsync(S2, xi_y->d, sizeof(double2) * 9 * vol, cudaMemcpyDeviceToDevice, c->stream));
+    JW_CUDA(fft2d_planes<double>(S1, 18, N, 1, scale, c->tw, c->stream));
+    k_pos_combine<<<blocks_for(vol), kThreads, 0, c->stream>>>(A->d, S1, S2, c->d_pos_tab, vol);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(fft2d_planes<double>(A->d, 9, N, 0, scale, c->tw, c->stream));
+    k_pos_rotate<<<blocks_for(vol), kThreads, 0, c->stream>>>(S1, S2, V->d, xi_x->d, xi_y->d, vol);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(fft2d_planes<double>(S1, 18, N, 1, scale, c->tw, c->stream));
+    k_pos_combine<<<blocks_for(vol), kThreads, 0, c->stream>>>(B->d, S1, S2, c->d_pos_tab, vol);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(fft2d_planes<double>(B->d, 9, N, 0, scale, c->tw, c->stream));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_set_correlations_for_coupling_constant(jw_context* c, jw_field* corr) {
+    JW_CHECK(c && corr && corr->ctx == c && corr->t == 1);
+    const int N = c->N;
+    const long vol = (long)N * N;
+    const double w = std::pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    const double f = 4.0 * M_PI / (11.0 - 2.0 * 3.0 / 3.0);
+    std::vector<double2> h(vol);
+    for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+            // momenta::set (momenta.h:90-124)
+            const double sx = std::sin(M_PI * x / (1.0 * N)), sy = std::sin(M_PI * y / (1.0 * N));
+            const double ph2 = 4.0 * std::pow(sx, 2.0) + 4.0 * std::pow(sy, 2.0);
+            const double cc = f / std::log(std::pow(w + std::pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2), 0.2));
+            h[(long)x * N + y] = make_double2(cc / std::sqrt((double)(N * N)), 0.0);
+        }
+    JW_CUDA(cudaStreamSynchronize(c->stream));
+    JW_CUDA(cudaMemcpy(corr->d, h.data(), sizeof(double2) * vol, cudaMemcpyHostToDevice));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, jw_cholesky** out) {
+    JW_CHECK(c && corr && corr->ctx == c && corr->t == 1 && out);
+    *out = nullptr;
+    const int N = c->N;
+    const long n = (long)N * N;
+    const size_t bytesL = sizeof(double2) * (size_t)n * n;
+    int n_chunks = (int)((n + kTC - 1) / kTC);
+    const size_t bytesX = sizeof(double) * (size_t)n * kMaxR;
+    const size_t bytesP = sizeof(double2) * (size_t)n_chunks * n * kMaxR;
+    size_t free_b = 0, total_b = 0;
+    JW_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (bytesL + bytesX + bytesP + ((size_t)1 << 30) > free_b) return JW_ENOMEM;
+    if (!c->cublas) {
+        cublasHandle_t h = nullptr;
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return JW_ECUDA;
+        c->cublas = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(c->cublas);
+    if (cublasSetStream(h, c->stream) != CUBLAS_STATUS_SUCCESS) return JW_ECUDA;
+    jw_cholesky* L = new jw_cholesky();
+    L->ctx = c;
+    L->n = n;
+    L->n_chunks = n_chunks;
+    if (cudaMalloc(&L->d_L, bytesL) != cudaSuccess || cudaMalloc(&L->d_X, bytesX) != cudaSuccess ||
+        cudaMalloc(&L->d_P, bytesP) != cudaSuccess) {
+        cholesky_free(L);
+        return JW_ENOMEM;
+    }
+    // apply work list, longest units first
+    std::vector<int2> units;
+    const long strips = (n + kTR - 1) / kTR;
+    for (long s = 0; s < strips; ++s) {
+        const long last = std::min(n, (s + 1) * kTR) - 1;
+        for (long ch = 0; ch <= last / kTC; ++ch) units.push_back(make_int2((int)s, (int)ch));
+    }
+    auto work = [&](int2 u) { return std::min((long)(u.y + 1) * kTC, std::min(n, (long)(u.x + 1) * kTR)) - (long)u.y * kTC; };
+    std::stable_sort(units.begin(), units.end(), [&](int2 a, int2 b) { return work(a) > work(b); });
+    L->n_units = (int)units.size();
+    if (cudaMalloc(&L->d_units, sizeof(int2) * units.size()) != cudaSuccess) {
+        cholesky_free(L);
+        return JW_ENOMEM;
+    }
+    auto fail = [&](jw_status s) {
+        cudaStreamSynchronize(c->stream);
+        cholesky_free(L);
+        return s;
+    };
+    if (cudaMemcpy(L->d_units, units.data(), sizeof(int2) * units.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(JW_ECUDA);
+    k_chol_fill<<<148 * 16, kThreads, 0, c->stream>>>(L->d_L, corr->d, N, n);
+    if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), minus_one = make_cuDoubleComplex(-1.0, 0.0);
+    for (long k0 = 0; k0 < n; k0 += kDiagBlock) {
+        const long b = std::min((long)kDiagBlock, n - k0);
+        double2* Akk = L->d_L + k0 * n + k0;
+        k_chol_diag<<<1, 1024, 0, c->stream>>>(Akk, n, (int)b);
+        if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
+        const long rest = n - k0 - b;
+        if (rest == 0) break;
+        // column-major view: U = L^T is upper; panel U(k0:k0+b, k0+b:n) <- U_kk^-T panel
+        cuDoubleComplex* Ukk = reinterpret_cast<cuDoubleComplex*>(Akk);
+        cuDoubleComplex* Upan = reinterpret_cast<cuDoubleComplex*>(L->d_L + (k0 + b) * n + k0);
+        cuDoubleComplex* Utr = reinterpret_cast<cuDoubleComplex*>(L->d_L + (k0 + b) * n + (k0 + b));
+        if (cublasZtrsm_64(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, b, rest, &one,
+                           Ukk, n, Upan, n) != CUBLAS_STATUS_SUCCESS)
+            return fail(JW_ECUDA);
+        // trailing S(k0+b:, k0+b:) -= panel^T panel (upper, complex symmetric)
+        if (cublasZsyrk_64(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, rest, b, &minus_one, Upan, n, &one, Utr, n) !=
+            CUBLAS_STATUS_SUCCESS)
+            return fail(JW_ECUDA);
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(JW_ECUDA);
+    c->choleskies.push_back(L);
+    *out = L;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_cholesky_destroy(jw_cholesky* L) {
+    if (!L) return JW_OK;
+    jw_context* c = L->ctx;
+    cudaStreamSynchronize(c->stream);
+    c->choleskies.erase(std::remove(c->choleskies.begin(), c->choleskies.end(), L), c->choleskies.end());
+    cholesky_free(L);
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_cholesky_get(const jw_cholesky* L, double* host) {
+    JW_CHECK(L && host);
+    JW_CUDA(cudaStreamSynchronize(L->ctx->stream));
+    JW_CUDA(cudaMemcpy(host, L->d_L, sizeof(double2) * (size_t)L->n * L->n, cudaMemcpyDeviceToHost));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_multiply_by_cholesky(jw_context* c, jw_field* xi, const jw_cholesky* L) {
+    JW_CHECK(c && xi && xi->ctx == c && L && L->ctx == c);
+    const long n = L->n;
+    k_chol_gather_field<<<blocks_for(n), kThreads, 0, c->stream>>>(xi->d, L->d_X, n, xi->t);
+    JW_CUDA(cudaGetLastError());
+    jw_status s;
+    if (xi->t == 9) {
+        s = launch_apply<18>(L, c->stream);
+        if (s) return s;
+        k_chol_finish_field<18><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
+    } else {
+        s = launch_apply<2>(L, c->stream);
+        if (s) return s;
+        k_chol_finish_field<2><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
+    }
+    JW_CUDA(cudaGetLastError());
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_reduce_hatta(jw_context* c, const jw_field* corr, jw_field* sum, jw_field* err, int xr,
+                                    int yr) {
+    JW_CHECK(c && same_ctx(corr, sum) && same_ctx(sum, err) && corr->ctx == c);
+    JW_CHECK(corr->t == 1 && sum->t == 1 && err->t == 1 && sum != err && corr != sum && corr != err);
+    JW_CHECK(xr >= 0 && xr < c->N && yr >= 0 && yr < c->N);
+    k_reduce_hatta<<<1, 1, 0, c->stream>>>(corr->d, sum->d, err->d, (long)xr * c->N + yr);
+    JW_CUDA(cudaGetLastError());
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_evolve_position(jw_context* c, jw_field* V, uint64_t step0, int n, int rr,
+                                       const jw_cholesky* L) {
+    JW_CHECK(c && V && V->ctx == c && V->t == 9 && n >= 0 && rr >= 0);
+    const jw_config& cfg = c->cfg;
+    const int coupling = cfg.CouplingChoice;
+    JW_CHECK(valid_coupling(coupling));
+    const bool correlated = coupling == JW_NOISE_COUPLING_CONSTANT;
+    if (correlated) JW_CHECK(L && L->ctx == c);
+    jw_field *xx = nullptr, *xy = nullptr, *A = nullptr, *B = nullptr;
+    jw_status s = JW_OK;
+    jw_field** all[4] = {&xx, &xy, &A, &B};
+    for (auto p : all)
+        if (!s) s = jw_field_create(c, 9, p);
+    for (int k = 0; k < n && s == JW_OK; ++k) {
+        const uint64_t step = step0 + (uint64_t)k;
+        if (correlated) s = cholesky_noise(c, L, xx, xy, step);
+        else s = jw_generate_gaussian(c, xx, xy, step, 0);
+        if (!s) s = jw_prepare_A_and_B(c, A, B, xx, xy, V, rr, coupling, cfg.KernelChoice);
+        if (!s) s = jw_update_uf(c, V, B, A, cfg.step);
+    }
+    for (auto p : all) jw_field_destroy(*p);
+    return s;
+}

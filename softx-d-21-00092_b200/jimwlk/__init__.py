@@ -113,6 +113,15 @@ def _load():
         "jw_print": ([_vp, ctypes.c_int, _vp, _vp, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
         "jw_initial_condition": ([_vp, _vp], ctypes.c_int),
         "jw_evolve_momentum": ([_vp, _vp, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
+        "jw_prepare_A_and_B": ([_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+                               ctypes.c_int),
+        "jw_set_correlations_for_coupling_constant": ([_vp, _vp], ctypes.c_int),
+        "jw_cholesky_decompose": ([_vp, _vp, ctypes.POINTER(_vp)], ctypes.c_int),
+        "jw_cholesky_destroy": ([_vp], ctypes.c_int),
+        "jw_cholesky_get": ([_vp, _dp], ctypes.c_int),
+        "jw_multiply_by_cholesky": ([_vp, _vp, _vp], ctypes.c_int),
+        "jw_reduce_hatta": ([_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "jw_evolve_position": ([_vp, _vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
         "jw_engine_create": ([ctypes.POINTER(jw_engine_options), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
         "jw_engine_destroy": ([_vp], ctypes.c_int),
         "jw_engine_sync": ([_vp], ctypes.c_int),
@@ -251,6 +260,56 @@ class Context:
 
     def evolve_momentum(self, V, step0: int, n: int):
         _ck(_lib.jw_evolve_momentum(self._h, V._h, step0, n), "jw_evolve_momentum")
+
+    # position-space evolution (main_optimized.cpp:271-304)
+    def prepare_A_and_B(self, A, B, xi_x, xi_y, V, rr: int, coupling: int, kernel: int):
+        _ck(_lib.jw_prepare_A_and_B(self._h, A._h, B._h, xi_x._h, xi_y._h, V._h, rr, coupling, kernel),
+            "jw_prepare_A_and_B")
+
+    def set_correlations_for_coupling_constant(self, corr):
+        _ck(_lib.jw_set_correlations_for_coupling_constant(self._h, corr._h),
+            "jw_set_correlations_for_coupling_constant")
+
+    def cholesky(self, corr) -> "Cholesky":
+        """gmatrix::decompose of the backward-transformed correlation `corr`."""
+        return Cholesky(self, corr)
+
+    def multiply_by_cholesky(self, xi, L: "Cholesky"):
+        _ck(_lib.jw_multiply_by_cholesky(self._h, xi._h, L._h), "jw_multiply_by_cholesky")
+
+    def reduce_hatta(self, corr, sum_, err, xr: int, yr: int):
+        _ck(_lib.jw_reduce_hatta(self._h, corr._h, sum_._h, err._h, xr, yr), "jw_reduce_hatta")
+
+    def evolve_position(self, V, step0: int, n: int, rr: int = 0, L: "Cholesky | None" = None):
+        _ck(_lib.jw_evolve_position(self._h, V._h, step0, n, rr, L._h if L is not None else None),
+            "jw_evolve_position")
+
+
+class Cholesky:
+    """The device Cholesky factor of the site-site correlation (jw_cholesky)."""
+
+    def __init__(self, ctx: Context, corr: "Field"):
+        self.ctx = ctx
+        self._h = _vp()
+        _ck(_lib.jw_cholesky_decompose(ctx._h, corr._h, ctypes.byref(self._h)), "jw_cholesky_decompose")
+        ctx._fields.add(self)
+
+    def get(self) -> np.ndarray:
+        n = self.ctx.N * self.ctx.N
+        a = np.empty((n, n), np.complex128)
+        _ck(_lib.jw_cholesky_get(self._h, a.ctypes.data_as(_dp)), "jw_cholesky_get")
+        return a
+
+    def close(self):
+        if self._h and self.ctx._h:
+            _lib.jw_cholesky_destroy(self._h)
+        self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Field:
