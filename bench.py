@@ -135,28 +135,117 @@ def parse_evolution_times(text: str):
     return [float(x) for x in re.findall(r"Evolution time:\s*([0-9.eE+-]+)", text)]
 
 
-def run_reference_main(steps: int, warmup: int, nthreads: int | None = None):
-    """The reference's main_optimized on one 512^2 event: returns seconds per
-    Langevin step (mean over the last `steps` of warmup + steps)."""
-    if not os.path.exists(REF_MAIN):
-        return None, "reference binary oracle/_ref/main_optimized_omp_512 not built"
+def run_reference_main(steps: int, warmup: int, nthreads: int | None = None, n_side: int = N,
+                       evolution: str = "MOMENTUM_EVOLUTION", coupling: str = "SQRT_COUPLING_CONSTANT",
+                       with_wall: bool = False):
+    """The reference's main_optimized on one n_side^2 event: returns seconds per
+    Langevin step (mean over the last `steps` of warmup + steps) and, with
+    with_wall, the run's wall time outside the initial condition and the
+    steps (the set-up, which holds the Cholesky decomposition)."""
+    exe = os.path.join(REPO, "oracle", "_ref", f"main_optimized_omp_{n_side}")
+    if not os.path.exists(exe):
+        return None, f"reference binary oracle/_ref/main_optimized_omp_{n_side} not built"
     with tempfile.TemporaryDirectory() as d:
         cfg = os.path.join(d, "config")
         with open(cfg, "w") as fh:
             # 1 MV slice: the initial condition is outside the per-step timing;
             # SQRT coupling takes the reference's parallel generate_gaussian.
-            fh.write(f"stat = 1\nmu = {MU}\nmass = {MASS}\nelementaryWilsonLines = 1\nfile_name = bench\n"
-                     f"langevin_steps = {warmup + steps}\nmeasurements = 1\nstep = {STEP}\n"
-                     "EvolutionChoice = MOMENTUM_EVOLUTION\nCouplingChoice = SQRT_COUPLING_CONSTANT\n"
-                     "KernelChoice = SIN_KERNEL\n")
+            fh.write(f"stat = 1\nmu = {0.5 * n_side}\nmass = {MASS}\nelementaryWilsonLines = 1\n"
+                     f"file_name = bench\nlangevin_steps = {warmup + steps}\nmeasurements = 1\nstep = {STEP}\n"
+                     f"EvolutionChoice = {evolution}\nCouplingChoice = {coupling}\nKernelChoice = SIN_KERNEL\n")
         env = dict(os.environ)
         env["OMP_NUM_THREADS"] = str(nthreads or os.cpu_count())
-        r = subprocess.run([REF_MAIN, "1", "1", cfg], cwd=d, capture_output=True, text=True, env=env,
-                           timeout=3600)
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, "1", "1", cfg], cwd=d, capture_output=True, text=True, env=env, timeout=3600)
+        wall = time.perf_counter() - t0
         t = parse_evolution_times(r.stdout)
         if len(t) < warmup + steps:
             return None, f"reference run produced {len(t)} step timings (rc={r.returncode})"
+        if with_wall:
+            ic = [float(x) for x in re.findall(r"Initial condition time:\s*([0-9.eE+-]+)", r.stdout)]
+            return (statistics.mean(t[warmup:]), wall - sum(t) - sum(ic)), None
         return statistics.mean(t[warmup:]), None
+
+
+POS_N, POS_SLICES, POS_STEPS, POS_EVERY = 256, 100, 500, 50
+POS_STEP = DS / math.pi ** 2  # running coupling: alpha_s(r) enters through the correlated noise
+POS_CPU_N = 32
+
+
+def position_leg(jw, device: int, steps: int = POS_STEPS, every: int = POS_EVERY):
+    """Position-space evolution with Cholesky-correlated noise (the reference's
+    POSITION_EVOLUTION + NOISE_COUPLING_CONSTANT path, main_optimized.cpp:
+    145-157, 271-304) on one 256^2 event in FP64: MV initial condition with
+    Ny = 100 slices, the 68.7 GB factor, `steps` steps measured every `every`
+    (C(k), S(r), Q_s).  The factor apply streams the lower triangle of L once
+    per step: 16 n (n + 1) / 2 bytes, n = N^2."""
+    import torch
+    cfg = jw.config_defaults(Nx=POS_N, Ny=POS_N, seed=11, mu=0.5 * POS_N, mass=MASS,
+                             elementaryWilsonLines=POS_SLICES, step=POS_STEP, EvolutionChoice=jw.POSITION_EVOLUTION,
+                             CouplingChoice=jw.NOISE_COUPLING_CONSTANT, KernelChoice=jw.SIN_KERNEL)
+    ctx = jw.Context(cfg, device)
+    s = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    V = ctx.field()
+    a.record(s)
+    ctx.initial_condition(V)
+    b.record(s)
+    b.synchronize()
+    ic_ms = a.elapsed_time(b)
+    corr = ctx.field(1)
+    ctx.set_correlations_for_coupling_constant(corr)
+    ctx.execute2D(corr, 0)
+    ctx.sync()
+    t0 = time.perf_counter()
+    L = ctx.cholesky(corr)  # returns after the decomposition has finished
+    dec_s = time.perf_counter() - t0
+    ctx.evolve_position(V, 0, 0, 0, L)  # allocates the step's work fields
+    Vk, c = ctx.field(), ctx.field(1)
+    evo_ms, qs, done = 0.0, [], 0
+    while done < steps:
+        k = min(every, steps - done)
+        a.record(s)
+        ctx.evolve_position(V, done, k, 0, L)
+        b.record(s)
+        b.synchronize()
+        evo_ms += a.elapsed_time(b)
+        done += k
+        Vk.copy_from(V)
+        ctx.execute2D(Vk, 1)
+        ctx.trace(Vk, c)
+        ctx.average_and_symmetrize(c)
+        qs.append(ctx.dipole(c)[3])
+    status = ctx.sync()
+    Vh = V.get().reshape(-1, 3, 3)
+    drift = float(np.abs(Vh @ np.conj(np.transpose(Vh, (0, 2, 1))) - np.eye(3)).max())
+    ctx.close()
+    n = POS_N * POS_N
+    lbytes = 16.0 * n * (n + 1) / 2
+    step_ms = evo_ms / steps
+    out = {"workload": f"1 event {POS_N}^2, POSITION_EVOLUTION + NOISE_COUPLING_CONSTANT (Cholesky-correlated "
+                       f"noise), SIN kernel, FP64, Ny = {POS_SLICES}, {steps} steps, measured every {every}",
+           "status": status, "initial_condition_ms": ic_ms, "cholesky_decompose_s": dec_s,
+           "cholesky_tflops_fp64": 4.0 * n ** 3 / 3.0 / dec_s / 1e12, "cholesky_bytes": 16.0 * n * n,
+           "step_ms": step_ms, "site_steps_per_s": n / (step_ms / 1e3),
+           "factor_stream_gbs": lbytes / (step_ms / 1e3) / 1e9,
+           "factor_stream_note": "lower triangle of L per step / whole-step time (the apply is ~96% of a step)",
+           "Qs_every_50": qs, "unitarity_drift": drift}
+    # the reference's own position path on a bounded sample (32^2), extrapolated by V^2 per step and V^3
+    # for the decomposition; 256^2 itself is out of reach on the CPU
+    r, why = run_reference_main(2, 0, n_side=POS_CPU_N, evolution="POSITION_EVOLUTION",
+                                coupling="NOISE_COUPLING_CONSTANT", with_wall=True)
+    if r is not None:
+        t_step, t_setup = r
+        scale = (POS_N / POS_CPU_N) ** 2
+        out["cpu_baseline"] = {"value": POS_CPU_N ** 2 / t_step, "unit": "site-steps/s", "cores": os.cpu_count(),
+                               "kind": "reference",
+                               "sample": f"main_optimized at {POS_CPU_N}^2, POSITION + NOISE, 2 steps; set-up "
+                                         f"(Cholesky) {t_setup:.2f} s",
+                               "extrapolated_256_step_s": t_step * scale ** 2,
+                               "extrapolated_256_decompose_s": t_setup * scale ** 3}
+    else:
+        out["cpu_baseline"] = {"value": None, "unit": "site-steps/s", "cores": 0, "kind": "reference", "sample": why}
+    return out
 
 
 def quantize_n(n: float) -> int:
@@ -395,6 +484,7 @@ def main_arm(args):
         line["serve"] = serve_leg(jw, local, args.serve_requests, 200.0, 2026)
         line["serve"]["vs_fp64_plain"] = line["serve"]["site_steps_per_s"] / plain
         line["uneven"] = uneven_leg(jw, local, 48)
+        line["position"] = position_leg(jw, local)
         # CPU baseline: the reference's own main on a bounded sample
         t, why = run_reference_main(2, 1)
         if t is not None:

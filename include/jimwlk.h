@@ -177,6 +177,16 @@ jw_status jw_average_and_symmetrize(jw_context* ctx, jw_field* corr);
 jw_status jw_average_and_symmetrize_noalloc(double* corr, int N, void* stream);
 /* gfield::reduce(sum, err, mpi) (field.h:1521-1536): sum += corr, err += corr^2. */
 jw_status jw_reduce(jw_context* ctx, const jw_field* corr, jw_field* sum, jw_field* err);
+/* No counterpart in the reference, which writes C(k) only (print).  The
+ * dipole of one symmetrised correlator corr (t = 1, after jw_trace and
+ * jw_average_and_symmetrize): S(x, y) = (N^2/3) sum_k corr(k) exp(+2 pi i
+ * k.(x, y)/N), i.e. (1/3N^2) sum_z tr V(z) V(z + (x, y))^dagger; its angular
+ * average over bins b = floor(|r| + 1/2) <= N/2 of minimum-image distances;
+ * and Q_s = sqrt(2)/r_s with S(r_s) = exp(-1/2), linear between the bins that
+ * bracket it (0 if none).  S_xy (N*N doubles, x-major) and the bins
+ * (nbins_cap >= N/2 + 1) are optional. */
+jw_status jw_dipole(jw_context* ctx, const jw_field* corr, double* S_xy, double* S_bins, double* r_bins, int* counts,
+                    int nbins_cap, int* nbins, double* Qs);
 /* print(measurement, sum, err, momenta, x, mpi, fileroot) (field.h:2521-2547):
  * appends to <fileroot>_<Nx>_<Ny>_mpi1_r0.dat. */
 jw_status jw_print(jw_context* ctx, int measurement, const jw_field* sum, const jw_field* err, double x,

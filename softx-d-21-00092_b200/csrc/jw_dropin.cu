@@ -246,6 +246,12 @@ __global__ void k_reduce(const double2* __restrict__ c, double2* __restrict__ su
     err[i] = cadd(err[i], sq);
 }
 
+// (N^2/3) corr: the dipole's Wiener-Khinchin prefactor, into a scratch plane.
+__global__ void k_dipole_scale(const double2* __restrict__ c, double2* __restrict__ out, long vol, double scale) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < vol) out[i] = cscale(c[i], scale);
+}
+
 __global__ void k_set_unit(double2* __restrict__ V, int N) {
     const long vol = (long)N * N;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -499,6 +505,22 @@ JW_EXPORT jw_status jw_reduce(jw_context* c, const jw_field* corr, jw_field* sum
     const int N = c->N;
     k_reduce<<<blocks_for((long)N * N), kThreads, 0, c->stream>>>(corr->d, sum->d, err->d, N);
     JW_CUDA(cudaGetLastError());
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_dipole(jw_context* c, const jw_field* corr, double* S_xy, double* S_bins, double* r_bins,
+                              int* counts, int nbins_cap, int* nbins, double* Qs) {
+    JW_CHECK(c && corr && corr->ctx == c && corr->t == 1);
+    const int N = c->N;
+    const long vol = (long)N * N;
+    if (S_bins && nbins_cap < N / 2 + 1) return JW_EINVAL;
+    k_dipole_scale<<<blocks_for(vol), kThreads, 0, c->stream>>>(corr->d, c->d_tmp, vol, (double)N * N / 3.0);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(fft2d_planes<double>(c->d_tmp, 1, N, 0, 1.0, c->tw, c->stream));
+    std::vector<double2> h(vol);
+    JW_CUDA(cudaMemcpyAsync(h.data(), c->d_tmp, sizeof(double2) * vol, cudaMemcpyDeviceToHost, c->stream));
+    JW_CUDA(cudaStreamSynchronize(c->stream));
+    dipole_bins(h.data(), N, S_xy, S_bins, r_bins, counts, nbins, Qs);
     return JW_OK;
 }
 

@@ -882,37 +882,11 @@ JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, in
     return JW_OK;
 }
 
-// Dipole in position space from an event's accumulated correlator (the mean
-// over its measurements): S(r) = (N^2/3) sum_k C(k) exp(+2 pi i k.r/N) (the
-// Wiener-Khinchin form of (1/3N^2) sum_x tr V(x) V^dagger(x+r)), then the
-// angular average over bins b = floor(|r| + 1/2), |r| the minimum-image length,
-// b <= N/2, and Q_s = sqrt(2)/r_s with S(r_s) = exp(-1/2) interpolated linearly
-// between the first pair of bins that brackets it (0 if none).
-JW_EXPORT jw_status jw_engine_dipole(jw_engine* e, int id, double* S_xy, double* S_bins, double* r_bins,
-                                     int* counts, int nbins_cap, int* nbins, double* Qs) {
-    JW_CHECK(e);
-    auto it = e->events.find(id);
-    if (it == e->events.end()) return JW_ENOTFOUND;
-    const Event& ev = it->second;
-    const int N = ev.N;
+namespace jw {
+void dipole_bins(const double2* h, int N, double* S_xy, double* S_bins, double* r_bins, int* counts, int* nbins,
+                 double* Qs) {
     const long vol = (long)N * N;
     const int nb = N / 2 + 1;
-    if (S_bins && nbins_cap < nb) return JW_EINVAL;
-    Group& g = *e->groups[N];
-    jw_status s = ensure_workspace(e, g, 1);
-    if (s) return s;
-    EventDev d{};
-    JW_CUDA(cudaMemcpyAsync(&d, g.d_ev + ev.slot, sizeof(EventDev), cudaMemcpyDeviceToHost, e->stream));
-    JW_CUDA(cudaStreamSynchronize(e->stream));
-    if (d.nmeas <= 0) return JW_EINVAL;
-    double2* plane = reinterpret_cast<double2*>(g.ws);
-    const double scale = (double)N * (double)N / 3.0 / d.nmeas;
-    k_dipole_prep<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ev.acc, plane, vol, scale);
-    JW_CUDA(cudaGetLastError());
-    JW_CUDA(fft2d_planes<double>(plane, 1, N, 0, 1.0, g.tw, e->stream));
-    std::vector<double2> h(vol);
-    JW_CUDA(cudaMemcpyAsync(h.data(), plane, sizeof(double2) * vol, cudaMemcpyDeviceToHost, e->stream));
-    JW_CUDA(cudaStreamSynchronize(e->stream));
     if (S_xy)
         for (long i = 0; i < vol; ++i) S_xy[i] = h[i].x;
     std::vector<double> sb(nb, 0.0), rb(nb, 0.0);
@@ -951,5 +925,40 @@ JW_EXPORT jw_status jw_engine_dipole(jw_engine* e, int id, double* S_xy, double*
             }
         *Qs = q;
     }
+}
+}  // namespace jw
+
+// Dipole in position space from an event's accumulated correlator (the mean
+// over its measurements): S(r) = (N^2/3) sum_k C(k) exp(+2 pi i k.r/N) (the
+// Wiener-Khinchin form of (1/3N^2) sum_x tr V(x) V^dagger(x+r)), then the
+// angular average over bins b = floor(|r| + 1/2), |r| the minimum-image length,
+// b <= N/2, and Q_s = sqrt(2)/r_s with S(r_s) = exp(-1/2) interpolated linearly
+// between the first pair of bins that brackets it (0 if none).
+JW_EXPORT jw_status jw_engine_dipole(jw_engine* e, int id, double* S_xy, double* S_bins, double* r_bins,
+                                     int* counts, int nbins_cap, int* nbins, double* Qs) {
+    JW_CHECK(e);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const Event& ev = it->second;
+    const int N = ev.N;
+    const long vol = (long)N * N;
+    const int nb = N / 2 + 1;
+    if (S_bins && nbins_cap < nb) return JW_EINVAL;
+    Group& g = *e->groups[N];
+    jw_status s = ensure_workspace(e, g, 1);
+    if (s) return s;
+    EventDev d{};
+    JW_CUDA(cudaMemcpyAsync(&d, g.d_ev + ev.slot, sizeof(EventDev), cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    if (d.nmeas <= 0) return JW_EINVAL;
+    double2* plane = reinterpret_cast<double2*>(g.ws);
+    const double scale = (double)N * (double)N / 3.0 / d.nmeas;
+    k_dipole_prep<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ev.acc, plane, vol, scale);
+    JW_CUDA(cudaGetLastError());
+    JW_CUDA(fft2d_planes<double>(plane, 1, N, 0, 1.0, g.tw, e->stream));
+    std::vector<double2> h(vol);
+    JW_CUDA(cudaMemcpyAsync(h.data(), plane, sizeof(double2) * vol, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    dipole_bins(h.data(), N, S_xy, S_bins, r_bins, counts, nbins, Qs);
     return JW_OK;
 }

@@ -64,11 +64,18 @@ struct jw_context {
     double2* d_pos_scratch = nullptr;  // 18 planes
     void* cublas = nullptr;         // cublasHandle_t (Cholesky decomposition)
     std::vector<jw_cholesky*> choleskies;  // live factors, released by jw_context_destroy
+    jw_field* pos_work[4] = {};     // xi_x, xi_y, A, B of jw_evolve_position (in `fields`)
 };
 
 namespace jw {
 // Frees what jw_position.cu attached to the context.
 void position_release(jw_context* c);
+// S(x, y) = h[x N + y].x (a plane already transformed to position space) ->
+// angular bins b = floor(|r| + 1/2) <= N/2 over minimum-image distances and
+// Q_s = sqrt(2)/r_s at S(r_s) = exp(-1/2), linear between the bracketing bins
+// (0 if none).  Every output pointer may be null.
+void dipole_bins(const double2* h, int N, double* S_xy, double* S_bins, double* r_bins, int* counts, int* nbins,
+                 double* Qs);
 }
 
 struct jw_field {

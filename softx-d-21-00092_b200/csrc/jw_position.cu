@@ -18,13 +18,14 @@
 // kernel factors each 128 x 128 diagonal block, and cuBLAS ZTRSM / ZSYRK (the
 // complex-symmetric, non-conjugating rank-k update) handle the panel and the
 // trailing matrix.  Applying L streams its lower triangle once per call
-// through a register-blocked FP64 kernel (k_chol_apply): each CTA owns 128
+// on the FP64 tensor cores (k_chol_apply, mma.sync m8n8k4): each CTA owns 128
 // rows and one 4096-column chunk, stages 128 x 16 tiles of L with cp.async,
-// and multiplies them with up to 18 real right-hand sides.  For the Langevin
-// noise the right-hand sides are the 16 unit normals of each site (the
-// Gell-Mann embedding is linear and is applied after L), so the kernel reads
-// 16 B of L per 32 FP64 FMAs and is bound by HBM.  Partial products of the
-// chunks are summed in a fixed order, so results are deterministic.
+// and multiplies them with 8, 16 or 24 real right-hand sides.  For the
+// Langevin noise the right-hand sides are the 16 unit normals of each site
+// (the Gell-Mann embedding is linear and is applied after L), so the kernel
+// does 32 FP64 FMAs per 16 B of L: HBM-bound when the tensor pipe runs above
+// about 70% of its peak.  Partial products of the chunks are summed in a
+// fixed order, so results are deterministic.
 #include <cublas_v2.h>
 
 #include <algorithm>
@@ -51,11 +52,11 @@ namespace {
 constexpr int kThreads = 256;
 inline unsigned blocks_for(long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
-// Cholesky apply tiling: 128 rows per CTA (one per thread), 16 columns per
-// staged tile, 4096 columns per chunk; at most 18 real right-hand sides.
-constexpr int kTR = 128, kKT = 16, kTC = 4096, kMaxR = 18;
-constexpr int kRowBytes = kKT * 16 + 16;  // padded shared row: conflict-free 16-byte loads across rows
-template <int R> constexpr int apply_stage_bytes() { return kTR * kRowBytes + kKT * R * 8; }
+// Cholesky apply tiling: 128 rows per CTA, 16 columns per staged tile, three
+// stages, 4096 columns per chunk; right-hand sides in multiples of 8 (at most 24).
+constexpr int kTR = 128, kKT = 16, kTC = 4096, kStages = 3, kMaxR = 24;
+template <int NT> constexpr int apply_x_row_bytes() { return NT * 64 + 32; }  // padded: conflict-free B fragments
+template <int NT> constexpr int apply_stage_bytes() { return kTR * kKT * 16 + kKT * apply_x_row_bytes<NT>(); }
 constexpr int kDiagBlock = 128;
 
 __device__ __forceinline__ void cpa16(void* smem, const void* gmem) {
@@ -197,71 +198,102 @@ __global__ void __launch_bounds__(1024) k_chol_diag(double2* __restrict__ a, lon
     }
 }
 
+// One FP64 tensor-core product D(8x8) += A(8x4) B(4x8) (mma.sync m8n8k4):
+// lane (g = lane/4, q = lane%4) supplies A[g][q] and B[q][g] and holds
+// D[g][2q], D[g][2q+1].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 // P[chunk][row][c] = sum over the chunk's columns k of L(row, k) X(k, c):
-// complex L times R real right-hand sides.  One CTA per (row strip, chunk)
-// unit, grid-strided; one output row per thread; tiles of 128 rows x 16
-// columns of L double-buffered in shared memory with cp.async.
-template <int R>
-__global__ void __launch_bounds__(kTR) k_chol_apply(const double2* __restrict__ L, const double* __restrict__ X,
+// complex L times RP = 8 NT real right-hand sides on the FP64 tensor cores.
+// One CTA (4 warps) per (row strip, chunk) unit, grid-strided.  A stage holds
+// 128 rows x 16 complex columns of L (32 KB, each row's 16-byte chunks XOR-
+// swizzled by bit 2 on odd rows so that the fragment loads of two rows hit
+// disjoint banks) and 16 rows of X (padded rows); three stages in flight with
+// cp.async.  Warp w owns complex rows 32w..32w+31 as four groups of eight;
+// each group is two m-tiles, the real and the imaginary parts of L, which
+// share one 16-byte fragment load and the B fragments, so that each thread
+// ends with matching real and imaginary parts of its outputs.
+template <int NT>
+__global__ void __launch_bounds__(kTR, 2) k_chol_apply(const double2* __restrict__ L, const double* __restrict__ X,
                                                     double2* __restrict__ P, const int2* __restrict__ units,
                                                     int n_units, long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int SB = apply_stage_bytes<R>();
-    const int tid = threadIdx.x;
+    constexpr int RP = 8 * NT;
+    constexpr int XS = apply_x_row_bytes<NT>();
+    constexpr int SB = apply_stage_bytes<NT>();
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int g = lane >> 2, q = lane & 3;
     for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
-        const int2 w = units[u];
-        const long row0 = (long)w.x * kTR;
-        const long k0 = (long)w.y * kTC;
+        const int2 wk = units[u];
+        const long row0 = (long)wk.x * kTR;
+        const long k0 = (long)wk.y * kTC;
         const long kend = min(k0 + kTC, min(n, row0 + kTR));  // columns past the strip's last row are zero
         const int nt = (int)((kend - k0) / kKT);               // n, kTR and kTC are multiples of kKT
-        auto stage = [&](int t, int s) {
-            unsigned char* sl = smem + s * SB;
-            double* sx = reinterpret_cast<double*>(sl + kTR * kRowBytes);
+        auto stage = [&](int t) {
+            unsigned char* sl = smem + (t % kStages) * SB;
+            unsigned char* sx = sl + kTR * kKT * 16;
             const long kb = k0 + (long)t * kKT;
 #pragma unroll
             for (int j = 0; j < kKT; ++j) {
                 const int c = tid + j * kTR;
                 const int r = c / kKT, e = c % kKT;
-                if (row0 + r < n) cpa16(sl + r * kRowBytes + e * 16, L + (row0 + r) * n + kb + e);
+                if (row0 + r < n) cpa16(sl + r * (kKT * 16) + ((e ^ ((r & 1) << 2)) << 4), L + (row0 + r) * n + kb + e);
             }
-            for (int c = tid; c < kKT * R / 2; c += kTR) cpa16(sx + 2 * c, X + kb * R + 2 * c);
-            cpa_commit();
+            for (int c = tid; c < kKT * RP / 2; c += kTR) {
+                const int r = c / (RP / 2), e = c % (RP / 2);
+                cpa16(sx + r * XS + e * 16, X + (kb + r) * RP + 2 * e);
+            }
         };
-        double ar[R], ai[R];
+        double dr[4][NT][2], di[4][NT][2];
 #pragma unroll
-        for (int c = 0; c < R; ++c) ar[c] = ai[c] = 0.0;
-        stage(0, 0);
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int m = 0; m < NT; ++m) dr[j][m][0] = dr[j][m][1] = di[j][m][0] = di[j][m][1] = 0.0;
+        stage(0);
+        cpa_commit();
+        if (nt > 1) stage(1);
+        cpa_commit();
         for (int t = 0; t < nt; ++t) {
-            if (t + 1 < nt) {
-                stage(t + 1, (t + 1) & 1);
-                cpa_wait<1>();
-            } else {
-                cpa_wait<0>();
-            }
+            cpa_wait<1>();  // stage t has landed (one later group may be in flight)
             __syncthreads();
-            const unsigned char* sl = smem + (t & 1) * SB;
-            const double* sx = reinterpret_cast<const double*>(sl + kTR * kRowBytes);
-            const double2* lr = reinterpret_cast<const double2*>(sl + tid * kRowBytes);
+            if (t + 2 < nt) stage(t + 2);  // into the buffer computed at t - 1
+            cpa_commit();
+            const unsigned char* sl = smem + (t % kStages) * SB;
+            const unsigned char* sx = sl + kTR * kKT * 16;
 #pragma unroll
-            for (int kk = 0; kk < kKT; ++kk) {
-                const double2 l = lr[kk];
-                const double2* xr = reinterpret_cast<const double2*>(sx + kk * R);
+            for (int ks = 0; ks < kKT / 4; ++ks) {
+                const int k = 4 * ks + q;
+                double b[NT];
 #pragma unroll
-                for (int c = 0; c < R / 2; ++c) {
-                    const double2 x = xr[c];
-                    ar[2 * c] = fma(l.x, x.x, ar[2 * c]);
-                    ai[2 * c] = fma(l.y, x.x, ai[2 * c]);
-                    ar[2 * c + 1] = fma(l.x, x.y, ar[2 * c + 1]);
-                    ai[2 * c + 1] = fma(l.y, x.y, ai[2 * c + 1]);
+                for (int m = 0; m < NT; ++m) b[m] = *reinterpret_cast<const double*>(sx + k * XS + (8 * m + g) * 8);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int a = 32 * w + 8 * j + g;
+                    const double2 l = *reinterpret_cast<const double2*>(sl + a * (kKT * 16) + ((k ^ ((a & 1) << 2)) << 4));
+#pragma unroll
+                    for (int m = 0; m < NT; ++m) {
+                        dmma(dr[j][m][0], dr[j][m][1], l.x, b[m]);
+                        dmma(di[j][m][0], di[j][m][1], l.y, b[m]);
+                    }
                 }
             }
-            __syncthreads();
         }
-        const long row = row0 + tid;
-        if (row < n) {
-            double2* p = P + ((long)w.y * n + row) * R;
+        __syncthreads();  // every warp is done with the buffers before the next unit refills them
 #pragma unroll
-            for (int c = 0; c < R; ++c) p[c] = make_double2(ar[c], ai[c]);
+        for (int j = 0; j < 4; ++j) {
+            const long row = row0 + 32 * w + 8 * j + g;
+            if (row < n) {
+                double2* p = P + ((long)wk.y * n + row) * RP;
+#pragma unroll
+                for (int m = 0; m < NT; ++m) {
+                    p[8 * m + 2 * q] = make_double2(dr[j][m][0], di[j][m][0]);
+                    p[8 * m + 2 * q + 1] = make_double2(dr[j][m][1], di[j][m][1]);
+                }
+            }
         }
     }
 }
@@ -272,21 +304,23 @@ __device__ __forceinline__ int chunks_of_row(long row, long n) {
     return (int)(last / kTC) + 1;
 }
 
-// Real right-hand sides of a field: X(i, k) = Re xi_k(i), X(i, t + k) = Im xi_k(i).
-__global__ void k_chol_gather_field(const double2* __restrict__ xi, double* __restrict__ X, long n, int t) {
+// Real right-hand sides of a field, RP per site: X(i, k) = Re xi_k(i),
+// X(i, t + k) = Im xi_k(i), zero beyond 2t.
+__global__ void k_chol_gather_field(const double2* __restrict__ xi, double* __restrict__ X, long n, int t, int RP) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    for (int c = 2 * t; c < RP; ++c) X[i * RP + c] = 0.0;
     for (int k = 0; k < t; ++k) {
         const double2 v = xi[k * n + i];
-        X[i * 2 * t + k] = v.x;
-        X[i * 2 * t + t + k] = v.y;
+        X[i * RP + k] = v.x;
+        X[i * RP + t + k] = v.y;
     }
 }
 
 // xi_k = Y_k + i Y_{t+k}, Y = sum of the chunk partials in chunk order.
-template <int R>
+template <int t, int RP>
 __global__ void k_chol_finish_field(const double2* __restrict__ P, double2* __restrict__ xi, long n) {
-    constexpr int t = R / 2;
+    constexpr int R = 2 * t;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 y[R];
@@ -294,7 +328,7 @@ __global__ void k_chol_finish_field(const double2* __restrict__ P, double2* __re
     for (int c = 0; c < R; ++c) y[c] = make_double2(0.0, 0.0);
     const int nc = chunks_of_row(i, n);
     for (int ch = 0; ch < nc; ++ch) {
-        const double2* p = P + ((long)ch * n + i) * R;
+        const double2* p = P + ((long)ch * n + i) * RP;
 #pragma unroll
         for (int c = 0; c < R; ++c) y[c] = cadd(y[c], p[c]);
     }
@@ -401,12 +435,12 @@ int apply_grid(const void* fn, int smem, int units) {
     return std::max(1, std::min(units, sms * std::max(per, 1)));
 }
 
-template <int R>
+template <int NT>
 jw_status launch_apply(const jw_cholesky* L, cudaStream_t s) {
-    constexpr int smem = 2 * apply_stage_bytes<R>();
-    JW_CUDA(cudaFuncSetAttribute(k_chol_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int grid = apply_grid((const void*)k_chol_apply<R>, smem, L->n_units);
-    k_chol_apply<R><<<grid, kTR, smem, s>>>(L->d_L, L->d_X, L->d_P, L->d_units, L->n_units, L->n);
+    constexpr int smem = kStages * apply_stage_bytes<NT>();
+    JW_CUDA(cudaFuncSetAttribute(k_chol_apply<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int grid = apply_grid((const void*)k_chol_apply<NT>, smem, L->n_units);
+    k_chol_apply<NT><<<grid, kTR, smem, s>>>(L->d_L, L->d_X, L->d_P, L->d_units, L->n_units, L->n);
     JW_CUDA(cudaGetLastError());
     return JW_OK;
 }
@@ -424,7 +458,7 @@ jw_status cholesky_noise(jw_context* c, const jw_cholesky* L, jw_field* xx, jw_f
     const long n = L->n;
     k_chol_noise_X<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_X, n, c->cfg.seed, step);
     JW_CUDA(cudaGetLastError());
-    jw_status s = launch_apply<16>(L, c->stream);
+    jw_status s = launch_apply<2>(L, c->stream);
     if (s) return s;
     k_chol_finish_noise<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xx->d, xy->d, n);
     JW_CUDA(cudaGetLastError());
@@ -593,17 +627,18 @@ JW_EXPORT jw_status jw_cholesky_get(const jw_cholesky* L, double* host) {
 JW_EXPORT jw_status jw_multiply_by_cholesky(jw_context* c, jw_field* xi, const jw_cholesky* L) {
     JW_CHECK(c && xi && xi->ctx == c && L && L->ctx == c);
     const long n = L->n;
-    k_chol_gather_field<<<blocks_for(n), kThreads, 0, c->stream>>>(xi->d, L->d_X, n, xi->t);
+    const int RP = xi->t == 9 ? 24 : 8;
+    k_chol_gather_field<<<blocks_for(n), kThreads, 0, c->stream>>>(xi->d, L->d_X, n, xi->t, RP);
     JW_CUDA(cudaGetLastError());
     jw_status s;
     if (xi->t == 9) {
-        s = launch_apply<18>(L, c->stream);
+        s = launch_apply<3>(L, c->stream);
         if (s) return s;
-        k_chol_finish_field<18><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
+        k_chol_finish_field<9, 24><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
     } else {
-        s = launch_apply<2>(L, c->stream);
+        s = launch_apply<1>(L, c->stream);
         if (s) return s;
-        k_chol_finish_field<2><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
+        k_chol_finish_field<1, 8><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
     }
     JW_CUDA(cudaGetLastError());
     return JW_OK;
@@ -622,16 +657,18 @@ JW_EXPORT jw_status jw_reduce_hatta(jw_context* c, const jw_field* corr, jw_fiel
 JW_EXPORT jw_status jw_evolve_position(jw_context* c, jw_field* V, uint64_t step0, int n, int rr,
                                        const jw_cholesky* L) {
     JW_CHECK(c && V && V->ctx == c && V->t == 9 && n >= 0 && rr >= 0);
+    for (jw_field* w : c->pos_work) JW_CHECK(V != w);
     const jw_config& cfg = c->cfg;
     const int coupling = cfg.CouplingChoice;
     JW_CHECK(valid_coupling(coupling));
     const bool correlated = coupling == JW_NOISE_COUPLING_CONSTANT;
     if (correlated) JW_CHECK(L && L->ctx == c);
-    jw_field *xx = nullptr, *xy = nullptr, *A = nullptr, *B = nullptr;
+    // work fields kept in the context: repeated calls allocate nothing
     jw_status s = JW_OK;
-    jw_field** all[4] = {&xx, &xy, &A, &B};
-    for (auto p : all)
-        if (!s) s = jw_field_create(c, 9, p);
+    for (int k = 0; k < 4 && !s; ++k)
+        if (!c->pos_work[k]) s = jw_field_create(c, 9, &c->pos_work[k]);
+    if (s) return s;
+    jw_field *xx = c->pos_work[0], *xy = c->pos_work[1], *A = c->pos_work[2], *B = c->pos_work[3];
     for (int k = 0; k < n && s == JW_OK; ++k) {
         const uint64_t step = step0 + (uint64_t)k;
         if (correlated) s = cholesky_noise(c, L, xx, xy, step);
@@ -639,6 +676,5 @@ JW_EXPORT jw_status jw_evolve_position(jw_context* c, jw_field* V, uint64_t step
         if (!s) s = jw_prepare_A_and_B(c, A, B, xx, xy, V, rr, coupling, cfg.KernelChoice);
         if (!s) s = jw_update_uf(c, V, B, A, cfg.step);
     }
-    for (auto p : all) jw_field_destroy(*p);
     return s;
 }

@@ -120,6 +120,8 @@ def _load():
         "jw_cholesky_destroy": ([_vp], ctypes.c_int),
         "jw_cholesky_get": ([_vp, _dp], ctypes.c_int),
         "jw_multiply_by_cholesky": ([_vp, _vp, _vp], ctypes.c_int),
+        "jw_dipole": ([_vp, _vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                       ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
         "jw_reduce_hatta": ([_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "jw_evolve_position": ([_vp, _vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
         "jw_engine_create": ([ctypes.POINTER(jw_engine_options), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
@@ -276,6 +278,20 @@ class Context:
 
     def multiply_by_cholesky(self, xi, L: "Cholesky"):
         _ck(_lib.jw_multiply_by_cholesky(self._h, xi._h, L._h), "jw_multiply_by_cholesky")
+
+    def dipole(self, corr, with_xy: bool = False):
+        """S(r) bins, r bins, counts, Q_s (and S(x, y)) of a symmetrised correlator."""
+        N = self.N
+        nb = N // 2 + 1
+        Sb, rb = np.zeros(nb), np.zeros(nb)
+        cb = np.zeros(nb, np.int32)
+        nbins, qs = ctypes.c_int(), ctypes.c_double()
+        Sxy = np.zeros((N, N)) if with_xy else None
+        _ck(_lib.jw_dipole(self._h, corr._h, Sxy.ctypes.data_as(_dp) if with_xy else None, Sb.ctypes.data_as(_dp),
+                           rb.ctypes.data_as(_dp), cb.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), nb,
+                           ctypes.byref(nbins), ctypes.byref(qs)), "jw_dipole")
+        out = (Sb, rb, cb, qs.value)
+        return out + (Sxy,) if with_xy else out
 
     def reduce_hatta(self, corr, sum_, err, xr: int, yr: int):
         _ck(_lib.jw_reduce_hatta(self._h, corr._h, sum_._h, err._h, xr, yr), "jw_reduce_hatta")

@@ -92,6 +92,18 @@ def test_evolve_position_matches_reference(jw, gold, name):
     assert rel(c.get()[..., 0], fx["corr"]) <= 1e-12
 
 
+def test_dipole_matches_oracle(jw, gold, oracle):
+    """jw_dipole (S(r) bins, Q_s) of the measured correlator against the oracle's definition."""
+    fx = gold("position_sqrt_sin_N16")
+    ctx, cp, kn = fixture_ctx(jw, fx)
+    c = ctx.field(1).set(fx["corr"][..., None])
+    Sb, rb, cb, qs, Sxy = ctx.dipole(c, with_xy=True)
+    So, Sbo, rbo, cbo, qso = oracle.dipole(fx["corr"])
+    assert np.abs(Sxy - So).max() <= 1e-13 and np.abs(Sb - Sbo).max() <= 1e-13
+    assert np.array_equal(cb, cbo) and np.abs(rb - rbo).max() <= 1e-13
+    assert abs(qs - qso) <= 1e-12 * max(abs(qso), 1.0)
+
+
 @pytest.mark.parametrize("N,kernel,rr", [(16, 1, 5), (16, 0, 2), (32, 1, 8)])
 def test_hatta_matches_oracle(jw, oracle, N, kernel, rr):
     """HATTA coupling: the SQRT formula at min(r2, rr) (the reference's own
