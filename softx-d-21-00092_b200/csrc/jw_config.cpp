@@ -58,6 +58,8 @@ JW_EXPORT jw_status jw_config_read(jw_config* c, const char* path) {
     if (!std::strcmp(coupling, "SQRT_COUPLING_CONSTANT")) c->CouplingChoice = JW_SQRT_COUPLING_CONSTANT;
     if (!std::strcmp(coupling, "NOISE_COUPLING_CONSTANT")) c->CouplingChoice = JW_NOISE_COUPLING_CONSTANT;
     if (!std::strcmp(coupling, "HATTA_COUPLING_CONSTANT")) c->CouplingChoice = JW_HATTA_COUPLING_CONSTANT;
+    // this library's fixed coupling (no reference spelling exists)
+    if (!std::strcmp(coupling, "FIXED_COUPLING_CONSTANT")) c->CouplingChoice = JW_FIXED_COUPLING_CONSTANT;
     if (!std::strcmp(kernel, "LINEAR_KERNEL")) c->KernelChoice = JW_LINEAR_KERNEL;
     if (!std::strcmp(kernel, "SIN_KERNEL")) c->KernelChoice = JW_SIN_KERNEL;
     return ok ? JW_OK : JW_EINVAL;

@@ -1,0 +1,209 @@
+// jimwlk_main.cpp -- main_optimized.cpp on one GPU: the same configuration
+// file, the same sequence (statistics -> MV initial condition -> [Hatta loop
+// over distances] -> Langevin steps -> measurements) and the same output
+// table (output_optimized_<Nx>_<Ny>_mpi1_r0.dat), with the reference's
+// progress lines.
+//
+//   jimwlk_main <px> <py> <config> [--N n] [--device d] [--seed s] [--call-for-call]
+//
+// <px> <py> are the reference's MPI grid arguments (ignored: one GPU holds the
+// lattice).  --N sets the lattice side (the reference fixes it at compile
+// time, 64 by default).  By default each Langevin step is one fused library
+// call (jw_evolve_momentum / jw_evolve_position); --call-for-call runs the
+// body of main_optimized.cpp:232-304 literally, one adapter call per
+// reference call.  Both draw the same noise: Langevin step n of the run uses
+// stream index n, MV slice n stream index n, in the reference's order.
+// Exit status 0 on success (the reference returns 1).
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "jimwlk.hpp"
+
+using namespace jimwlk;
+
+namespace {
+
+struct timer {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double seconds() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+int usage() {
+    std::fprintf(stderr,
+                 "usage: jimwlk_main <px> <py> <config> [--N n] [--device d] [--seed s] [--call-for-call]\n");
+    return 2;
+}
+
+}  // namespace
+
+int main(int argc, char* argv[]) {
+    if (argc < 4) return usage();
+    int N = 64, device_id = 0;
+    bool call_for_call = false, seed_given = false;
+    uint64_t seed = 1;
+    for (int i = 4; i < argc; ++i) {
+        if (!std::strcmp(argv[i], "--N") && i + 1 < argc) N = std::atoi(argv[++i]);
+        else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) device_id = std::atoi(argv[++i]);
+        else if (!std::strcmp(argv[i], "--seed") && i + 1 < argc) {
+            seed = std::strtoull(argv[++i], nullptr, 10);
+            seed_given = true;
+        } else if (!std::strcmp(argv[i], "--call-for-call")) call_for_call = true;
+        else return usage();
+    }
+    try {
+        std::printf("INITIALIZATION\n");
+        config cnfg(N);
+        cnfg.read_config_from_file(argv[3]);
+        if (seed_given) cnfg.seed = seed;
+        if (cnfg.langevin_steps < 1 || cnfg.measurements < 1 || cnfg.langevin_steps / cnfg.measurements < 1) {
+            std::fprintf(stderr, "jimwlk_main: need 1 <= measurements <= langevin_steps\n");
+            return 2;
+        }
+        mpi_class mpi(argc, argv);
+        mpi.mpi_init(&cnfg);
+        mpi.mpi_exchange_grid();
+        momenta momtable(&cnfg, &mpi);
+        momtable.set();
+        positions postable(&cnfg, &mpi);
+        postable.set();
+        device dev(cnfg, device_id);
+        MV_class MVmodel(1.0, cnfg.mu / cnfg.Nx, cnfg.elementaryWilsonLines);
+        fftw2D fourier2(dev);
+        fourier2.init2D();
+
+        std::printf("ALLOCATION\n");
+        lfield<double, 9> f(dev), uf(dev), xi_local_x(dev), xi_local_y(dev), A_local(dev), B_local(dev), uftmp(dev);
+        lfield<double, 9> uxiulocal_x(dev), uxiulocal_y(dev), uf_copy(dev);
+        lfield<double, 1> zero(dev), corr(dev);
+        // the reference allocates one accumulator per step (main_optimized.cpp:131-132);
+        // only the first `measurements` are ever used
+        std::vector<std::unique_ptr<lfield<double, 1>>> sum, err;
+        for (int i = 0; i < cnfg.measurements; ++i) {
+            sum.emplace_back(new lfield<double, 1>(zero));
+            err.emplace_back(new lfield<double, 1>(zero));
+        }
+
+        const Evolution evo = cnfg.EvolutionChoice;
+        const Coupling cp = cnfg.CouplingChoice;
+        // fixed coupling: NOISE kernel factor 1 with plain noise
+        const Coupling kernel_cp = cp == FIXED_COUPLING_CONSTANT ? NOISE_COUPLING_CONSTANT : cp;
+        std::unique_ptr<gmatrix<double>> cholesky;
+        if (evo == POSITION_EVOLUTION && cp == NOISE_COUPLING_CONSTANT) {  // :145-157
+            corr.setCorrelationsForCouplingConstant(&momtable);
+            fourier2.execute2D(&corr, 0);
+            cholesky.reset(new gmatrix<double>(dev));
+            cholesky->decompose(&corr);
+            std::printf("cholesky decomposition finished\n");
+        }
+        const int Nx = cnfg.Nx, Ny = cnfg.Ny;
+        const int every = cnfg.langevin_steps / cnfg.measurements;
+
+        for (int stat = 0; stat < cnfg.stat; ++stat) {
+            timer ts;
+            std::printf("Gatherting stat sample no. %i\n", stat);
+            timer ti;
+            uf.setToUnit();
+            for (int i = 0; i < MVmodel.Ny_parameter; ++i) {  // :180-191
+                f.setMVModel(&MVmodel);
+                fourier2.execute2D(&f, 1);
+                f.solvePoisson(cnfg.mass * MVmodel.g_parameter * MVmodel.g_parameter * MVmodel.mu_parameter,
+                               MVmodel.g_parameter, &momtable);
+                fourier2.execute2D(&f, 0);
+                uf *= f;
+            }
+            dev.sync();
+            std::printf("Initial condition time: %g\n", ti.seconds());
+
+            const int upper_bound_x = cp == HATTA_COUPLING_CONSTANT ? Nx : 1;  // :200-216
+            for (int ix = 0; ix < upper_bound_x; ++ix) {
+                const int lower_bound_y = cp == HATTA_COUPLING_CONSTANT ? ix - 1 : 0;
+                const int upper_bound_y = cp == HATTA_COUPLING_CONSTANT ? ix + 2 : 1;
+                for (int iy = lower_bound_y; iy < upper_bound_y; ++iy) {
+                    if (iy < 0 || iy >= Ny) continue;
+                    double dix = ix, diy = iy;
+                    if (dix >= Nx / 2) dix -= Nx;
+                    if (dix < -Nx / 2) dix += Nx;
+                    if (diy >= Ny / 2) diy -= Ny;
+                    if (diy < -Ny / 2) diy += Ny;
+                    const int rr_hatta = (int)(dix * dix + diy * diy);
+                    uftmp = uf;
+                    for (int langevin = 0; langevin < cnfg.langevin_steps; ++langevin) {
+                        timer te;
+                        std::printf("Performing evolution step no. %i\n", langevin);
+                        if (!call_for_call) {
+                            const uint64_t step_index = dev.noise_step++;
+                            if (evo == MOMENTUM_EVOLUTION)
+                                check(jw_evolve_momentum(dev.ctx, uftmp.f, step_index, 1), "jw_evolve_momentum");
+                            else
+                                check(jw_evolve_position(dev.ctx, uftmp.f, step_index, 1, rr_hatta,
+                                                         cholesky ? cholesky->L : nullptr),
+                                      "jw_evolve_position");
+                        } else {
+                            // :243-304, one adapter call per reference call
+                            if (evo == MOMENTUM_EVOLUTION && cp == NOISE_COUPLING_CONSTANT)
+                                generate_gaussian_with_noise_coupling_constant(&xi_local_x, &xi_local_y, &momtable,
+                                                                               &mpi, &cnfg);
+                            else
+                                generate_gaussian(&xi_local_x, &xi_local_y, &mpi, &cnfg);
+                            if (evo == MOMENTUM_EVOLUTION) {
+                                fourier2.execute2D(&xi_local_x, 1);
+                                fourier2.execute2D(&xi_local_y, 1);
+                                prepare_A_local(&A_local, &xi_local_x, &xi_local_y, &momtable, &mpi, kernel_cp,
+                                                cnfg.KernelChoice);
+                                fourier2.execute2D(&A_local, 0);
+                                fourier2.execute2D(&xi_local_x, 0);
+                                fourier2.execute2D(&xi_local_y, 0);
+                                uxiulocal(&uxiulocal_x, &uxiulocal_y, &uftmp, &xi_local_x, &xi_local_y);
+                                fourier2.execute2D(&uxiulocal_x, 1);
+                                fourier2.execute2D(&uxiulocal_y, 1);
+                                prepare_A_local(&B_local, &uxiulocal_x, &uxiulocal_y, &momtable, &mpi, kernel_cp,
+                                                cnfg.KernelChoice);
+                                fourier2.execute2D(&B_local, 0);
+                            } else {
+                                // the gathers are identities on one GPU
+                                if (cp == NOISE_COUPLING_CONSTANT) {
+                                    xi_local_x.multiplyByCholesky(cholesky.get());
+                                    xi_local_y.multiplyByCholesky(cholesky.get());
+                                }
+                                prepare_A_and_B(&xi_local_x, &xi_local_y, &A_local, &B_local, &uftmp, &postable,
+                                                rr_hatta, cp, cnfg.KernelChoice);
+                            }
+                            update_uf(&uftmp, &B_local, &A_local, cnfg.step);
+                        }
+                        dev.sync();
+                        std::printf("Evolution time: %g\n", te.seconds());
+
+                        if (langevin % every == 0) {  // :314-336
+                            const int time = (int)(langevin * cnfg.measurements / cnfg.langevin_steps);
+                            uf_copy = uftmp;
+                            fourier2.execute2D(&uf_copy, 1);
+                            uf_copy.trace(&corr);
+                            corr.average_and_symmetrize();
+                            if (cp == HATTA_COUPLING_CONSTANT)
+                                corr.reduce_hatta(sum[time].get(), err[time].get(), &mpi, ix, iy);
+                            else
+                                corr.reduce(sum[time].get(), err[time].get(), &mpi);
+                        }
+                    }
+                }
+            }
+            dev.sync();
+            std::printf("Statistics time: %g\n", ts.seconds());
+        }
+        const std::string file_name = "output_optimized";
+        for (int i = cnfg.measurements - 1; i < cnfg.measurements; ++i)
+            print(i, sum[i].get(), err[i].get(), &momtable, 1.0 / 3.0 / cnfg.stat, &mpi, file_name);
+        dev.sync();
+    } catch (const error& e) {
+        std::fprintf(stderr, "jimwlk_main: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -109,6 +109,55 @@ def fixture_position(o: Oracle, N: int, seed: int, coupling: str, kernel: str, s
     return out
 
 
+DRIVER_RUNS = {
+    # name: (N, seed, config fields)
+    "driver_sqrt_sin_N16": (16, 41, dict(stat=2, mu=8.0, mass=0.04, wilson_lines=6, langevin_steps=12,
+                                         measurements=4, step=0.0004, evolution="MOMENTUM_EVOLUTION",
+                                         coupling="SQRT_COUPLING_CONSTANT", kernel="SIN_KERNEL")),
+    "driver_noise_sin_N16": (16, 42, dict(stat=1, mu=8.0, mass=0.04, wilson_lines=6, langevin_steps=8,
+                                          measurements=2, step=0.0004, evolution="MOMENTUM_EVOLUTION",
+                                          coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL")),
+    "driver_sqrt_linear_N16": (16, 43, dict(stat=1, mu=8.0, mass=0.04, wilson_lines=6, langevin_steps=6,
+                                            measurements=3, step=0.0004, evolution="MOMENTUM_EVOLUTION",
+                                            coupling="SQRT_COUPLING_CONSTANT", kernel="LINEAR_KERNEL")),
+    "driver_position_cholesky_N16": (16, 44, dict(stat=1, mu=8.0, mass=0.04, wilson_lines=6, langevin_steps=4,
+                                                  measurements=2, step=0.0004, evolution="POSITION_EVOLUTION",
+                                                  coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL")),
+}
+
+
+def fixture_driver(o: Oracle, N: int, seed: int, cfg: dict) -> dict:
+    """The reference's main_optimized (oracle/_ref/main_optimized_inject_<N>,
+    serial, noise injected) on a config, fed the library's noise stream in the
+    reference's draw order: per statistics sample the MV slices (stream index
+    stat * Ny + i), then the Langevin steps (running index).  Returns the
+    config text and the output table it writes."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle", "_ref", f"main_optimized_inject_{N}")
+    text = config_text(file_name="output", **cfg)
+    ny, steps, stats = cfg["wilson_lines"], cfg["langevin_steps"], cfg["stat"]
+    chunks, g = [], 0
+    for s in range(stats):
+        chunks += [o.mv_normals(seed, s * ny + i, N).ravel() for i in range(ny)]
+        for _ in range(steps):
+            chunks.append(o.langevin_normals(seed, g, N).ravel())
+            g += 1
+    with tempfile.TemporaryDirectory() as d:
+        zf = os.path.join(d, "noise.bin")
+        np.concatenate(chunks).astype(np.float64).tofile(zf)
+        cf = os.path.join(d, "config")
+        with open(cf, "w") as fh:
+            fh.write(text)
+        r = subprocess.run([exe, "1", "1", cf], cwd=d, capture_output=True, text=True,
+                           env=dict(os.environ, JW_INJECT_FILE=zf), timeout=600)
+        if r.returncode not in (0, 1):
+            raise SystemExit(f"reference main failed ({r.returncode}): {r.stderr[-500:]}")
+        with open(os.path.join(d, f"output_optimized_{N}_{N}_mpi1_r0.dat")) as fh:
+            dat = fh.read()
+    return {"N": N, "seed": seed, "config": text, "dat": dat}
+
+
 def check_oracle_position(o: Oracle, fx: dict) -> float:
     N, seed = int(fx["N"]), int(fx["seed"])
     cp = 1 if str(fx["coupling"]) == "NOISE_COUPLING_CONSTANT" else 0
@@ -174,6 +223,10 @@ def main() -> None:
         print(f"{name}: oracle vs reference max deviation {d:.3e}")
         if d > 1e-12:
             raise SystemExit(f"oracle disagrees with the reference on {name}")
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fx.items()})
+    for name, (N, seed, cfg) in DRIVER_RUNS.items():
+        fx = fixture_driver(o, N, seed, cfg)
+        print(f"{name}: {len(fx['dat'].splitlines())} output lines")
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fx.items()})
 
 

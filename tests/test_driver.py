@@ -1,0 +1,107 @@
+"""The main_optimized-equivalent driver (softx-d-21-00092_b200/host/): its noise
+order and output table against the reference's own main_optimized run on the
+same configuration and noise (tests/golden/driver_*.npz, written by
+oracle/_ref/main_optimized_inject_16).  The CPU test replays the driver's
+sequence on the oracle and must reproduce the reference's table text exactly;
+the GPU test runs the driver binary."""
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from jwref import f32
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(REPO, "softx-d-21-00092_b200", "bin", "jimwlk_main")
+NAMES = ["driver_sqrt_sin_N16", "driver_noise_sin_N16", "driver_sqrt_linear_N16", "driver_position_cholesky_N16"]
+COUPLING = {"SQRT_COUPLING_CONSTANT": 0, "NOISE_COUPLING_CONSTANT": 1, "HATTA_COUPLING_CONSTANT": 2}
+
+
+def parse_config(text: str) -> dict:
+    kv = dict(line.split(" = ", 1) for line in text.strip().splitlines())
+    return {"stat": int(kv["stat"]), "mu": f32(float(kv["mu"])), "mass": f32(float(kv["mass"])),
+            "ny": int(kv["elementaryWilsonLines"]), "steps": int(kv["langevin_steps"]),
+            "meas": int(kv["measurements"]), "step": f32(float(kv["step"])), "evolution": kv["EvolutionChoice"],
+            "coupling": COUPLING[kv["CouplingChoice"]], "kernel": 1 if kv["KernelChoice"] == "SIN_KERNEL" else 0}
+
+
+def table(N: int, measurement: int, s: np.ndarray, e: np.ndarray, x: float) -> str:
+    """print (field.h:2521-2547) for |kx - ky| <= 4."""
+    out = []
+    for xx in range(N):
+        for yy in range(N):
+            if abs(xx - yy) <= 4:
+                ph2 = 4.0 * math.pow(math.sin(math.pi * xx / N), 2.0) + 4.0 * math.pow(math.sin(math.pi * yy / N), 2.0)
+                out.append("%i %i %i \t %f %e %e\n" % (measurement, xx, yy, math.sqrt(ph2), x * ph2 * s[xx, yy].real,
+                                                        x * ph2 * e[xx, yy].real))
+    return "".join(out)
+
+
+def parse_dat(text: str) -> np.ndarray:
+    return np.array([[float(v) for v in line.split()] for line in text.strip().splitlines()])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_replays_reference_main(oracle, gold, name):
+    fx = gold(name)
+    N, seed = int(fx["N"]), int(fx["seed"])
+    c = parse_config(str(fx["config"]))
+    L = oracle.cholesky(oracle.correlations(N)) if (c["evolution"] == "POSITION_EVOLUTION" and
+                                                     c["coupling"] == 1) else None
+    every = c["steps"] // c["meas"]
+    sums = [np.zeros((N, N), np.complex128) for _ in range(c["meas"])]
+    errs = [np.zeros((N, N), np.complex128) for _ in range(c["meas"])]
+    g = 1.0
+    mu = c["mu"] / N
+    step_index = 0
+    for s in range(c["stat"]):
+        V = np.zeros((N, N, 9), np.complex128)
+        V[..., 0] = V[..., 4] = V[..., 8] = 1.0
+        for i in range(c["ny"]):
+            f = oracle.set_mv_model(oracle.mv_normals(seed, s * c["ny"] + i, N), g * mu / math.sqrt(c["ny"]))
+            f = oracle.execute2D(f, 1)
+            f = oracle.solve_poisson(f, c["mass"] * g * g * mu, g)
+            f = oracle.execute2D(f, 0)
+            V = oracle.mul_exp(V, f)
+        for lv in range(c["steps"]):
+            if c["evolution"] == "MOMENTUM_EVOLUTION":
+                V = oracle.evolve_momentum(V, 1, step_index, c["step"], c["coupling"], c["kernel"], seed)
+            else:
+                V = oracle.evolve_position(V, 1, step_index, c["step"], c["coupling"], c["kernel"], 0, L, seed)
+            step_index += 1
+            if lv % every == 0:
+                t = lv * c["meas"] // c["steps"]
+                _, sums[t], errs[t] = oracle.measure(V, sums[t], errs[t])
+    m = c["meas"] - 1
+    assert table(N, m, sums[m], errs[m], 1.0 / 3.0 / c["stat"]) == str(fx["dat"])
+
+
+def test_driver_usage_without_arguments():
+    if not os.path.exists(DRIVER):
+        pytest.skip("driver not built (make -C softx-d-21-00092_b200)")
+    r = subprocess.run([DRIVER], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["fused", "call-for-call"])
+@pytest.mark.parametrize("name", NAMES)
+def test_driver_matches_reference_main(gold, tmp_path, name, mode):
+    fx = gold(name)
+    N, seed = int(fx["N"]), int(fx["seed"])
+    cfg = tmp_path / "config"
+    cfg.write_text(str(fx["config"]))
+    args = [DRIVER, "1", "1", str(cfg), "--N", str(N), "--seed", str(seed)]
+    if mode == "call-for-call":
+        args.append("--call-for-call")
+    r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "Evolution time:" in r.stdout and "Initial condition time:" in r.stdout
+    got = parse_dat((tmp_path / f"output_optimized_{N}_{N}_mpi1_r0.dat").read_text())
+    want = parse_dat(str(fx["dat"]))
+    assert got.shape == want.shape
+    assert np.array_equal(got[:, :3], want[:, :3])
+    # the table prints 7 significant digits
+    assert np.allclose(got[:, 3:], want[:, 3:], rtol=2e-6, atol=1e-12)
