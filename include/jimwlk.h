@@ -201,7 +201,7 @@ jw_status jw_initial_condition(jw_context* ctx, jw_field* V);
 jw_status jw_evolve_momentum(jw_context* ctx, jw_field* V, uint64_t step0, int n);
 
 /* ------------------------------------------------------------------ position-space evolution */
-/* The loop of main_optimized.cpp:290-301 over every site, i.e.
+/* The loop of main_optimized.cpp:287-300 over every site, i.e.
  * prepare_A_and_B_local(x, y, x_global, y_global, xi_x, xi_y, A, B, uf,
  * positions, rr, Coupling, Kernel) (field.h:2368-2519) for all (x, y):
  *   A(x) = sum_y [k_x(x-y) xi_x(y) + k_y(x-y) xi_y(y)]

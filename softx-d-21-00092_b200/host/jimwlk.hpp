@@ -18,7 +18,7 @@
 //    the reference's generator, but reproducible;
 //  - errors throw jimwlk::error (the reference returns 1 and goes on);
 //  - prepare_A_and_B replaces the per-site loop of prepare_A_and_B_local
-//    (main_optimized.cpp:290-301) by one call for all sites.
+//    (main_optimized.cpp:287-300) by one call for all sites.
 #pragma once
 
 #include <complex>
@@ -311,7 +311,7 @@ int update_uf(lfield<T, 9>* uf, lfield<T, 9>* B, lfield<T, 9>* A, double step) {
     check(jw_update_uf(uf->dev->ctx, uf->f, B->f, A->f, step), "jw_update_uf");
     return 1;
 }
-// prepare_A_and_B_local for every site (main_optimized.cpp:290-301).
+// prepare_A_and_B_local for every site (main_optimized.cpp:287-300).
 template <class T>
 int prepare_A_and_B(gfield<T, 9>* xi_x, gfield<T, 9>* xi_y, lfield<T, 9>* A, lfield<T, 9>* B, gfield<T, 9>* uf,
                     positions*, int rr, Coupling p, Kernel k) {
