@@ -311,25 +311,32 @@ cudaError_t launch_mv_slice(jw_engine* e, Group& g, const int* d_slots, int nb, 
 }
 
 template <int N>
-cudaError_t launch_measure(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
+cudaError_t launch_measure_kernels(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
     const long vol = (long)N * N;
     double2* M = reinterpret_cast<double2*>(ws);
     double* corr = reinterpret_cast<double*>(M + (size_t)9 * vol * nb);
-    constexpr int RT = row_threads<N>();
-    constexpr int C = p2_cols<double, N>();
-    constexpr int ROWS = meas_rows_per_cta<N>();
-    const size_t sm1 = sizeof(double2) * padded_len(ROWS * N);
-    const size_t sm2 = sizeof(double2) * padded_len(N * C);
+    constexpr int RW = meas_rows16<N>();
+    const size_t sm1 = meas_rows16_smem<N>();
+    const size_t sm2 = meas_cols_smem<N>();
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_meas_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
         cudaFuncSetAttribute(k_meas_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
         configured = true;
     }
-    (void)RT;
-    k_meas_rows<N><<<dim3((unsigned)((9L * N + ROWS - 1) / ROWS), nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, M,
-                                                                                           g.tw.d64);
-    k_meas_cols<N><<<dim3(N / C, nb), C * (N / 8), sm2, e->stream>>>(d_slots, M, corr, g.tw.d64);
+    k_meas_rows<N><<<dim3((unsigned)((9L * N + RW - 1) / RW), nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, M,
+                                                                                       g.tw.d64);
+    k_meas_cols<N><<<dim3(N / mx_cols<N>(), nb), meas_cols_threads<N>(), sm2, e->stream>>>(d_slots, M, corr,
+                                                                                          g.tw.d64);
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_measure(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
+    const long vol = (long)N * N;
+    double* corr = reinterpret_cast<double*>(reinterpret_cast<double2*>(ws) + (size_t)9 * vol * nb);
+    cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws);
+    if (err != cudaSuccess) return err;
     k_meas_reduce<N><<<dim3((unsigned)((vol + 255) / 256), nb), 256, 0, e->stream>>>(g.d_ev, d_slots, corr);
     return cudaGetLastError();
 }
@@ -338,21 +345,9 @@ template <int N>
 cudaError_t launch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws,
                                    double* ens) {
     const long vol = (long)N * N;
-    double2* M = reinterpret_cast<double2*>(ws);
-    double* corr = reinterpret_cast<double*>(M + (size_t)9 * vol * nb);
-    constexpr int C = p2_cols<double, N>();
-    constexpr int ROWS = meas_rows_per_cta<N>();
-    const size_t sm1 = sizeof(double2) * padded_len(ROWS * N);
-    const size_t sm2 = sizeof(double2) * padded_len(N * C);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_meas_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-        cudaFuncSetAttribute(k_meas_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-        configured = true;
-    }
-    k_meas_rows<N><<<dim3((unsigned)((9L * N + ROWS - 1) / ROWS), nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, M,
-                                                                                           g.tw.d64);
-    k_meas_cols<N><<<dim3(N / C, nb), C * (N / 8), sm2, e->stream>>>(d_slots, M, corr, g.tw.d64);
+    double* corr = reinterpret_cast<double*>(reinterpret_cast<double2*>(ws) + (size_t)9 * vol * nb);
+    cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws);
+    if (err != cudaSuccess) return err;
     k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, nb, ens);
     return cudaGetLastError();
 }

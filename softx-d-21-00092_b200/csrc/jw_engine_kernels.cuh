@@ -442,71 +442,6 @@ __global__ void __launch_bounds__(row_threads<N>()) k_mv_pass3(EventDev* __restr
     if (fl) atomicOr(flags, fl);
 }
 
-// ------------------------------------------------------------------ measurement (FP64)
-// rows of V's 9 planes, forward, out of place into M: the 9*N rows of an
-// event are contiguous, ROWS of them per CTA
-template <int N> constexpr int meas_rows_per_cta() { return (2048 / N) > 0 ? (2048 / N) : 1; }
-
-template <int N>
-__global__ void __launch_bounds__(256) k_meas_rows(const EventDev* __restrict__ ev, const int* __restrict__ slots,
-                                                   double2* __restrict__ M, const double2* __restrict__ tw) {
-    constexpr int ROWS = meas_rows_per_cta<N>();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* sm = reinterpret_cast<double2*>(smem_raw);
-    const int b = blockIdx.y;
-    const EventDev& e = ev[slots[b]];
-    const long vol = (long)N * N;
-    const long row0 = (long)blockIdx.x * ROWS;
-    const int nr = (int)min((long)ROWS, 9L * N - row0);
-    const double2* in = e.V + row0 * N;
-    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) sm[pad(i)] = in[i];
-    __syncthreads();
-    constexpr int TPS = N / 8;
-    const int r = threadIdx.x / TPS;
-    fft_smem<double, N>(sm, RowIdx{r * N}, threadIdx.x % TPS, r < nr, -1.0, tw);
-    double2* out = M + (long)b * 9 * vol + row0 * N;
-    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) out[i] = sm[pad(i)];
-}
-
-// columns: sum over the 9 components of |X|^2 / N^6  (trace, field.h:1375-1432)
-template <int N>
-__global__ void __launch_bounds__(p2_cols<double, N>() * (N / 8)) k_meas_cols(const int* __restrict__ slots,
-                                                                               const double2* __restrict__ M,
-                                                                               double* __restrict__ corr,
-                                                                               const double2* __restrict__ tw) {
-    constexpr int C = p2_cols<double, N>();
-    constexpr int PER = 8;  // tile elements per thread: N*C / (C*N/8)
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* t0 = reinterpret_cast<double2*>(smem_raw);
-    const int c0 = blockIdx.x * C, b = blockIdx.y;
-    const long vol = (long)N * N;
-    double acc[PER];
-#pragma unroll
-    for (int q = 0; q < PER; ++q) acc[q] = 0.0;
-    const int c = threadIdx.x % C, t = threadIdx.x / C;
-    for (int comp = 0; comp < 9; ++comp) {
-        const double2* in = M + ((long)b * 9 + comp) * vol + c0;
-        for (int i = threadIdx.x; i < N * C; i += blockDim.x) t0[pad(i)] = in[(long)(i / C) * N + (i % C)];
-        __syncthreads();
-        fft_smem<double, N>(t0, ColIdx<C>{c}, t, true, -1.0, tw);
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const double2 v = t0[pad(threadIdx.x + q * blockDim.x)];
-            acc[q] += v.x * v.x + v.y * v.y;
-        }
-        __syncthreads();
-    }
-    const double n2 = (double)N * (double)N;
-    const double inv = 1.0 / (n2 * n2 * n2);
-    double* out = corr + (long)b * vol + c0;
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int i = threadIdx.x + q * blockDim.x;
-        out[(long)(i / C) * N + (i % C)] = acc[q] * inv;
-    }
-    (void)slots;
-}
-
 // average_and_symmetrize (field.h:1460-1492) + reduce (field.h:1521-1536) with
 // compensated (Neumaier) FP64 accumulation of sum and sum of squares.
 __device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {

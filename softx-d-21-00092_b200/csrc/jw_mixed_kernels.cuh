@@ -294,4 +294,97 @@ __global__ void __launch_bounds__(row_threads<N>(), 2) k_mix_pass3(EventDev* __r
     if (x == 0 && threadIdx.x == 0) e.step += 1;
 }
 
+// ------------------------------------------------------------------ measurement (FP64)
+// C(k) = sum over the 9 entries of |FFT(V_ij)(k)|^2 / N^6 (lfield::trace,
+// field.h:1375-1432, after the unitary forward transform), with the 16-byte
+// element core on double2: a row pass writes the 9 row-transformed planes to
+// the workspace M, a column pass transforms them and accumulates the trace.
+
+// rows: 4096-element tiles (8 rows at N = 512) of the event's 9N contiguous
+// rows, staged with cp.async
+template <int N> constexpr int meas_rows16() { return N >= 4096 ? 1 : 4096 / N; }
+template <int N> constexpr size_t meas_rows16_smem() { return 16 * (size_t)padded_len16(meas_rows16<N>() * N); }
+
+template <int N>
+__global__ void __launch_bounds__(256) k_meas_rows(const EventDev* __restrict__ ev, const int* __restrict__ slots,
+                                                   double2* __restrict__ M, const double2* __restrict__ tw) {
+    constexpr int RW = meas_rows16<N>();
+    constexpr int TPS = N / 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int b = blockIdx.y;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const long row0 = (long)blockIdx.x * RW;
+    const int nr = (int)min((long)RW, 9L * N - row0);
+    const double2* in = e.V + row0 * N;
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) cp_async<16>(&sm[pad16(i)], &in[i]);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const int spr = blockDim.x / TPS, r = threadIdx.x / TPS;
+    for (int p0 = 0; p0 < nr; p0 += spr) {
+        const int pr = p0 + r;
+        fft16<double, N>(sm, RowIdx16{pr * N}, threadIdx.x % TPS, r < spr && pr < nr, -1.0, tw);
+    }
+    double2* out = M + (long)b * 9 * vol + row0 * N;
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) out[i] = sm[pad16(i)];
+}
+
+// columns: tiles of C columns, the 9 components double-buffered with cp.async
+template <int N> constexpr int meas_cols_threads() { return mx_cols<N>() * (N / 8); }
+template <int N> constexpr size_t meas_cols_smem() { return 2 * 16 * (size_t)mx_tile_len<N>(); }
+
+template <int N>
+__global__ void __launch_bounds__(meas_cols_threads<N>()) k_meas_cols(const int* __restrict__ slots,
+                                                                       const double2* __restrict__ M,
+                                                                       double* __restrict__ corr,
+                                                                       const double2* __restrict__ tw) {
+    constexpr int C = mx_cols<N>();
+    constexpr int TH = meas_cols_threads<N>();
+    constexpr int PER = N * C / TH;  // = 8
+    constexpr int RSTEP = TH / C;    // = N / 8
+    constexpr int TL = mx_tile_len<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* tile[2] = {reinterpret_cast<double2*>(smem_raw), reinterpret_cast<double2*>(smem_raw) + TL};
+    const int c0 = blockIdx.x * C, b = blockIdx.y;
+    const long vol = (long)N * N;
+    const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
+    const ColIdx16P<C> cidx{cc};
+    auto stage = [&](int comp, double2* t) {
+        const double2* in = M + ((long)b * 9 + comp) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) cp_async<16>(&t[cidx(r0 + q * RSTEP)], in + (long)q * RSTEP * N);
+        cp_async_commit();
+    };
+    double acc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) acc[q] = 0.0;
+    stage(0, tile[0]);
+#pragma unroll 1
+    for (int comp = 0; comp < 9; ++comp) {
+        if (comp + 1 < 9) {
+            stage(comp + 1, tile[(comp + 1) & 1]);  // the buffer read at comp - 1
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        double2* t = tile[comp & 1];
+        fft16<double, N>(t, cidx, r0, true, -1.0, tw);
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const double2 v = t[cidx(r0 + q * RSTEP)];
+            acc[q] += v.x * v.x + v.y * v.y;
+        }
+        __syncthreads();
+    }
+    const double n2 = (double)N * (double)N;
+    const double inv = 1.0 / (n2 * n2 * n2);
+    double* out = corr + (long)b * vol + c0 + cc;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
+    (void)slots;
+}
+
 }  // namespace jw
