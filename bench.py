@@ -60,6 +60,37 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def init_dist(backend: str = "nccl", timeout_s: int = 120) -> None:
+    """One process per GPU (torchrun sets RANK/WORLD_SIZE/MASTER_*); a short
+    timeout ends ranks that wait for a rank that died."""
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+
+def max_over_ranks(x: float) -> float:
+    """The slowest rank's time (every rank calls it at the same point)."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier() -> None:
+    import torch.distributed as dist
+    if dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+
+
+def event_seeds(rank: int, events: int) -> list:
+    """Each rank evolves its own events (weak scaling): seeds never repeat across ranks."""
+    return [1_000_003 * (rank + 1) + i for i in range(events)]
+
+
 def measured_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -367,28 +398,14 @@ def main_arm(args):
 
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier_max(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        init_dist("nccl")
+    barrier_max = max_over_ranks
 
     events = args.events
     n_side = args.n
     eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch)
     ids = [eng.add_event(n_side, ny_slices=NY_SLICES, mu=0.5 * n_side, mass=MASS, step=STEP,
-                         coupling=jw.FIXED_COUPLING_CONSTANT, seed=1_000_003 * (rank + 1) + i) for i in range(events)]
+                         coupling=jw.FIXED_COUPLING_CONSTANT, seed=sd) for sd in event_seeds(rank, events)]
     eng.init_mv(ids)
     eng.step(ids, args.warmup)
     if eng.sync() != jw.OK:
