@@ -267,9 +267,17 @@ typedef struct jw_event_desc {
     double mu;            /* config mu (mu_MV = mu/N, g = 1) */
     double mass;          /* config mass (Poisson mass = mass * mu_MV) */
     double step;          /* Langevin step (config step) */
-    int coupling;         /* JW_SQRT_COUPLING_CONSTANT or JW_NOISE_COUPLING_CONSTANT */
-    int kernel;           /* JW_SIN_KERNEL or JW_LINEAR_KERNEL */
+    int coupling;         /* JW_SQRT_, JW_NOISE_, JW_FIXED_ (and, in position space, JW_HATTA_) COUPLING_CONSTANT */
+    int kernel;           /* JW_SIN_KERNEL (the engine's only kernel) */
     uint64_t seed;        /* noise stream key of this event */
+    /* 0: momentum-space steps (main_optimized.cpp:249-269).  Nonzero:
+     * position-space steps (:271-302, jw_prepare_A_and_B) with plain noise;
+     * coupling SQRT, FIXED (factor 1) or HATTA at min(r^2, rr).  NOISE in
+     * position space needs the Cholesky factor and is JW_EUNSUPPORTED here
+     * (use jw_evolve_position). */
+    int position_space;
+    int rr;               /* Hatta distance squared (position space, HATTA) */
+    uint64_t step0;       /* noise index of the event's first step (default 0) */
 } jw_event_desc;
 
 typedef struct jw_engine jw_engine;
@@ -297,8 +305,14 @@ jw_status jw_engine_measure(jw_engine* e, const int* ids, int n);
 jw_status jw_engine_get_correlator(jw_engine* e, int event_id, double* sum, double* err, int* nmeas);
 /* Reset an event's accumulators. */
 jw_status jw_engine_reset_correlator(jw_engine* e, int event_id);
-/* Steps taken so far by an event (its next noise index). */
+/* An event's next noise index: step0 plus the steps taken so far. */
 jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
+/* For each event ids[i], its accumulated symmetrised correlator at one
+ * momentum (xr[i], yr[i]): sum[i] (real part) and err[i] (sum of squares),
+ * i.e. what gfield::reduce_hatta (field.h:1538-1564) adds for a Hatta branch
+ * measured once since its last reset. */
+jw_status jw_engine_correlator_at(jw_engine* e, const int* ids, int n, const int* xr, const int* yr, double* sum,
+                                  double* err);
 /* Dipole in position space from the event's accumulated correlator (mean over
  * its measurements; the reference stops at C(k), field.h:2521-2547):
  * S(r) = (N^2/3) sum_k C(k) exp(+2 pi i k.r/N), optionally all N*N values

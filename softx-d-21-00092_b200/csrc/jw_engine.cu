@@ -41,7 +41,12 @@ struct Event {
     jw_event_desc desc{};
     double2* V = nullptr;
     double* acc = nullptr;
+    double* k64 = nullptr;   // the event's own kernel tables (position space)
+    float* k32 = nullptr;
 };
+
+// Per-event table bytes of a position-space event: [2][N*N] in FP64 and FP32.
+size_t position_table_bytes(int N) { return (sizeof(double) + sizeof(float)) * 2 * (size_t)N * N; }
 
 template <typename T> size_t step_ws_bytes(int N) { return sizeof(C2<T>) * 24 * (size_t)N * N; }
 size_t meas_ws_bytes(int N) { return (sizeof(double2) * 9 + sizeof(double)) * (size_t)N * N; }
@@ -78,6 +83,31 @@ void kernel_table(int N, int coupling, std::vector<double>& t) {
             t[i] = -2.0 * M_PI * std::sqrt(cc) * std::sin(2.0 * M_PI * ix / (1.0 * N)) / ph2 * inv;
             t[vol + i] = -2.0 * M_PI * std::sqrt(cc) * std::sin(2.0 * M_PI * iy / (1.0 * N)) / ph2 * inv;
         }
+}
+
+// prepare_A_and_B_local's kernel (field.h:2368-2519) as a multiplier in
+// momentum space: the raw DFT of the real position kernel k_i(d)
+// (positions.h:105-150); for the SIN kernel k_i is odd in d_i and even in the
+// other coordinate, so the DFT is imaginary.  Stored like kernel_table:
+// imag(DFT k_i) / N^2.
+__global__ void k_position_table(const double2* __restrict__ dft, double* __restrict__ k64, float* __restrict__ k32,
+                                 long n2, double inv) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n2) return;
+    const double v = dft[i].y * inv;
+    k64[i] = v;
+    k32[i] = (float)v;
+}
+
+// One accumulator site of an event: acc[site] and the plane stride.
+struct AccSite {
+    const double* p;
+    long vol;
+};
+__global__ void k_gather_acc(const AccSite* __restrict__ a, int n, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int q = 0; q < 4; ++q) out[4 * i + q] = a[i].p[q * a[i].vol];
 }
 
 // generate_gaussian_with_noise_coupling_constant's factor at the momentum
@@ -535,7 +565,8 @@ JW_EXPORT void* jw_engine_stream(jw_engine* e) { return e ? (void*)e->stream : n
 JW_EXPORT size_t jw_engine_event_bytes(const jw_engine* e, const jw_event_desc* d) {
     if (!e || !d || !supported_n(d->N)) return 0;
     const size_t vol = (size_t)d->N * d->N;
-    return vol * (sizeof(double2) * 9 + sizeof(double) * 4) + ws_per_event(e, d->N);
+    return vol * (sizeof(double2) * 9 + sizeof(double) * 4) + ws_per_event(e, d->N) +
+           (d->position_space ? position_table_bytes(d->N) : 0);
 }
 
 JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, int* event_id) {
@@ -543,13 +574,20 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     *event_id = -1;
     if (!engine_supported(e->opt.precision, d->N)) return JW_EUNSUPPORTED;
     if (d->kernel != JW_SIN_KERNEL) return JW_EUNSUPPORTED;
-    if (d->coupling != JW_SQRT_COUPLING_CONSTANT && d->coupling != JW_NOISE_COUPLING_CONSTANT &&
-        d->coupling != JW_FIXED_COUPLING_CONSTANT)
+    if (d->position_space) {
+        if (d->coupling != JW_SQRT_COUPLING_CONSTANT && d->coupling != JW_HATTA_COUPLING_CONSTANT &&
+            d->coupling != JW_FIXED_COUPLING_CONSTANT)
+            return JW_EUNSUPPORTED;
+        JW_CHECK(d->rr >= 0);
+    } else if (d->coupling != JW_SQRT_COUPLING_CONSTANT && d->coupling != JW_NOISE_COUPLING_CONSTANT &&
+               d->coupling != JW_FIXED_COUPLING_CONSTANT) {
         return JW_EUNSUPPORTED;
+    }
     JW_CHECK(d->ny_slices >= 0 && d->step >= 0.0 && std::isfinite(d->mu) && std::isfinite(d->mass) &&
              std::isfinite(d->step));
     const size_t vol = (size_t)d->N * d->N;
-    const size_t own = vol * (sizeof(double2) * 9 + sizeof(double) * 4);
+    const size_t own = vol * (sizeof(double2) * 9 + sizeof(double) * 4) +
+                       (d->position_space ? position_table_bytes(d->N) : 0);
     if (e->bytes_in_use + own + ws_per_event(e, d->N) > e->budget) return JW_ENOMEM;
     Group* g = nullptr;
     jw_status s = group_get(e, d->N, &g);
@@ -574,6 +612,45 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
         cudaFree(ev.V);
         return JW_ENOMEM;
     }
+    if (d->position_space) {
+        // k_i(d) on the host, its DFT on the device in FP64 (the staging buffer
+        // holds the two planes), imag / N^2 into the event's tables
+        double2* tmp = nullptr;
+        if (cudaMalloc(&ev.k64, sizeof(double) * 2 * vol) != cudaSuccess ||
+            cudaMalloc(&ev.k32, sizeof(float) * 2 * vol) != cudaSuccess ||
+            cudaMalloc(&tmp, sizeof(double2) * 2 * vol) != cudaSuccess) {
+            cudaFree(ev.V);
+            cudaFree(ev.acc);
+            if (ev.k64) cudaFree(ev.k64);
+            if (ev.k32) cudaFree(ev.k32);
+            if (tmp) cudaFree(tmp);
+            return JW_ENOMEM;
+        }
+        std::vector<double2> h(2 * vol);
+        for (int x = 0; x < d->N; ++x)
+            for (int y = 0; y < d->N; ++y) {
+                double kx, ky;
+                position_kernel_host(x, y, d->N, d->rr, d->coupling, d->kernel, &kx, &ky);
+                h[(size_t)x * d->N + y] = make_double2(kx, 0.0);
+                h[vol + (size_t)x * d->N + y] = make_double2(ky, 0.0);
+            }
+        cudaError_t ce = cudaMemcpyAsync(tmp, h.data(), sizeof(double2) * 2 * vol, cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess) ce = fft2d_planes<double>(tmp, 2, d->N, 1, 1.0, g->tw, e->stream);
+        if (ce == cudaSuccess) {
+            k_position_table<<<(unsigned)((2 * vol + 255) / 256), 256, 0, e->stream>>>(
+                tmp, ev.k64, ev.k32, (long)(2 * vol), 1.0 / ((double)d->N * d->N));
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+        cudaFree(tmp);
+        if (ce != cudaSuccess) {
+            cudaFree(ev.V);
+            cudaFree(ev.acc);
+            cudaFree(ev.k64);
+            cudaFree(ev.k32);
+            return JW_ECUDA;
+        }
+    }
     e->bytes_in_use += own;
     k_set_unit_planes<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ev.V, (long)vol);
     JW_CUDA(cudaMemsetAsync(ev.acc, 0, sizeof(double) * 4 * vol, e->stream));
@@ -581,12 +658,14 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     h.V = ev.V;
     h.acc = ev.acc;
     const int cp = d->coupling;
-    h.k64 = g->k64[cp];
-    h.k32 = g->k32[cp];
-    h.nf64 = cp == JW_NOISE_COUPLING_CONSTANT ? g->nf64 : nullptr;
-    h.nf32 = cp == JW_NOISE_COUPLING_CONSTANT ? g->nf32 : nullptr;
+    h.k64 = d->position_space ? ev.k64 : g->k64[cp];
+    h.k32 = d->position_space ? ev.k32 : g->k32[cp];
+    // the site-indexed noise factor belongs to momentum-space NOISE coupling only
+    const bool nf = !d->position_space && cp == JW_NOISE_COUPLING_CONSTANT;
+    h.nf64 = nf ? g->nf64 : nullptr;
+    h.nf32 = nf ? g->nf32 : nullptr;
     h.seed = d->seed;
-    h.step = 0;
+    h.step = d->step0;
     h.sqrt_eps = std::sqrt(d->step);
     const double gg = 1.0, mu = d->mu / d->N;
     h.mv_sigma = d->ny_slices > 0 ? gg * mu / std::sqrt((double)d->ny_slices) : 0.0;
@@ -607,6 +686,8 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
         g->owner[slot] = -1;
         cudaFree(ev.V);
         cudaFree(ev.acc);
+        if (ev.k64) cudaFree(ev.k64);
+        if (ev.k32) cudaFree(ev.k32);
         e->bytes_in_use -= own;
         return s;
     }
@@ -625,8 +706,11 @@ JW_EXPORT jw_status jw_engine_remove_event(jw_engine* e, int id) {
     g.owner[ev.slot] = -1;
     cudaFree(ev.V);
     cudaFree(ev.acc);
+    if (ev.k64) cudaFree(ev.k64);
+    if (ev.k32) cudaFree(ev.k32);
     const size_t vol = (size_t)ev.N * ev.N;
-    e->bytes_in_use -= vol * (sizeof(double2) * 9 + sizeof(double) * 4);
+    e->bytes_in_use -= vol * (sizeof(double2) * 9 + sizeof(double) * 4) +
+                       (ev.desc.position_space ? position_table_bytes(ev.N) : 0);
     e->events.erase(it);
     return JW_OK;
 }
@@ -787,6 +871,42 @@ JW_EXPORT jw_status jw_engine_reset_correlator(jw_engine* e, int id) {
     JW_CUDA(cudaMemcpyAsync(&e->groups[ev.N]->d_ev[ev.slot].nmeas, &zero, sizeof(int), cudaMemcpyHostToDevice,
                             e->stream));
     JW_CUDA(cudaStreamSynchronize(e->stream));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_correlator_at(jw_engine* e, const int* ids, int n, const int* xr, const int* yr,
+                                            double* sum, double* err) {
+    JW_CHECK(e && ids && xr && yr && n >= 0 && (sum || err));
+    for (int i = 0; i < n; ++i) {
+        auto it = e->events.find(ids[i]);
+        if (it == e->events.end()) return JW_ENOTFOUND;
+        JW_CHECK(xr[i] >= 0 && xr[i] < it->second.N && yr[i] >= 0 && yr[i] < it->second.N);
+    }
+    if (n == 0) return JW_OK;
+    // one gather on the device: per event the address of acc[site] and the
+    // plane stride go up, four doubles per event (sum, compensation, err,
+    // compensation) come back in one copy
+    const size_t up = sizeof(AccSite) * n, down = sizeof(double) * 4 * n;
+    jw_status st = ensure_stage(e, up + down);
+    if (st) return st;
+    AccSite* hs = reinterpret_cast<AccSite*>(e->h_pinned);
+    for (int i = 0; i < n; ++i) {
+        const Event& ev = e->events[ids[i]];
+        const long vol = (long)ev.N * ev.N;
+        hs[i] = AccSite{ev.acc + (long)xr[i] * ev.N + yr[i], vol};
+    }
+    unsigned char* ds = reinterpret_cast<unsigned char*>(e->d_stage);
+    JW_CUDA(cudaMemcpyAsync(ds, hs, up, cudaMemcpyHostToDevice, e->stream));
+    double* dout = reinterpret_cast<double*>(ds + up);
+    k_gather_acc<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(reinterpret_cast<const AccSite*>(ds), n, dout);
+    JW_CUDA(cudaGetLastError());
+    std::vector<double> h(4 * (size_t)n);
+    JW_CUDA(cudaMemcpyAsync(h.data(), dout, down, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    for (int i = 0; i < n; ++i) {
+        if (sum) sum[i] = h[4 * (size_t)i] + h[4 * (size_t)i + 1];
+        if (err) err[i] = h[4 * (size_t)i + 2] + h[4 * (size_t)i + 3];
+    }
     return JW_OK;
 }
 

@@ -70,6 +70,9 @@ struct jw_context {
 namespace jw {
 // Frees what jw_position.cu attached to the context.
 void position_release(jw_context* c);
+// The position kernel k_x, k_y at distance (dxi, dyi) (positions.h:105-150,
+// field.h:2402-2470), host FP64 with the reference's expressions.
+void position_kernel_host(int dxi, int dyi, int N, int rr, int coupling, int kernel, double* kx, double* ky);
 // S(x, y) = h[x N + y].x (a plane already transformed to position space) ->
 // angular bins b = floor(|r| + 1/2) <= N/2 over minimum-image distances and
 // Q_s = sqrt(2)/r_s at S(r_s) = exp(-1/2), linear between the bracketing bins

@@ -67,10 +67,12 @@ __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_gro
 template <int K>
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
 
+}  // namespace
+
 // ---- position kernel (positions.h:105-150, field.h:2402-2462), host FP64
 // with the reference's own expressions so that the tabulated values are the
 // reference's bit for bit.
-void position_kernel_host(int dxi, int dyi, int N, int rr, int coupling, int kernel, double* kx, double* ky) {
+void jw::position_kernel_host(int dxi, int dyi, int N, int rr, int coupling, int kernel, double* kx, double* ky) {
     double dx, dy, rrr;
     if (kernel == JW_SIN_KERNEL) {
         dx = 0.5 * N * std::sin(2.0 * M_PI * dxi / (1.0 * N)) / M_PI;
@@ -102,6 +104,8 @@ void position_kernel_host(int dxi, int dyi, int N, int rr, int coupling, int ker
         *ky = sc * dy / rrr;
     }
 }
+
+namespace {
 
 // out_k = K_x X_k + K_y Y_k for the 9 components (k-space product of the convolution).
 __global__ void k_pos_combine(double2* __restrict__ out, const double2* __restrict__ X, const double2* __restrict__ Y,

@@ -201,8 +201,15 @@ void worker_loop(jw_server* s) {
             for (auto it = s->queue.begin(); it != s->queue.end();) {
                 if (s->opt.max_active > 0 && (int)(s->active.size() + admitted.size()) >= s->opt.max_active) break;
                 Request* r = &s->reqs[*it];
-                jw_event_desc d{r->d.N, r->d.ny_slices, r->d.mu, r->d.mass, r->d.step, r->d.coupling, r->d.kernel,
-                                r->d.seed};
+                jw_event_desc d{};
+                d.N = r->d.N;
+                d.ny_slices = r->d.ny_slices;
+                d.mu = r->d.mu;
+                d.mass = r->d.mass;
+                d.step = r->d.step;
+                d.coupling = r->d.coupling;
+                d.kernel = r->d.kernel;
+                d.seed = r->d.seed;
                 int eid = -1;
                 const jw_status st = s->be->add(d, &eid);
                 if (st == JW_OK) {

@@ -48,7 +48,8 @@ class jw_engine_options(ctypes.Structure):
 class jw_event_desc(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("ny_slices", ctypes.c_int), ("mu", ctypes.c_double), ("mass", ctypes.c_double),
                 ("step", ctypes.c_double), ("coupling", ctypes.c_int), ("kernel", ctypes.c_int),
-                ("seed", ctypes.c_uint64)]
+                ("seed", ctypes.c_uint64), ("position_space", ctypes.c_int), ("rr", ctypes.c_int),
+                ("step0", ctypes.c_uint64)]
 
 
 class jw_server_options(ctypes.Structure):
@@ -138,6 +139,8 @@ def _load():
         "jw_engine_measure": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
         "jw_engine_get_correlator": ([_vp, ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "jw_engine_reset_correlator": ([_vp, ctypes.c_int], ctypes.c_int),
+        "jw_engine_correlator_at": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), _dp, _dp], ctypes.c_int),
         "jw_engine_event_steps": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
         "jw_server_create": ([ctypes.POINTER(jw_server_options), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
         "jw_server_destroy": ([_vp], ctypes.c_int),
@@ -413,8 +416,9 @@ class Engine:
 
     def add_event(self, N: int, ny_slices: int = 50, mu: float | None = None, mass: float = 0.04,
                   step: float = 0.0004, coupling: int = FIXED_COUPLING_CONSTANT, kernel: int = SIN_KERNEL,
-                  seed: int = 1) -> int:
-        d = jw_event_desc(N, ny_slices, 0.5 * N if mu is None else mu, mass, step, coupling, kernel, seed)
+                  seed: int = 1, position_space: bool = False, rr: int = 0, step0: int = 0) -> int:
+        d = jw_event_desc(N, ny_slices, 0.5 * N if mu is None else mu, mass, step, coupling, kernel, seed,
+                          int(position_space), rr, step0)
         eid = ctypes.c_int(-1)
         _ck(_lib.jw_engine_add_event(self._h, ctypes.byref(d), ctypes.byref(eid)), "jw_engine_add_event")
         self.N[eid.value] = N
@@ -425,7 +429,8 @@ class Engine:
         N = kw["N"]
         d = jw_event_desc(N, kw.get("ny_slices", 50), kw.get("mu", 0.5 * N), kw.get("mass", 0.04),
                           kw.get("step", 0.0004), kw.get("coupling", FIXED_COUPLING_CONSTANT),
-                          kw.get("kernel", SIN_KERNEL), kw.get("seed", 1))
+                          kw.get("kernel", SIN_KERNEL), kw.get("seed", 1), int(kw.get("position_space", False)),
+                          kw.get("rr", 0), kw.get("step0", 0))
         eid = ctypes.c_int(-1)
         st = _lib.jw_engine_add_event(self._h, ctypes.byref(d), ctypes.byref(eid))
         if st == OK:
@@ -468,6 +473,16 @@ class Engine:
         _ck(_lib.jw_engine_get_correlator(self._h, eid, s.ctypes.data_as(_dp), e.ctypes.data_as(_dp),
                                           ctypes.byref(n)), "jw_engine_get_correlator")
         return s, e, n.value
+
+    def correlator_at(self, ids, xr, yr):
+        """(sum, err) of each event's accumulated correlator at (xr[i], yr[i])."""
+        arr, n = _ids(ids)
+        x = (ctypes.c_int * n)(*[int(v) for v in xr])
+        y = (ctypes.c_int * n)(*[int(v) for v in yr])
+        s_, e_ = np.zeros(n), np.zeros(n)
+        _ck(_lib.jw_engine_correlator_at(self._h, arr, n, x, y, s_.ctypes.data_as(_dp), e_.ctypes.data_as(_dp)),
+            "jw_engine_correlator_at")
+        return s_, e_
 
     def reset_correlator(self, eid: int):
         _ck(_lib.jw_engine_reset_correlator(self._h, eid), "jw_engine_reset_correlator")
