@@ -4,16 +4,19 @@
 // table (output_optimized_<Nx>_<Ny>_mpi1_r0.dat), with the reference's
 // progress lines.
 //
-//   jimwlk_main <px> <py> <config> [--N n] [--device d] [--seed s] [--call-for-call]
+//   jimwlk_main <px> <py> <config> [--N n] [--device d] [--seed s] [--call-for-call] [--mixed]
 //
 // <px> <py> are the reference's MPI grid arguments (ignored: one GPU holds the
 // lattice).  --N sets the lattice side (the reference fixes it at compile
 // time, 64 by default).  By default each Langevin step is one fused library
-// call (jw_evolve_momentum / jw_evolve_position); --call-for-call runs the
-// body of main_optimized.cpp:232-304 literally, one adapter call per
-// reference call.  Both draw the same noise: Langevin step n of the run uses
-// stream index n, MV slice n stream index n, in the reference's order.
-// Exit status 0 on success (the reference returns 1).
+// call (jw_evolve_momentum / jw_evolve_position), and the Hatta branches
+// (HATTA coupling, main_optimized.cpp:200-216) run together as events of the
+// batched engine, one per (ix, iy), stepped in one launch sequence (FP64, or
+// mixed precision with --mixed).  --call-for-call runs the body of
+// main_optimized.cpp:232-304 literally, one adapter call per reference call,
+// branch after branch.  All modes draw the same noise: Langevin step n of the
+// run (branches in the reference's order) uses stream index n, MV slice n
+// stream index n.  Exit status 0 on success (the reference returns 1).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -35,9 +38,84 @@ struct timer {
     }
 };
 
+// The Hatta branches of one statistics sample (main_optimized.cpp:200-216,
+// 331-332) as events of the batched engine: branch b = (ix, iy) starts from
+// the initial condition uf, evolves with rr = |(ix, iy)|^2 (wrapped) and noise
+// indices from dev.noise_step + b * langevin_steps on, and adds its
+// symmetrised correlator at (ix, iy) to sum[t], err[t] at each measurement.
+void run_hatta_batched(device& dev, const config& cnfg, lfield<double, 9>& uf,
+                       std::vector<std::unique_ptr<lfield<double, 1>>>& sum,
+                       std::vector<std::unique_ptr<lfield<double, 1>>>& err, int device_id, bool mixed) {
+    const int Nx = cnfg.Nx, Ny = cnfg.Ny, steps = cnfg.langevin_steps;
+    struct Branch { int ix, iy, rr; };
+    std::vector<Branch> br;
+    for (int ix = 0; ix < Nx; ++ix)
+        for (int iy = ix - 1; iy < ix + 2; ++iy) {
+            if (iy < 0 || iy >= Ny) continue;
+            double dix = ix, diy = iy;
+            if (dix >= Nx / 2) dix -= Nx;
+            if (dix < -Nx / 2) dix += Nx;
+            if (diy >= Ny / 2) diy -= Ny;
+            if (diy < -Ny / 2) diy += Ny;
+            br.push_back({ix, iy, (int)(dix * dix + diy * diy)});
+        }
+    jw_engine_options o{};
+    o.precision = mixed ? JW_PRECISION_MIXED : JW_PRECISION_FP64;
+    jw_engine* e = nullptr;
+    check(jw_engine_create(&o, device_id, &e), "jw_engine_create");
+    struct Guard { jw_engine* e; ~Guard() { jw_engine_destroy(e); } } guard{e};
+    const std::vector<std::complex<double>> V0 = uf.get();
+    std::vector<int> ids(br.size()), xs(br.size()), ys(br.size());
+    for (size_t b = 0; b < br.size(); ++b) {
+        jw_event_desc d{};
+        d.N = Nx;
+        d.ny_slices = 0;
+        d.mu = cnfg.mu;
+        d.mass = cnfg.mass;
+        d.step = cnfg.step;
+        d.coupling = JW_HATTA_COUPLING_CONSTANT;
+        d.kernel = cnfg.KernelChoice;
+        d.seed = cnfg.seed;
+        d.position_space = cnfg.EvolutionChoice == POSITION_EVOLUTION;
+        d.rr = br[b].rr;
+        d.step0 = dev.noise_step + (uint64_t)b * steps;
+        check(jw_engine_add_event(e, &d, &ids[b]), "jw_engine_add_event");
+        check(jw_engine_set_V(e, ids[b], reinterpret_cast<const double*>(V0.data())), "jw_engine_set_V");
+        xs[b] = br[b].ix;
+        ys[b] = br[b].iy;
+    }
+    const int n = (int)ids.size();
+    const int every = cnfg.langevin_steps / cnfg.measurements;
+    std::vector<double> vs(n), ve(n);
+    for (int langevin = 0; langevin < steps; ++langevin) {
+        timer te;
+        std::printf("Performing evolution step no. %i (%d Hatta branches)\n", langevin, n);
+        check(jw_engine_step(e, ids.data(), n, 1), "jw_engine_step");
+        check(jw_engine_sync(e), "jw_engine_sync");
+        std::printf("Evolution time: %g\n", te.seconds());
+        if (langevin % every == 0) {
+            const int time = (int)(langevin * cnfg.measurements / cnfg.langevin_steps);
+            check(jw_engine_measure(e, ids.data(), n), "jw_engine_measure");
+            check(jw_engine_correlator_at(e, ids.data(), n, xs.data(), ys.data(), vs.data(), ve.data()),
+                  "jw_engine_correlator_at");
+            for (int b = 0; b < n; ++b) check(jw_engine_reset_correlator(e, ids[b]), "jw_engine_reset_correlator");
+            // reduce_hatta (field.h:1538-1564): one site per branch
+            std::vector<std::complex<double>> hs = sum[time]->get(), he = err[time]->get();
+            for (int b = 0; b < n; ++b) {
+                const long i = (long)xs[b] * Ny + ys[b];
+                hs[i] += vs[b];
+                he[i] += ve[b];
+            }
+            sum[time]->set(hs);
+            err[time]->set(he);
+        }
+    }
+    dev.noise_step += (uint64_t)n * steps;
+}
+
 int usage() {
-    std::fprintf(stderr,
-                 "usage: jimwlk_main <px> <py> <config> [--N n] [--device d] [--seed s] [--call-for-call]\n");
+    std::fprintf(stderr, "usage: jimwlk_main <px> <py> <config> [--N n] [--device d] [--seed s] [--call-for-call] "
+                         "[--mixed]\n");
     return 2;
 }
 
@@ -46,7 +124,7 @@ int usage() {
 int main(int argc, char* argv[]) {
     if (argc < 4) return usage();
     int N = 64, device_id = 0;
-    bool call_for_call = false, seed_given = false;
+    bool call_for_call = false, seed_given = false, mixed = false;
     uint64_t seed = 1;
     for (int i = 4; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--N") && i + 1 < argc) N = std::atoi(argv[++i]);
@@ -55,6 +133,7 @@ int main(int argc, char* argv[]) {
             seed = std::strtoull(argv[++i], nullptr, 10);
             seed_given = true;
         } else if (!std::strcmp(argv[i], "--call-for-call")) call_for_call = true;
+        else if (!std::strcmp(argv[i], "--mixed")) mixed = true;
         else return usage();
     }
     try {
@@ -121,6 +200,12 @@ int main(int argc, char* argv[]) {
             dev.sync();
             std::printf("Initial condition time: %g\n", ti.seconds());
 
+            if (cp == HATTA_COUPLING_CONSTANT && !call_for_call) {
+                run_hatta_batched(dev, cnfg, uf, sum, err, device_id, mixed);
+                dev.sync();
+                std::printf("Statistics time: %g\n", ts.seconds());
+                continue;
+            }
             const int upper_bound_x = cp == HATTA_COUPLING_CONSTANT ? Nx : 1;  // :200-216
             for (int ix = 0; ix < upper_bound_x; ++ix) {
                 const int lower_bound_y = cp == HATTA_COUPLING_CONSTANT ? ix - 1 : 0;

@@ -78,6 +78,50 @@ def test_oracle_replays_reference_main(oracle, gold, name):
     assert table(N, m, sums[m], errs[m], 1.0 / 3.0 / c["stat"]) == str(fx["dat"])
 
 
+HATTA_CONFIG = ("stat = 1\nmu = 8\nmass = 0.04\nelementaryWilsonLines = 4\nfile_name = output\n"
+                "langevin_steps = 3\nmeasurements = 3\nstep = 0.0004\nEvolutionChoice = POSITION_EVOLUTION\n"
+                "CouplingChoice = HATTA_COUPLING_CONSTANT\nKernelChoice = SIN_KERNEL\n")
+
+
+def hatta_table(oracle, N: int, seed: int) -> str:
+    """The driver's Hatta run replayed on the oracle: branches (ix, iy) in the
+    reference's order (main_optimized.cpp:200-216), each from the initial
+    condition with rr = |(ix, iy)|^2 and its own block of noise indices,
+    reduce_hatta at (ix, iy) (field.h:1538-1564).  The reference leaves the
+    HATTA coupling uninitialised, so this is the formula's intent, not a
+    reference output."""
+    c = parse_config(HATTA_CONFIG)
+    g, mu = 1.0, c["mu"] / N
+    V0 = np.zeros((N, N, 9), np.complex128)
+    V0[..., 0] = V0[..., 4] = V0[..., 8] = 1.0
+    for i in range(c["ny"]):
+        f = oracle.set_mv_model(oracle.mv_normals(seed, i, N), g * mu / math.sqrt(c["ny"]))
+        f = oracle.solve_poisson(oracle.execute2D(f, 1), c["mass"] * g * g * mu, g)
+        V0 = oracle.mul_exp(V0, oracle.execute2D(f, 0))
+    every = c["steps"] // c["meas"]
+    sums = [np.zeros((N, N), np.complex128) for _ in range(c["meas"])]
+    errs = [np.zeros((N, N), np.complex128) for _ in range(c["meas"])]
+    step_index = 0
+    for ix in range(N):
+        for iy in range(ix - 1, ix + 2):
+            if not 0 <= iy < N:
+                continue
+            dix = ix - N if ix >= N // 2 else ix
+            diy = iy - N if iy >= N // 2 else iy
+            rr = dix * dix + diy * diy
+            V = V0.copy()
+            for lv in range(c["steps"]):
+                V = oracle.evolve_position(V, 1, step_index, c["step"], 2, c["kernel"], rr, None, seed)
+                step_index += 1
+                if lv % every == 0:
+                    t = lv * c["meas"] // c["steps"]
+                    corr, _, _ = oracle.measure(V)
+                    sums[t][ix, iy] += corr[ix, iy].real
+                    errs[t][ix, iy] += corr[ix, iy].real ** 2
+    m = c["meas"] - 1
+    return table(N, m, sums[m], errs[m], 1.0 / 3.0 / c["stat"])
+
+
 def test_driver_usage_without_arguments():
     if not os.path.exists(DRIVER):
         pytest.skip("driver not built (make -C softx-d-21-00092_b200)")
@@ -105,3 +149,20 @@ def test_driver_matches_reference_main(gold, tmp_path, name, mode):
     assert np.array_equal(got[:, :3], want[:, :3])
     # the table prints 7 significant digits
     assert np.allclose(got[:, 3:], want[:, 3:], rtol=2e-6, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["batched", "batched-mixed", "call-for-call"])
+def test_driver_hatta_matches_oracle(oracle, tmp_path, mode):
+    N, seed = 8, 5
+    cfg = tmp_path / "config"
+    cfg.write_text(HATTA_CONFIG)
+    args = [DRIVER, "1", "1", str(cfg), "--N", str(N), "--seed", str(seed)]
+    args += {"batched": [], "batched-mixed": ["--mixed"], "call-for-call": ["--call-for-call"]}[mode]
+    r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = parse_dat((tmp_path / f"output_optimized_{N}_{N}_mpi1_r0.dat").read_text())
+    want = parse_dat(hatta_table(oracle, N, seed))
+    assert np.array_equal(got[:, :3], want[:, :3])
+    rtol = 2e-6 if mode != "batched-mixed" else 2e-4
+    assert np.allclose(got[:, 3:], want[:, 3:], rtol=rtol, atol=1e-14)
