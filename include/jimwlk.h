@@ -305,6 +305,11 @@ jw_status jw_engine_measure(jw_engine* e, const int* ids, int n);
 jw_status jw_engine_get_correlator(jw_engine* e, int event_id, double* sum, double* err, int* nmeas);
 /* Reset an event's accumulators. */
 jw_status jw_engine_reset_correlator(jw_engine* e, int event_id);
+/* Reset the accumulators of n events (one synchronisation). */
+jw_status jw_engine_reset_correlators(jw_engine* e, const int* ids, int n);
+/* V of event dst <- V of event src (same N), on the device: e.g. the Hatta
+ * branches' common start uftmp = uf (main_optimized.cpp:230). */
+jw_status jw_engine_copy_V(jw_engine* e, int dst, int src);
 /* An event's next noise index: step0 plus the steps taken so far. */
 jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
 /* For each event ids[i], its accumulated symmetrised correlator at one

@@ -85,6 +85,46 @@ void kernel_table(int N, int coupling, std::vector<double>& t) {
         }
 }
 
+// The position kernel k_i(d) (positions.h:105-150, field.h:2402-2470) on the
+// device for all d, as complex planes [2][N*N] (real parts), with the same
+// expressions as the host copy in jw_position.cu.
+__global__ void k_position_kernel(double2* __restrict__ out, int N, int rr, int coupling, int kernel) {
+    const long vol = (long)N * N;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    const int dxi = (int)(i / N), dyi = (int)(i % N);
+    const double pi = 3.141592653589793;
+    double dx, dy, rrr;
+    if (kernel == JW_SIN_KERNEL) {
+        dx = 0.5 * N * sin(2.0 * pi * dxi / (1.0 * N)) / pi;
+        dy = 0.5 * N * sin(2.0 * pi * dyi / (1.0 * N)) / pi;
+        const double sx = N * sin(pi * dxi / (1.0 * N)) / pi, sy = N * sin(pi * dyi / (1.0 * N)) / pi;
+        rrr = sx * sx + sy * sy;
+    } else {
+        dx = dxi;
+        if (dx >= N / 2) dx = dx - N;
+        if (dx < -N / 2) dx = dx + N;
+        dy = dyi;
+        if (dy >= N / 2) dy = dy - N;
+        if (dy < -N / 2) dy = dy + N;
+        rrr = 1.0 * (dx * dx + dy * dy);
+    }
+    double rrrmin = rrr;
+    if (coupling == JW_HATTA_COUPLING_CONSTANT) rrrmin = (rrr <= rr) ? rrr : rr;
+    const double lambda = pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    double sc = 1.0;
+    if (coupling == JW_SQRT_COUPLING_CONSTANT || coupling == JW_HATTA_COUPLING_CONSTANT)
+        sc = sqrt(4.0 * pi / ((11.0 - 2.0 * 3.0 / 3.0) *
+                              log(pow(lambda + 1.26 / pow(6.0 * 6.0 * rrrmin / N / N, 1.0 / 0.2), 0.2))));
+    double kx = 0.0, ky = 0.0;
+    if (rrr > 10e-9) {
+        kx = sc * dx / rrr;
+        ky = sc * dy / rrr;
+    }
+    out[i] = make_double2(kx, 0.0);
+    out[vol + i] = make_double2(ky, 0.0);
+}
+
 // prepare_A_and_B_local's kernel (field.h:2368-2519) as a multiplier in
 // momentum space: the raw DFT of the real position kernel k_i(d)
 // (positions.h:105-150); for the SIN kernel k_i is odd in d_i and even in the
@@ -613,8 +653,7 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
         return JW_ENOMEM;
     }
     if (d->position_space) {
-        // k_i(d) on the host, its DFT on the device in FP64 (the staging buffer
-        // holds the two planes), imag / N^2 into the event's tables
+        // k_i(d), its DFT in FP64, imag / N^2 into the event's tables
         double2* tmp = nullptr;
         if (cudaMalloc(&ev.k64, sizeof(double) * 2 * vol) != cudaSuccess ||
             cudaMalloc(&ev.k32, sizeof(float) * 2 * vol) != cudaSuccess ||
@@ -626,15 +665,9 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
             if (tmp) cudaFree(tmp);
             return JW_ENOMEM;
         }
-        std::vector<double2> h(2 * vol);
-        for (int x = 0; x < d->N; ++x)
-            for (int y = 0; y < d->N; ++y) {
-                double kx, ky;
-                position_kernel_host(x, y, d->N, d->rr, d->coupling, d->kernel, &kx, &ky);
-                h[(size_t)x * d->N + y] = make_double2(kx, 0.0);
-                h[vol + (size_t)x * d->N + y] = make_double2(ky, 0.0);
-            }
-        cudaError_t ce = cudaMemcpyAsync(tmp, h.data(), sizeof(double2) * 2 * vol, cudaMemcpyHostToDevice, e->stream);
+        k_position_kernel<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(tmp, d->N, d->rr, d->coupling,
+                                                                                d->kernel);
+        cudaError_t ce = cudaGetLastError();
         if (ce == cudaSuccess) ce = fft2d_planes<double>(tmp, 2, d->N, 1, 1.0, g->tw, e->stream);
         if (ce == cudaSuccess) {
             k_position_table<<<(unsigned)((2 * vol + 255) / 256), 256, 0, e->stream>>>(
@@ -871,6 +904,32 @@ JW_EXPORT jw_status jw_engine_reset_correlator(jw_engine* e, int id) {
     JW_CUDA(cudaMemcpyAsync(&e->groups[ev.N]->d_ev[ev.slot].nmeas, &zero, sizeof(int), cudaMemcpyHostToDevice,
                             e->stream));
     JW_CUDA(cudaStreamSynchronize(e->stream));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_copy_V(jw_engine* e, int dst, int src) {
+    JW_CHECK(e);
+    auto a = e->events.find(dst), b = e->events.find(src);
+    if (a == e->events.end() || b == e->events.end()) return JW_ENOTFOUND;
+    JW_CHECK(a->second.N == b->second.N);
+    if (dst == src) return JW_OK;
+    JW_CUDA(cudaMemcpyAsync(a->second.V, b->second.V, sizeof(double2) * 9 * (size_t)a->second.N * a->second.N,
+                            cudaMemcpyDeviceToDevice, e->stream));
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_reset_correlators(jw_engine* e, const int* ids, int n) {
+    JW_CHECK(e && (ids || n == 0) && n >= 0);
+    for (int i = 0; i < n; ++i)
+        if (e->events.find(ids[i]) == e->events.end()) return JW_ENOTFOUND;
+    const int zero = 0;
+    for (int i = 0; i < n; ++i) {
+        const Event& ev = e->events[ids[i]];
+        JW_CUDA(cudaMemsetAsync(ev.acc, 0, sizeof(double) * 4 * (size_t)ev.N * ev.N, e->stream));
+        JW_CUDA(cudaMemcpyAsync(&e->groups[ev.N]->d_ev[ev.slot].nmeas, &zero, sizeof(int), cudaMemcpyHostToDevice,
+                                e->stream));
+    }
+    JW_CUDA(cudaStreamSynchronize(e->stream));  // `zero` lives on this frame
     return JW_OK;
 }
 

@@ -80,7 +80,8 @@ void run_hatta_batched(device& dev, const config& cnfg, lfield<double, 9>& uf,
         d.rr = br[b].rr;
         d.step0 = dev.noise_step + (uint64_t)b * steps;
         check(jw_engine_add_event(e, &d, &ids[b]), "jw_engine_add_event");
-        check(jw_engine_set_V(e, ids[b], reinterpret_cast<const double*>(V0.data())), "jw_engine_set_V");
+        if (b == 0) check(jw_engine_set_V(e, ids[b], reinterpret_cast<const double*>(V0.data())), "jw_engine_set_V");
+        else check(jw_engine_copy_V(e, ids[b], ids[0]), "jw_engine_copy_V");  // uftmp = uf
         xs[b] = br[b].ix;
         ys[b] = br[b].iy;
     }
@@ -98,7 +99,7 @@ void run_hatta_batched(device& dev, const config& cnfg, lfield<double, 9>& uf,
             check(jw_engine_measure(e, ids.data(), n), "jw_engine_measure");
             check(jw_engine_correlator_at(e, ids.data(), n, xs.data(), ys.data(), vs.data(), ve.data()),
                   "jw_engine_correlator_at");
-            for (int b = 0; b < n; ++b) check(jw_engine_reset_correlator(e, ids[b]), "jw_engine_reset_correlator");
+            check(jw_engine_reset_correlators(e, ids.data(), n), "jw_engine_reset_correlators");
             // reduce_hatta (field.h:1538-1564): one site per branch
             std::vector<std::complex<double>> hs = sum[time]->get(), he = err[time]->get();
             for (int b = 0; b < n; ++b) {

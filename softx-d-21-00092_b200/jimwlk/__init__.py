@@ -139,6 +139,8 @@ def _load():
         "jw_engine_measure": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
         "jw_engine_get_correlator": ([_vp, ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "jw_engine_reset_correlator": ([_vp, ctypes.c_int], ctypes.c_int),
+        "jw_engine_copy_V": ([_vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "jw_engine_reset_correlators": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
         "jw_engine_correlator_at": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), _dp, _dp], ctypes.c_int),
         "jw_engine_event_steps": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
@@ -473,6 +475,13 @@ class Engine:
         _ck(_lib.jw_engine_get_correlator(self._h, eid, s.ctypes.data_as(_dp), e.ctypes.data_as(_dp),
                                           ctypes.byref(n)), "jw_engine_get_correlator")
         return s, e, n.value
+
+    def copy_V(self, dst: int, src: int):
+        _ck(_lib.jw_engine_copy_V(self._h, dst, src), "jw_engine_copy_V")
+
+    def reset_correlators(self, ids):
+        arr, n = _ids(ids)
+        _ck(_lib.jw_engine_reset_correlators(self._h, arr, n), "jw_engine_reset_correlators")
 
     def correlator_at(self, ids, xr, yr):
         """(sum, err) of each event's accumulated correlator at (xr[i], yr[i])."""

@@ -71,7 +71,7 @@ def test_hatta_branches_batched(jw, oracle):
     ids = []
     for b, (ix, iy, rr) in enumerate(branches):
         eid = pos_event(eng, N, seed, HATTA, rr=rr, step0=b * steps)
-        eng.set_V(eid, V0)
+        eng.copy_V(eid, base)
         ids.append(eid)
     eng.step(ids, steps)
     eng.measure(ids)
@@ -84,6 +84,9 @@ def test_hatta_branches_batched(jw, oracle):
         assert s[k] == full[ix, iy].real and e[k] == full_err[ix, iy].real
         c, _, _ = oracle.measure(want)
         assert abs(s[k] - c[ix, iy].real) <= 1e-12 * abs(c).max()
+    eng.reset_correlators(ids)
+    s, e = eng.correlator_at(ids, [b[0] for b in branches], [b[1] for b in branches])
+    assert not s.any() and not e.any()
 
 
 def test_position_engine_rejects_what_it_cannot_do(jw):
