@@ -122,6 +122,11 @@ jw_status jw_field_set(jw_field* f, const double* host);
 jw_status jw_field_get(const jw_field* f, double* host);
 /* lfield::operator= (field.h:301-318). */
 jw_status jw_field_copy(jw_field* dst, const jw_field* src);
+/* No counterpart in the reference (it has no checkpoints).  A field to and
+ * from a file: a 16-byte header ("JWFIELD1", int32 N, int32 t) and then
+ * 2*t*N*N native doubles in the reference layout.  Loading checks N and t. */
+jw_status jw_field_save(const jw_field* f, const char* path);
+jw_status jw_field_load(jw_field* f, const char* path);
 /* lfield::setToUnit / setToZero (field.h:181-211). */
 jw_status jw_field_set_unit(jw_field* f);
 jw_status jw_field_set_zero(jw_field* f);
@@ -310,6 +315,14 @@ jw_status jw_engine_reset_correlators(jw_engine* e, const int* ids, int n);
 /* V of event dst <- V of event src (same N), on the device: e.g. the Hatta
  * branches' common start uftmp = uf (main_optimized.cpp:230). */
 jw_status jw_engine_copy_V(jw_engine* e, int dst, int src);
+/* No counterpart in the reference.  Checkpoint of one event: its descriptor,
+ * next noise index, measurement count, V (reference layout) and FP64
+ * accumulators, so that a loaded event continues bit for bit.  File: the
+ * header ("JWEVENT1", jw_event_desc, uint64 step, int32 nmeas, int32 0), then
+ * 18*N*N doubles of V and 4*N*N doubles of accumulators (sum, compensation,
+ * err, compensation).  Loading adds a new event and returns its id. */
+jw_status jw_engine_save_event(jw_engine* e, int event_id, const char* path);
+jw_status jw_engine_load_event(jw_engine* e, const char* path, int* event_id);
 /* An event's next noise index: step0 plus the steps taken so far. */
 jw_status jw_engine_event_steps(jw_engine* e, int event_id, uint64_t* steps);
 /* For each event ids[i], its accumulated symmetrised correlator at one

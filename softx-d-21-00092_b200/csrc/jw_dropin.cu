@@ -384,6 +384,46 @@ JW_EXPORT jw_status jw_field_get(const jw_field* f, double* host) {
     return JW_OK;
 }
 
+namespace {
+struct FieldFileHeader {
+    char magic[8];  // "JWFIELD1"
+    int32_t N;
+    int32_t t;
+};
+constexpr char kFieldMagic[8] = {'J', 'W', 'F', 'I', 'E', 'L', 'D', '1'};
+}  // namespace
+
+JW_EXPORT jw_status jw_field_save(const jw_field* f, const char* path) {
+    JW_CHECK(f && path);
+    const long vol = (long)f->ctx->N * f->ctx->N;
+    std::vector<double> h(2 * (size_t)f->t * vol);
+    jw_status s = jw_field_get(f, h.data());
+    if (s) return s;
+    FieldFileHeader hd{};
+    std::memcpy(hd.magic, kFieldMagic, 8);
+    hd.N = f->ctx->N;
+    hd.t = f->t;
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return JW_EINVAL;
+    bool ok = std::fwrite(&hd, sizeof hd, 1, fp) == 1 && std::fwrite(h.data(), sizeof(double), h.size(), fp) == h.size();
+    ok = (std::fclose(fp) == 0) && ok;
+    return ok ? JW_OK : JW_EINVAL;
+}
+
+JW_EXPORT jw_status jw_field_load(jw_field* f, const char* path) {
+    JW_CHECK(f && path);
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return JW_EINVAL;
+    FieldFileHeader hd{};
+    const long vol = (long)f->ctx->N * f->ctx->N;
+    std::vector<double> h(2 * (size_t)f->t * vol);
+    bool ok = std::fread(&hd, sizeof hd, 1, fp) == 1 && std::memcmp(hd.magic, kFieldMagic, 8) == 0 &&
+              hd.N == f->ctx->N && hd.t == f->t && std::fread(h.data(), sizeof(double), h.size(), fp) == h.size();
+    std::fclose(fp);
+    if (!ok) return JW_EINVAL;
+    return jw_field_set(f, h.data());
+}
+
 JW_EXPORT jw_status jw_field_copy(jw_field* dst, const jw_field* src) {
     JW_CHECK(same_ctx(dst, src) && dst->t == src->t);
     if (dst == src) return JW_OK;

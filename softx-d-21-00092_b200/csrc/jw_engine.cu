@@ -780,6 +780,79 @@ JW_EXPORT jw_status jw_engine_get_V(jw_engine* e, int id, double* host) {
     return JW_OK;
 }
 
+// ---- checkpoints: [header][V, reference layout][4 accumulator planes]
+namespace {
+struct EventFileHeader {
+    char magic[8];         // "JWEVENT1"
+    jw_event_desc desc;
+    uint64_t step;         // next noise index
+    int32_t nmeas;
+    int32_t reserved;
+};
+constexpr char kEventMagic[8] = {'J', 'W', 'E', 'V', 'E', 'N', 'T', '1'};
+}  // namespace
+
+JW_EXPORT jw_status jw_engine_save_event(jw_engine* e, int id, const char* path) {
+    JW_CHECK(e && path);
+    auto it = e->events.find(id);
+    if (it == e->events.end()) return JW_ENOTFOUND;
+    const Event& ev = it->second;
+    const long vol = (long)ev.N * ev.N;
+    std::vector<double> V(18 * (size_t)vol), acc(4 * (size_t)vol);
+    jw_status s = jw_engine_get_V(e, id, V.data());
+    if (s) return s;
+    EventDev d{};
+    JW_CUDA(cudaMemcpyAsync(acc.data(), ev.acc, sizeof(double) * 4 * vol, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaMemcpyAsync(&d, e->groups[ev.N]->d_ev + ev.slot, sizeof(EventDev), cudaMemcpyDeviceToHost,
+                            e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    EventFileHeader h{};
+    std::memcpy(h.magic, kEventMagic, 8);
+    h.desc = ev.desc;
+    h.step = d.step;
+    h.nmeas = d.nmeas;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return JW_EINVAL;
+    bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 && std::fwrite(V.data(), sizeof(double), V.size(), f) == V.size() &&
+              std::fwrite(acc.data(), sizeof(double), acc.size(), f) == acc.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? JW_OK : JW_EINVAL;
+}
+
+JW_EXPORT jw_status jw_engine_load_event(jw_engine* e, const char* path, int* event_id) {
+    JW_CHECK(e && path && event_id);
+    *event_id = -1;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return JW_EINVAL;
+    EventFileHeader h{};
+    if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, kEventMagic, 8) != 0 || !supported_n(h.desc.N)) {
+        std::fclose(f);
+        return JW_EINVAL;
+    }
+    const long vol = (long)h.desc.N * h.desc.N;
+    std::vector<double> V(18 * (size_t)vol), acc(4 * (size_t)vol);
+    const bool ok = std::fread(V.data(), sizeof(double), V.size(), f) == V.size() &&
+                    std::fread(acc.data(), sizeof(double), acc.size(), f) == acc.size();
+    std::fclose(f);
+    if (!ok) return JW_EINVAL;
+    int id = -1;
+    jw_status s = jw_engine_add_event(e, &h.desc, &id);
+    if (s) return s;
+    s = jw_engine_set_V(e, id, V.data());
+    if (s) {
+        jw_engine_remove_event(e, id);
+        return s;
+    }
+    const Event& ev = e->events[id];
+    EventDev* dev = e->groups[ev.N]->d_ev + ev.slot;
+    JW_CUDA(cudaMemcpyAsync(ev.acc, acc.data(), sizeof(double) * 4 * vol, cudaMemcpyHostToDevice, e->stream));
+    JW_CUDA(cudaMemcpyAsync(&dev->step, &h.step, sizeof h.step, cudaMemcpyHostToDevice, e->stream));
+    JW_CUDA(cudaMemcpyAsync(&dev->nmeas, &h.nmeas, sizeof h.nmeas, cudaMemcpyHostToDevice, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    *event_id = id;
+    return JW_OK;
+}
+
 JW_EXPORT jw_status jw_engine_init_mv(jw_engine* e, const int* ids, int n) {
     JW_CHECK(e);
     std::map<int, std::vector<int>> by_n;

@@ -98,6 +98,10 @@ def _load():
         "jw_field_set": ([_vp, _dp], ctypes.c_int),
         "jw_field_get": ([_vp, _dp], ctypes.c_int),
         "jw_field_copy": ([_vp, _vp], ctypes.c_int),
+        "jw_field_save": ([_vp, ctypes.c_char_p], ctypes.c_int),
+        "jw_field_load": ([_vp, ctypes.c_char_p], ctypes.c_int),
+        "jw_engine_save_event": ([_vp, ctypes.c_int, ctypes.c_char_p], ctypes.c_int),
+        "jw_engine_load_event": ([_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "jw_field_set_unit": ([_vp], ctypes.c_int),
         "jw_field_set_zero": ([_vp], ctypes.c_int),
         "jw_execute2D": ([_vp, _vp, ctypes.c_int], ctypes.c_int),
@@ -368,6 +372,13 @@ class Field:
         _ck(_lib.jw_field_get(self._h, a.ctypes.data_as(_dp)), "jw_field_get")
         return a
 
+    def save(self, path: str):
+        _ck(_lib.jw_field_save(self._h, os.fsencode(path)), "jw_field_save")
+
+    def load(self, path: str) -> "Field":
+        _ck(_lib.jw_field_load(self._h, os.fsencode(path)), "jw_field_load")
+        return self
+
     def copy_from(self, other: "Field"):
         _ck(_lib.jw_field_copy(self._h, other._h), "jw_field_copy")
 
@@ -475,6 +486,19 @@ class Engine:
         _ck(_lib.jw_engine_get_correlator(self._h, eid, s.ctypes.data_as(_dp), e.ctypes.data_as(_dp),
                                           ctypes.byref(n)), "jw_engine_get_correlator")
         return s, e, n.value
+
+    def save_event(self, eid: int, path: str):
+        _ck(_lib.jw_engine_save_event(self._h, eid, os.fsencode(path)), "jw_engine_save_event")
+
+    def load_event(self, path: str) -> int:
+        eid = ctypes.c_int(-1)
+        _ck(_lib.jw_engine_load_event(self._h, os.fsencode(path), ctypes.byref(eid)), "jw_engine_load_event")
+        d = jw_event_desc()
+        with open(path, "rb") as fh:
+            fh.seek(8)
+            fh.readinto(d)
+        self.N[eid.value] = d.N
+        return eid.value
 
     def copy_V(self, dst: int, src: int):
         _ck(_lib.jw_engine_copy_V(self._h, dst, src), "jw_engine_copy_V")
