@@ -380,9 +380,28 @@ cudaError_t launch_mv_slice(jw_engine* e, Group& g, const int* d_slots, int nb, 
     return cudaGetLastError();
 }
 
+// The correlator planes of a measurement: FP64 transforms for the FP64
+// engine, FP32 pair planes (FP64 sums) for the mixed one.  Returns the
+// per-event correlators' location in the workspace.
 template <int N>
-cudaError_t launch_measure_kernels(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
+cudaError_t launch_measure_kernels(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws,
+                                   double** corr_out) {
     const long vol = (long)N * N;
+    if (e->opt.precision == JW_PRECISION_MIXED) {
+        float4* M = reinterpret_cast<float4*>(ws);
+        double* corr = reinterpret_cast<double*>(M + (size_t)5 * vol * nb);
+        const size_t sm1 = meas32_rows_smem<N>(), sm2 = mx_p2_smem<N>();
+        static bool configured = false;
+        if (!configured) {
+            cudaFuncSetAttribute(k_meas32_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+            cudaFuncSetAttribute(k_meas32_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+            configured = true;
+        }
+        k_meas32_rows<N><<<dim3(N, nb), meas32_rows_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, M, g.tw.d32);
+        k_meas32_cols<N><<<dim3(N / mx_cols<N>(), nb), mx_p2_threads<N>(), sm2, e->stream>>>(M, corr, g.tw.d32);
+        *corr_out = corr;
+        return cudaGetLastError();
+    }
     double2* M = reinterpret_cast<double2*>(ws);
     double* corr = reinterpret_cast<double*>(M + (size_t)9 * vol * nb);
     constexpr int RW = meas_rows16<N>();
@@ -398,14 +417,15 @@ cudaError_t launch_measure_kernels(jw_engine* e, Group& g, const int* d_slots, i
                                                                                        g.tw.d64);
     k_meas_cols<N><<<dim3(N / mx_cols<N>(), nb), meas_cols_threads<N>(), sm2, e->stream>>>(d_slots, M, corr,
                                                                                           g.tw.d64);
+    *corr_out = corr;
     return cudaGetLastError();
 }
 
 template <int N>
 cudaError_t launch_measure(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
     const long vol = (long)N * N;
-    double* corr = reinterpret_cast<double*>(reinterpret_cast<double2*>(ws) + (size_t)9 * vol * nb);
-    cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws);
+    double* corr = nullptr;
+    cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws, &corr);
     if (err != cudaSuccess) return err;
     k_meas_reduce<N><<<dim3((unsigned)((vol + 255) / 256), nb), 256, 0, e->stream>>>(g.d_ev, d_slots, corr);
     return cudaGetLastError();
@@ -415,8 +435,8 @@ template <int N>
 cudaError_t launch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws,
                                    double* ens) {
     const long vol = (long)N * N;
-    double* corr = reinterpret_cast<double*>(reinterpret_cast<double2*>(ws) + (size_t)9 * vol * nb);
-    cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws);
+    double* corr = nullptr;
+    cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws, &corr);
     if (err != cudaSuccess) return err;
     k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, nb, ens);
     return cudaGetLastError();

@@ -387,4 +387,105 @@ __global__ void __launch_bounds__(meas_cols_threads<N>()) k_meas_cols(const int*
     (void)slots;
 }
 
+// ---- measurement, mixed precision: the 9 entries of V as 5 FP32 pair planes
+// (V_0, V_1), (V_2, V_3), (V_4, V_5), (V_6, V_7), (V_8, 0), transformed like
+// the step's pair planes; |.|^2 is summed in FP64.  Workspace: 80 B/site.
+template <int N> constexpr int meas32_rows_threads() {
+    return (N >= 64 && 5 * (N / 8) <= 1024) ? 5 * (N / 8) : 256;
+}
+template <int N> constexpr size_t meas32_rows_smem() { return 16 * (size_t)padded_len16(5 * N); }
+
+template <int N>
+__global__ void __launch_bounds__(meas32_rows_threads<N>(), N <= 512 ? 2 : 1) k_meas32_rows(const EventDev* __restrict__ ev,
+                                                                          const int* __restrict__ slots,
+                                                                          float4* __restrict__ M,
+                                                                          const float2* __restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* sm = reinterpret_cast<float4*>(smem_raw);
+    const int x = blockIdx.x, b = blockIdx.y;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const double2* V = e.V + (long)x * N;
+    // the row's 9 N entries in batches of 4 independent loads per thread;
+    // entry (k, y) goes to half (k & 1) of pair element (k >> 1, y)
+    constexpr int TH = meas32_rows_threads<N>();
+    constexpr int B = 4;
+    for (int base = 0; base < 9 * N; base += TH * B) {
+        double2 v[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int i = base + threadIdx.x + u * TH;
+            if (i < 9 * N) v[u] = V[(long)(i / N) * vol + (i % N)];
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int i = base + threadIdx.x + u * TH;
+            if (i < 9 * N) {
+                const int k = i / N, y = i - k * N;
+                reinterpret_cast<float2*>(&sm[pad16((k >> 1) * N + y)])[k & 1] =
+                    make_float2((float)v[u].x, (float)v[u].y);
+            }
+        }
+    }
+    for (int y = threadIdx.x; y < N; y += TH)
+        reinterpret_cast<float2*>(&sm[pad16(4 * N + y)])[1] = make_float2(0.0f, 0.0f);
+    __syncthreads();
+    fft16_rows<N, 5>(sm, -1.0f, tw);
+    float4* out = M + (long)b * 5 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 5 * N; i += blockDim.x) {
+        const int p = i / N, y = i - p * N;
+        out[p * vol + y] = sm[pad16(i)];
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(mx_p2_threads<N>(), 3) k_meas32_cols(const float4* __restrict__ M,
+                                                                    double* __restrict__ corr,
+                                                                    const float2* __restrict__ tw) {
+    constexpr int C = mx_cols<N>();
+    constexpr int TH = mx_p2_threads<N>();
+    constexpr int PER = N * C / TH;  // = 8
+    constexpr int RSTEP = TH / C;    // = N / 8
+    constexpr int TL = mx_tile_len<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* tile[2] = {reinterpret_cast<float4*>(smem_raw), reinterpret_cast<float4*>(smem_raw) + TL};
+    const int c0 = blockIdx.x * C, b = blockIdx.y;
+    const long vol = (long)N * N;
+    const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
+    const ColIdx16P<C> cidx{cc};
+    auto stage = [&](int p, float4* t) {
+        const float4* in = M + ((long)b * 5 + p) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) cp_async<16>(&t[cidx(r0 + q * RSTEP)], in + (long)q * RSTEP * N);
+        cp_async_commit();
+    };
+    double acc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) acc[q] = 0.0;
+    stage(0, tile[0]);
+#pragma unroll 1
+    for (int p = 0; p < 5; ++p) {
+        if (p + 1 < 5) {
+            stage(p + 1, tile[(p + 1) & 1]);  // the buffer read at p - 1
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        float4* t = tile[p & 1];
+        fft16<float, N>(t, cidx, r0, true, -1.0f, tw);
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const float4 v = t[cidx(r0 + q * RSTEP)];
+            acc[q] += ((double)v.x * v.x + (double)v.y * v.y) + ((double)v.z * v.z + (double)v.w * v.w);
+        }
+        __syncthreads();
+    }
+    const double n2 = (double)N * (double)N;
+    const double inv = 1.0 / (n2 * n2 * n2);
+    double* out = corr + (long)b * vol + c0 + cc;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
+}
+
 }  // namespace jw
