@@ -198,6 +198,9 @@ def run_reference_main(steps: int, warmup: int, nthreads: int | None = None, n_s
         return statistics.mean(t[warmup:]), None
 
 
+# serving: each tick advances the requests with the least remaining work first,
+# up to 64 x 512^2 lattice sites (one bench batch)
+SERVE_TICK_SITES = 64 * 512 * 512
 POS_N, POS_SLICES, POS_STEPS, POS_EVERY = 256, 100, 500, 50
 POS_STEP = DS / math.pi ** 2  # running coupling: alpha_s(r) enters through the correlated noise
 POS_CPU_N = 32
@@ -284,7 +287,7 @@ def quantize_n(n: float) -> int:
     return int(2 ** int(round(math.log2(n))))
 
 
-def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int):
+def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sites: int = 0):
     """Continuous batching under Poisson arrivals: requests (N log-uniform on
     [64, 2048] rounded to a power of two, Ny in {50, 100}, steps uniform on
     [10, 2000], g^2 mu a uniform on [0.3, 0.8], per-request seed) submitted at
@@ -298,7 +301,7 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int):
         N = quantize_n(math.exp(rng.uniform(math.log(64), math.log(2048))))
         reqs.append(dict(N=N, ny_slices=int(rng.choice([50, 100])), steps=int(rng.integers(10, 2001)),
                          mu=float(rng.uniform(0.3, 0.8)) * N, seed=10_000 + i))
-    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=16, device=device)
+    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=16, device=device, tick_sites=tick_sites)
     rids = [None] * n_requests
 
     def feeder():
@@ -328,8 +331,10 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int):
             "site_steps_per_s": site_steps / (t_last - t_first), "wall_s": t_last - t_first,
             "max_resident": stats.max_active,
             "offered_site_steps_per_s": site_steps / arrivals[-1],
+            "tick_sites": tick_sites,
             "what": "Poisson arrivals, N log-uniform 64..2048 rounded to powers of two, steps U[10,2000], "
-                    "Ny in {50,100}, mixed precision, continuous batching"}
+                    "Ny in {50,100}, mixed precision, continuous batching"
+                    + (", least remaining work first per tick" if tick_sites else "")}
 
 
 def uneven_leg(jw, device: int, seed: int):
@@ -498,7 +503,7 @@ def main_arm(args):
                               "what": "jw_evolve_momentum, reference call structure, FP64, one 512^2 event",
                               "mixed_batched_over_plain": value / plain}
         ctx.close()
-        line["serve"] = serve_leg(jw, local, args.serve_requests, 200.0, 2026)
+        line["serve"] = serve_leg(jw, local, args.serve_requests, 200.0, 2026, tick_sites=SERVE_TICK_SITES)
         line["serve"]["vs_fp64_plain"] = line["serve"]["site_steps_per_s"] / plain
         line["uneven"] = uneven_leg(jw, local, 48)
         line["position"] = position_leg(jw, local)

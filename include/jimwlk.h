@@ -371,6 +371,13 @@ typedef struct jw_server_options {
     int max_active;             /* resident events (0 = no limit beyond memory) */
     int fake_device;            /* 1: host-only stand-in backend (no GPU; scheduler tests) */
     double fake_ns_per_site_step;
+    /* 0: every resident request advances at every tick.  Otherwise a tick
+     * advances the resident requests with the least remaining work (sites x
+     * (remaining steps + pending MV slices)) first, as many as fit in this
+     * many lattice sites (at least one), and a request's MV initial condition
+     * runs when it is first chosen: short requests finish early instead of
+     * sharing every tick with long ones. */
+    size_t tick_sites;
 } jw_server_options;
 
 typedef struct jw_request_desc {

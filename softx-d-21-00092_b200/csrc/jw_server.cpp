@@ -6,9 +6,13 @@
 // owns the device:
 //   admit   first fit over the queue by device footprint (the engine's budget);
 //           requests that do not fit wait, later smaller ones may pass them;
-//   tick    every resident event advances together, one launch group per
-//           lattice size, by k = min(max_steps_per_tick, fewest remaining
-//           steps in the group) steps;
+//   tick    the chosen resident events advance together, one launch group
+//           per lattice size, by k = min(max_steps_per_tick, fewest remaining
+//           steps in the group) steps.  Chosen are all of them, or with
+//           options.tick_sites the ones with the least remaining work first
+//           (shortest remaining work, as many as fit in tick_sites lattice
+//           sites, at least one); an event's MV initial condition runs when it
+//           is first chosen;
 //   retire  finished events are measured, their S(r) copied out and their
 //           device memory released, which lets queued requests in.
 // Requests that arrive while others are on the GPU join at the next tick.
@@ -144,6 +148,7 @@ struct Request {
     bool done = false;
     int eid = -1;
     long remaining = 0;
+    bool mv = false;  // MV initial condition done
     double t_submit = 0, t_admit = 0, t_done = 0;
     std::vector<double> sb, rb;
     double qs = 0;
@@ -232,23 +237,57 @@ void worker_loop(jw_server* s) {
             s->max_active_seen = std::max(s->max_active_seen, (int)(s->active.size() + admitted.size()));
         }
         // device work runs outside the lock: only this thread uses the backend
-        if (!admitted.empty()) {
-            std::vector<int> eids;
-            for (Request* r : admitted) eids.push_back(r->eid);
-            const jw_status st = s->be->init_mv(eids);
-            if (st) {
-                for (Request* r : admitted) {
-                    s->be->remove(r->eid);
-                    retire(s, r, st);
-                }
-            } else {
-                for (Request* r : admitted) s->active.push_back(r);
+        for (Request* r : admitted) s->active.push_back(r);
+        if (s->active.empty()) continue;
+        // choose this tick's events
+        std::vector<Request*> sel;
+        if (s->opt.tick_sites == 0) {
+            sel = s->active;
+        } else {
+            auto work = [](const Request* r) {
+                return (double)r->d.N * r->d.N * (double)(r->remaining + (r->mv ? 0 : r->d.ny_slices));
+            };
+            std::vector<Request*> order = s->active;
+            std::stable_sort(order.begin(), order.end(),
+                             [&](const Request* a, const Request* b) { return work(a) < work(b); });
+            double sites = 0;
+            for (Request* r : order) {
+                const double n2 = (double)r->d.N * r->d.N;
+                if (!sel.empty() && sites + n2 > (double)s->opt.tick_sites) continue;
+                sel.push_back(r);
+                sites += n2;
             }
         }
-        if (s->active.empty()) continue;
+        // MV initial conditions of the chosen events that have none yet
+        {
+            std::vector<int> eids;
+            std::vector<Request*> fresh;
+            for (Request* r : sel)
+                if (!r->mv) {
+                    eids.push_back(r->eid);
+                    fresh.push_back(r);
+                }
+            if (!eids.empty()) {
+                const jw_status st = s->be->init_mv(eids);
+                for (Request* r : fresh) r->mv = (st == JW_OK);
+                if (st) {
+                    std::vector<Request*> keep;
+                    for (Request* r : s->active) {
+                        if (std::find(fresh.begin(), fresh.end(), r) != fresh.end()) {
+                            s->be->remove(r->eid);
+                            retire(s, r, st);
+                        } else {
+                            keep.push_back(r);
+                        }
+                    }
+                    s->active.swap(keep);
+                    continue;
+                }
+            }
+        }
         // tick: one launch group per lattice size
         std::map<int, std::vector<Request*>> by_n;
-        for (Request* r : s->active) by_n[r->d.N].push_back(r);
+        for (Request* r : sel) by_n[r->d.N].push_back(r);
         double ss = 0;
         jw_status tick_status = JW_OK;
         for (auto& kv : by_n) {
@@ -274,7 +313,7 @@ void worker_loop(jw_server* s) {
             if (tick_status != JW_OK) {
                 s->be->remove(r->eid);
                 retire(s, r, tick_status);
-            } else if (r->remaining <= 0) {
+            } else if (r->remaining <= 0 && r->mv) {
                 std::vector<double> sb, rb;
                 double qs = 0;
                 const jw_status st = s->be->finish(r->eid, sb, rb, &qs);

@@ -55,7 +55,7 @@ class jw_event_desc(ctypes.Structure):
 class jw_server_options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("reunitarize", ctypes.c_int), ("max_bytes", ctypes.c_size_t),
                 ("max_steps_per_tick", ctypes.c_int), ("max_active", ctypes.c_int), ("fake_device", ctypes.c_int),
-                ("fake_ns_per_site_step", ctypes.c_double)]
+                ("fake_ns_per_site_step", ctypes.c_double), ("tick_sites", ctypes.c_size_t)]
 
 
 class jw_request_desc(ctypes.Structure):
@@ -563,9 +563,9 @@ class Server:
 
     def __init__(self, precision: int = PRECISION_MIXED, max_bytes: int = 0, max_steps_per_tick: int = 8,
                  max_active: int = 0, reunitarize: bool = False, fake_device: bool = False,
-                 fake_ns_per_site_step: float = 0.0, device: int = 0):
+                 fake_ns_per_site_step: float = 0.0, device: int = 0, tick_sites: int = 0):
         o = jw_server_options(precision, int(reunitarize), max_bytes, max_steps_per_tick, max_active,
-                              int(fake_device), fake_ns_per_site_step)
+                              int(fake_device), fake_ns_per_site_step, tick_sites)
         self._h = _vp()
         _ck(_lib.jw_server_create(ctypes.byref(o), device, ctypes.byref(self._h)), "jw_server_create")
 

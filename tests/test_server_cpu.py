@@ -103,3 +103,24 @@ def test_concurrent_submitters(jw):
     assert len(out) == 20 and all(st == jw.OK for st, _ in out)
     assert srv.stats().completed == 20
     srv.close()
+
+
+@pytest.mark.parametrize("tick_sites", [0, 3 * 64 * 64])
+def test_shortest_remaining_work_first(jw, tick_sites):
+    """A long request (512^2 x 100 steps) and three short ones (64^2 x 200).
+    Every resident request at every tick (tick_sites = 0): the long one needs
+    13 ticks of 8 steps and the short ones 25, so the long one finishes first.
+    With tick_sites = 3 * 64^2 the short ones (less remaining work) take the
+    ticks until they are done, and the long one finishes last."""
+    srv = jw.Server(fake_device=True, max_bytes=1 << 30, fake_ns_per_site_step=20.0, max_steps_per_tick=8,
+                    tick_sites=tick_sites)
+    long_ = srv.submit(512, 100, seed=1)
+    short = [srv.submit(64, 200, seed=2 + i) for i in range(3)]
+    t_long = srv.wait(long_, timeout=60)[1].t_done
+    t_short = [srv.wait(r, timeout=60)[1].t_done for r in short]
+    if tick_sites:
+        assert max(t_short) < t_long
+    else:
+        assert t_long < min(t_short)
+    assert srv.stats().completed == 4
+    srv.close()
