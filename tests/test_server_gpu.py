@@ -27,9 +27,12 @@ def run(jw, reqs, **opt):
     return out, st
 
 
+@pytest.mark.parametrize("tick_sites", [0, 2 * 64 * 64])
 @pytest.mark.parametrize("precision", [1, 0])
-def test_each_result_same_alone_and_in_mix(jw, precision):
-    mixed, st = run(jw, MIX, precision=precision, max_steps_per_tick=4)
+def test_each_result_same_alone_and_in_mix(jw, precision, tick_sites):
+    """Also with the least-remaining-work-first ticks (tick_sites), which step
+    different subsets of the resident requests at each tick."""
+    mixed, st = run(jw, MIX, precision=precision, max_steps_per_tick=4, tick_sites=tick_sites)
     assert st.completed == len(MIX) and st.max_active >= 2
     for r, (status, res, sb, rb) in zip(MIX, mixed):
         assert status == jw.OK
