@@ -358,6 +358,48 @@ def uneven_leg(jw, device: int, seed: int):
                     "one server, MV initial conditions included"}
 
 
+def c1_leg(jw, device: int):
+    """C1, the reference's CPU-runnable case: one FP64 event at 64^2, MV initial
+    condition (g^2 mu a = 0.5, m a = 0.02, Ny = 50), 100 fixed-coupling steps
+    (alpha_s = 0.15, ds = 1e-4) through the call-for-call layer, then C(k), S(r)
+    and Q_s.  Beside it the reference's main_optimized at 64^2 (all host
+    threads), per Langevin step."""
+    import torch
+    n = 64
+    cfg = jw.config_defaults(Nx=n, Ny=n, seed=1, mu=0.5 * n, mass=MASS, elementaryWilsonLines=NY_SLICES, step=STEP,
+                             CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
+    ctx = jw.Context(cfg, device)
+    s = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    V, Vk, c = ctx.field(), ctx.field(), ctx.field(1)
+    ctx.evolve_momentum(V, 0, 0)
+    torch.cuda.synchronize()
+    ev[0].record(s)
+    ctx.initial_condition(V)
+    ev[1].record(s)
+    ctx.evolve_momentum(V, 0, 100)
+    ev[2].record(s)
+    Vk.copy_from(V)
+    ctx.execute2D(Vk, 1)
+    ctx.trace(Vk, c)
+    ctx.average_and_symmetrize(c)
+    ev[3].record(s)
+    ev[3].synchronize()
+    qs = ctx.dipole(c)[3]
+    status = ctx.sync()
+    ctx.close()
+    ic, steps, meas = (ev[i].elapsed_time(ev[i + 1]) for i in range(3))
+    out = {"workload": "1 event 64^2 FP64, MV Ny = 50, 100 fixed-coupling steps, measurement (call-for-call layer)",
+           "status": status, "total_ms": ic + steps + meas, "initial_condition_ms": ic, "steps_ms": steps,
+           "measure_ms": meas, "site_steps_per_s": n * n * 100 / (steps / 1e3), "Qs": qs}
+    t, why = run_reference_main(10, 2, n_side=n)
+    out["cpu_baseline"] = ({"value": n * n / t, "unit": "site-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                            "sample": f"main_optimized at {n}^2, 10 steps after 2 warm-up, SQRT coupling"}
+                           if t is not None else {"value": None, "unit": "site-steps/s", "cores": 0,
+                                                  "kind": "reference", "sample": why})
+    return out
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -507,6 +549,7 @@ def main_arm(args):
         line["serve"]["vs_fp64_plain"] = line["serve"]["site_steps_per_s"] / plain
         line["uneven"] = uneven_leg(jw, local, 48)
         line["position"] = position_leg(jw, local)
+        line["c1"] = c1_leg(jw, local)
         # CPU baseline: the reference's own main on a bounded sample
         t, why = run_reference_main(2, 1)
         if t is not None:

@@ -588,11 +588,14 @@ JW_EXPORT jw_status jw_evolve_momentum(jw_context* c, jw_field* V, uint64_t step
     JW_CHECK(c && V && V->ctx == c && V->t == 9 && n >= 0);
     const jw_config& cfg = c->cfg;
     if (cfg.CouplingChoice == JW_HATTA_COUPLING_CONSTANT) return JW_EUNSUPPORTED;
-    jw_field *xx = nullptr, *xy = nullptr, *A = nullptr, *B = nullptr, *ux = nullptr, *uy = nullptr;
+    for (jw_field* w : c->mom_work) JW_CHECK(V != w);
+    // work fields kept in the context: repeated calls allocate nothing
     jw_status s = JW_OK;
-    jw_field** all[6] = {&xx, &xy, &A, &B, &ux, &uy};
-    for (auto p : all)
-        if (!s) s = jw_field_create(c, 9, p);
+    for (int k = 0; k < 6 && !s; ++k)
+        if (!c->mom_work[k]) s = jw_field_create(c, 9, &c->mom_work[k]);
+    if (s) return s;
+    jw_field *xx = c->mom_work[0], *xy = c->mom_work[1], *A = c->mom_work[2], *B = c->mom_work[3],
+             *ux = c->mom_work[4], *uy = c->mom_work[5];
     const int with_coupling = cfg.CouplingChoice == JW_NOISE_COUPLING_CONSTANT;
     const int kc = cfg.CouplingChoice == JW_FIXED_COUPLING_CONSTANT ? JW_NOISE_COUPLING_CONSTANT : cfg.CouplingChoice;
     for (int k = 0; k < n && s == JW_OK; ++k) {
@@ -610,7 +613,6 @@ JW_EXPORT jw_status jw_evolve_momentum(jw_context* c, jw_field* V, uint64_t step
         if (!s) s = jw_execute2D(c, B, 0);
         if (!s) s = jw_update_uf(c, V, B, A, cfg.step);
     }
-    for (auto p : all) jw_field_destroy(*p);
     return s;
 }
 

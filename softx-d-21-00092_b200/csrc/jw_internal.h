@@ -65,6 +65,7 @@ struct jw_context {
     void* cublas = nullptr;         // cublasHandle_t (Cholesky decomposition)
     std::vector<jw_cholesky*> choleskies;  // live factors, released by jw_context_destroy
     jw_field* pos_work[4] = {};     // xi_x, xi_y, A, B of jw_evolve_position (in `fields`)
+    jw_field* mom_work[6] = {};     // xi_x, xi_y, A, B, ux, uy of jw_evolve_momentum (in `fields`)
 };
 
 namespace jw {
