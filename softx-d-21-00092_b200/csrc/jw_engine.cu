@@ -329,7 +329,7 @@ cudaError_t launch_mix_step(jw_engine* e, Group& g, const int* d_slots, int nb, 
     k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), sm2, e->stream>>>(g.d_ev, d_slots, P, Q,
                                                                                           g.tw.d32);
     if (t) { cudaEventRecord(t[3], e->stream); cudaEventRecord(t[4], e->stream); }
-    k_mix_pass3<N><<<dim3(N, nb), row_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32, e->d_flags);
+    k_mix_pass3<N><<<dim3(N, nb), mx_p3_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32, e->d_flags);
     if (t) cudaEventRecord(t[5], e->stream);
     return cudaGetLastError();
 }

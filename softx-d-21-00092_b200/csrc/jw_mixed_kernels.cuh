@@ -21,18 +21,20 @@
 
 namespace jw {
 
-// pass 1 stages V in chunks of 256 sites (36 KB) so that two CTAs fit per SM at N = 512
-template <int N> constexpr int mx_vc() { return N < 256 ? N : 256; }
+// pass 1 stages V in chunks of 256 sites (36 KB) so that two CTAs fit per SM at N = 512;
+// at N = 2048 (half the pair rows per CTA) 512 threads take 512-site chunks
+template <int N> constexpr int mx_vc() { return N >= 2048 ? 512 : (N < 256 ? N : 256); }
 template <int N> constexpr int mx_groups() {
     return (16 * padded_len16(8 * N) + 16 * 9 * mx_vc<N>()) > 220 * 1024 ? 2 : 1;
 }
-template <int N> constexpr int mx_p1_threads() { return 256; }
+template <int N> constexpr int mx_p1_threads() { return N >= 2048 ? 512 : 256; }
 template <int N> constexpr size_t mx_p1_smem() {
     return 16 * (size_t)padded_len16(8 / mx_groups<N>() * N) + 16 * 9 * (size_t)mx_vc<N>();
 }
 // pass 2 tile width: 4 columns (64-byte rows, padded) while two tiles fit in 80 KB
+// (160 KB from N = 1024 on: one CTA of 512 threads, rows of 64 or 32 bytes)
 template <int N> constexpr int mx_cols() {
-    constexpr int cap = 32768 / (N * 16);
+    constexpr int cap = (N >= 1024 ? 65536 : 32768) / (N * 16);
     constexpr int c = cap >= 4 ? 4 : (cap >= 1 ? cap : 1);
     return c < N ? c : N;
 }
@@ -48,8 +50,12 @@ template <int N> constexpr int mx_tile_len() {
     return mx_cols<N>() >= 8 ? N * mx_cols<N>() : N * mx_cols<N>() + (N / 8) * mx_cols<N>();
 }
 template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile_len<N>(); }
+// pass 3: V staged in chunks of mx_p3_vc sites (128 at N = 1024, so that two CTAs
+// fit), mx_p3_threads threads
+template <int N> constexpr int mx_p3_vc() { return N == 1024 ? 128 : v_chunk<N>(); }
+template <int N> constexpr int mx_p3_threads() { return row_threads<N>(); }
 template <int N> constexpr size_t mx_p3_smem() {
-    return 16 * (size_t)padded_len16(4 * N) + 16 * 9 * (size_t)v_chunk<N>();
+    return 16 * (size_t)padded_len16(4 * N) + 16 * 9 * (size_t)mx_p3_vc<N>();
 }
 
 // V sites [c0, c0 + VC) of row x into smV[k][VC] (16-byte copies)
@@ -231,12 +237,12 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
 
 // ------------------------------------------------------------------ pass 3
 template <int N>
-__global__ void __launch_bounds__(row_threads<N>(), 2) k_mix_pass3(EventDev* __restrict__ ev,
+__global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 ? 2 : 1) k_mix_pass3(EventDev* __restrict__ ev,
                                                                     const int* __restrict__ slots,
                                                                     const float4* __restrict__ Q,
                                                                     const float2* __restrict__ tw,
                                                                     int* __restrict__ flags) {
-    constexpr int VC = v_chunk<N>();
+    constexpr int VC = mx_p3_vc<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
     double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(4 * N));
@@ -247,7 +253,7 @@ __global__ void __launch_bounds__(row_threads<N>(), 2) k_mix_pass3(EventDev* __r
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    stage_v<N>(smV, e.V, vol, x, 0);
+    stage_v_chunk<N, VC>(smV, e.V, vol, x, 0);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(row_threads<N>(), 2) k_mix_pass3(EventDev* __r
     for (int c0 = 0; c0 < N; c0 += VC) {
         if (c0 > 0) {
             __syncthreads();
-            stage_v<N>(smV, e.V, vol, x, c0);
+            stage_v_chunk<N, VC>(smV, e.V, vol, x, c0);
             cp_async_commit();
         }
         cp_async_wait<0>();
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(meas32_rows_threads<N>(), N <= 512 ? 2 : 1) k_
 }
 
 template <int N>
-__global__ void __launch_bounds__(mx_p2_threads<N>(), 3) k_meas32_cols(const float4* __restrict__ M,
+__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 3 : 1) k_meas32_cols(const float4* __restrict__ M,
                                                                     double* __restrict__ corr,
                                                                     const float2* __restrict__ tw) {
     constexpr int C = mx_cols<N>();
