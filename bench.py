@@ -326,7 +326,8 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
     stats = srv.stats()
     srv.close()
     site_steps = sum(r["N"] ** 2 * r["steps"] for r in reqs)
-    return {"requests": n_requests, "ok": ok, "rate_req_per_s": rate,
+    mix = [(r["N"], r["ny_slices"], r["steps"]) for r in reqs]
+    return {"requests": n_requests, "ok": ok, "rate_req_per_s": rate, "_mix": mix,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "site_steps_per_s": site_steps / (t_last - t_first), "wall_s": t_last - t_first,
             "max_resident": stats.max_active,
@@ -335,6 +336,34 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
             "what": "Poisson arrivals, N log-uniform 64..2048 rounded to powers of two, steps U[10,2000], "
                     "Ny in {50,100}, mixed precision, continuous batching"
                     + (", least remaining work first per tick" if tick_sites else "")}
+
+
+def plain_fp64_times(jw, device: int, sizes) -> dict:
+    """The plain FP64 form per lattice size: one event at a time through the
+    call-for-call layer (the reference's call structure), ms per MV slice and
+    per Langevin step, timed with CUDA events."""
+    import torch
+    out = {}
+    for n in sizes:
+        cfg = jw.config_defaults(Nx=n, Ny=n, seed=3, mu=0.5 * n, mass=MASS, elementaryWilsonLines=2, step=STEP,
+                                 CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
+        ctx = jw.Context(cfg, device)
+        s = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        V = ctx.field()
+        ctx.initial_condition(V)
+        ctx.evolve_momentum(V, 0, 1)
+        ctx.sync()
+        k = 3 if n >= 1024 else 10
+        a.record(s)
+        ctx.initial_condition(V)
+        b.record(s)
+        ctx.evolve_momentum(V, 1, k)
+        c.record(s)
+        c.synchronize()
+        out[n] = {"slice_ms": a.elapsed_time(b) / 2, "step_ms": b.elapsed_time(c) / k}
+        ctx.close()
+    return out
 
 
 def uneven_leg(jw, device: int, seed: int):
@@ -547,6 +576,16 @@ def main_arm(args):
         ctx.close()
         line["serve"] = serve_leg(jw, local, args.serve_requests, 200.0, 2026, tick_sites=SERVE_TICK_SITES)
         line["serve"]["vs_fp64_plain"] = line["serve"]["site_steps_per_s"] / plain
+        # the plain FP64 form one request at a time on the same mix: MV slices and steps per request
+        mix = line["serve"].pop("_mix")
+        per_n = plain_fp64_times(jw, local, sorted({m[0] for m in mix}))
+        t_plain = sum(ny * per_n[n]["slice_ms"] + steps * per_n[n]["step_ms"] for n, ny, steps in mix) / 1e3
+        mix_rate = sum(n * n * steps for n, _, steps in mix) / t_plain
+        line["serve"]["fp64_plain_mix"] = {
+            "site_steps_per_s": mix_rate, "seconds": t_plain,
+            "per_n_ms": {str(n): v for n, v in per_n.items()},
+            "what": "each request of the same mix alone, MV slices + steps through the call-for-call FP64 layer"}
+        line["serve"]["vs_fp64_plain_mix"] = line["serve"]["site_steps_per_s"] / mix_rate
         line["uneven"] = uneven_leg(jw, local, 48)
         line["position"] = position_leg(jw, local)
         line["c1"] = c1_leg(jw, local)

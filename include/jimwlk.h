@@ -405,6 +405,10 @@ typedef struct jw_server_stats {
     double site_steps;          /* Langevin site-steps executed */
     int max_active;             /* most events resident at once */
     double now;                 /* server clock, seconds */
+    /* worker wall time, seconds, by phase: admission (device allocation),
+     * MV initial conditions, Langevin ticks (launch to completion), retiring
+     * (final measurement, S(r), release) */
+    double t_admit, t_mv, t_step, t_retire;
 } jw_server_stats;
 
 typedef struct jw_server jw_server;

@@ -59,31 +59,50 @@ bool engine_supported(int precision, int N) {
 }
 
 // prepare_A_local's kernel (field.h:1998-2075) for the SIN kernel, imaginary
-// parts of K_x and K_y divided by N^2 (the two unitary transforms).
-void kernel_table(int N, int coupling, std::vector<double>& t) {
+// parts of K_x and K_y divided by N^2 (the two unitary transforms), into
+// t64 / t32 ([2][N*N]); computed on the device when a group first needs it.
+__global__ void k_kernel_table(double* __restrict__ t64, float* __restrict__ t32, int N, int coupling) {
     const long vol = (long)N * N;
-    t.assign(2 * vol, 0.0);
-    const double inv = 1.0 / ((double)N * (double)N);
-    for (int ix = 0; ix < N; ++ix)
-        for (int iy = 0; iy < N; ++iy) {
-            const long i = (long)ix * N + iy;
-            int xx = ix, yy = iy;
-            if (xx >= N / 2) xx -= N;
-            if (yy >= N / 2) yy -= N;
-            const double px = 2.0 * M_PI * xx / (1.0 * N), py = 2.0 * M_PI * yy / (1.0 * N);
-            if (!(std::fabs(px * px + py * py) > 10e-9)) continue;
-            const double sx = std::sin(M_PI * ix / (1.0 * N)), sy = std::sin(M_PI * iy / (1.0 * N));
-            const double ph2 = 4.0 * std::pow(sx, 2.0) + 4.0 * std::pow(sy, 2.0);
-            double cc = 1.0;
-            if (coupling == JW_SQRT_COUPLING_CONSTANT)
-                cc = 4.0 * M_PI / ((11.0 - 2.0 * 3.0 / 3.0) *
-                                   std::log(std::pow(std::pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2) +
-                                                         std::pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2),
-                                                     0.2)));
-            t[i] = -2.0 * M_PI * std::sqrt(cc) * std::sin(2.0 * M_PI * ix / (1.0 * N)) / ph2 * inv;
-            t[vol + i] = -2.0 * M_PI * std::sqrt(cc) * std::sin(2.0 * M_PI * iy / (1.0 * N)) / ph2 * inv;
-        }
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    const double pi = 3.141592653589793;
+    const int ix = (int)(i / N), iy = (int)(i % N);
+    int xx = ix, yy = iy;
+    if (xx >= N / 2) xx -= N;
+    if (yy >= N / 2) yy -= N;
+    const double px = 2.0 * pi * xx / (1.0 * N), py = 2.0 * pi * yy / (1.0 * N);
+    double kx = 0.0, ky = 0.0;
+    if (fabs(px * px + py * py) > 10e-9) {
+        const double inv = 1.0 / ((double)N * (double)N);
+        const double ph2 = phat2_d(ix, iy, N);
+        double cc = 1.0;
+        if (coupling == JW_SQRT_COUPLING_CONSTANT)
+            cc = 4.0 * pi / ((11.0 - 2.0 * 3.0 / 3.0) *
+                             log(pow(pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2) + pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2),
+                                     0.2)));
+        kx = -2.0 * pi * sqrt(cc) * sin(2.0 * pi * ix / (1.0 * N)) / ph2 * inv;
+        ky = -2.0 * pi * sqrt(cc) * sin(2.0 * pi * iy / (1.0 * N)) / ph2 * inv;
+    }
+    t64[i] = kx;
+    t64[vol + i] = ky;
+    t32[i] = (float)kx;
+    t32[vol + i] = (float)ky;
 }
+
+// generate_gaussian_with_noise_coupling_constant's factor at the momentum
+// index equal to the site index (field.h:2267-2273).
+__global__ void k_noise_factor_table(double* __restrict__ t64, float* __restrict__ t32, int N) {
+    const long vol = (long)N * N;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    const double tmp = pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
+    const double tmp2 = 4.0 * 3.141592653589793 / (11.0 - 2.0 * 3.0 / 3.0);
+    const double ph2 = phat2_d((int)(i / N), (int)(i % N), N);
+    const double f = sqrt(tmp2 / log(pow(tmp + pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2), 0.2)));
+    t64[i] = f;
+    t32[i] = (float)f;
+}
+
 
 // The position kernel k_i(d) (positions.h:105-150, field.h:2402-2470) on the
 // device for all d, as complex planes [2][N*N] (real parts), with the same
@@ -150,28 +169,7 @@ __global__ void k_gather_acc(const AccSite* __restrict__ a, int n, double* __res
     for (int q = 0; q < 4; ++q) out[4 * i + q] = a[i].p[q * a[i].vol];
 }
 
-// generate_gaussian_with_noise_coupling_constant's factor at the momentum
-// index equal to the site index (field.h:2267-2273).
-void noise_factor_table(int N, std::vector<double>& t) {
-    t.resize((size_t)N * N);
-    const double tmp = std::pow(15.0 * 15.0 / 6.0 / 6.0, 1.0 / 0.2);
-    const double tmp2 = 4.0 * M_PI / (11.0 - 2.0 * 3.0 / 3.0);
-    for (int ix = 0; ix < N; ++ix)
-        for (int iy = 0; iy < N; ++iy) {
-            const double sx = std::sin(M_PI * ix / (1.0 * N)), sy = std::sin(M_PI * iy / (1.0 * N));
-            const double ph2 = 4.0 * std::pow(sx, 2.0) + 4.0 * std::pow(sy, 2.0);
-            t[(size_t)ix * N + iy] =
-                std::sqrt(tmp2 / std::log(std::pow(tmp + std::pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2), 0.2)));
-        }
-}
 
-template <typename T>
-cudaError_t upload_table(const std::vector<double>& h, T** d) {
-    std::vector<T> c(h.begin(), h.end());
-    cudaError_t e = cudaMalloc(d, sizeof(T) * c.size());
-    if (e != cudaSuccess) return e;
-    return cudaMemcpy(*d, c.data(), sizeof(T) * c.size(), cudaMemcpyHostToDevice);
-}
 
 // mean symmetrised correlator times N^2/3 as a complex plane (dipole S(r) input)
 __global__ void k_dipole_prep(const double* __restrict__ acc, double2* __restrict__ out, long vol, double scale) {
@@ -219,6 +217,8 @@ struct jw_engine {
     size_t stage_bytes = 0;
     double2* h_pinned = nullptr;  // pinned host staging
     size_t pinned_bytes = 0;
+    std::map<size_t, std::vector<void*>> pool;  // buffers of removed events, by size
+    size_t pool_bytes = 0;
 };
 
 namespace {
@@ -230,19 +230,74 @@ size_t ws_per_event(const jw_engine* e, int N) {
     return std::max(std::max(s, meas_ws_bytes(N)), mv_ws_bytes(N));
 }
 
+// Event buffers (V, accumulators, tables) of removed events are kept by size
+// for the next event of that size, so that a serving loop does not call
+// cudaMalloc and cudaFree (which synchronise the device) per request.  The
+// pool holds at most what the budget leaves free and is released when an
+// allocation would otherwise fail.
+void pool_release(jw_engine* e) {
+    if (e->pool_bytes == 0) return;
+    cudaStreamSynchronize(e->stream);
+    for (auto& kv : e->pool)
+        for (void* p : kv.second) cudaFree(p);
+    e->pool.clear();
+    e->pool_bytes = 0;
+}
+
+void* ev_alloc(jw_engine* e, size_t bytes) {
+    auto it = e->pool.find(bytes);
+    if (it != e->pool.end() && !it->second.empty()) {
+        void* p = it->second.back();
+        it->second.pop_back();
+        e->pool_bytes -= bytes;
+        return p;
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    cudaGetLastError();  // an allocation failure is not sticky: clear it
+    pool_release(e);
+    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    cudaGetLastError();
+    return nullptr;
+}
+
+// Stream-ordered reuse: every use of an event buffer is on the engine stream.
+void ev_free(jw_engine* e, void* p, size_t bytes) {
+    if (!p) return;
+    if (e->bytes_in_use + e->pool_bytes + bytes <= e->budget) {
+        e->pool[bytes].push_back(p);
+        e->pool_bytes += bytes;
+    } else {
+        cudaFree(p);
+    }
+}
+
+// The workspace of a group grows geometrically (at least doubling), within
+// the budget, so that admitting events one by one reallocates it rarely.
 jw_status ensure_workspace(jw_engine* e, Group& g, int nev) {
     if (g.ws_events >= nev) return JW_OK;
     const size_t per = ws_per_event(e, g.N);
     const size_t old = per * (size_t)g.ws_events;
-    const size_t need = per * (size_t)nev;
+    int want = std::max(nev, 2 * g.ws_events);
+    if (e->opt.max_batch > 0) want = std::min(want, std::max(nev, e->opt.max_batch));
+    if (e->bytes_in_use - old + per * (size_t)want > e->budget) want = nev;
+    const size_t need = per * (size_t)want;
     if (e->bytes_in_use - old + need > e->budget) return JW_ENOMEM;
     JW_CUDA(cudaStreamSynchronize(e->stream));
     if (g.ws) cudaFree(g.ws);
     g.ws = nullptr;
     g.ws_events = 0;
     e->bytes_in_use -= old;
-    if (cudaMalloc(&g.ws, need) != cudaSuccess) return JW_ENOMEM;
-    g.ws_events = nev;
+    if (cudaMalloc(&g.ws, need) != cudaSuccess) {
+        cudaGetLastError();
+        pool_release(e);
+        if (cudaMalloc(&g.ws, need) != cudaSuccess) {
+            cudaGetLastError();
+            g.ws = nullptr;
+            return JW_ENOMEM;
+        }
+    }
+    g.ws_events = want;
     e->bytes_in_use += need;
     return JW_OK;
 }
@@ -256,6 +311,36 @@ jw_status ensure_slots(Group& g, int n) {
     return JW_OK;
 }
 
+// The momentum-space kernel table of `coupling` (and, for NOISE, the noise
+// factor), built on the device the first time an event of the group needs it.
+jw_status ensure_tables(jw_engine* e, Group& g, int coupling) {
+    const long vol = (long)g.N * g.N;
+    const unsigned blocks = (unsigned)((vol + 255) / 256);
+    if (!g.k64[coupling]) {
+        if (cudaMalloc(&g.k64[coupling], sizeof(double) * 2 * vol) != cudaSuccess ||
+            cudaMalloc(&g.k32[coupling], sizeof(float) * 2 * vol) != cudaSuccess) {
+            if (g.k64[coupling]) cudaFree(g.k64[coupling]);
+            g.k64[coupling] = nullptr;
+            g.k32[coupling] = nullptr;
+            return JW_ENOMEM;
+        }
+        k_kernel_table<<<blocks, 256, 0, e->stream>>>(g.k64[coupling], g.k32[coupling], g.N, coupling);
+        JW_CUDA(cudaGetLastError());
+    }
+    if (coupling == JW_NOISE_COUPLING_CONSTANT && !g.nf64) {
+        if (cudaMalloc(&g.nf64, sizeof(double) * vol) != cudaSuccess ||
+            cudaMalloc(&g.nf32, sizeof(float) * vol) != cudaSuccess) {
+            if (g.nf64) cudaFree(g.nf64);
+            g.nf64 = nullptr;
+            g.nf32 = nullptr;
+            return JW_ENOMEM;
+        }
+        k_noise_factor_table<<<blocks, 256, 0, e->stream>>>(g.nf64, g.nf32, g.N);
+        JW_CUDA(cudaGetLastError());
+    }
+    return JW_OK;
+}
+
 jw_status group_get(jw_engine* e, int N, Group** out) {
     auto it = e->groups.find(N);
     if (it != e->groups.end()) {
@@ -265,15 +350,6 @@ jw_status group_get(jw_engine* e, int N, Group** out) {
     auto g = std::make_unique<Group>();
     g->N = N;
     JW_CUDA(twiddles_create(N, &g->tw));
-    std::vector<double> t;
-    for (int c : {JW_SQRT_COUPLING_CONSTANT, JW_NOISE_COUPLING_CONSTANT, JW_FIXED_COUPLING_CONSTANT}) {
-        kernel_table(N, c, t);
-        JW_CUDA(upload_table(t, &g->k64[c]));
-        JW_CUDA(upload_table(t, &g->k32[c]));
-    }
-    noise_factor_table(N, t);
-    JW_CUDA(upload_table(t, &g->nf64));
-    JW_CUDA(upload_table(t, &g->nf32));
     *out = g.get();
     e->groups[N] = std::move(g);
     return JW_OK;
@@ -601,7 +677,10 @@ JW_EXPORT jw_status jw_engine_destroy(jw_engine* e) {
     for (auto& kv : e->events) {
         cudaFree(kv.second.V);
         cudaFree(kv.second.acc);
+        if (kv.second.k64) cudaFree(kv.second.k64);
+        if (kv.second.k32) cudaFree(kv.second.k32);
     }
+    pool_release(e);
     for (auto& kv : e->groups) group_destroy(*kv.second);
     if (e->d_flags) cudaFree(e->d_flags);
     if (e->d_stage) cudaFree(e->d_stage);
@@ -652,6 +731,7 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     Group* g = nullptr;
     jw_status s = group_get(e, d->N, &g);
     if (s) return s;
+    if (!d->position_space && (s = ensure_tables(e, *g, d->coupling))) return s;
     int slot = -1;
     for (int k = 0; k < (int)g->owner.size(); ++k)
         if (g->owner[k] < 0) {
@@ -667,22 +747,26 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     ev.N = d->N;
     ev.slot = slot;
     ev.desc = *d;
-    if (cudaMalloc(&ev.V, sizeof(double2) * 9 * vol) != cudaSuccess) return JW_ENOMEM;
-    if (cudaMalloc(&ev.acc, sizeof(double) * 4 * vol) != cudaSuccess) {
-        cudaFree(ev.V);
+    const size_t bV = sizeof(double2) * 9 * vol, bA = sizeof(double) * 4 * vol;
+    const size_t b64 = sizeof(double) * 2 * vol, b32 = sizeof(float) * 2 * vol, bT = sizeof(double2) * 2 * vol;
+    ev.V = static_cast<double2*>(ev_alloc(e, bV));
+    ev.acc = static_cast<double*>(ev_alloc(e, bA));
+    if (!ev.V || !ev.acc) {
+        ev_free(e, ev.V, bV);
+        ev_free(e, ev.acc, bA);
         return JW_ENOMEM;
     }
     if (d->position_space) {
         // k_i(d), its DFT in FP64, imag / N^2 into the event's tables
-        double2* tmp = nullptr;
-        if (cudaMalloc(&ev.k64, sizeof(double) * 2 * vol) != cudaSuccess ||
-            cudaMalloc(&ev.k32, sizeof(float) * 2 * vol) != cudaSuccess ||
-            cudaMalloc(&tmp, sizeof(double2) * 2 * vol) != cudaSuccess) {
-            cudaFree(ev.V);
-            cudaFree(ev.acc);
-            if (ev.k64) cudaFree(ev.k64);
-            if (ev.k32) cudaFree(ev.k32);
-            if (tmp) cudaFree(tmp);
+        ev.k64 = static_cast<double*>(ev_alloc(e, b64));
+        ev.k32 = static_cast<float*>(ev_alloc(e, b32));
+        double2* tmp = static_cast<double2*>(ev_alloc(e, bT));
+        if (!ev.k64 || !ev.k32 || !tmp) {
+            ev_free(e, ev.V, bV);
+            ev_free(e, ev.acc, bA);
+            ev_free(e, ev.k64, b64);
+            ev_free(e, ev.k32, b32);
+            ev_free(e, tmp, bT);
             return JW_ENOMEM;
         }
         k_position_kernel<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(tmp, d->N, d->rr, d->coupling,
@@ -695,12 +779,12 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
             ce = cudaGetLastError();
         }
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-        cudaFree(tmp);
+        ev_free(e, tmp, bT);
         if (ce != cudaSuccess) {
-            cudaFree(ev.V);
-            cudaFree(ev.acc);
-            cudaFree(ev.k64);
-            cudaFree(ev.k32);
+            ev_free(e, ev.V, bV);
+            ev_free(e, ev.acc, bA);
+            ev_free(e, ev.k64, b64);
+            ev_free(e, ev.k32, b32);
             return JW_ECUDA;
         }
     }
@@ -737,11 +821,11 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     s = ensure_workspace(e, *g, chunk_size(e, resident));
     if (s) {
         g->owner[slot] = -1;
-        cudaFree(ev.V);
-        cudaFree(ev.acc);
-        if (ev.k64) cudaFree(ev.k64);
-        if (ev.k32) cudaFree(ev.k32);
         e->bytes_in_use -= own;
+        ev_free(e, ev.V, bV);
+        ev_free(e, ev.acc, bA);
+        ev_free(e, ev.k64, b64);
+        ev_free(e, ev.k32, b32);
         return s;
     }
     e->events[ev.id] = ev;
@@ -757,13 +841,13 @@ JW_EXPORT jw_status jw_engine_remove_event(jw_engine* e, int id) {
     Event& ev = it->second;
     Group& g = *e->groups[ev.N];
     g.owner[ev.slot] = -1;
-    cudaFree(ev.V);
-    cudaFree(ev.acc);
-    if (ev.k64) cudaFree(ev.k64);
-    if (ev.k32) cudaFree(ev.k32);
     const size_t vol = (size_t)ev.N * ev.N;
     e->bytes_in_use -= vol * (sizeof(double2) * 9 + sizeof(double) * 4) +
                        (ev.desc.position_space ? position_table_bytes(ev.N) : 0);
+    ev_free(e, ev.V, sizeof(double2) * 9 * vol);
+    ev_free(e, ev.acc, sizeof(double) * 4 * vol);
+    ev_free(e, ev.k64, sizeof(double) * 2 * vol);
+    ev_free(e, ev.k32, sizeof(float) * 2 * vol);
     e->events.erase(it);
     return JW_OK;
 }

@@ -173,6 +173,7 @@ struct jw_server {
     int64_t submitted = 0, completed = 0, failed = 0;
     double site_steps = 0;
     int max_active_seen = 0;
+    double t_admit = 0, t_mv = 0, t_step = 0, t_retire = 0;  // worker phases (under mu)
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
 
@@ -203,6 +204,7 @@ void worker_loop(jw_server* s) {
                 continue;
             }
             // first fit over the queue
+            const double ta = s->now();
             for (auto it = s->queue.begin(); it != s->queue.end();) {
                 if (s->opt.max_active > 0 && (int)(s->active.size() + admitted.size()) >= s->opt.max_active) break;
                 Request* r = &s->reqs[*it];
@@ -235,6 +237,7 @@ void worker_loop(jw_server* s) {
                 }
             }
             s->max_active_seen = std::max(s->max_active_seen, (int)(s->active.size() + admitted.size()));
+            s->t_admit += s->now() - ta;
         }
         // device work runs outside the lock: only this thread uses the backend
         for (Request* r : admitted) s->active.push_back(r);
@@ -268,14 +271,20 @@ void worker_loop(jw_server* s) {
                     fresh.push_back(r);
                 }
             if (!eids.empty()) {
+                const double tm = s->now();
                 const jw_status st = s->be->init_mv(eids);
-                for (Request* r : fresh) r->mv = (st == JW_OK);
-                if (st) {
+                const jw_status sy = s->be->sync();
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    s->t_mv += s->now() - tm;
+                }
+                for (Request* r : fresh) r->mv = (st == JW_OK && sy == JW_OK);
+                if (st || sy) {
                     std::vector<Request*> keep;
                     for (Request* r : s->active) {
                         if (std::find(fresh.begin(), fresh.end(), r) != fresh.end()) {
                             s->be->remove(r->eid);
-                            retire(s, r, st);
+                            retire(s, r, st ? st : sy);
                         } else {
                             keep.push_back(r);
                         }
@@ -286,6 +295,7 @@ void worker_loop(jw_server* s) {
             }
         }
         // tick: one launch group per lattice size
+        const double tt = s->now();
         std::map<int, std::vector<Request*>> by_n;
         for (Request* r : sel) by_n[r->d.N].push_back(r);
         double ss = 0;
@@ -303,9 +313,11 @@ void worker_loop(jw_server* s) {
         }
         const jw_status sst = s->be->sync();
         if (!tick_status) tick_status = sst;
+        const double tr = s->now();
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->site_steps += ss;
+            s->t_step += tr - tt;
         }
         // retire finished events (all of this tick's events if the tick failed)
         std::vector<Request*> keep;
@@ -330,6 +342,10 @@ void worker_loop(jw_server* s) {
             }
         }
         s->active.swap(keep);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->t_retire += s->now() - tr;
+        }
     }
 }
 
@@ -438,5 +454,9 @@ JW_EXPORT jw_status jw_server_get_stats(jw_server* s, jw_server_stats* st) {
     st->site_steps = s->site_steps;
     st->max_active = s->max_active_seen;
     st->now = s->now();
+    st->t_admit = s->t_admit;
+    st->t_mv = s->t_mv;
+    st->t_step = s->t_step;
+    st->t_retire = s->t_retire;
     return JW_OK;
 }

@@ -73,7 +73,8 @@ class jw_request_result(ctypes.Structure):
 class jw_server_stats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("queued", ctypes.c_int64), ("site_steps", ctypes.c_double), ("max_active", ctypes.c_int),
-                ("now", ctypes.c_double)]
+                ("now", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_mv", ctypes.c_double),
+                ("t_step", ctypes.c_double), ("t_retire", ctypes.c_double)]
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
