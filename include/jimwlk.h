@@ -264,6 +264,8 @@ typedef struct jw_engine_options {
     int reunitarize;      /* project V back onto SU(3) after every step (FP64) */
     size_t max_bytes;     /* device-memory budget for events and workspaces; 0 = 90% of free */
     int max_batch;        /* events advanced per launch group (0 = all) */
+    size_t max_batch_sites; /* and at most this many lattice sites per launch group (0 = no limit;
+                               at least one event), which also bounds each size's workspace */
 } jw_engine_options;
 
 typedef struct jw_event_desc {

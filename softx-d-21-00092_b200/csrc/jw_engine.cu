@@ -272,6 +272,8 @@ void ev_free(jw_engine* e, void* p, size_t bytes) {
     }
 }
 
+int chunk_size(const jw_engine* e, int count, int N);
+
 // The workspace of a group grows geometrically (at least doubling), within
 // the budget, so that admitting events one by one reallocates it rarely.
 jw_status ensure_workspace(jw_engine* e, Group& g, int nev) {
@@ -279,7 +281,7 @@ jw_status ensure_workspace(jw_engine* e, Group& g, int nev) {
     const size_t per = ws_per_event(e, g.N);
     const size_t old = per * (size_t)g.ws_events;
     int want = std::max(nev, 2 * g.ws_events);
-    if (e->opt.max_batch > 0) want = std::min(want, std::max(nev, e->opt.max_batch));
+    want = std::min(want, std::max(nev, chunk_size(e, 1 << 30, g.N)));
     if (e->bytes_in_use - old + per * (size_t)want > e->budget) want = nev;
     const size_t need = per * (size_t)want;
     if (e->bytes_in_use - old + need > e->budget) return JW_ENOMEM;
@@ -614,9 +616,13 @@ jw_status collect(jw_engine* e, const int* ids, int n, std::map<int, std::vector
     return JW_OK;
 }
 
-int chunk_size(const jw_engine* e, int count) {
+int chunk_size(const jw_engine* e, int count, int N) {
     int c = count;
     if (e->opt.max_batch > 0) c = std::min(c, e->opt.max_batch);
+    if (e->opt.max_batch_sites > 0) {
+        const size_t per = std::max<size_t>(1, e->opt.max_batch_sites / ((size_t)N * N));
+        c = (int)std::min<size_t>((size_t)c, per);
+    }
     return std::max(c, 1);
 }
 
@@ -818,7 +824,7 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     // workspace for every resident event of this size stepping in one launch group
     int resident = 0;
     for (int o : g->owner) resident += o >= 0;
-    s = ensure_workspace(e, *g, chunk_size(e, resident));
+    s = ensure_workspace(e, *g, chunk_size(e, resident, d->N));
     if (s) {
         g->owner[slot] = -1;
         e->bytes_in_use -= own;
@@ -969,7 +975,7 @@ JW_EXPORT jw_status jw_engine_init_mv(jw_engine* e, const int* ids, int n) {
         for (int slot : kv.second) by_ny[e->events[g.owner[slot]].desc.ny_slices].push_back(slot);
         for (auto& nv : by_ny) {
             const std::vector<int>& slots = nv.second;
-            const int cs = chunk_size(e, (int)slots.size());
+            const int cs = chunk_size(e, (int)slots.size(), g.N);
             if ((s = ensure_workspace(e, g, cs))) return s;
             if ((s = upload_slots(e, g, slots))) return s;
             for (size_t c0 = 0; c0 < slots.size(); c0 += cs) {
@@ -994,7 +1000,7 @@ JW_EXPORT jw_status jw_engine_step(jw_engine* e, const int* ids, int n, int nste
     std::vector<Work> work;
     for (auto& kv : by_n) {
         Group& g = *e->groups[kv.first];
-        const int cs = chunk_size(e, (int)kv.second.size());
+        const int cs = chunk_size(e, (int)kv.second.size(), kv.first);
         if ((s = ensure_workspace(e, g, cs))) return s;
         if ((s = upload_slots(e, g, kv.second))) return s;
         for (int c0 = 0; c0 < (int)kv.second.size(); c0 += cs)
@@ -1042,7 +1048,7 @@ JW_EXPORT jw_status jw_engine_measure(jw_engine* e, const int* ids, int n) {
     if (s) return s;
     for (auto& kv : by_n) {
         Group& g = *e->groups[kv.first];
-        const int cs = chunk_size(e, (int)kv.second.size());
+        const int cs = chunk_size(e, (int)kv.second.size(), kv.first);
         if ((s = ensure_workspace(e, g, cs))) return s;
         if ((s = upload_slots(e, g, kv.second))) return s;
         for (int c0 = 0; c0 < (int)kv.second.size(); c0 += cs)
@@ -1167,7 +1173,7 @@ JW_EXPORT jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int
     Group& g = *e->groups[by_n.begin()->first];
     const std::vector<int>& slots = by_n.begin()->second;
     const long vol = (long)g.N * g.N;
-    const int cs = chunk_size(e, (int)slots.size());
+    const int cs = chunk_size(e, (int)slots.size(), g.N);
     if ((s = ensure_workspace(e, g, cs))) return s;
     if ((s = upload_slots(e, g, slots))) return s;
     if ((s = ensure_stage(e, sizeof(double) * 4 * vol))) return s;
@@ -1197,7 +1203,7 @@ JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, in
     Group& g = *e->groups[by_n.begin()->first];
     const std::vector<int>& slots = by_n.begin()->second;
     const int nb = (int)slots.size();
-    const int cs = chunk_size(e, nb);
+    const int cs = chunk_size(e, nb, g.N);
     const int nch = (nb + cs - 1) / cs;
     if ((s = ensure_workspace(e, g, cs))) return s;
     if ((s = upload_slots(e, g, slots))) return s;

@@ -42,7 +42,7 @@ class jw_config(ctypes.Structure):
 
 class jw_engine_options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("reunitarize", ctypes.c_int), ("max_bytes", ctypes.c_size_t),
-                ("max_batch", ctypes.c_int)]
+                ("max_batch", ctypes.c_int), ("max_batch_sites", ctypes.c_size_t)]
 
 
 class jw_event_desc(ctypes.Structure):
@@ -400,8 +400,8 @@ class Engine:
     """The batched engine (jw_engine): resident events advanced by fused kernels."""
 
     def __init__(self, precision: int = PRECISION_MIXED, reunitarize: bool = False, max_bytes: int = 0,
-                 max_batch: int = 0, device: int = 0):
-        self.opt = jw_engine_options(precision, int(reunitarize), max_bytes, max_batch)
+                 max_batch: int = 0, device: int = 0, max_batch_sites: int = 0):
+        self.opt = jw_engine_options(precision, int(reunitarize), max_bytes, max_batch, max_batch_sites)
         self._h = _vp()
         _ck(_lib.jw_engine_create(ctypes.byref(self.opt), device, ctypes.byref(self._h)), "jw_engine_create")
         self.N = {}
