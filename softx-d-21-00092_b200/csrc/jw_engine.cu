@@ -441,20 +441,18 @@ cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsi
 template <int N>
 cudaError_t launch_mv_slice(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws, int slice) {
     double2* P = reinterpret_cast<double2*>(ws);
-    constexpr int RT = row_threads<N>();
-    constexpr int C = p2_cols<double, N>();
-    const size_t sm1 = sizeof(double2) * padded_len(4 * N);
-    const size_t sm2 = sizeof(double2) * padded_len(N * C);
+    const size_t r = mv16_row_smem<N>(), c = mv16_col_smem<N>();
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_mv_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-        cudaFuncSetAttribute(k_mv_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-        cudaFuncSetAttribute(k_mv_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_mv16_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r);
+        cudaFuncSetAttribute(k_mv16_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c);
+        cudaFuncSetAttribute(k_mv16_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r);
         configured = true;
     }
-    k_mv_pass1<N><<<dim3(N, nb), RT, sm1, e->stream>>>(g.d_ev, d_slots, slice, P, g.tw.d64);
-    k_mv_pass2<N><<<dim3(N / C, 4, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, g.tw.d64);
-    k_mv_pass3<N><<<dim3(N, nb), RT, sm1, e->stream>>>(g.d_ev, d_slots, P, g.tw.d64, e->d_flags);
+    k_mv16_pass1<N><<<dim3(N, nb), mv16_threads<N>(), r, e->stream>>>(g.d_ev, d_slots, slice, P, g.tw.d64);
+    k_mv16_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), c, e->stream>>>(g.d_ev, d_slots, P,
+                                                                                         g.tw.d64);
+    k_mv16_pass3<N><<<dim3(N, nb), mv16_threads<N>(), r, e->stream>>>(g.d_ev, d_slots, P, g.tw.d64, e->d_flags);
     return cudaGetLastError();
 }
 

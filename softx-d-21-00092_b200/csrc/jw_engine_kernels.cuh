@@ -346,102 +346,6 @@ __global__ void __launch_bounds__(row_threads<N>(), 2) k_step_pass3(EventDev* __
     if (x == 0 && threadIdx.x == 0) e.step += 1;
 }
 
-// ------------------------------------------------------------------ MV initial condition (FP64)
-// slice pass 1: rho_a = sigma z_a packed as 4 sequences rho_{2s} + i rho_{2s+1}, row transform.
-template <int N>
-__global__ void __launch_bounds__(row_threads<N>()) k_mv_pass1(const EventDev* __restrict__ ev,
-                                                                const int* __restrict__ slots, int slice,
-                                                                double2* __restrict__ P,
-                                                                const double2* __restrict__ tw) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* sm = reinterpret_cast<double2*>(smem_raw);
-    const int x = blockIdx.x, b = blockIdx.y;
-    const EventDev& e = ev[slots[b]];
-    const long vol = (long)N * N;
-    for (int y = threadIdx.x; y < N; y += blockDim.x) {
-        double z[8];
-        mv_normals<double>(e.seed, (uint32_t)slice, (uint32_t)((long)x * N + y), z);
-#pragma unroll
-        for (int s = 0; s < 4; ++s)
-            sm[pad(s * N + y)] = make_double2(z[2 * s] * e.mv_sigma + 0.0, z[2 * s + 1] * e.mv_sigma + 0.0);
-    }
-    __syncthreads();
-    fft_rows_smem<double, N, 4>(sm, -1.0, tw);
-    double2* out = P + (long)b * 4 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x) out[(long)(i / N) * vol + (i % N)] = sm[pad(i)];
-}
-
-// slice pass 2: column transform, x -g/(-phat2 + m^2)/N^2 (solvePoisson, field.h:867-877), inverse.
-template <int N>
-__global__ void __launch_bounds__(p2_cols<double, N>() * (N / 8)) k_mv_pass2(const EventDev* __restrict__ ev,
-                                                                              const int* __restrict__ slots,
-                                                                              double2* __restrict__ P,
-                                                                              const double2* __restrict__ tw) {
-    constexpr int C = p2_cols<double, N>();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* t0 = reinterpret_cast<double2*>(smem_raw);
-    const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
-    const EventDev& e = ev[slots[b]];
-    const long vol = (long)N * N;
-    double2* io = P + ((long)b * 4 + j) * vol + c0;
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) t0[pad(i)] = io[(long)(i / C) * N + (i % C)];
-    __syncthreads();
-    const int c = threadIdx.x % C, t = threadIdx.x / C;
-    fft_smem<double, N>(t0, ColIdx<C>{c}, t, true, -1.0, tw);
-    const double inv = 1.0 / ((double)N * (double)N);
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) {
-        const int kx = i / C, ky = c0 + i % C;
-        const double fac = -1.0 * e.mv_g / (-phat2_d(kx, ky, N) + e.mv_mass2) * inv;
-        t0[pad(i)] = cscale(t0[pad(i)], fac);
-    }
-    __syncthreads();
-    fft_smem<double, N>(t0, ColIdx<C>{c}, t, true, 1.0, tw);
-    for (int i = threadIdx.x; i < N * C; i += blockDim.x) io[(long)(i / C) * N + (i % C)] = t0[pad(i)];
-}
-
-// slice pass 3: inverse row transform, f = sum_a f_a L_a, V <- V exp(+i f) (field.h:337-365).
-template <int N>
-__global__ void __launch_bounds__(row_threads<N>()) k_mv_pass3(EventDev* __restrict__ ev,
-                                                                const int* __restrict__ slots,
-                                                                const double2* __restrict__ P,
-                                                                const double2* __restrict__ tw,
-                                                                int* __restrict__ flags) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* sm = reinterpret_cast<double2*>(smem_raw);
-    const int x = blockIdx.x, b = blockIdx.y;
-    EventDev& e = ev[slots[b]];
-    const long vol = (long)N * N;
-    const double2* in = P + (long)b * 4 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x) sm[pad(i)] = in[(long)(i / N) * vol + (i % N)];
-    __syncthreads();
-    fft_rows_smem<double, N, 4>(sm, 1.0, tw);
-    int fl = 0;
-    for (int y = threadIdx.x; y < N; y += blockDim.x) {
-        double f[8];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const double2 u = sm[pad(s * N + y)];
-            f[2 * s] = u.x;
-            f[2 * s + 1] = u.y;
-        }
-        double2 m[9], v[9], r[9];
-        embed_lambda<double>(f, m);
-        expi_ch(m, 1.0);
-        const int st = 0;
-        const long site = (long)x * N + y;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
-        mul3(v, m, r);
-        if (st) fl |= JW_FLAG_NOCONV;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            if (!isfinite(r[k].x) || !isfinite(r[k].y)) fl |= JW_FLAG_NAN;
-            e.V[k * vol + site] = r[k];
-        }
-    }
-    if (fl) atomicOr(flags, fl);
-}
-
 // average_and_symmetrize (field.h:1460-1492) + reduce (field.h:1521-1536) with
 // compensated (Neumaier) FP64 accumulation of sum and sum of squares.
 __device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {

@@ -494,4 +494,136 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     for (int q = 0; q < PER; ++q) out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
 }
 
+// ---- MV slice (setMVModel / solvePoisson / operator*=, field.h:683-757,
+// 867-877, 337-365) in FP64 on the 16-byte-element core: the 8 charge
+// coefficients of a site as 4 complex planes (r0 + i r1, ..., r6 + i r7); row
+// transform, column transform x Poisson factor x inverse column transform,
+// inverse row transform, V <- V exp(+i f).  The Poisson factor
+// -g/(-phat2 + m^2) is -g/m^2 at k = 0 (2500 for m a = 0.02): FP32 transforms
+// would put its rounding into V, so the slices stay FP64 in both precisions.
+template <int N> constexpr int mv16_threads() {
+    return 4 * (N / 8) < 64 ? 64 : (4 * (N / 8) > 256 ? 256 : 4 * (N / 8));
+}
+template <int N> constexpr size_t mv16_row_smem() { return 16 * (size_t)padded_len16(4 * N); }
+template <int N> constexpr size_t mv16_col_smem() { return 16 * (size_t)mx_tile_len<N>(); }
+
+// NP rows of the padded row buffer, in rounds of blockDim / (N/8) rows.
+template <int N, int NP>
+__device__ __forceinline__ void fft16_rows_d(double2* sm, double sign, const double2* __restrict__ tw) {
+    constexpr int TPS = N / 8;
+    const int spr = blockDim.x / TPS;
+    const int r = threadIdx.x / TPS;
+    for (int p0 = 0; p0 < NP; p0 += spr) {
+        const int pr = p0 + r;
+        fft16<double, N>(sm, RowIdx16{pr * N}, threadIdx.x % TPS, r < spr && pr < NP, sign, tw);
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(mv16_threads<N>()) k_mv16_pass1(const EventDev* __restrict__ ev,
+                                                                  const int* __restrict__ slots, int slice,
+                                                                  double2* __restrict__ P,
+                                                                  const double2* __restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int x = blockIdx.x, b = blockIdx.y;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        double z[8];
+        mv_normals<double>(e.seed, (uint32_t)slice, (uint32_t)((long)x * N + y), z);
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            sm[pad16(s * N + y)] = make_double2(z[2 * s] * e.mv_sigma + 0.0, z[2 * s + 1] * e.mv_sigma + 0.0);
+    }
+    __syncthreads();
+    fft16_rows_d<N, 4>(sm, -1.0, tw);
+    double2* out = P + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x) {
+        const int p = i / N, y = i - p * N;
+        out[p * vol + y] = sm[pad16(i)];
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 2 : 1) k_mv16_pass2(
+    const EventDev* __restrict__ ev, const int* __restrict__ slots, double2* __restrict__ P,
+    const double2* __restrict__ tw) {
+    constexpr int C = mx_cols<N>();
+    constexpr int TH = mx_p2_threads<N>();
+    constexpr int PER = N * C / TH;  // = 8
+    constexpr int RSTEP = TH / C;    // = N / 8
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* t = reinterpret_cast<double2*>(smem_raw);
+    const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
+    const ColIdx16P<C> cidx{cc};
+    double2* io = P + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) cp_async<16>(&t[cidx(r0 + q * RSTEP)], io + (long)q * RSTEP * N);
+    cp_async_commit();
+    // -g / (-phat2 + m^2) / N^2 at (kx, ky) = (r0 + q RSTEP, c0 + cc)
+    double fac[PER];
+    const double inv = 1.0 / ((double)N * (double)N);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) fac[q] = -1.0 * e.mv_g / (-phat2_d(r0 + q * RSTEP, c0 + cc, N) + e.mv_mass2) * inv;
+    cp_async_wait<0>();
+    __syncthreads();
+    fft16<double, N>(t, cidx, r0, true, -1.0, tw);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int i = cidx(r0 + q * RSTEP);
+        t[i] = cscale(t[i], fac[q]);
+    }
+    __syncthreads();
+    fft16<double, N>(t, cidx, r0, true, 1.0, tw);
+#pragma unroll 2
+    for (int q = 0; q < PER; ++q) io[(long)q * RSTEP * N] = t[cidx(r0 + q * RSTEP)];
+}
+
+template <int N>
+__global__ void __launch_bounds__(mv16_threads<N>()) k_mv16_pass3(EventDev* __restrict__ ev,
+                                                                  const int* __restrict__ slots,
+                                                                  const double2* __restrict__ P,
+                                                                  const double2* __restrict__ tw,
+                                                                  int* __restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int x = blockIdx.x, b = blockIdx.y;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const double2* in = P + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
+        cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    fft16_rows_d<N, 4>(sm, 1.0, tw);
+    int fl = 0;
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        double f[8];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double2 u = sm[pad16(s * N + y)];
+            f[2 * s] = u.x;
+            f[2 * s + 1] = u.y;
+        }
+        double2 m[9], v[9], r[9];
+        embed_lambda<double>(f, m);
+        expi_ch(m, 1.0);  // exp(+i f)
+        const long site = (long)x * N + y;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
+        mul3(v, m, r);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            if (!isfinite(r[k].x) || !isfinite(r[k].y)) fl |= JW_FLAG_NAN;
+            e.V[k * vol + site] = r[k];
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+}
+
 }  // namespace jw
