@@ -347,8 +347,16 @@ jw_status jw_engine_dipole(jw_engine* e, int event_id, double* S_xy, double* S_b
  * symmetrised correlators of main_optimized.cpp:321-334 summed over the events
  * as gfield::reduce sums them over stats (field.h:1521-1536), written to host
  * arrays sum and err (N*N complex each, reference layout t = 1).  The events'
- * own accumulators are not touched. */
+ * own accumulators are not touched.  Page-locked arrays (cudaMallocHost,
+ * cudaHostRegister) receive the result by direct device-to-host copies. */
 jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double* sum, double* err);
+/* jw_engine_step(ids, nsteps) followed by jw_engine_measure_ensemble(ids):
+ * the body of main_optimized.cpp's Langevin loop (evolution :234-304, then the
+ * measurement :317-336) as one call, with the same results.  In mixed
+ * precision up to 1024^2 the last step's third pass also row-transforms the new
+ * V for the measurement, so V is not read again. */
+jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, int nsteps, double* sum,
+                                          double* err);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
  * event around each fused kernel launch; returns the milliseconds per step
  * spent in each of the three kernels (summed over launch groups, pass_ms[3])

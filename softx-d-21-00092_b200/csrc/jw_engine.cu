@@ -26,6 +26,7 @@ struct Group {
     std::vector<int> owner;          // event id per slot, -1 if free
     int* d_slots = nullptr;          // slot lists of the current call
     int slots_cap = 0;
+    std::vector<int> h_slots;        // what d_slots holds
     unsigned char* ws = nullptr;     // workspace, ws_events events
     int ws_events = 0;
     double* k64[kCouplings] = {};    // kernel tables per coupling ([2][N*N])
@@ -49,7 +50,7 @@ struct Event {
 size_t position_table_bytes(int N) { return (sizeof(double) + sizeof(float)) * 2 * (size_t)N * N; }
 
 template <typename T> size_t step_ws_bytes(int N) { return sizeof(C2<T>) * 24 * (size_t)N * N; }
-size_t meas_ws_bytes(int N) { return (sizeof(double2) * 9 + sizeof(double)) * (size_t)N * N; }
+size_t meas_ws_bytes(int N) { return (sizeof(double2) * 9 + 2 * sizeof(double)) * (size_t)N * N; }
 size_t mv_ws_bytes(int N) { return sizeof(double2) * 4 * (size_t)N * N; }
 
 bool engine_supported(int precision, int N) {
@@ -308,6 +309,7 @@ jw_status ensure_slots(Group& g, int n) {
     if (g.slots_cap >= n) return JW_OK;
     if (g.d_slots) cudaFree(g.d_slots);
     g.d_slots = nullptr;
+    g.h_slots.clear();
     if (cudaMalloc(&g.d_slots, sizeof(int) * n) != cudaSuccess) return JW_ENOMEM;
     g.slots_cap = n;
     return JW_OK;
@@ -407,9 +409,63 @@ cudaError_t launch_mix_step(jw_engine* e, Group& g, const int* d_slots, int nb, 
     k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), sm2, e->stream>>>(g.d_ev, d_slots, P, Q,
                                                                                           g.tw.d32);
     if (t) { cudaEventRecord(t[3], e->stream); cudaEventRecord(t[4], e->stream); }
-    k_mix_pass3<N><<<dim3(N, nb), mx_p3_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32, e->d_flags);
+    k_mix_pass3<N><<<dim3(N, nb), mx_p3_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32, e->d_flags,
+                                                                        nullptr);
     if (t) cudaEventRecord(t[5], e->stream);
     return cudaGetLastError();
+}
+
+// One mixed step whose pass 3 also row-transforms the new V for the ensemble
+// measurement (the measurement planes land where P was), then the column pass
+// and the ensemble reduction: the same result as a step followed by
+// launch_measure_ensemble, without re-reading V.
+template <int N>
+cudaError_t launch_mix_step_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
+    if constexpr (!mx_p3_meas_fits<N>()) {
+        return cudaErrorInvalidValue;
+    } else {
+        const long vol = (long)N * N;
+        float4* P = reinterpret_cast<float4*>(g.ws);
+        float4* Q = P + (size_t)8 * vol * nb;
+        float4* M = P;
+        double* corr = reinterpret_cast<double*>(M + (size_t)5 * vol * nb);
+        const size_t sm1 = mx_p1_smem<N>(), sm2 = mx_p2_smem<N>(), sm3 = mx_p3_smem<N, true>();
+        static bool configured = false;
+        if (!configured) {
+            cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+            cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+            cudaFuncSetAttribute(k_mix_pass3<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
+            cudaFuncSetAttribute(k_meas32_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+            configured = true;
+        }
+        k_mix_pass1<N><<<dim3(N, mx_groups<N>(), nb), mx_p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P,
+                                                                                            g.tw.d32);
+        k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), sm2, e->stream>>>(g.d_ev, d_slots, P, Q,
+                                                                                              g.tw.d32);
+        k_mix_pass3<N, true><<<dim3(N, nb), mx_p3_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32,
+                                                                                  e->d_flags, M);
+        k_meas32_cols<N><<<dim3(N / mx_cols<N>(), nb), mx_p2_threads<N>(), sm2, e->stream>>>(M, corr, corr + vol * nb,
+                                                                                            g.tw.d32);
+        k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, corr + vol * nb, nb,
+                                                                                         ens);
+        return cudaGetLastError();
+    }
+}
+
+bool fused_measure_supported(int precision, int N) {
+    if (precision != JW_PRECISION_MIXED) return false;
+    switch (N) {
+        case 8: return mx_p3_meas_fits<8>();
+        case 16: return mx_p3_meas_fits<16>();
+        case 32: return mx_p3_meas_fits<32>();
+        case 64: return mx_p3_meas_fits<64>();
+        case 128: return mx_p3_meas_fits<128>();
+        case 256: return mx_p3_meas_fits<256>();
+        case 512: return mx_p3_meas_fits<512>();
+        case 1024: return mx_p3_meas_fits<1024>();
+        case 2048: return mx_p3_meas_fits<2048>();
+        default: return false;
+    }
 }
 
 template <typename T, int N>
@@ -474,7 +530,8 @@ cudaError_t launch_measure_kernels(jw_engine* e, Group& g, const int* d_slots, i
             configured = true;
         }
         k_meas32_rows<N><<<dim3(N, nb), meas32_rows_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, M, g.tw.d32);
-        k_meas32_cols<N><<<dim3(N / mx_cols<N>(), nb), mx_p2_threads<N>(), sm2, e->stream>>>(M, corr, g.tw.d32);
+        k_meas32_cols<N><<<dim3(N / mx_cols<N>(), nb), mx_p2_threads<N>(), sm2, e->stream>>>(M, corr, corr + vol * nb,
+                                                                                            g.tw.d32);
         *corr_out = corr;
         return cudaGetLastError();
     }
@@ -492,7 +549,7 @@ cudaError_t launch_measure_kernels(jw_engine* e, Group& g, const int* d_slots, i
     k_meas_rows<N><<<dim3((unsigned)((9L * N + RW - 1) / RW), nb), 256, sm1, e->stream>>>(g.d_ev, d_slots, M,
                                                                                        g.tw.d64);
     k_meas_cols<N><<<dim3(N / mx_cols<N>(), nb), meas_cols_threads<N>(), sm2, e->stream>>>(d_slots, M, corr,
-                                                                                          g.tw.d64);
+                                                                                          corr + vol * nb, g.tw.d64);
     *corr_out = corr;
     return cudaGetLastError();
 }
@@ -503,7 +560,8 @@ cudaError_t launch_measure(jw_engine* e, Group& g, const int* d_slots, int nb, u
     double* corr = nullptr;
     cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws, &corr);
     if (err != cudaSuccess) return err;
-    k_meas_reduce<N><<<dim3((unsigned)((vol + 255) / 256), nb), 256, 0, e->stream>>>(g.d_ev, d_slots, corr);
+    k_meas_reduce<N><<<dim3((unsigned)((vol + 255) / 256), nb), 256, 0, e->stream>>>(g.d_ev, d_slots, corr,
+                                                                                   corr + vol * nb);
     return cudaGetLastError();
 }
 
@@ -514,7 +572,7 @@ cudaError_t launch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, 
     double* corr = nullptr;
     cudaError_t err = launch_measure_kernels<N>(e, g, d_slots, nb, ws, &corr);
     if (err != cudaSuccess) return err;
-    k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, nb, ens);
+    k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, corr + vol * nb, nb, ens);
     return cudaGetLastError();
 }
 
@@ -553,6 +611,10 @@ cudaError_t dispatch_mv(jw_engine* e, Group& g, const int* d_slots, int nb, int 
 }
 cudaError_t dispatch_measure(jw_engine* e, Group& g, const int* d_slots, int nb) {
     JW_DISPATCH_N(g.N, (launch_measure<NN>(e, g, d_slots, nb, g.ws)))
+}
+
+cudaError_t dispatch_step_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
+    JW_DISPATCH_N(g.N, (launch_mix_step_measure_ensemble<NN>(e, g, d_slots, nb, ens)))
 }
 
 cudaError_t dispatch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
@@ -624,11 +686,16 @@ int chunk_size(const jw_engine* e, int count, int N) {
     return std::max(c, 1);
 }
 
+// The device slot list of a call; unchanged lists (the same events stepped
+// and measured call after call) are not uploaded again.
 jw_status upload_slots(jw_engine* e, Group& g, const std::vector<int>& slots) {
+    if (g.d_slots && g.h_slots == slots) return JW_OK;
     jw_status s = ensure_slots(g, (int)slots.size());
     if (s) return s;
+    g.h_slots.clear();
     JW_CUDA(cudaMemcpyAsync(g.d_slots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, e->stream));
     JW_CUDA(cudaStreamSynchronize(e->stream));
+    g.h_slots = slots;
     return JW_OK;
 }
 
@@ -647,6 +714,39 @@ jw_status ensure_stage(jw_engine* e, size_t bytes) {
         if (cudaMallocHost(&e->h_pinned, bytes) != cudaSuccess) return JW_ENOMEM;
         e->pinned_bytes = bytes;
     }
+    return JW_OK;
+}
+
+// True when both ends of [p, p + bytes) are page-locked host memory
+// (cudaMallocHost, cudaHostAlloc, cudaHostRegister).  Only the copy path
+// depends on it: cudaMemcpyAsync into pageable memory is correct too.
+bool host_pinned(const void* p, size_t bytes) {
+    for (const char* q : {static_cast<const char*>(p), static_cast<const char*>(p) + bytes - 1}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
+
+// Two device planes of vol complex doubles (d_out, d_out + vol) to the
+// caller's host arrays: straight into page-locked arrays, through the pinned
+// stage otherwise.
+jw_status copy_out_host(jw_engine* e, const double2* d_out, long vol, double* a, double* b) {
+    const size_t bytes = sizeof(double2) * (size_t)vol;
+    if (host_pinned(a, bytes) && host_pinned(b, bytes)) {
+        JW_CUDA(cudaMemcpyAsync(a, d_out, bytes, cudaMemcpyDeviceToHost, e->stream));
+        JW_CUDA(cudaMemcpyAsync(b, d_out + vol, bytes, cudaMemcpyDeviceToHost, e->stream));
+        JW_CUDA(cudaStreamSynchronize(e->stream));
+        return JW_OK;
+    }
+    JW_CUDA(cudaMemcpyAsync(e->h_pinned, d_out, 2 * bytes, cudaMemcpyDeviceToHost, e->stream));
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    std::memcpy(a, e->h_pinned, bytes);
+    std::memcpy(b, e->h_pinned + vol, bytes);
     return JW_OK;
 }
 
@@ -1174,21 +1274,44 @@ JW_EXPORT jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int
     const int cs = chunk_size(e, (int)slots.size(), g.N);
     if ((s = ensure_workspace(e, g, cs))) return s;
     if ((s = upload_slots(e, g, slots))) return s;
-    if ((s = ensure_stage(e, sizeof(double) * 4 * vol))) return s;
+    if ((s = ensure_stage(e, sizeof(double) * 8 * vol))) return s;
     double* ens = reinterpret_cast<double*>(e->d_stage);
+    double2* out = reinterpret_cast<double2*>(ens + 4 * vol);
     JW_CUDA(cudaMemsetAsync(ens, 0, sizeof(double) * 4 * vol, e->stream));
     for (int c0 = 0; c0 < (int)slots.size(); c0 += cs)
         JW_CUDA(dispatch_measure_ensemble(e, g, g.d_slots + c0, std::min(cs, (int)slots.size() - c0), ens));
-    double* h = reinterpret_cast<double*>(e->h_pinned);
-    JW_CUDA(cudaMemcpyAsync(h, ens, sizeof(double) * 4 * vol, cudaMemcpyDeviceToHost, e->stream));
-    JW_CUDA(cudaStreamSynchronize(e->stream));
-    for (long i = 0; i < vol; ++i) {
-        sum[2 * i] = h[i] + h[vol + i];
-        sum[2 * i + 1] = 0.0;
-        err[2 * i] = h[2 * vol + i] + h[3 * vol + i];
-        err[2 * i + 1] = 0.0;
+    k_ens_finalize<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ens, vol, out);
+    JW_CUDA(cudaGetLastError());
+    return copy_out_host(e, out, vol, sum, err);
+}
+
+JW_EXPORT jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, int nsteps, double* sum,
+                                                    double* err) {
+    JW_CHECK(e && sum && err && n > 0 && nsteps >= 1);
+    std::map<int, std::vector<int>> by_n;
+    jw_status s = collect(e, ids, n, by_n);
+    if (s) return s;
+    if (by_n.size() != 1) return JW_EINVAL;  // one lattice size per ensemble
+    if (!fused_measure_supported(e->opt.precision, by_n.begin()->first)) {
+        if ((s = jw_engine_step(e, ids, n, nsteps))) return s;
+        return jw_engine_measure_ensemble(e, ids, n, sum, err);
     }
-    return JW_OK;
+    if (nsteps > 1 && (s = jw_engine_step(e, ids, n, nsteps - 1))) return s;
+    Group& g = *e->groups[by_n.begin()->first];
+    const std::vector<int>& slots = by_n.begin()->second;
+    const long vol = (long)g.N * g.N;
+    const int cs = chunk_size(e, (int)slots.size(), g.N);
+    if ((s = ensure_workspace(e, g, cs))) return s;
+    if ((s = upload_slots(e, g, slots))) return s;
+    if ((s = ensure_stage(e, sizeof(double) * 8 * vol))) return s;
+    double* ens = reinterpret_cast<double*>(e->d_stage);
+    double2* out = reinterpret_cast<double2*>(ens + 4 * vol);
+    JW_CUDA(cudaMemsetAsync(ens, 0, sizeof(double) * 4 * vol, e->stream));
+    for (int c0 = 0; c0 < (int)slots.size(); c0 += cs)
+        JW_CUDA(dispatch_step_measure_ensemble(e, g, g.d_slots + c0, std::min(cs, (int)slots.size() - c0), ens));
+    k_ens_finalize<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ens, vol, out);
+    JW_CUDA(cudaGetLastError());
+    return copy_out_host(e, out, vol, sum, err);
 }
 
 JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms,

@@ -354,19 +354,29 @@ __device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
     s = t;
 }
 
+// corr and corrT hold each event's correlator and its transpose
+// (corrT[q][p] = corr[p][q]), so that every load below is coalesced.
+template <int N>
+__device__ __forceinline__ double symmetrized(const double* __restrict__ cb, const double* __restrict__ cbT,
+                                              int x, int y) {
+    const int a = (N - x) % N, bb = (N - y) % N;
+    auto tsym = [&](int p, int q) {
+        const long o = (long)p * N + q;
+        return 0.5 * (__ldg(cb + o) + __ldg(cbT + o));
+    };
+    return 0.25 * (((tsym(x, y) + tsym(a, y)) + tsym(x, bb)) + tsym(a, bb));
+}
+
 template <int N>
 __global__ void k_meas_reduce(EventDev* __restrict__ ev, const int* __restrict__ slots,
-                              const double* __restrict__ corr) {
+                              const double* __restrict__ corr, const double* __restrict__ corrT) {
     const long vol = (long)N * N;
     const int b = blockIdx.y;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     EventDev& e = ev[slots[b]];
     if (i < vol) {
-        const double* cb = corr + (long)b * vol;
         const int x = (int)(i / N), y = (int)(i % N);
-        const int a = (N - x) % N, bb = (N - y) % N;
-        auto tsym = [&](int p, int q) { return 0.5 * (cb[(long)p * N + q] + cb[(long)q * N + p]); };
-        const double s = 0.25 * (((tsym(x, y) + tsym(a, y)) + tsym(x, bb)) + tsym(a, bb));
+        const double s = symmetrized<N>(corr + (long)b * vol, corrT + (long)b * vol, x, y);
         double* acc = e.acc;
         double s0 = acc[i], s1 = acc[vol + i], e0 = acc[2 * vol + i], e1 = acc[3 * vol + i];
         neumaier_add(s0, s1, s);
@@ -383,17 +393,16 @@ __global__ void k_meas_reduce(EventDev* __restrict__ ev, const int* __restrict__
 // batch and add their sum and sum of squares (over events) into ens[4][N*N]
 // (sum, compensation, err, compensation) -- gfield::reduce over stats.
 template <int N>
-__global__ void k_meas_reduce_ensemble(const double* __restrict__ corr, int nb, double* __restrict__ ens) {
+__global__ void k_meas_reduce_ensemble(const double* __restrict__ corr, const double* __restrict__ corrT, int nb,
+                                       double* __restrict__ ens) {
     const long vol = (long)N * N;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= vol) return;
     const int x = (int)(i / N), y = (int)(i % N);
-    const int a = (N - x) % N, bb = (N - y) % N;
     double s0 = ens[i], s1 = ens[vol + i], e0 = ens[2 * vol + i], e1 = ens[3 * vol + i];
+#pragma unroll 4
     for (int b = 0; b < nb; ++b) {
-        const double* cb = corr + (long)b * vol;
-        auto tsym = [&](int p, int q) { return 0.5 * (cb[(long)p * N + q] + cb[(long)q * N + p]); };
-        const double s = 0.25 * (((tsym(x, y) + tsym(a, y)) + tsym(x, bb)) + tsym(a, bb));
+        const double s = symmetrized<N>(corr + (long)b * vol, corrT + (long)b * vol, x, y);
         neumaier_add(s0, s1, s);
         neumaier_add(e0, e1, s * s);
     }
@@ -401,6 +410,15 @@ __global__ void k_meas_reduce_ensemble(const double* __restrict__ corr, int nb, 
     ens[vol + i] = s1;
     ens[2 * vol + i] = e0;
     ens[3 * vol + i] = e1;
+}
+
+// The ensemble's compensated sums as the reference's complex fields
+// (sum, err), each vol complex doubles with zero imaginary part.
+__global__ void k_ens_finalize(const double* __restrict__ ens, long vol, double2* __restrict__ out) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vol) return;
+    out[i] = make_double2(ens[i] + ens[vol + i], 0.0);
+    out[vol + i] = make_double2(ens[2 * vol + i] + ens[3 * vol + i], 0.0);
 }
 
 }  // namespace jw

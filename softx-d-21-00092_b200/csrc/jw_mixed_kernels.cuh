@@ -54,9 +54,13 @@ template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile
 // fit), mx_p3_threads threads
 template <int N> constexpr int mx_p3_vc() { return N == 1024 ? 128 : v_chunk<N>(); }
 template <int N> constexpr int mx_p3_threads() { return row_threads<N>(); }
-template <int N> constexpr size_t mx_p3_smem() {
-    return 16 * (size_t)padded_len16(4 * N) + 16 * 9 * (size_t)mx_p3_vc<N>();
+// MEAS: pass 3 also leaves the row-transformed measurement planes of the new V
+// (5 FP32 pair planes, as k_meas32_rows writes them) in a fifth row of shared
+// memory; up to 1024^2, where two such CTAs still fit on an SM
+template <int N, bool MEAS = false> constexpr size_t mx_p3_smem() {
+    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N) + 16 * 9 * (size_t)mx_p3_vc<N>();
 }
+template <int N> constexpr bool mx_p3_meas_fits() { return mx_p3_smem<N, true>() <= 112 * 1024; }
 
 // V sites [c0, c0 + VC) of row x into smV[k][VC] (16-byte copies)
 template <int N, int VC>
@@ -236,16 +240,17 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
 }
 
 // ------------------------------------------------------------------ pass 3
-template <int N>
+template <int N, bool MEAS = false>
 __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 ? 2 : 1) k_mix_pass3(EventDev* __restrict__ ev,
                                                                     const int* __restrict__ slots,
                                                                     const float4* __restrict__ Q,
                                                                     const float2* __restrict__ tw,
-                                                                    int* __restrict__ flags) {
+                                                                    int* __restrict__ flags,
+                                                                    float4* __restrict__ M) {
     constexpr int VC = mx_p3_vc<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
-    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(4 * N));
+    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N));
     const int x = blockIdx.x, b = blockIdx.y;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
@@ -294,10 +299,28 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 
                 if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
                 e.V[k * vol + site] = v[k];
             }
+            if constexpr (MEAS) {
+                // entries 2p, 2p + 1 of the new V as pair element (p, y); this
+                // thread alone has read or written column y of the row buffer
+#pragma unroll
+                for (int p = 0; p < 5; ++p) {
+                    const double2 hi = p < 4 ? v[2 * p + 1] : make_double2(0.0, 0.0);
+                    sm[pad16(p * N + y)] = make_float4((float)v[2 * p].x, (float)v[2 * p].y, (float)hi.x, (float)hi.y);
+                }
+            }
         }
     }
     if (fl) atomicOr(flags, fl);
     if (x == 0 && threadIdx.x == 0) e.step += 1;
+    if constexpr (MEAS) {
+        __syncthreads();
+        fft16_rows<N, 5>(sm, -1.0f, tw);
+        float4* out = M + (long)b * 5 * vol + (long)x * N;
+        for (int i = threadIdx.x; i < 5 * N; i += blockDim.x) {
+            const int p = i / N, y = i - p * N;
+            out[p * vol + y] = sm[pad16(i)];
+        }
+    }
 }
 
 // ------------------------------------------------------------------ measurement (FP64)
@@ -345,6 +368,7 @@ template <int N>
 __global__ void __launch_bounds__(meas_cols_threads<N>()) k_meas_cols(const int* __restrict__ slots,
                                                                        const double2* __restrict__ M,
                                                                        double* __restrict__ corr,
+                                                                       double* __restrict__ corrT,
                                                                        const double2* __restrict__ tw) {
     constexpr int C = mx_cols<N>();
     constexpr int TH = meas_cols_threads<N>();
@@ -388,8 +412,12 @@ __global__ void __launch_bounds__(meas_cols_threads<N>()) k_meas_cols(const int*
     const double n2 = (double)N * (double)N;
     const double inv = 1.0 / (n2 * n2 * n2);
     double* out = corr + (long)b * vol + c0 + cc;
+    double* outT = corrT + (long)b * vol + (long)(c0 + cc) * N + r0;
 #pragma unroll
-    for (int q = 0; q < PER; ++q) out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
+    for (int q = 0; q < PER; ++q) {
+        out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
+        outT[q * RSTEP] = acc[q] * inv;
+    }
     (void)slots;
 }
 
@@ -447,6 +475,7 @@ __global__ void __launch_bounds__(meas32_rows_threads<N>(), N <= 512 ? 2 : 1) k_
 template <int N>
 __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 3 : 1) k_meas32_cols(const float4* __restrict__ M,
                                                                     double* __restrict__ corr,
+                                                                    double* __restrict__ corrT,
                                                                     const float2* __restrict__ tw) {
     constexpr int C = mx_cols<N>();
     constexpr int TH = mx_p2_threads<N>();
@@ -490,8 +519,12 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     const double n2 = (double)N * (double)N;
     const double inv = 1.0 / (n2 * n2 * n2);
     double* out = corr + (long)b * vol + c0 + cc;
+    double* outT = corrT + (long)b * vol + (long)(c0 + cc) * N + r0;
 #pragma unroll
-    for (int q = 0; q < PER; ++q) out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
+    for (int q = 0; q < PER; ++q) {
+        out[(long)(r0 + q * RSTEP) * N] = acc[q] * inv;
+        outT[q * RSTEP] = acc[q] * inv;
+    }
 }
 
 // ---- MV slice (setMVModel / solvePoisson / operator*=, field.h:683-757,

@@ -158,6 +158,8 @@ def _load():
         "jw_engine_dipole": ([_vp, ctypes.c_int, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                               ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
         "jw_engine_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp], ctypes.c_int),
+        "jw_engine_step_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
+                                            ctypes.c_int),
         "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
                                  ctypes.c_int),
     }
@@ -534,6 +536,18 @@ class Engine:
         arr, n = _ids(ids)
         _ck(_lib.jw_engine_measure_ensemble(self._h, arr, n, s.ctypes.data_as(_dp), e.ctypes.data_as(_dp)),
             "jw_engine_measure_ensemble")
+        return s, e
+
+    def step_measure_ensemble(self, ids, nsteps: int = 1, sum_out: np.ndarray | None = None,
+                              err_out: np.ndarray | None = None):
+        """nsteps Langevin steps of the events, then one ensemble measurement."""
+        ids = list(ids)
+        N = self.N[ids[0]]
+        s = np.empty((N, N), np.complex128) if sum_out is None else sum_out
+        e = np.empty((N, N), np.complex128) if err_out is None else err_out
+        arr, n = _ids(ids)
+        _ck(_lib.jw_engine_step_measure_ensemble(self._h, arr, n, int(nsteps), s.ctypes.data_as(_dp),
+                                                 e.ctypes.data_as(_dp)), "jw_engine_step_measure_ensemble")
         return s, e
 
     def step_timed(self, ids, nsteps: int):
