@@ -52,13 +52,16 @@ template <int N> constexpr int mx_tile_len() {
 template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile_len<N>(); }
 // pass 3: V staged in chunks of mx_p3_vc sites (128 at N = 1024, so that two CTAs
 // fit), mx_p3_threads threads
-template <int N> constexpr int mx_p3_vc() { return N == 1024 ? 128 : v_chunk<N>(); }
+template <int N, bool MEAS = false> constexpr int mx_p3_vc() {
+    return N == 1024 ? 128 : (MEAS && N == 512 ? 256 : v_chunk<N>());
+}
 template <int N> constexpr int mx_p3_threads() { return row_threads<N>(); }
 // MEAS: pass 3 also leaves the row-transformed measurement planes of the new V
 // (5 FP32 pair planes, as k_meas32_rows writes them) in a fifth row of shared
-// memory; up to 1024^2, where two such CTAs still fit on an SM
+// memory, with V chunks of 256 sites at 512^2; up to 1024^2, where two such
+// CTAs still fit on an SM
 template <int N, bool MEAS = false> constexpr size_t mx_p3_smem() {
-    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N) + 16 * 9 * (size_t)mx_p3_vc<N>();
+    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N) + 16 * 9 * (size_t)mx_p3_vc<N, MEAS>();
 }
 template <int N> constexpr bool mx_p3_meas_fits() { return mx_p3_smem<N, true>() <= 112 * 1024; }
 
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 
                                                                     const float2* __restrict__ tw,
                                                                     int* __restrict__ flags,
                                                                     float4* __restrict__ M) {
-    constexpr int VC = mx_p3_vc<N>();
+    constexpr int VC = mx_p3_vc<N, MEAS>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
     double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N));

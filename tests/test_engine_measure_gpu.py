@@ -65,6 +65,7 @@ def test_ensemble_is_sum_of_event_measurements(jw, precision):
 @pytest.mark.parametrize("precision,N,events,max_batch", [
     ("mixed", 64, 5, 2),      # fused, three launch groups
     ("mixed", 512, 3, 0),     # fused
+    ("mixed", 1024, 2, 0),    # fused
     ("mixed", 2048, 1, 0),    # step, then the separate measurement kernels
     ("fp64", 64, 3, 0),       # FP64 engine: step, then the FP64 measurement
 ])
