@@ -278,6 +278,132 @@ __device__ __forceinline__ void fft16_passes(typename Elem16<T>::E* sm, const Id
     }
 }
 
+// Register hand-off.  After the last pass thread t holds the elements
+// t + m N/8 (m = 0..7) of its sequences, and the first pass reads exactly those
+// elements.  So a transform can end in registers (for an elementwise step, a
+// reduction or a store) and the next one start from them, without the shared-
+// memory round trip.  reg[l][m] is element t + m N/8 of sequence l.
+template <typename T, int N, int Ns, int R, bool IN, bool OUT, typename IdxF>
+__device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
+                                                 bool active, T sign, const C2<T>* __restrict__ tw,
+                                                 C2<T> (&reg)[Elem16<T>::VL][8]) {
+    using V = C2<T>;
+    constexpr int VL = Elem16<T>::VL;
+    constexpr int B = 8 / R;
+    constexpr int NB = N / R;
+    constexpr int TPS = N / 8;
+    constexpr int TWS = N / (Ns * R);
+    static_assert(!IN || Ns == 1, "register input feeds the first pass");
+    static_assert(!OUT || Ns * R == N, "register output comes from the last pass");
+    V v[VL][8];
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int b = t + q * TPS;
+            const int k = b & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if constexpr (IN) {
+#pragma unroll
+                    for (int l = 0; l < VL; ++l) v[l][q * R + r] = reg[l][q + r * B];  // element b + r NB
+                } else {
+                    V u[VL];
+                    unpack16(sm[idx(b + r * NB)], u);
+#pragma unroll
+                    for (int l = 0; l < VL; ++l) v[l][q * R + r] = u[l];
+                }
+            }
+            if (Ns > 1) {
+                V w[8];
+                w[1] = tw_load(tw, k * TWS, sign);
+                if constexpr (R >= 4) w[2] = tw_load(tw, 2 * k * TWS, sign);
+                if constexpr (R == 4) w[3] = cmul(w[1], w[2]);
+                if constexpr (R == 8) {
+                    w[4] = tw_load(tw, 4 * k * TWS, sign);
+                    w[3] = cmul(w[1], w[2]);
+                    w[5] = cmul(w[4], w[1]);
+                    w[6] = cmul(w[4], w[2]);
+                    w[7] = cmul(w[4], w[3]);
+                }
+#pragma unroll
+                for (int r = 1; r < R; ++r)
+#pragma unroll
+                    for (int l = 0; l < VL; ++l) v[l][q * R + r] = cmul(v[l][q * R + r], w[r]);
+            }
+#pragma unroll
+            for (int l = 0; l < VL; ++l) {
+                if constexpr (R == 8) {
+                    bfly8<V, T>(v[l], sign);
+                } else if constexpr (R == 4) {
+                    bfly4<V, T>(v[l][q * 4 + 0], v[l][q * 4 + 1], v[l][q * 4 + 2], v[l][q * 4 + 3], sign);
+                } else {
+                    bfly2<V, T>(v[l][q * 2 + 0], v[l][q * 2 + 1]);
+                }
+            }
+        }
+    }
+    if constexpr (OUT) {
+        // output b + r Ns = t + (q + r B) N/8; the caller synchronises before
+        // the buffer is written again
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < B; ++q)
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int l = 0; l < VL; ++l) reg[l][q + r * B] = v[l][q * R + r];
+        }
+    } else {
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < B; ++q) {
+                const int b = t + q * TPS;
+                const int k = b & (Ns - 1);
+                const int base = (b / Ns) * Ns * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    V u[VL];
+#pragma unroll
+                    for (int l = 0; l < VL; ++l) u[l] = v[l][q * R + r];
+                    sm[idx(base + r * Ns)] = pack16(u);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int N, int Ns, bool IN, bool OUT, typename IdxF>
+__device__ __forceinline__ void fft16x_passes(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
+                                              const C2<T>* __restrict__ tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
+    if constexpr (Ns < N) {
+        constexpr int rem = N / Ns;
+        constexpr int R = rem >= 8 ? 8 : rem;
+        stockham_pass16x<T, N, Ns, R, IN && Ns == 1, OUT && Ns * R == N>(sm, idx, t, active, sign, tw, reg);
+        fft16x_passes<T, N, Ns * R, IN, OUT>(sm, idx, t, active, sign, tw, reg);
+    }
+}
+
+// fft16 with the first pass reading reg (IN) and/or the last pass writing reg
+// (OUT) instead of sm; sm still carries the passes in between.
+template <typename T, int N, bool IN, bool OUT, typename IdxF>
+__device__ __forceinline__ void fft16x(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
+                                       const C2<T>* __restrict__ tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
+    static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two N >= 8");
+    fft16x_passes<T, N, 1, IN, OUT>(sm, idx, t, active, sign, tw, reg);
+}
+
+__device__ __forceinline__ void reg_get(const float4& e, float2 (&reg)[2][8], int m) {
+    reg[0][m] = make_float2(e.x, e.y);
+    reg[1][m] = make_float2(e.z, e.w);
+}
+__device__ __forceinline__ float4 reg_put(const float2 (&reg)[2][8], int m) {
+    return make_float4(reg[0][m].x, reg[0][m].y, reg[1][m].x, reg[1][m].y);
+}
+__device__ __forceinline__ void reg_get(const double2& e, double2 (&reg)[1][8], int m) { reg[0][m] = e; }
+__device__ __forceinline__ double2 reg_put(const double2 (&reg)[1][8], int m) { return reg[0][m]; }
+
 // Transform the VL sequences held in the elements sm[idx(e)], e < N, with
 // thread t < N/8; all threads of the CTA must call it.
 template <typename T, int N, typename IdxF>

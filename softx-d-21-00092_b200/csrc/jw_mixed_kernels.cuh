@@ -114,6 +114,28 @@ __device__ __forceinline__ void fft16_rows(float4* sm, float sign, const float2*
     }
 }
 
+// np rows of the padded row buffer, transformed, the last pass storing row p
+// straight to out + p stride (no shared-memory round trip for the result)
+template <typename T, int N>
+__device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int np, T sign,
+                                                 const C2<T>* __restrict__ tw, typename Elem16<T>::E* __restrict__ out,
+                                                 long stride) {
+    constexpr int TPS = N / 8;
+    const int spr = blockDim.x / TPS;
+    const int r = threadIdx.x / TPS, t = threadIdx.x % TPS;
+    for (int p0 = 0; p0 < np; p0 += spr) {
+        const int p = p0 + r;
+        const bool act = r < spr && p < np;
+        C2<T> rv[Elem16<T>::VL][8];
+        fft16x<T, N, false, true>(sm, RowIdx16{p * N}, t, act, sign, tw, rv);
+        if (act) {
+            typename Elem16<T>::E* o = out + (long)p * stride + t;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) o[(long)m * TPS] = reg_put(rv, m);
+        }
+    }
+}
+
 // ------------------------------------------------------------------ pass 1
 template <int N>
 __global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev* __restrict__ ev,
@@ -179,17 +201,17 @@ __global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev
         }
     }
     __syncthreads();
-    fft16_rows<N, NP>(sm, -1.0f, tw);
-    float4* out = P + ((long)b * 8 + NP * g) * vol + (long)x * N;
-    for (int i = threadIdx.x; i < NP * N; i += blockDim.x) {
-        const int p = i / N, y = i - p * N;
-        out[p * vol + y] = sm[pad16(i)];
-    }
+    fft16_rows_store<float, N>(sm, NP, -1.0f, tw, P + ((long)b * 8 + NP * g) * vol + (long)x * N, vol);
 }
 
 // ------------------------------------------------------------------ pass 2
+// Column transforms of planes j (n_x, packed) and 4 + j (n_y), W = (i K_x) X +
+// (i K_y) Y per column element, inverse transform of W.  Thread (cc, r0)
+// holds rows r0 + m N/8 of column cc between the transforms (fft16x), so the
+// plane-j transform starts from global loads, the kernel product and the
+// inverse start from registers and the inverse ends in the store.
 template <int N>
-__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 3 : 1) k_mix_pass2(const EventDev* __restrict__ ev,
+__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 2 : 1) k_mix_pass2(const EventDev* __restrict__ ev,
                                                                    const int* __restrict__ slots,
                                                                    const float4* __restrict__ P,
                                                                    float4* __restrict__ Q,
@@ -197,6 +219,7 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     constexpr int C = mx_cols<N>();
     constexpr int TH = mx_p2_threads<N>();
     constexpr int PER = N * C / TH;  // = 8
+    static_assert(PER == 8, "one radix-8 lane per thread and column");
     constexpr int TL = mx_tile_len<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* ta = reinterpret_cast<float4*>(smem_raw);
@@ -210,12 +233,11 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     const float4* ina = P + ((long)b * 8 + j) * vol + c0 + (long)r0 * N + cc;
     const float4* inb = P + ((long)b * 8 + 4 + j) * vol + c0 + (long)r0 * N + cc;
 #pragma unroll 1
-    for (int q = 0; q < PER; ++q) {
-        const int row = r0 + q * RSTEP;
-        cp_async<16>(&ta[cidx(row)], ina + (long)q * RSTEP * N);
-        cp_async<16>(&tb[cidx(row)], inb + (long)q * RSTEP * N);
-    }
+    for (int q = 0; q < PER; ++q) cp_async<16>(&tb[cidx(r0 + q * RSTEP)], inb + (long)q * RSTEP * N);
     cp_async_commit();
+    float2 ra[2][8];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) reg_get(__ldg(ina + (long)q * RSTEP * N), ra, q);
     const float* kt = e.k32 + c0 + (long)r0 * N + cc;
     float kx[PER], ky[PER];
 #pragma unroll
@@ -223,23 +245,23 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
         kx[q] = __ldg(kt + (long)q * RSTEP * N);
         ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
     }
+    // (i kx) X + (i ky) Y, X and Y the two halves of a plane element
+    fft16x<float, N, true, true>(ta, cidx, r0, true, -1.0f, tw, ra);
+    float2 w[2][8];
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+        w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
     cp_async_wait<0>();
     __syncthreads();
-    fft16<float, N>(ta, cidx, r0, true, -1.0f, tw);
-    fft16<float, N>(tb, cidx, r0, true, -1.0f, tw);
+    fft16x<float, N, false, true>(tb, cidx, r0, true, -1.0f, tw, ra);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int i = cidx(r0 + q * RSTEP);
-        const float4 a = ta[i], bb = tb[i];
-        // (i kx) X + (i ky) Y  and  (i kx) BX + (i ky) BY
-        ta[i] = make_float4(-kx[q] * a.y - ky[q] * a.w, kx[q] * a.x + ky[q] * a.z,
-                            -kx[q] * bb.y - ky[q] * bb.w, kx[q] * bb.x + ky[q] * bb.z);
-    }
-    __syncthreads();
-    fft16<float, N>(ta, cidx, r0, true, 1.0f, tw);
+    for (int q = 0; q < PER; ++q)
+        w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+    // every thread has passed a barrier since its last read of ta
+    fft16x<float, N, true, true>(ta, cidx, r0, true, 1.0f, tw, w);
     float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
-#pragma unroll 2
-    for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = ta[cidx(r0 + q * RSTEP)];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = reg_put(w, q);
 }
 
 // ------------------------------------------------------------------ pass 3
@@ -317,12 +339,7 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 
     if (x == 0 && threadIdx.x == 0) e.step += 1;
     if constexpr (MEAS) {
         __syncthreads();
-        fft16_rows<N, 5>(sm, -1.0f, tw);
-        float4* out = M + (long)b * 5 * vol + (long)x * N;
-        for (int i = threadIdx.x; i < 5 * N; i += blockDim.x) {
-            const int p = i / N, y = i - p * N;
-            out[p * vol + y] = sm[pad16(i)];
-        }
+        fft16_rows_store<float, N>(sm, 5, -1.0f, tw, M + (long)b * 5 * vol + (long)x * N, vol);
     }
 }
 
@@ -341,7 +358,6 @@ template <int N>
 __global__ void __launch_bounds__(256) k_meas_rows(const EventDev* __restrict__ ev, const int* __restrict__ slots,
                                                    double2* __restrict__ M, const double2* __restrict__ tw) {
     constexpr int RW = meas_rows16<N>();
-    constexpr int TPS = N / 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* sm = reinterpret_cast<double2*>(smem_raw);
     const int b = blockIdx.y;
@@ -354,13 +370,7 @@ __global__ void __launch_bounds__(256) k_meas_rows(const EventDev* __restrict__ 
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
-    const int spr = blockDim.x / TPS, r = threadIdx.x / TPS;
-    for (int p0 = 0; p0 < nr; p0 += spr) {
-        const int pr = p0 + r;
-        fft16<double, N>(sm, RowIdx16{pr * N}, threadIdx.x % TPS, r < spr && pr < nr, -1.0, tw);
-    }
-    double2* out = M + (long)b * 9 * vol + row0 * N;
-    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) out[i] = sm[pad16(i)];
+    fft16_rows_store<double, N>(sm, nr, -1.0, tw, M + (long)b * 9 * vol + row0 * N, N);
 }
 
 // columns: tiles of C columns, the 9 components double-buffered with cp.async
@@ -403,13 +413,10 @@ __global__ void __launch_bounds__(meas_cols_threads<N>()) k_meas_cols(const int*
             cp_async_wait<0>();
         }
         __syncthreads();
-        double2* t = tile[comp & 1];
-        fft16<double, N>(t, cidx, r0, true, -1.0, tw);
+        double2 rv[1][8];
+        fft16x<double, N, false, true>(tile[comp & 1], cidx, r0, true, -1.0, tw, rv);
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const double2 v = t[cidx(r0 + q * RSTEP)];
-            acc[q] += v.x * v.x + v.y * v.y;
-        }
+        for (int q = 0; q < PER; ++q) acc[q] += rv[0][q].x * rv[0][q].x + rv[0][q].y * rv[0][q].y;
         __syncthreads();
     }
     const double n2 = (double)N * (double)N;
@@ -467,12 +474,7 @@ __global__ void __launch_bounds__(meas32_rows_threads<N>(), N <= 512 ? 2 : 1) k_
     for (int y = threadIdx.x; y < N; y += TH)
         reinterpret_cast<float2*>(&sm[pad16(4 * N + y)])[1] = make_float2(0.0f, 0.0f);
     __syncthreads();
-    fft16_rows<N, 5>(sm, -1.0f, tw);
-    float4* out = M + (long)b * 5 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 5 * N; i += blockDim.x) {
-        const int p = i / N, y = i - p * N;
-        out[p * vol + y] = sm[pad16(i)];
-    }
+    fft16_rows_store<float, N>(sm, 5, -1.0f, tw, M + (long)b * 5 * vol + (long)x * N, vol);
 }
 
 template <int N>
@@ -510,13 +512,12 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
             cp_async_wait<0>();
         }
         __syncthreads();
-        float4* t = tile[p & 1];
-        fft16<float, N>(t, cidx, r0, true, -1.0f, tw);
+        float2 rv[2][8];
+        fft16x<float, N, false, true>(tile[p & 1], cidx, r0, true, -1.0f, tw, rv);
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const float4 v = t[cidx(r0 + q * RSTEP)];
-            acc[q] += ((double)v.x * v.x + (double)v.y * v.y) + ((double)v.z * v.z + (double)v.w * v.w);
-        }
+        for (int q = 0; q < PER; ++q)
+            acc[q] += ((double)rv[0][q].x * rv[0][q].x + (double)rv[0][q].y * rv[0][q].y) +
+                      ((double)rv[1][q].x * rv[1][q].x + (double)rv[1][q].y * rv[1][q].y);
         __syncthreads();
     }
     const double n2 = (double)N * (double)N;
@@ -573,14 +574,12 @@ __global__ void __launch_bounds__(mv16_threads<N>()) k_mv16_pass1(const EventDev
             sm[pad16(s * N + y)] = make_double2(z[2 * s] * e.mv_sigma + 0.0, z[2 * s + 1] * e.mv_sigma + 0.0);
     }
     __syncthreads();
-    fft16_rows_d<N, 4>(sm, -1.0, tw);
-    double2* out = P + (long)b * 4 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x) {
-        const int p = i / N, y = i - p * N;
-        out[p * vol + y] = sm[pad16(i)];
-    }
+    fft16_rows_store<double, N>(sm, 4, -1.0, tw, P + (long)b * 4 * vol + (long)x * N, vol);
 }
 
+// column transform, Poisson factor and inverse column transform with the
+// register hand-off of fft16x: global loads feed the first pass, the factor
+// and the inverse start from registers, the inverse ends in the store
 template <int N>
 __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 2 : 1) k_mv16_pass2(
     const EventDev* __restrict__ ev, const int* __restrict__ slots, double2* __restrict__ P,
@@ -589,6 +588,7 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     constexpr int TH = mx_p2_threads<N>();
     constexpr int PER = N * C / TH;  // = 8
     constexpr int RSTEP = TH / C;    // = N / 8
+    static_assert(PER == 8, "one radix-8 lane per thread and column");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* t = reinterpret_cast<double2*>(smem_raw);
     const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
@@ -597,26 +597,19 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
     const ColIdx16P<C> cidx{cc};
     double2* io = P + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
+    double2 rv[1][8];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) cp_async<16>(&t[cidx(r0 + q * RSTEP)], io + (long)q * RSTEP * N);
-    cp_async_commit();
+    for (int q = 0; q < PER; ++q) rv[0][q] = io[(long)q * RSTEP * N];
+    fft16x<double, N, true, true>(t, cidx, r0, true, -1.0, tw, rv);
     // -g / (-phat2 + m^2) / N^2 at (kx, ky) = (r0 + q RSTEP, c0 + cc)
-    double fac[PER];
     const double inv = 1.0 / ((double)N * (double)N);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) fac[q] = -1.0 * e.mv_g / (-phat2_d(r0 + q * RSTEP, c0 + cc, N) + e.mv_mass2) * inv;
-    cp_async_wait<0>();
-    __syncthreads();
-    fft16<double, N>(t, cidx, r0, true, -1.0, tw);
+    for (int q = 0; q < PER; ++q)
+        rv[0][q] = cscale(rv[0][q], -1.0 * e.mv_g / (-phat2_d(r0 + q * RSTEP, c0 + cc, N) + e.mv_mass2) * inv);
+    // the inverse's first pass synchronises before it writes t
+    fft16x<double, N, true, true>(t, cidx, r0, true, 1.0, tw, rv);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int i = cidx(r0 + q * RSTEP);
-        t[i] = cscale(t[i], fac[q]);
-    }
-    __syncthreads();
-    fft16<double, N>(t, cidx, r0, true, 1.0, tw);
-#pragma unroll 2
-    for (int q = 0; q < PER; ++q) io[(long)q * RSTEP * N] = t[cidx(r0 + q * RSTEP)];
+    for (int q = 0; q < PER; ++q) io[(long)q * RSTEP * N] = rv[0][q];
 }
 
 template <int N>
