@@ -48,12 +48,14 @@ MASS = 0.04           # m a = 0.02 = mass * mu_MV
 ALPHA_S, DS = 0.15, 1e-4
 STEP = ALPHA_S * DS / math.pi ** 2
 METRIC = "lattice site-steps/s"
-# algorithmic HBM bytes per site of each fused kernel (mixed precision):
+# algorithmic HBM bytes per site of each kernel kind (mixed precision):
 #   pass 1: read V (9 complex FP64 = 144 B) + write 16 FP32 complex planes (128 B)
 #   pass 2: read 16 planes (128 B) + write 8 planes (64 B)
 #   pass 3: read 8 planes (64 B) + read and write V (288 B)
-PASS_BYTES = {"k_mix_pass1<512>": 272, "k_mix_pass2<512>": 192, "k_mix_pass3<512>": 352}
-PASS_NAMES = ["k_mix_pass1<512>", "k_mix_pass2<512>", "k_mix_pass3<512>"]
+#   pass 3 + next pass 1: read 8 planes (64 B), read and write V (288 B), write 16 planes (128 B)
+# A run of K steps is pass 1, K - 1 times (pass 2, pass 3 + next pass 1), pass 2, pass 3.
+KIND_BYTES = {"pass1": 272, "pass2": 192, "pass3": 352, "pass31": 480}
+KIND_KERNEL = {"pass1": "k_mix_pass1", "pass2": "k_mix_pass2", "pass3": "k_mix_pass3", "pass31": "k_mix_pass31"}
 
 
 def dist_env():
@@ -488,11 +490,11 @@ def main_arm(args):
         raise RuntimeError("device error during warm-up")
     sites = events * n_side * n_side
 
-    # ---- timed region: K steps, a CUDA event around every fused kernel
+    # ---- timed region: K steps, a CUDA event around every kernel
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        pass_ms, total_ms = eng.step_timed(ids, args.steps)
+        kernels, total_ms = eng.step_timed(ids, args.steps)
     torch.cuda.synchronize()
     status = eng.sync()
     if status != jw.OK:
@@ -530,18 +532,23 @@ def main_arm(args):
     h2d = 4 * events                   # the event id list
     d2h = 2 * n_side * n_side * 16     # sum and err, complex
 
-    # ---- roofline of the dominant kernel
+    # ---- roofline of the dominant kernel (the largest share of the timed region)
     peak, peak_kind = measured_peaks()
-    dom = int(np.argmax(pass_ms))
-    name = PASS_NAMES[dom]
-    alg_bytes = PASS_BYTES[name] * sites
-    achieved = alg_bytes / (pass_ms[dom] / 1e3) / 1e9
+    launched = {k: v for k, v in kernels.items() if v[1] > 0}
+    dom = max(launched, key=lambda k: launched[k][0])
+    name = f"{KIND_KERNEL[dom]}<{n_side}>"
+    per_launch = {k: ms / cnt for k, (ms, cnt) in launched.items()}
+    alg_bytes = KIND_BYTES[dom] * sites
+    achieved = alg_bytes / (per_launch[dom] / 1e3) / 1e9
     traffic = profiled_traffic().get(name)
+    kernel_time = sum(ms for ms, _ in launched.values())
     roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic * sites if traffic else None,
             "algorithmic_bytes": alg_bytes,
-            "pass_ms": {n: m for n, m in zip(PASS_NAMES, pass_ms)},
-            "pass_frac": {n: PASS_BYTES[n] * sites / (m / 1e3) / 1e9 / peak for n, m in zip(PASS_NAMES, pass_ms)}}
+            "kernels": {f"{KIND_KERNEL[k]}<{n_side}>": {
+                "launches": cnt, "ms_per_launch": per_launch[k], "share": ms / kernel_time,
+                "hbm_frac": KIND_BYTES[k] * sites / (per_launch[k] / 1e3) / 1e9 / peak}
+                for k, (ms, cnt) in launched.items()}}
 
     line = {
         "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world, "steps": args.steps,
@@ -557,7 +564,7 @@ def main_arm(args):
                 "what": "jw_engine_step_measure_ensemble per step (one step + ensemble measurement to host arrays)",
                 "two_calls": {"value": world * sites * k_e2e / (two_ms / 1e3), "ms_per_step": two_ms / k_e2e,
                               "what": "jw_engine_step + jw_engine_measure_ensemble per step"}},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": sum(cnt for _, cnt in launched.values()),
         "clocks": clocks,
         "roofline": roof,
     }

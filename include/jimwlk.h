@@ -358,10 +358,13 @@ jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double
 jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, int nsteps, double* sum,
                                           double* err);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
- * event around each fused kernel launch; returns the milliseconds per step
- * spent in each of the three kernels (summed over launch groups, pass_ms[3])
- * and the total time from the first launch to the last. */
-jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms, double* total_ms);
+ * event around each kernel launch.  kernel_ms[4] receives the milliseconds
+ * spent in each kernel kind and launches[4] its launch count: pass 1, pass 2,
+ * pass 3, and pass 3 fused with the next step's pass 1 (mixed precision runs
+ * nsteps steps as pass 1, nsteps - 1 times (pass 2, fused pass), pass 2,
+ * pass 3); total_ms is the time from the first launch to the last. */
+jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* kernel_ms, int* launches,
+                               double* total_ms);
 
 /* ------------------------------------------------------------------ serving */
 /* Continuous-batching evolution server over the engine.  A request is one

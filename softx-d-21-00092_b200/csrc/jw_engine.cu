@@ -389,67 +389,148 @@ void group_destroy(Group& g) {
 }
 
 // --------------------------------------------------------------- launches
-template <int N>
-cudaError_t launch_mix_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws, cudaEvent_t* t) {
-    const long vol = (long)N * N;
-    float4* P = reinterpret_cast<float4*>(ws);
-    float4* Q = P + (size_t)8 * vol * nb;
-    const size_t sm1 = mx_p1_smem<N>(), sm2 = mx_p2_smem<N>(), sm3 = mx_p3_smem<N>();
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-        cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-        cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
-        configured = true;
+// Kernel kinds of a timed run (jw_engine_step_timed's kernel_ms order).
+enum { KIND_P1 = 0, KIND_P2 = 1, KIND_P3 = 2, KIND_P31 = 3, KIND_COUNT = 4 };
+
+// CUDA events around launches, for jw_engine_step_timed.
+struct LaunchTimes {
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> ev;  // start, end of each timed launch
+    std::vector<int> kind;
+    void start(int k) {
+        cudaEvent_t a = nullptr;
+        cudaEventCreate(&a);
+        cudaEventRecord(a, stream);
+        ev.push_back(a);
+        kind.push_back(k);
     }
-    if (t) cudaEventRecord(t[0], e->stream);
-    k_mix_pass1<N><<<dim3(N, mx_groups<N>(), nb), mx_p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P,
-                                                                                        g.tw.d32);
-    if (t) { cudaEventRecord(t[1], e->stream); cudaEventRecord(t[2], e->stream); }
-    k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), sm2, e->stream>>>(g.d_ev, d_slots, P, Q,
-                                                                                          g.tw.d32);
-    if (t) { cudaEventRecord(t[3], e->stream); cudaEventRecord(t[4], e->stream); }
-    k_mix_pass3<N><<<dim3(N, nb), mx_p3_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32, e->d_flags,
-                                                                        nullptr);
-    if (t) cudaEventRecord(t[5], e->stream);
-    return cudaGetLastError();
+    void stop() {
+        cudaEvent_t b = nullptr;
+        cudaEventCreate(&b);
+        cudaEventRecord(b, stream);
+        ev.push_back(b);
+    }
+    ~LaunchTimes() {
+        for (cudaEvent_t x : ev) cudaEventDestroy(x);
+    }
+};
+
+template <int N>
+void mix_configure() {
+    static bool configured = false;
+    if (configured) return;
+    cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
+    cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p2_smem<N>());
+    cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p3_smem<N>());
+    if constexpr (mx_p3_meas_fits<N>())
+        cudaFuncSetAttribute(k_mix_pass3<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)mx_p3_smem<N, true>());
+    if constexpr (mx_fuse31<N>())
+        cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
+    cudaFuncSetAttribute(k_meas32_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p2_smem<N>());
+    configured = true;
 }
 
-// One mixed step whose pass 3 also row-transforms the new V for the ensemble
-// measurement (the measurement planes land where P was), then the column pass
-// and the ensemble reduction: the same result as a step followed by
-// launch_measure_ensemble, without re-reading V.
+// One mixed-precision kernel of a launch group.  The workspace holds P (8 pair
+// planes per event) and then Q (4 pair planes per event); the measuring pass 3
+// writes its 5 row-transformed planes where P was.
 template <int N>
-cudaError_t launch_mix_step_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
-    if constexpr (!mx_p3_meas_fits<N>()) {
-        return cudaErrorInvalidValue;
-    } else {
-        const long vol = (long)N * N;
-        float4* P = reinterpret_cast<float4*>(g.ws);
-        float4* Q = P + (size_t)8 * vol * nb;
-        float4* M = P;
-        double* corr = reinterpret_cast<double*>(M + (size_t)5 * vol * nb);
-        const size_t sm1 = mx_p1_smem<N>(), sm2 = mx_p2_smem<N>(), sm3 = mx_p3_smem<N, true>();
-        static bool configured = false;
-        if (!configured) {
-            cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-            cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-            cudaFuncSetAttribute(k_mix_pass3<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
-            cudaFuncSetAttribute(k_meas32_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-            configured = true;
+void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bool meas, LaunchTimes* tm) {
+    const long vol = (long)N * N;
+    float4* P = reinterpret_cast<float4*>(g.ws);
+    float4* Q = P + (size_t)8 * vol * nb;
+    if (tm) tm->start(kind);
+    switch (kind) {
+        case KIND_P1:
+            k_mix_pass1<N><<<dim3(N, mx_groups<N>(), nb), mx_p1_threads<N>(), mx_p1_smem<N>(), e->stream>>>(
+                g.d_ev, d_slots, P, g.tw.d32);
+            break;
+        case KIND_P2:
+            k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), mx_p2_smem<N>(), e->stream>>>(
+                g.d_ev, d_slots, P, Q, g.tw.d32);
+            break;
+        case KIND_P3:
+            if constexpr (mx_p3_meas_fits<N>()) {
+                if (meas) {
+                    k_mix_pass3<N, true><<<dim3(N, nb), mx_p3_threads<N>(), mx_p3_smem<N, true>(), e->stream>>>(
+                        g.d_ev, d_slots, Q, g.tw.d32, e->d_flags, P);
+                    break;
+                }
+            }
+            k_mix_pass3<N><<<dim3(N, nb), mx_p3_threads<N>(), mx_p3_smem<N>(), e->stream>>>(g.d_ev, d_slots, Q,
+                                                                                            g.tw.d32, e->d_flags,
+                                                                                            nullptr);
+            break;
+        case KIND_P31:
+            if constexpr (mx_fuse31<N>())
+                k_mix_pass31<N><<<dim3(N, nb), mx_p31_threads<N>(), mx_p31_smem<N>(), e->stream>>>(
+                    g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
+            break;
+        default:
+            break;
+    }
+    if (tm) tm->stop();
+}
+
+// nsteps >= 1 mixed steps of one launch group: pass 1, then nsteps - 1 times
+// (pass 2, pass 3 + next pass 1), then pass 2 and pass 3.  Where pass 1 splits
+// its rows over two CTAs (2048^2) the middle is (pass 2, pass 3, pass 1).
+// With ens the last pass 3 also row-transforms the new V, and the column pass
+// and the ensemble reduction into ens follow (the same result as the steps
+// followed by launch_measure_ensemble).  The middle is captured once as a CUDA
+// graph and replayed when it repeats and nothing is timed.  Launch groups that
+// share the workspace run one after another, each through all its steps.
+template <int N>
+cudaError_t launch_mix_run(jw_engine* e, Group& g, const int* d_slots, int nb, int nsteps, double* ens,
+                           LaunchTimes* tm) {
+    if (nsteps < 1) return cudaErrorInvalidValue;
+    if (ens && !mx_p3_meas_fits<N>()) return cudaErrorInvalidValue;
+    mix_configure<N>();
+    auto middle = [&]() {
+        mix_launch<N>(e, g, d_slots, nb, KIND_P2, false, tm);
+        if constexpr (mx_fuse31<N>()) {
+            mix_launch<N>(e, g, d_slots, nb, KIND_P31, false, tm);
+        } else {
+            mix_launch<N>(e, g, d_slots, nb, KIND_P3, false, tm);
+            mix_launch<N>(e, g, d_slots, nb, KIND_P1, false, tm);
         }
-        k_mix_pass1<N><<<dim3(N, mx_groups<N>(), nb), mx_p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P,
-                                                                                            g.tw.d32);
-        k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), sm2, e->stream>>>(g.d_ev, d_slots, P, Q,
-                                                                                              g.tw.d32);
-        k_mix_pass3<N, true><<<dim3(N, nb), mx_p3_threads<N>(), sm3, e->stream>>>(g.d_ev, d_slots, Q, g.tw.d32,
-                                                                                  e->d_flags, M);
-        k_meas32_cols<N><<<dim3(N / mx_cols<N>(), nb), mx_p2_threads<N>(), sm2, e->stream>>>(M, corr, corr + vol * nb,
-                                                                                            g.tw.d32);
+    };
+    mix_launch<N>(e, g, d_slots, nb, KIND_P1, false, tm);
+    const int reps = nsteps - 1;
+    if (reps >= 3 && !tm) {
+        middle();
+        cudaError_t ce = cudaGetLastError();
+        if (ce != cudaSuccess) return ce;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if ((ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return ce;
+        middle();
+        const cudaError_t launched = cudaGetLastError();
+        ce = cudaStreamEndCapture(e->stream, &graph);
+        if (launched != cudaSuccess || ce != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return launched != cudaSuccess ? launched : ce;
+        }
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        for (int r = 1; r < reps && ce == cudaSuccess; ++r) ce = cudaGraphLaunch(exec, e->stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return ce;
+    } else {
+        for (int r = 0; r < reps; ++r) middle();
+    }
+    mix_launch<N>(e, g, d_slots, nb, KIND_P2, false, tm);
+    mix_launch<N>(e, g, d_slots, nb, KIND_P3, ens != nullptr, tm);
+    if (ens) {
+        const long vol = (long)N * N;
+        const float4* M = reinterpret_cast<const float4*>(g.ws);
+        double* corr = reinterpret_cast<double*>(g.ws + sizeof(float4) * 5 * (size_t)vol * nb);
+        k_meas32_cols<N><<<dim3(N / mx_cols<N>(), nb), mx_p2_threads<N>(), mx_p2_smem<N>(), e->stream>>>(
+            M, corr, corr + vol * nb, g.tw.d32);
         k_meas_reduce_ensemble<N><<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(corr, corr + vol * nb, nb,
                                                                                          ens);
-        return cudaGetLastError();
     }
+    return cudaGetLastError();
 }
 
 bool fused_measure_supported(int precision, int N) {
@@ -470,7 +551,7 @@ bool fused_measure_supported(int precision, int N) {
 
 template <typename T, int N>
 cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
-    if constexpr (sizeof(T) == 4) return launch_mix_step<N>(e, g, d_slots, nb, ws, nullptr);
+    if constexpr (sizeof(T) == 4) return launch_mix_run<N>(e, g, d_slots, nb, 1, nullptr, nullptr);
     using V2 = C2<T>;
     const long vol = (long)N * N;
     V2* P = reinterpret_cast<V2*>(ws);
@@ -613,52 +694,58 @@ cudaError_t dispatch_measure(jw_engine* e, Group& g, const int* d_slots, int nb)
     JW_DISPATCH_N(g.N, (launch_measure<NN>(e, g, d_slots, nb, g.ws)))
 }
 
-cudaError_t dispatch_step_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
-    JW_DISPATCH_N(g.N, (launch_mix_step_measure_ensemble<NN>(e, g, d_slots, nb, ens)))
+cudaError_t dispatch_mix_run(jw_engine* e, Group& g, const int* d_slots, int nb, int nsteps, double* ens,
+                             LaunchTimes* tm) {
+    JW_DISPATCH_N(g.N, (launch_mix_run<NN>(e, g, d_slots, nb, nsteps, ens, tm)))
 }
 
 cudaError_t dispatch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, int nb, double* ens) {
     JW_DISPATCH_N(g.N, (launch_measure_ensemble<NN>(e, g, d_slots, nb, g.ws, ens)))
 }
 
-template <typename T, int N>
-cudaError_t launch_step_timed(jw_engine* e, Group& g, const int* d_slots, int nb, cudaEvent_t* t) {
-    if constexpr (sizeof(T) == 4) return launch_mix_step<N>(e, g, d_slots, nb, g.ws, t);
-    using V2 = C2<T>;
+// One timed FP64 step (the mixed steps are timed through launch_mix_run).
+template <int N>
+cudaError_t launch_step_timed64(jw_engine* e, Group& g, const int* d_slots, int nb, LaunchTimes* tm) {
+    using V2 = double2;
     const long vol = (long)N * N;
     V2* P = reinterpret_cast<V2*>(g.ws);
     V2* Q = P + (size_t)16 * vol * nb;
-    const V2* tw = (const V2*)(sizeof(T) == 8 ? (const void*)g.tw.d64 : (const void*)g.tw.d32);
+    const V2* tw = g.tw.d64;
     constexpr int RT = row_threads<N>();
-    constexpr int C = p2_cols<T, N>();
-    const size_t sm1 = p1_smem_bytes<T, N>();
-    const size_t sm2 = p2_smem<T, N>();
-    const size_t sm3 = p3_smem<T, N>();
-    cudaEventRecord(t[0], e->stream);
-    k_step_pass1<T, N><<<dim3(N, p1_groups<T, N>(), nb), p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots, P, tw);
-    cudaEventRecord(t[1], e->stream);
-    cudaEventRecord(t[2], e->stream);
-    k_step_pass2<T, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);
-    cudaEventRecord(t[3], e->stream);
-    cudaEventRecord(t[4], e->stream);
-    k_step_pass3<T, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, d_slots, Q, tw, e->d_flags);
-    cudaEventRecord(t[5], e->stream);
+    constexpr int C = p2_cols<double, N>();
+    const size_t sm1 = p1_smem_bytes<double, N>();
+    const size_t sm2 = p2_smem<double, N>();
+    const size_t sm3 = p3_smem<double, N>();
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_step_pass1<double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_step_pass2<double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        cudaFuncSetAttribute(k_step_pass3<double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
+        configured = true;
+    }
+    tm->start(KIND_P1);
+    k_step_pass1<double, N><<<dim3(N, p1_groups<double, N>(), nb), p1_threads<N>(), sm1, e->stream>>>(g.d_ev, d_slots,
+                                                                                                    P, tw);
+    tm->stop();
+    tm->start(KIND_P2);
+    k_step_pass2<double, N><<<dim3(N / C, 8, nb), C * (N / 8), sm2, e->stream>>>(g.d_ev, d_slots, P, Q, tw);
+    tm->stop();
+    tm->start(KIND_P3);
+    k_step_pass3<double, N><<<dim3(N, nb), RT, sm3, e->stream>>>(g.d_ev, d_slots, Q, tw, e->d_flags);
+    tm->stop();
     return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t dispatch_pass_timed(jw_engine* e, Group& g, const int* d_slots, int nb, cudaEvent_t* t) {
-    if (sizeof(T) == 8 && g.N > 1024) return cudaErrorInvalidValue;
+cudaError_t dispatch_step_timed64(jw_engine* e, Group& g, const int* d_slots, int nb, LaunchTimes* tm) {
     switch (g.N) {
-        case 8: return launch_step_timed<T, 8>(e, g, d_slots, nb, t);
-        case 16: return launch_step_timed<T, 16>(e, g, d_slots, nb, t);
-        case 32: return launch_step_timed<T, 32>(e, g, d_slots, nb, t);
-        case 64: return launch_step_timed<T, 64>(e, g, d_slots, nb, t);
-        case 128: return launch_step_timed<T, 128>(e, g, d_slots, nb, t);
-        case 256: return launch_step_timed<T, 256>(e, g, d_slots, nb, t);
-        case 512: return launch_step_timed<T, 512>(e, g, d_slots, nb, t);
-        case 1024: return launch_step_timed<T, 1024>(e, g, d_slots, nb, t);
-        case 2048: return launch_step_timed<T, (sizeof(T) == 8 ? 1024 : 2048)>(e, g, d_slots, nb, t);
+        case 8: return launch_step_timed64<8>(e, g, d_slots, nb, tm);
+        case 16: return launch_step_timed64<16>(e, g, d_slots, nb, tm);
+        case 32: return launch_step_timed64<32>(e, g, d_slots, nb, tm);
+        case 64: return launch_step_timed64<64>(e, g, d_slots, nb, tm);
+        case 128: return launch_step_timed64<128>(e, g, d_slots, nb, tm);
+        case 256: return launch_step_timed64<256>(e, g, d_slots, nb, tm);
+        case 512: return launch_step_timed64<512>(e, g, d_slots, nb, tm);
+        case 1024: return launch_step_timed64<1024>(e, g, d_slots, nb, tm);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1104,7 +1191,12 @@ JW_EXPORT jw_status jw_engine_step(jw_engine* e, const int* ids, int n, int nste
         for (int c0 = 0; c0 < (int)kv.second.size(); c0 += cs)
             work.push_back({&g, std::min(cs, (int)kv.second.size() - c0), c0});
     }
-    // one step of every chunk, captured once as a graph and replayed
+    if (e->opt.precision == JW_PRECISION_MIXED) {
+        for (const Work& w : work)
+            JW_CUDA(dispatch_mix_run(e, *w.g, w.g->d_slots + w.off, w.nb, nsteps, nullptr, nullptr));
+        return JW_OK;
+    }
+    // FP64: one step of every chunk, captured once as a graph and replayed
     auto record = [&]() -> cudaError_t {
         for (const Work& w : work) {
             cudaError_t ce = dispatch_step(e, *w.g, w.g->d_slots + w.off, w.nb);
@@ -1296,7 +1388,6 @@ JW_EXPORT jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids
         if ((s = jw_engine_step(e, ids, n, nsteps))) return s;
         return jw_engine_measure_ensemble(e, ids, n, sum, err);
     }
-    if (nsteps > 1 && (s = jw_engine_step(e, ids, n, nsteps - 1))) return s;
     Group& g = *e->groups[by_n.begin()->first];
     const std::vector<int>& slots = by_n.begin()->second;
     const long vol = (long)g.N * g.N;
@@ -1308,15 +1399,15 @@ JW_EXPORT jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids
     double2* out = reinterpret_cast<double2*>(ens + 4 * vol);
     JW_CUDA(cudaMemsetAsync(ens, 0, sizeof(double) * 4 * vol, e->stream));
     for (int c0 = 0; c0 < (int)slots.size(); c0 += cs)
-        JW_CUDA(dispatch_step_measure_ensemble(e, g, g.d_slots + c0, std::min(cs, (int)slots.size() - c0), ens));
+        JW_CUDA(dispatch_mix_run(e, g, g.d_slots + c0, std::min(cs, (int)slots.size() - c0), nsteps, ens, nullptr));
     k_ens_finalize<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ens, vol, out);
     JW_CUDA(cudaGetLastError());
     return copy_out_host(e, out, vol, sum, err);
 }
 
-JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* pass_ms,
-                                         double* total_ms) {
-    JW_CHECK(e && nsteps > 0 && pass_ms && total_ms);
+JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* kernel_ms,
+                                         int* launches, double* total_ms) {
+    JW_CHECK(e && nsteps > 0 && kernel_ms && launches && total_ms);
     std::map<int, std::vector<int>> by_n;
     jw_status s = collect(e, ids, n, by_n);
     if (s) return s;
@@ -1325,38 +1416,38 @@ JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, in
     const std::vector<int>& slots = by_n.begin()->second;
     const int nb = (int)slots.size();
     const int cs = chunk_size(e, nb, g.N);
-    const int nch = (nb + cs - 1) / cs;
     if ((s = ensure_workspace(e, g, cs))) return s;
     if ((s = upload_slots(e, g, slots))) return s;
-    JW_CUDA(dispatch_step(e, g, g.d_slots, std::min(cs, nb)));  // kernel attributes, outside the timing
-    const int per_step = 6 * nch;
-    std::vector<cudaEvent_t> ev((size_t)per_step * nsteps);
-    for (auto& x : ev) JW_CUDA(cudaEventCreate(&x));
     const bool mixed = e->opt.precision == JW_PRECISION_MIXED;
+    LaunchTimes tm;
+    tm.stream = e->stream;
     cudaError_t ce = cudaSuccess;
-    for (int k = 0; k < nsteps && ce == cudaSuccess; ++k)
-        for (int c = 0; c < nch && ce == cudaSuccess; ++c) {
-            cudaEvent_t* t = &ev[(size_t)k * per_step + 6 * c];
-            const int nbc = std::min(cs, nb - c * cs);
-            ce = mixed ? dispatch_pass_timed<float>(e, g, g.d_slots + c * cs, nbc, t)
-                       : dispatch_pass_timed<double>(e, g, g.d_slots + c * cs, nbc, t);
+    for (int c = 0; c * cs < nb && ce == cudaSuccess; ++c) {
+        const int nbc = std::min(cs, nb - c * cs);
+        if (mixed) {
+            ce = dispatch_mix_run(e, g, g.d_slots + c * cs, nbc, nsteps, nullptr, &tm);
+        } else {
+            for (int k = 0; k < nsteps && ce == cudaSuccess; ++k)
+                ce = dispatch_step_timed64(e, g, g.d_slots + c * cs, nbc, &tm);
         }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-    double p[3] = {0, 0, 0}, tot = 0;
-    if (ce == cudaSuccess) {
-        float a;
-        for (size_t b = 0; b < ev.size(); b += 6)
-            for (int q = 0; q < 3; ++q) {
-                cudaEventElapsedTime(&a, ev[b + 2 * q], ev[b + 2 * q + 1]);
-                p[q] += a;
-            }
-        cudaEventElapsedTime(&a, ev.front(), ev.back());
-        tot = a;
     }
-    for (auto& x : ev) cudaEventDestroy(x);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     JW_CUDA(ce);
-    for (int q = 0; q < 3; ++q) pass_ms[q] = p[q] / nsteps;  // per step, summed over launch groups
-    *total_ms = tot;
+    for (int k = 0; k < KIND_COUNT; ++k) {
+        kernel_ms[k] = 0.0;
+        launches[k] = 0;
+    }
+    float a = 0.0f;
+    for (size_t i = 0; i < tm.kind.size(); ++i) {
+        JW_CUDA(cudaEventElapsedTime(&a, tm.ev[2 * i], tm.ev[2 * i + 1]));
+        kernel_ms[tm.kind[i]] += a;
+        launches[tm.kind[i]] += 1;
+    }
+    *total_ms = 0.0;
+    if (!tm.ev.empty()) {
+        JW_CUDA(cudaEventElapsedTime(&a, tm.ev.front(), tm.ev.back()));
+        *total_ms = a;
+    }
     return JW_OK;
 }
 

@@ -47,7 +47,7 @@ struct EventDev {
     const double* nf64;         // per-site noise factor (NOISE coupling) or null
     const float* nf32;
     unsigned long long seed;
-    unsigned long long step;    // next Langevin step index (advanced by pass 3)
+    unsigned long long step;    // next Langevin step index (advanced by pass 2 in mixed precision, pass 3 in FP64)
     double sqrt_eps;            // sqrt(step)
     double mv_sigma;            // g mu / sqrt(ny_slices)
     double mv_mass2;            // (mass * g^2 * mu)^2

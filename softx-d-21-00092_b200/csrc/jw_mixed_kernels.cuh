@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev
 // plane-j transform starts from global loads, the kernel product and the
 // inverse start from registers and the inverse ends in the store.
 template <int N>
-__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 2 : 1) k_mix_pass2(const EventDev* __restrict__ ev,
+__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 2 : 1) k_mix_pass2(EventDev* __restrict__ ev,
                                                                    const int* __restrict__ slots,
                                                                    const float4* __restrict__ P,
                                                                    float4* __restrict__ Q,
@@ -226,6 +226,9 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
     float4* tb = ta + TL;
     const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
     const EventDev& e = ev[slots[b]];
+    // the step index advances here: pass 1 of this step has read it, and the
+    // next step's noise (pass 1, or pass 3 + 1) reads the new value
+    if (blockIdx.x == 0 && j == 0 && threadIdx.x == 0) ev[slots[b]].step += 1;
     const long vol = (long)N * N;
     const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
     constexpr int RSTEP = TH / C;  // = N / 8
@@ -265,6 +268,36 @@ __global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 
 }
 
 // ------------------------------------------------------------------ pass 3
+// The update of site y: V <- exp(+i sqrt(eps) B) V exp(-i sqrt(eps) A), A and B
+// from the inverse row transforms in column y of the row buffer, V the old
+// value staged in smV (chunk from c0).  Reports non-finite entries in fl.
+template <int N, int VC>
+__device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, const double2* smV, int y, int c0,
+                                        double se, double2 (&v)[9], int& fl) {
+    double a[8], bq[8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float4 u = sm[pad16(j * N + y)];
+        a[2 * j] = (double)u.x * se;
+        a[2 * j + 1] = (double)u.y * se;
+        bq[2 * j] = (double)u.z * -se;
+        bq[2 * j + 1] = (double)u.w * -se;
+    }
+    double2 mA[9], mB[9], tmp[9];
+    embed_lambda<double>(a, mA);
+    embed_lambda<double>(bq, mB);
+    expi_ch(mB, -1.0);  // exp(+i sqrt(eps) B)
+    expi_ch(mA, -1.0);  // exp(-i sqrt(eps) A)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] = smV[k * VC + (y - c0)];
+    mul3(mB, v, tmp);
+    mul3(tmp, mA, v);
+    if (e.reunit) reunitarize(v);
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+}
+
 template <int N, bool MEAS = false>
 __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 ? 2 : 1) k_mix_pass3(EventDev* __restrict__ ev,
                                                                     const int* __restrict__ slots,
@@ -299,31 +332,11 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 
         cp_async_wait<0>();
         __syncthreads();
         for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
-            double a[8], bq[8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float4 u = sm[pad16(j * N + y)];
-                a[2 * j] = (double)u.x * se;
-                a[2 * j + 1] = (double)u.y * se;
-                bq[2 * j] = (double)u.z * -se;
-                bq[2 * j + 1] = (double)u.w * -se;
-            }
-            double2 mA[9], mB[9], v[9], tmp[9];
-            embed_lambda<double>(a, mA);
-            embed_lambda<double>(bq, mB);
-            expi_ch(mB, -1.0);  // exp(+i sqrt(eps) B)
-            expi_ch(mA, -1.0);  // exp(-i sqrt(eps) A)
-#pragma unroll
-            for (int k = 0; k < 9; ++k) v[k] = smV[k * VC + (y - c0)];
-            mul3(mB, v, tmp);
-            mul3(tmp, mA, v);
-            if (e.reunit) reunitarize(v);
+            double2 v[9];
+            p3_site<N, VC>(e, sm, smV, y, c0, se, v, fl);
             const long site = (long)x * N + y;
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
-                e.V[k * vol + site] = v[k];
-            }
+            for (int k = 0; k < 9; ++k) e.V[k * vol + site] = v[k];
             if constexpr (MEAS) {
                 // entries 2p, 2p + 1 of the new V as pair element (p, y); this
                 // thread alone has read or written column y of the row buffer
@@ -336,11 +349,93 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 
         }
     }
     if (fl) atomicOr(flags, fl);
-    if (x == 0 && threadIdx.x == 0) e.step += 1;
     if constexpr (MEAS) {
         __syncthreads();
         fft16_rows_store<float, N>(sm, 5, -1.0f, tw, M + (long)b * 5 * vol + (long)x * N, vol);
     }
+}
+
+// ------------------------------------------------------------------ pass 3 + next pass 1
+// The end of one step and the start of the next for lattice row x, in one
+// kernel: the inverse row transforms of Q and the V update (pass 3), then, with
+// the new V still in registers, the next step's noise, V xi V^dagger and their
+// forward row transforms (pass 1).  This saves the V re-read of pass 1 and lets
+// pass 3's memory traffic overlap pass 1's arithmetic.  The new pair rows of
+// site y overwrite column y of the inverse transforms, which the same thread
+// has just consumed, so the row buffer is pass 1's (8 rows).  Pass 2 has
+// advanced the step index, so e.step is the next step's noise index.
+template <int N> constexpr bool mx_fuse31() { return mx_groups<N>() == 1; }
+template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
+template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>(); }
+
+template <int N>
+__global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_smem<N>() <= 112 * 1024 ? 2 : 1) k_mix_pass31(
+    EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q, float4* __restrict__ P,
+    const float2* __restrict__ tw, int* __restrict__ flags) {
+    static_assert(mx_fuse31<N>(), "one CTA holds all 8 pair rows");
+    constexpr int VC = mx_vc<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* sm = reinterpret_cast<float4*>(smem_raw);
+    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(8 * N));
+    const int x = blockIdx.x, b = blockIdx.y;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const float4* in = Q + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
+        cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    cp_async_commit();
+    stage_v_chunk<N, VC>(smV, e.V, vol, x, 0);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    fft16_rows<N, 4>(sm, 1.0f, tw);
+    const double se = e.sqrt_eps;
+    const float* nf = e.nf32;
+    int fl = 0;
+    for (int c0 = 0; c0 < N; c0 += VC) {
+        if (c0 > 0) {
+            __syncthreads();
+            stage_v_chunk<N, VC>(smV, e.V, vol, x, c0);
+            cp_async_commit();
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
+            const long site = (long)x * N + y;
+            float2 v32[9];
+            {
+                double2 v[9];
+                p3_site<N, VC>(e, sm, smV, y, c0, se, v, fl);
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    e.V[k * vol + site] = v[k];
+                    v32[k] = make_float2((float)v[k].x, (float)v[k].y);
+                }
+            }
+            float z[16];
+            langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+            const float f = nf ? nf[site] : 1.0f;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+                sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+            float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                n[k] = z[2 * k];
+                m[k] = z[2 * k + 1];
+            }
+            rotate_herm(v32, n, hx);
+            rotate_herm(v32, m, hy);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+                sm[pad16((4 + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+    __syncthreads();
+    fft16_rows_store<float, N>(sm, 8, -1.0f, tw, P + (long)b * 8 * vol + (long)x * N, vol);
 }
 
 // ------------------------------------------------------------------ measurement (FP64)

@@ -160,8 +160,8 @@ def _load():
         "jw_engine_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp], ctypes.c_int),
         "jw_engine_step_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
                                             ctypes.c_int),
-        "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
-                                 ctypes.c_int),
+        "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp,
+                                  ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -551,11 +551,14 @@ class Engine:
         return s, e
 
     def step_timed(self, ids, nsteps: int):
+        """nsteps steps with every kernel timed: ({kind: (total ms, launches)}, total ms)."""
         arr, n = _ids(ids)
-        p = (ctypes.c_double * 3)()
+        p = (ctypes.c_double * 4)()
+        c = (ctypes.c_int * 4)()
         tot = ctypes.c_double(0)
-        _ck(_lib.jw_engine_step_timed(self._h, arr, n, nsteps, p, ctypes.byref(tot)), "jw_engine_step_timed")
-        return list(p), tot.value
+        _ck(_lib.jw_engine_step_timed(self._h, arr, n, nsteps, p, c, ctypes.byref(tot)), "jw_engine_step_timed")
+        kinds = ("pass1", "pass2", "pass3", "pass31")
+        return {k: (p[i], c[i]) for i, k in enumerate(kinds)}, tot.value
 
     def dipole(self, eid: int, with_xy: bool = False):
         """(S_bins, r_bins, counts, Q_s[, S_xy]) from the event's accumulated correlator."""
