@@ -420,7 +420,7 @@ void mix_configure() {
     static bool configured = false;
     if (configured) return;
     cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
-    cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p2_smem<N>());
+    cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_s2_smem<N>());
     cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p3_smem<N>());
     if constexpr (mx_p3_meas_fits<N>())
         cudaFuncSetAttribute(k_mix_pass3<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -446,7 +446,7 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
                 g.d_ev, d_slots, P, g.tw.d32);
             break;
         case KIND_P2:
-            k_mix_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), mx_p2_smem<N>(), e->stream>>>(
+            k_mix_pass2<N><<<dim3(N / mx_s2_cols<N>(), 4, nb), mx_s2_threads<N>(), mx_s2_smem<N>(), e->stream>>>(
                 g.d_ev, d_slots, P, Q, g.tw.d32);
             break;
         case KIND_P3:

@@ -50,6 +50,14 @@ template <int N> constexpr int mx_tile_len() {
     return mx_cols<N>() >= 8 ? N * mx_cols<N>() : N * mx_cols<N>() + (N / 8) * mx_cols<N>();
 }
 template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile_len<N>(); }
+// the step's pass 2 (k_mix_pass2): its own tile width, two tiles (planes j, 4 + j)
+template <int N> constexpr int mx_s2_cols() { return mx_cols<N>(); }
+template <int N> constexpr int mx_s2_threads() { return mx_s2_cols<N>() * (N / 8); }
+template <int N> constexpr int mx_s2_tile_len() {
+    return mx_s2_cols<N>() >= 8 ? N * mx_s2_cols<N>() : N * mx_s2_cols<N>() + (N / 8) * mx_s2_cols<N>();
+}
+template <int N> constexpr size_t mx_s2_smem() { return 2 * 16 * (size_t)mx_s2_tile_len<N>(); }
+template <int N> constexpr int mx_s2_blocks() { return mx_s2_threads<N>() <= 256 ? 2 : 1; }
 // pass 3: V staged in chunks of mx_p3_vc sites (128 at N = 1024, so that two CTAs
 // fit), mx_p3_threads threads
 template <int N, bool MEAS = false> constexpr int mx_p3_vc() {
@@ -211,16 +219,16 @@ __global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev
 // plane-j transform starts from global loads, the kernel product and the
 // inverse start from registers and the inverse ends in the store.
 template <int N>
-__global__ void __launch_bounds__(mx_p2_threads<N>(), mx_p2_threads<N>() <= 256 ? 2 : 1) k_mix_pass2(EventDev* __restrict__ ev,
+__global__ void __launch_bounds__(mx_s2_threads<N>(), mx_s2_blocks<N>()) k_mix_pass2(EventDev* __restrict__ ev,
                                                                    const int* __restrict__ slots,
                                                                    const float4* __restrict__ P,
                                                                    float4* __restrict__ Q,
                                                                    const float2* __restrict__ tw) {
-    constexpr int C = mx_cols<N>();
-    constexpr int TH = mx_p2_threads<N>();
+    constexpr int C = mx_s2_cols<N>();
+    constexpr int TH = mx_s2_threads<N>();
     constexpr int PER = N * C / TH;  // = 8
     static_assert(PER == 8, "one radix-8 lane per thread and column");
-    constexpr int TL = mx_tile_len<N>();
+    constexpr int TL = mx_s2_tile_len<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* ta = reinterpret_cast<float4*>(smem_raw);
     float4* tb = ta + TL;
