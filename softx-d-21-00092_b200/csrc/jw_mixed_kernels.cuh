@@ -21,16 +21,15 @@
 
 namespace jw {
 
-// pass 1 stages V in chunks of 256 sites (36 KB) so that two CTAs fit per SM at N = 512;
-// at N = 2048 (half the pair rows per CTA) 512 threads take 512-site chunks
-template <int N> constexpr int mx_vc() { return N >= 2048 ? 512 : (N < 256 ? N : 256); }
-template <int N> constexpr int mx_groups() {
-    return (16 * padded_len16(8 * N) + 16 * 9 * mx_vc<N>()) > 220 * 1024 ? 2 : 1;
-}
+// Passes 1 and 3 hold whole rows of pair planes in shared memory; each thread
+// loads the V of its own sites straight into registers (a warp's loads of one
+// plane are contiguous), early enough that the noise or the exponentials of
+// the site cover the latency.  At N = 2048 the 8 pair rows of pass 1 take
+// 295 KB, so two CTAs (groups) share a row: noise rows and rotated rows.
+template <int N> constexpr int mx_groups() { return 16 * padded_len16(8 * N) > 220 * 1024 ? 2 : 1; }
 template <int N> constexpr int mx_p1_threads() { return N >= 2048 ? 512 : 256; }
-template <int N> constexpr size_t mx_p1_smem() {
-    return 16 * (size_t)padded_len16(8 / mx_groups<N>() * N) + 16 * 9 * (size_t)mx_vc<N>();
-}
+template <int N> constexpr size_t mx_p1_smem() { return 16 * (size_t)padded_len16(8 / mx_groups<N>() * N); }
+template <int N> constexpr int mx_p1_blocks() { return mx_p1_threads<N>() <= 256 && mx_p1_smem<N>() <= 113 * 1024 ? 2 : 1; }
 // pass 2 tile width: 4 columns (64-byte rows, padded) while two tiles fit in 80 KB
 // (160 KB from N = 1024 on: one CTA of 512 threads, rows of 64 or 32 bytes)
 template <int N> constexpr int mx_cols() {
@@ -58,29 +57,17 @@ template <int N> constexpr int mx_s2_tile_len() {
 }
 template <int N> constexpr size_t mx_s2_smem() { return 2 * 16 * (size_t)mx_s2_tile_len<N>(); }
 template <int N> constexpr int mx_s2_blocks() { return mx_s2_threads<N>() <= 256 ? 2 : 1; }
-// pass 3: V staged in chunks of mx_p3_vc sites (128 at N = 1024, so that two CTAs
-// fit), mx_p3_threads threads
-template <int N, bool MEAS = false> constexpr int mx_p3_vc() {
-    return N == 1024 ? 128 : (MEAS && N == 512 ? 256 : v_chunk<N>());
-}
+// pass 3: mx_p3_threads threads; the 4 inverse-transformed pair rows in shared
+// memory.  MEAS: pass 3 also leaves the row-transformed measurement planes of
+// the new V (5 FP32 pair planes, as k_meas32_rows writes them) in a fifth row.
 template <int N> constexpr int mx_p3_threads() { return row_threads<N>(); }
-// MEAS: pass 3 also leaves the row-transformed measurement planes of the new V
-// (5 FP32 pair planes, as k_meas32_rows writes them) in a fifth row of shared
-// memory, with V chunks of 256 sites at 512^2; up to 1024^2, where two such
-// CTAs still fit on an SM
 template <int N, bool MEAS = false> constexpr size_t mx_p3_smem() {
-    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N) + 16 * 9 * (size_t)mx_p3_vc<N, MEAS>();
+    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N);
 }
-template <int N> constexpr bool mx_p3_meas_fits() { return mx_p3_smem<N, true>() <= 112 * 1024; }
-
-// V sites [c0, c0 + VC) of row x into smV[k][VC] (16-byte copies)
-template <int N, int VC>
-__device__ __forceinline__ void stage_v_chunk(double2* smV, const double2* __restrict__ V, long vol, int x, int c0) {
-    for (int i = threadIdx.x; i < 9 * VC; i += blockDim.x) {
-        const int k = i / VC, yy = i - k * VC;
-        cp_async<16>(&smV[i], &V[k * vol + (long)x * N + c0 + yy]);
-    }
+template <int N, bool MEAS = false> constexpr int mx_p3_blocks() {
+    return mx_p3_threads<N>() <= 256 && mx_p3_smem<N, MEAS>() <= 113 * 1024 ? 2 : 1;
 }
+template <int N> constexpr bool mx_p3_meas_fits() { return mx_p3_smem<N, true>() <= 220 * 1024; }
 
 // Gell-Mann coefficients of R = V xi V^dagger, xi = sum_a n_a L_a: only the
 // upper triangle and the real diagonal of R are formed (R is Hermitian).
@@ -146,16 +133,14 @@ __device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int 
 
 // ------------------------------------------------------------------ pass 1
 template <int N>
-__global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev* __restrict__ ev,
-                                                                   const int* __restrict__ slots,
-                                                                   float4* __restrict__ P,
-                                                                   const float2* __restrict__ tw) {
-    constexpr int VC = mx_vc<N>();
+__global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_pass1(const EventDev* __restrict__ ev,
+                                                                                     const int* __restrict__ slots,
+                                                                                     float4* __restrict__ P,
+                                                                                     const float2* __restrict__ tw) {
     constexpr int G = mx_groups<N>();
     constexpr int NP = 8 / G;  // pair rows per CTA
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
-    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(NP * N));
     const int x = blockIdx.x, g = blockIdx.y, b = blockIdx.z;
     const EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
@@ -163,49 +148,38 @@ __global__ void __launch_bounds__(mx_p1_threads<N>()) k_mix_pass1(const EventDev
     const bool want_noise = (G == 1) || g == 0;
     const bool want_rot = (G == 1) || g == 1;
     const int rot_base = (G == 1) ? 4 : 0;
-    for (int c0 = 0; c0 < N; c0 += VC) {
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        double2 dv[9];
         if (want_rot) {
-            if (c0 > 0) __syncthreads();
-            stage_v_chunk<N, VC>(smV, e.V, vol, x, c0);
-            cp_async_commit();
+#pragma unroll
+            for (int k = 0; k < 9; ++k) dv[k] = __ldg(&e.V[k * vol + site]);  // in flight during the noise
         }
-        const bool have = threadIdx.x < VC;
-        const int y = c0 + threadIdx.x;
         float z[16];
-        if (have) {
-            const long site = (long)x * N + y;
-            langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-            const float f = nf ? nf[site] : 1.0f;
+        langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+        const float f = nf ? nf[site] : 1.0f;
 #pragma unroll
-            for (int k = 0; k < 16; ++k) z[k] *= f;
-            if (want_noise) {
+        for (int k = 0; k < 16; ++k) z[k] *= f;
+        if (want_noise) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
-                    sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
-            }
+            for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+                sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
         }
         if (want_rot) {
-            cp_async_wait<0>();
-            __syncthreads();
-            if (have) {
-                float n[8], m[8], hx[8], hy[8];
+            float n[8], m[8], hx[8], hy[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    n[k] = z[2 * k];
-                    m[k] = z[2 * k + 1];
-                }
-                float2 v[9];
-#pragma unroll
-                for (int k = 0; k < 9; ++k) {
-                    const double2 dv = smV[k * VC + threadIdx.x];
-                    v[k] = make_float2((float)dv.x, (float)dv.y);
-                }
-                rotate_herm(v, n, hx);
-                rotate_herm(v, m, hy);
-#pragma unroll
-                for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
-                    sm[pad16((rot_base + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+            for (int k = 0; k < 8; ++k) {
+                n[k] = z[2 * k];
+                m[k] = z[2 * k + 1];
             }
+            float2 v[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) v[k] = make_float2((float)dv[k].x, (float)dv[k].y);
+            rotate_herm(v, n, hx);
+            rotate_herm(v, m, hy);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+                sm[pad16((rot_base + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
         }
     }
     __syncthreads();
@@ -277,11 +251,15 @@ __global__ void __launch_bounds__(mx_s2_threads<N>(), mx_s2_blocks<N>()) k_mix_p
 
 // ------------------------------------------------------------------ pass 3
 // The update of site y: V <- exp(+i sqrt(eps) B) V exp(-i sqrt(eps) A), A and B
-// from the inverse row transforms in column y of the row buffer, V the old
-// value staged in smV (chunk from c0).  Reports non-finite entries in fl.
-template <int N, int VC>
-__device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, const double2* smV, int y, int c0,
-                                        double se, double2 (&v)[9], int& fl) {
+// from the inverse row transforms in column y of the row buffer.  The old V is
+// loaded first and arrives while exp(+i sqrt(eps) B) is formed; one
+// exponential is held at a time.  Reports non-finite entries in fl.
+template <int N>
+__device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, int y, long site, long vol, double se,
+                                        double2 (&v)[9], int& fl) {
+    double2 v0[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v0[k] = e.V[k * vol + site];
     double a[8], bq[8];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -291,15 +269,13 @@ __device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, con
         bq[2 * j] = (double)u.z * -se;
         bq[2 * j + 1] = (double)u.w * -se;
     }
-    double2 mA[9], mB[9], tmp[9];
-    embed_lambda<double>(a, mA);
-    embed_lambda<double>(bq, mB);
-    expi_ch(mB, -1.0);  // exp(+i sqrt(eps) B)
-    expi_ch(mA, -1.0);  // exp(-i sqrt(eps) A)
-#pragma unroll
-    for (int k = 0; k < 9; ++k) v[k] = smV[k * VC + (y - c0)];
-    mul3(mB, v, tmp);
-    mul3(tmp, mA, v);
+    double2 m[9], tmp[9];
+    embed_lambda<double>(bq, m);
+    expi_ch(m, -1.0);  // exp(+i sqrt(eps) B), formed while V arrives
+    mul3(m, v0, tmp);
+    embed_lambda<double>(a, m);
+    expi_ch(m, -1.0);  // exp(-i sqrt(eps) A)
+    mul3(tmp, m, v);
     if (e.reunit) reunitarize(v);
 #pragma unroll
     for (int k = 0; k < 9; ++k)
@@ -307,16 +283,14 @@ __device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, con
 }
 
 template <int N, bool MEAS = false>
-__global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 ? 2 : 1) k_mix_pass3(EventDev* __restrict__ ev,
-                                                                    const int* __restrict__ slots,
-                                                                    const float4* __restrict__ Q,
-                                                                    const float2* __restrict__ tw,
-                                                                    int* __restrict__ flags,
-                                                                    float4* __restrict__ M) {
-    constexpr int VC = mx_p3_vc<N, MEAS>();
+__global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k_mix_pass3(EventDev* __restrict__ ev,
+                                                                                         const int* __restrict__ slots,
+                                                                                         const float4* __restrict__ Q,
+                                                                                         const float2* __restrict__ tw,
+                                                                                         int* __restrict__ flags,
+                                                                                         float4* __restrict__ M) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
-    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N));
     const int x = blockIdx.x, b = blockIdx.y;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
@@ -324,35 +298,24 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_threads<N>() <= 256 
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    stage_v_chunk<N, VC>(smV, e.V, vol, x, 0);
-    cp_async_commit();
-    cp_async_wait<1>();
+    cp_async_wait<0>();
     __syncthreads();
     fft16_rows<N, 4>(sm, 1.0f, tw);
     const double se = e.sqrt_eps;
     int fl = 0;
-    for (int c0 = 0; c0 < N; c0 += VC) {
-        if (c0 > 0) {
-            __syncthreads();
-            stage_v_chunk<N, VC>(smV, e.V, vol, x, c0);
-            cp_async_commit();
-        }
-        cp_async_wait<0>();
-        __syncthreads();
-        for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
-            double2 v[9];
-            p3_site<N, VC>(e, sm, smV, y, c0, se, v, fl);
-            const long site = (long)x * N + y;
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        double2 v[9];
+        p3_site<N>(e, sm, y, site, vol, se, v, fl);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) e.V[k * vol + site] = v[k];
-            if constexpr (MEAS) {
-                // entries 2p, 2p + 1 of the new V as pair element (p, y); this
-                // thread alone has read or written column y of the row buffer
+        for (int k = 0; k < 9; ++k) e.V[k * vol + site] = v[k];
+        if constexpr (MEAS) {
+            // entries 2p, 2p + 1 of the new V as pair element (p, y); this
+            // thread alone has read or written column y of the row buffer
 #pragma unroll
-                for (int p = 0; p < 5; ++p) {
-                    const double2 hi = p < 4 ? v[2 * p + 1] : make_double2(0.0, 0.0);
-                    sm[pad16(p * N + y)] = make_float4((float)v[2 * p].x, (float)v[2 * p].y, (float)hi.x, (float)hi.y);
-                }
+            for (int p = 0; p < 5; ++p) {
+                const double2 hi = p < 4 ? v[2 * p + 1] : make_double2(0.0, 0.0);
+                sm[pad16(p * N + y)] = make_float4((float)v[2 * p].x, (float)v[2 * p].y, (float)hi.x, (float)hi.y);
             }
         }
     }
@@ -377,14 +340,12 @@ template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
 template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>(); }
 
 template <int N>
-__global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_smem<N>() <= 112 * 1024 ? 2 : 1) k_mix_pass31(
+__global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_pass31(
     EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q, float4* __restrict__ P,
     const float2* __restrict__ tw, int* __restrict__ flags) {
     static_assert(mx_fuse31<N>(), "one CTA holds all 8 pair rows");
-    constexpr int VC = mx_vc<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
-    double2* smV = reinterpret_cast<double2*>(smem_raw + 16 * (size_t)padded_len16(8 * N));
     const int x = blockIdx.x, b = blockIdx.y;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
@@ -392,54 +353,43 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_smem<N>() <= 112 * 
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    stage_v_chunk<N, VC>(smV, e.V, vol, x, 0);
-    cp_async_commit();
-    cp_async_wait<1>();
+    cp_async_wait<0>();
     __syncthreads();
     fft16_rows<N, 4>(sm, 1.0f, tw);
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
     int fl = 0;
-    for (int c0 = 0; c0 < N; c0 += VC) {
-        if (c0 > 0) {
-            __syncthreads();
-            stage_v_chunk<N, VC>(smV, e.V, vol, x, c0);
-            cp_async_commit();
-        }
-        cp_async_wait<0>();
-        __syncthreads();
-        for (int y = c0 + threadIdx.x; y < c0 + VC; y += blockDim.x) {
-            const long site = (long)x * N + y;
-            float2 v32[9];
-            {
-                double2 v[9];
-                p3_site<N, VC>(e, sm, smV, y, c0, se, v, fl);
+    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        float2 v32[9];
+        {
+            double2 v[9];
+            p3_site<N>(e, sm, y, site, vol, se, v, fl);
 #pragma unroll
-                for (int k = 0; k < 9; ++k) {
-                    e.V[k * vol + site] = v[k];
-                    v32[k] = make_float2((float)v[k].x, (float)v[k].y);
-                }
+            for (int k = 0; k < 9; ++k) {
+                e.V[k * vol + site] = v[k];
+                v32[k] = make_float2((float)v[k].x, (float)v[k].y);
             }
-            float z[16];
-            langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-            const float f = nf ? nf[site] : 1.0f;
-#pragma unroll
-            for (int k = 0; k < 16; ++k) z[k] *= f;
-#pragma unroll
-            for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
-                sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
-            float n[8], m[8], hx[8], hy[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                n[k] = z[2 * k];
-                m[k] = z[2 * k + 1];
-            }
-            rotate_herm(v32, n, hx);
-            rotate_herm(v32, m, hy);
-#pragma unroll
-            for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
-                sm[pad16((4 + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
         }
+        float z[16];
+        langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+        const float f = nf ? nf[site] : 1.0f;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) z[k] *= f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+            sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+        float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            n[k] = z[2 * k];
+            m[k] = z[2 * k + 1];
+        }
+        rotate_herm(v32, n, hx);
+        rotate_herm(v32, m, hy);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+            sm[pad16((4 + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
     }
     if (fl) atomicOr(flags, fl);
     __syncthreads();
