@@ -423,6 +423,30 @@ def c1_leg(jw, device: int):
     out = {"workload": "1 event 64^2 FP64, MV Ny = 50, 100 fixed-coupling steps, measurement (call-for-call layer)",
            "status": status, "total_ms": ic + steps + meas, "initial_condition_ms": ic, "steps_ms": steps,
            "measure_ms": meas, "site_steps_per_s": n * n * 100 / (steps / 1e3), "Qs": qs}
+    # the same event through the FP64 batched engine (fused kernels, graph replay)
+    eng = jw.Engine(precision=jw.PRECISION_FP64, device=device)
+    warm = eng.add_event(n, ny_slices=NY_SLICES, mu=0.5 * n, mass=MASS, step=STEP,
+                         coupling=jw.FIXED_COUPLING_CONSTANT, seed=2)
+    eng.init_mv([warm])
+    eng.step([warm], 3)
+    eng.measure([warm])
+    eid = eng.add_event(n, ny_slices=NY_SLICES, mu=0.5 * n, mass=MASS, step=STEP,
+                        coupling=jw.FIXED_COUPLING_CONSTANT, seed=1)
+    es = torch.cuda.ExternalStream(eng.stream)
+    torch.cuda.synchronize()
+    ev[0].record(es)
+    eng.init_mv([eid])
+    ev[1].record(es)
+    eng.step([eid], 100)
+    ev[2].record(es)
+    eng.measure([eid])
+    ev[3].record(es)
+    ev[3].synchronize()
+    estatus = eng.sync()
+    eng.close()
+    ic, steps, meas = (ev[i].elapsed_time(ev[i + 1]) for i in range(3))
+    out["engine_fp64"] = {"status": estatus, "total_ms": ic + steps + meas, "initial_condition_ms": ic,
+                          "steps_ms": steps, "measure_ms": meas, "site_steps_per_s": n * n * 100 / (steps / 1e3)}
     t, why = run_reference_main(10, 2, n_side=n)
     out["cpu_baseline"] = ({"value": n * n / t, "unit": "site-steps/s", "cores": os.cpu_count(), "kind": "reference",
                             "sample": f"main_optimized at {n}^2, 10 steps after 2 warm-up, SQRT coupling"}
