@@ -1,0 +1,74 @@
+"""GPU tests of the engine's multi-step runs.  A call of K mixed-precision steps
+runs pass 1, then K - 1 times (pass 2, pass 3 fused with the next pass 1), then
+pass 2 and pass 3; K calls of one step never use the fused kernel.  Both must
+give bit-identical lattices, as must any split of the steps into calls, the
+timed run, and chunked launch groups."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def jw():
+    import jimwlk
+    return jimwlk
+
+
+def make(jw, N, events, precision, max_batch=0):
+    eng = jw.Engine(precision=precision, max_batch=max_batch)
+    ids = [eng.add_event(N, ny_slices=2, mu=0.5 * N, mass=0.04, step=2e-3, coupling=jw.FIXED_COUPLING_CONSTANT,
+                         seed=11 + i) for i in range(events)]
+    eng.init_mv(ids)
+    return eng, ids
+
+
+@pytest.mark.parametrize("precision,N,events", [
+    ("mixed", 64, 3),      # fused pass 3 + 1
+    ("mixed", 512, 2),     # fused, two CTAs per SM
+    ("mixed", 1024, 1),    # fused, one CTA per SM
+    ("fp64", 64, 2),       # FP64 engine: per-step graph replay
+])
+def test_split_of_steps_into_calls_is_bitwise_invariant(jw, precision, N, events):
+    prec = jw.PRECISION_MIXED if precision == "mixed" else jw.PRECISION_FP64
+    splits = {"one call": [7], "single steps": [1] * 7, "3 + 4": [3, 4], "2 + 5": [2, 5]}
+    finals = {}
+    for name, parts in splits.items():
+        eng, ids = make(jw, N, events, prec)
+        for k in parts:
+            eng.step(ids, k)
+        assert eng.sync() == jw.OK
+        finals[name] = [eng.get_V(i) for i in ids]
+        assert all(eng.steps_taken(i) == 7 for i in ids)
+        eng.close()
+    # the same 7 steps through the timed run
+    eng, ids = make(jw, N, events, prec)
+    kernels, total = eng.step_timed(ids, 7)
+    assert eng.sync() == jw.OK and total > 0
+    finals["timed"] = [eng.get_V(i) for i in ids]
+    eng.close()
+    ref = finals["one call"]
+    assert np.abs(ref[0]).max() > 0
+    for name, vs in finals.items():
+        for a, b in zip(ref, vs):
+            assert np.array_equal(a, b), name
+    # launches of the timed run: mixed 1 + 7 + 1 + 6 (pass 1, pass 2, pass 3, pass 3+1)
+    counts = {k: c for k, (_, c) in kernels.items()}
+    if precision == "mixed":
+        assert counts == {"pass1": 1, "pass2": 7, "pass3": 1, "pass31": 6}
+    else:
+        assert counts == {"pass1": 7, "pass2": 7, "pass3": 7, "pass31": 0}
+
+
+def test_chunked_launch_groups_match_one_group(jw):
+    """max_batch splits the events into launch groups that each run all their
+    steps in turn; the lattices equal those of one launch group."""
+    a, ida = make(jw, 128, 5, jw.PRECISION_MIXED)
+    b, idb = make(jw, 128, 5, jw.PRECISION_MIXED, max_batch=2)
+    a.step(ida, 6)
+    b.step(idb, 6)
+    assert a.sync() == jw.OK and b.sync() == jw.OK
+    for i, j in zip(ida, idb):
+        assert np.array_equal(a.get_V(i), b.get_V(j))
+    a.close()
+    b.close()
