@@ -505,7 +505,7 @@ def main_arm(args):
 
     events = args.events
     n_side = args.n
-    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch)
+    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch, autotune=True)
     ids = [eng.add_event(n_side, ny_slices=NY_SLICES, mu=0.5 * n_side, mass=MASS, step=STEP,
                          coupling=jw.FIXED_COUPLING_CONSTANT, seed=sd) for sd in event_seeds(rank, events)]
     eng.init_mv(ids)
@@ -582,7 +582,8 @@ def main_arm(args):
                    "max_batch": args.max_batch,
                    "N": n_side, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "alpha_s": ALPHA_S, "ds": DS,
                    "step": STEP, "kernel": "SIN", "coupling": "fixed", "l2": "inputs ~5.6 GB per GPU > L2",
-                   "parallelism": f"events sharded, {world} rank(s)"},
+                   "parallelism": f"events sharded, {world} rank(s)",
+                   "autotuned_column_tile": eng.tuning(n_side)},
         "e2e": {"value": e2e_value, "unit": "site-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e,
                 "what": "jw_engine_step_measure_ensemble per step (one step + ensemble measurement to host arrays)",

@@ -266,6 +266,10 @@ typedef struct jw_engine_options {
     int max_batch;        /* events advanced per launch group (0 = all) */
     size_t max_batch_sites; /* and at most this many lattice sites per launch group (0 = no limit;
                                at least one event), which also bounds each size's workspace */
+    int autotune;         /* nonzero: the first mixed-precision run of each lattice size times
+                             every compiled column-tile width of the column pass on its own
+                             workspace and keeps the fastest (jw_engine_tuning); results do
+                             not depend on the choice.  0: the built-in default */
 } jw_engine_options;
 
 typedef struct jw_event_desc {
@@ -357,6 +361,14 @@ jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double
  * V for the measurement, so V is not read again. */
 jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, int nsteps, double* sum,
                                           double* err);
+/* The column-tile width the autotuner chose for lattice size N (columns per
+ * CTA of the mixed column pass), or 0 when it has not run for that size.
+ * JW_ENOTFOUND if the engine holds no event of that size. */
+jw_status jw_engine_tuning(jw_engine* e, int N, int* p2_cols);
+/* Fix the column-tile width of size N's column pass (1, 2, 4 or 8 where it
+ * fits, JW_EINVAL otherwise; 0 = the built-in default), for example a width
+ * found once by the autotuner and kept; the autotuner then skips that size. */
+jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
  * event around each kernel launch.  kernel_ms[4] receives the milliseconds
  * spent in each kernel kind and launches[4] its launch count: pass 1, pass 2,

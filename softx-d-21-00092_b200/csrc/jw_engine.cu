@@ -7,6 +7,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 #include "jw_engine_kernels.cuh"
@@ -33,6 +34,8 @@ struct Group {
     float* k32[kCouplings] = {};
     double* nf64 = nullptr;          // noise factor (NOISE coupling)
     float* nf32 = nullptr;
+    int p2_cols = 0;                 // mixed pass 2 column-tile width (0: the default)
+    bool tuned = false;              // the autotuner has run for this size
 };
 
 struct Event {
@@ -415,12 +418,40 @@ struct LaunchTimes {
     }
 };
 
+// f(std::integral_constant<int, C>) for every valid pass-2 tile width C.
+template <int N, typename F>
+void for_each_p2_cols(F&& f) {
+    if constexpr (mx_s2_valid<N, 1>()) f(std::integral_constant<int, 1>{});
+    if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, 2>{});
+    if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, 4>{});
+    if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, 8>{});
+}
+
+// Pass 2 with tile width `cols` (0: the default); advance = 0 leaves the step
+// index alone (timing launches of the autotuner).
+template <int N>
+void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, int advance) {
+    const long vol = (long)N * N;
+    float4* P = reinterpret_cast<float4*>(g.ws);
+    float4* Q = P + (size_t)8 * vol * nb;
+    if (cols == 0) cols = mx_s2_cols<N>();
+    for_each_p2_cols<N>([&](auto c) {
+        constexpr int C = decltype(c)::value;
+        if (C == cols)
+            k_mix_pass2<N, C><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
+                g.d_ev, d_slots, P, Q, g.tw.d32, advance);
+    });
+}
+
 template <int N>
 void mix_configure() {
     static bool configured = false;
     if (configured) return;
     cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
-    cudaFuncSetAttribute(k_mix_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_s2_smem<N>());
+    for_each_p2_cols<N>([](auto c) {
+        constexpr int C = decltype(c)::value;
+        cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_s2_smem<N, C>());
+    });
     cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p3_smem<N>());
     if constexpr (mx_p3_meas_fits<N>())
         cudaFuncSetAttribute(k_mix_pass3<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -446,8 +477,7 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
                 g.d_ev, d_slots, P, g.tw.d32);
             break;
         case KIND_P2:
-            k_mix_pass2<N><<<dim3(N / mx_s2_cols<N>(), 4, nb), mx_s2_threads<N>(), mx_s2_smem<N>(), e->stream>>>(
-                g.d_ev, d_slots, P, Q, g.tw.d32);
+            launch_pass2<N>(e, g, d_slots, nb, g.p2_cols, 1);
             break;
         case KIND_P3:
             if constexpr (mx_p3_meas_fits<N>()) {
@@ -480,12 +510,50 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
 // followed by launch_measure_ensemble).  The middle is captured once as a CUDA
 // graph and replayed when it repeats and nothing is timed.  Launch groups that
 // share the workspace run one after another, each through all its steps.
+// The autotuner: every valid pass-2 tile width runs 1 + 3 times on this launch
+// group's workspace (the step index frozen; pass 2 only maps P to Q, which the
+// run then recomputes), and the fastest by CUDA events is kept for the size.
+template <int N>
+cudaError_t tune_mix(jw_engine* e, Group& g, const int* d_slots, int nb) {
+    float best = 0.0f;
+    int best_cols = 0;
+    cudaError_t ce = cudaSuccess;
+    for_each_p2_cols<N>([&](auto c) {
+        constexpr int C = decltype(c)::value;
+        if (ce != cudaSuccess) return;
+        cudaEvent_t a = nullptr, b = nullptr;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        launch_pass2<N>(e, g, d_slots, nb, C, 0);
+        cudaEventRecord(a, e->stream);
+        for (int r = 0; r < 3; ++r) launch_pass2<N>(e, g, d_slots, nb, C, 0);
+        cudaEventRecord(b, e->stream);
+        ce = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (ce == cudaSuccess && (best_cols == 0 || ms < best)) {
+            best = ms;
+            best_cols = C;
+        }
+    });
+    if (ce != cudaSuccess) return ce;
+    g.p2_cols = best_cols;
+    g.tuned = true;
+    return cudaSuccess;
+}
+
 template <int N>
 cudaError_t launch_mix_run(jw_engine* e, Group& g, const int* d_slots, int nb, int nsteps, double* ens,
                            LaunchTimes* tm) {
     if (nsteps < 1) return cudaErrorInvalidValue;
     if (ens && !mx_p3_meas_fits<N>()) return cudaErrorInvalidValue;
     mix_configure<N>();
+    if (e->opt.autotune && !g.tuned) {
+        const cudaError_t ce = tune_mix<N>(e, g, d_slots, nb);
+        if (ce != cudaSuccess) return ce;
+    }
     auto middle = [&]() {
         mix_launch<N>(e, g, d_slots, nb, KIND_P2, false, tm);
         if constexpr (mx_fuse31<N>()) {
@@ -1403,6 +1471,49 @@ JW_EXPORT jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids
     k_ens_finalize<<<(unsigned)((vol + 255) / 256), 256, 0, e->stream>>>(ens, vol, out);
     JW_CUDA(cudaGetLastError());
     return copy_out_host(e, out, vol, sum, err);
+}
+
+namespace {
+template <int N>
+bool p2_cols_valid_n(int cols) {
+    bool ok = false;
+    for_each_p2_cols<N>([&](auto c) { ok = ok || decltype(c)::value == cols; });
+    return ok;
+}
+bool p2_cols_valid(int N, int cols) {
+    switch (N) {
+        case 8: return p2_cols_valid_n<8>(cols);
+        case 16: return p2_cols_valid_n<16>(cols);
+        case 32: return p2_cols_valid_n<32>(cols);
+        case 64: return p2_cols_valid_n<64>(cols);
+        case 128: return p2_cols_valid_n<128>(cols);
+        case 256: return p2_cols_valid_n<256>(cols);
+        case 512: return p2_cols_valid_n<512>(cols);
+        case 1024: return p2_cols_valid_n<1024>(cols);
+        case 2048: return p2_cols_valid_n<2048>(cols);
+        default: return false;
+    }
+}
+}  // namespace
+
+JW_EXPORT jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols) {
+    JW_CHECK(e);
+    auto it = e->groups.find(N);
+    if (it == e->groups.end()) return JW_ENOTFOUND;
+    if (p2_cols != 0 && !p2_cols_valid(N, p2_cols)) return JW_EINVAL;
+    JW_CUDA(cudaStreamSynchronize(e->stream));  // launches already queued keep their width
+    it->second->p2_cols = p2_cols;
+    it->second->tuned = true;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_tuning(jw_engine* e, int N, int* p2_cols) {
+    JW_CHECK(e && p2_cols);
+    auto it = e->groups.find(N);
+    if (it == e->groups.end()) return JW_ENOTFOUND;
+    const Group& g = *it->second;
+    *p2_cols = g.tuned ? g.p2_cols : 0;
+    return JW_OK;
 }
 
 JW_EXPORT jw_status jw_engine_step_timed(jw_engine* e, const int* ids, int n, int nsteps, double* kernel_ms,

@@ -49,14 +49,17 @@ template <int N> constexpr int mx_tile_len() {
     return mx_cols<N>() >= 8 ? N * mx_cols<N>() : N * mx_cols<N>() + (N / 8) * mx_cols<N>();
 }
 template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile_len<N>(); }
-// the step's pass 2 (k_mix_pass2): its own tile width, two tiles (planes j, 4 + j)
+// The step's pass 2 (k_mix_pass2) is built for every column-tile width C in
+// {1, 2, 4, 8} that fits (C N/8 <= 1024 threads, two tiles in 227 KB); the
+// engine's autotuner picks one per lattice size, mx_s2_cols is the default.
 template <int N> constexpr int mx_s2_cols() { return mx_cols<N>(); }
-template <int N> constexpr int mx_s2_threads() { return mx_s2_cols<N>() * (N / 8); }
-template <int N> constexpr int mx_s2_tile_len() {
-    return mx_s2_cols<N>() >= 8 ? N * mx_s2_cols<N>() : N * mx_s2_cols<N>() + (N / 8) * mx_s2_cols<N>();
+template <int N, int C> constexpr int mx_s2_threads() { return C * (N / 8); }
+template <int N, int C> constexpr int mx_s2_tile_len() { return C >= 8 ? N * C : N * C + (N / 8) * C; }
+template <int N, int C> constexpr size_t mx_s2_smem() { return 2 * 16 * (size_t)mx_s2_tile_len<N, C>(); }
+template <int N, int C> constexpr int mx_s2_blocks() { return mx_s2_threads<N, C>() <= 256 ? 2 : 1; }
+template <int N, int C> constexpr bool mx_s2_valid() {
+    return C <= N && mx_s2_threads<N, C>() <= 1024 && mx_s2_smem<N, C>() <= 227 * 1024;
 }
-template <int N> constexpr size_t mx_s2_smem() { return 2 * 16 * (size_t)mx_s2_tile_len<N>(); }
-template <int N> constexpr int mx_s2_blocks() { return mx_s2_threads<N>() <= 256 ? 2 : 1; }
 // pass 3: mx_p3_threads threads; the 4 inverse-transformed pair rows in shared
 // memory.  MEAS: pass 3 also leaves the row-transformed measurement planes of
 // the new V (5 FP32 pair planes, as k_meas32_rows writes them) in a fifth row.
@@ -192,25 +195,25 @@ __global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_p
 // holds rows r0 + m N/8 of column cc between the transforms (fft16x), so the
 // plane-j transform starts from global loads, the kernel product and the
 // inverse start from registers and the inverse ends in the store.
-template <int N>
-__global__ void __launch_bounds__(mx_s2_threads<N>(), mx_s2_blocks<N>()) k_mix_pass2(EventDev* __restrict__ ev,
+template <int N, int C>
+__global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k_mix_pass2(EventDev* __restrict__ ev,
                                                                    const int* __restrict__ slots,
                                                                    const float4* __restrict__ P,
                                                                    float4* __restrict__ Q,
-                                                                   const float2* __restrict__ tw) {
-    constexpr int C = mx_s2_cols<N>();
-    constexpr int TH = mx_s2_threads<N>();
+                                                                   const float2* __restrict__ tw, int advance) {
+    constexpr int TH = mx_s2_threads<N, C>();
     constexpr int PER = N * C / TH;  // = 8
     static_assert(PER == 8, "one radix-8 lane per thread and column");
-    constexpr int TL = mx_s2_tile_len<N>();
+    constexpr int TL = mx_s2_tile_len<N, C>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* ta = reinterpret_cast<float4*>(smem_raw);
     float4* tb = ta + TL;
     const int c0 = blockIdx.x * C, j = blockIdx.y, b = blockIdx.z;
     const EventDev& e = ev[slots[b]];
     // the step index advances here: pass 1 of this step has read it, and the
-    // next step's noise (pass 1, or pass 3 + 1) reads the new value
-    if (blockIdx.x == 0 && j == 0 && threadIdx.x == 0) ev[slots[b]].step += 1;
+    // next step's noise (pass 1, or pass 3 + 1) reads the new value (advance = 0:
+    // a timing launch of the autotuner)
+    if (advance && blockIdx.x == 0 && j == 0 && threadIdx.x == 0) ev[slots[b]].step += 1;
     const long vol = (long)N * N;
     const int cc = threadIdx.x % C, r0 = threadIdx.x / C;
     constexpr int RSTEP = TH / C;  // = N / 8

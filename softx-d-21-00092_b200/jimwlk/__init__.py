@@ -42,7 +42,7 @@ class jw_config(ctypes.Structure):
 
 class jw_engine_options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("reunitarize", ctypes.c_int), ("max_bytes", ctypes.c_size_t),
-                ("max_batch", ctypes.c_int), ("max_batch_sites", ctypes.c_size_t)]
+                ("max_batch", ctypes.c_int), ("max_batch_sites", ctypes.c_size_t), ("autotune", ctypes.c_int)]
 
 
 class jw_event_desc(ctypes.Structure):
@@ -160,6 +160,8 @@ def _load():
         "jw_engine_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp], ctypes.c_int),
         "jw_engine_step_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp, _dp],
                                             ctypes.c_int),
+        "jw_engine_tuning": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "jw_engine_set_tuning": ([_vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp,
                                   ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     }
@@ -402,8 +404,9 @@ class Engine:
     """The batched engine (jw_engine): resident events advanced by fused kernels."""
 
     def __init__(self, precision: int = PRECISION_MIXED, reunitarize: bool = False, max_bytes: int = 0,
-                 max_batch: int = 0, device: int = 0, max_batch_sites: int = 0):
-        self.opt = jw_engine_options(precision, int(reunitarize), max_bytes, max_batch, max_batch_sites)
+                 max_batch: int = 0, device: int = 0, max_batch_sites: int = 0, autotune: bool = False):
+        self.opt = jw_engine_options(precision, int(reunitarize), max_bytes, max_batch, max_batch_sites,
+                                     int(autotune))
         self._h = _vp()
         _ck(_lib.jw_engine_create(ctypes.byref(self.opt), device, ctypes.byref(self._h)), "jw_engine_create")
         self.N = {}
@@ -549,6 +552,15 @@ class Engine:
         _ck(_lib.jw_engine_step_measure_ensemble(self._h, arr, n, int(nsteps), s.ctypes.data_as(_dp),
                                                  e.ctypes.data_as(_dp)), "jw_engine_step_measure_ensemble")
         return s, e
+
+    def tuning(self, N: int) -> int:
+        """Column-tile width the autotuner chose for size N (0 if it has not run)."""
+        c = ctypes.c_int(0)
+        _ck(_lib.jw_engine_tuning(self._h, int(N), ctypes.byref(c)), "jw_engine_tuning")
+        return c.value
+
+    def set_tuning(self, N: int, p2_cols: int) -> None:
+        _ck(_lib.jw_engine_set_tuning(self._h, int(N), int(p2_cols)), "jw_engine_set_tuning")
 
     def step_timed(self, ids, nsteps: int):
         """nsteps steps with every kernel timed: ({kind: (total ms, launches)}, total ms)."""

@@ -72,3 +72,42 @@ def test_chunked_launch_groups_match_one_group(jw):
         assert np.array_equal(a.get_V(i), b.get_V(j))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("N", [64, 512, 2048])
+def test_autotuner_choice_does_not_change_results(jw, N):
+    """The autotuner picks a valid column-tile width on the first run of a size,
+    and every width gives the same lattice bit for bit."""
+    events = {64: 3, 512: 2, 2048: 1}[N]
+    eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+    eng.step(ids, 4)
+    ref = [eng.get_V(i) for i in ids]
+    eng.close()
+    tuned = jw.Engine(precision=jw.PRECISION_MIXED, autotune=True)
+    tids = [tuned.add_event(N, ny_slices=2, mu=0.5 * N, mass=0.04, step=2e-3, coupling=jw.FIXED_COUPLING_CONSTANT,
+                            seed=11 + i) for i in range(events)]
+    tuned.init_mv(tids)
+    assert tuned.tuning(N) == 0
+    tuned.step(tids, 4)
+    assert tuned.sync() == jw.OK
+    chosen = tuned.tuning(N)
+    assert chosen in (1, 2, 4, 8)
+    for a, i in zip(ref, tids):
+        assert np.array_equal(a, tuned.get_V(i))
+    assert all(tuned.steps_taken(i) == 4 for i in tids)
+    tuned.close()
+    widths = [c for c in (1, 2, 4, 8) if c <= N and c * (N // 8) <= 1024 and
+              2 * 16 * (N * c + (0 if c >= 8 else (N // 8) * c)) <= 227 * 1024]
+    assert chosen in widths
+    for c in widths:
+        eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+        eng.set_tuning(N, c)
+        eng.step(ids, 4)
+        assert eng.sync() == jw.OK
+        for a, i in zip(ref, ids):
+            assert np.array_equal(a, eng.get_V(i)), c
+        eng.close()
+    eng, ids = make(jw, N, 1, jw.PRECISION_MIXED)
+    with pytest.raises(RuntimeError):
+        eng.set_tuning(N, 3)
+    eng.close()
