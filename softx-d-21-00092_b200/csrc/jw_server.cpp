@@ -364,8 +364,9 @@ JW_EXPORT jw_status jw_server_create(const jw_server_options* opt, int device, j
         s->be = std::move(fb);
     } else {
         auto eb = std::make_unique<EngineBackend>();
-        // launch groups (and their workspaces) no larger than a tick
-        jw_engine_options eo{opt->precision, opt->reunitarize, opt->max_bytes, 0, opt->tick_sites};
+        // launch groups (and their workspaces) no larger than a tick; column
+        // tiles autotuned per lattice size
+        jw_engine_options eo{opt->precision, opt->reunitarize, opt->max_bytes, 0, opt->tick_sites, 1};
         const jw_status st = jw_engine_create(&eo, device, &eb->e);
         if (st) {
             delete s;
