@@ -307,7 +307,12 @@ jw_status jw_engine_init_mv(jw_engine* e, const int* ids, int n);
 /* Host V in the reference layout. */
 jw_status jw_engine_set_V(jw_engine* e, int event_id, const double* host);
 jw_status jw_engine_get_V(jw_engine* e, int event_id, double* host);
-/* Advance the listed events by nsteps Langevin steps each (fused kernels). */
+/* Advance the listed events by nsteps Langevin steps each (main_optimized.cpp:234-304
+ * per step).  Mixed precision runs the steps of each launch group as pass 1,
+ * then nsteps - 1 times (pass 2, pass 3 fused with the next pass 1), then pass 2
+ * and pass 3, with the repeated part replayed as a CUDA graph; any split of
+ * the steps into calls gives the same lattices bit for bit.  Asynchronous on
+ * the engine stream (jw_engine_sync reports device errors). */
 jw_status jw_engine_step(jw_engine* e, const int* ids, int n, int nsteps);
 /* Dipole measurement of the listed events: C(k) of main_optimized.cpp:321-334
  * accumulated (sum, sum of squares) into each event's FP64 accumulators. */
