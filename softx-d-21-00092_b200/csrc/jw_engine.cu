@@ -650,11 +650,15 @@ cudaError_t launch_mv_slice(jw_engine* e, Group& g, const int* d_slots, int nb, 
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_mv16_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r);
+        cudaFuncSetAttribute(k_mv16_pass1<N, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r);
         cudaFuncSetAttribute(k_mv16_pass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c);
         cudaFuncSetAttribute(k_mv16_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r);
         configured = true;
     }
-    k_mv16_pass1<N><<<dim3(N, nb), mv16_threads<N>(), r, e->stream>>>(g.d_ev, d_slots, slice, P, g.tw.d64);
+    if (e->opt.precision == JW_PRECISION_MIXED)
+        k_mv16_pass1<N, float><<<dim3(N, nb), mv16_threads<N>(), r, e->stream>>>(g.d_ev, d_slots, slice, P, g.tw.d64);
+    else
+        k_mv16_pass1<N><<<dim3(N, nb), mv16_threads<N>(), r, e->stream>>>(g.d_ev, d_slots, slice, P, g.tw.d64);
     k_mv16_pass2<N><<<dim3(N / mx_cols<N>(), 4, nb), mx_p2_threads<N>(), c, e->stream>>>(g.d_ev, d_slots, P,
                                                                                          g.tw.d64);
     k_mv16_pass3<N><<<dim3(N, nb), mv16_threads<N>(), r, e->stream>>>(g.d_ev, d_slots, P, g.tw.d64, e->d_flags);

@@ -612,7 +612,9 @@ __device__ __forceinline__ void fft16_rows_d(double2* sm, double sign, const dou
     }
 }
 
-template <int N>
+// NT = float: the 8 normals from the FP32 Box-Muller (mixed precision; relative
+// error ~1e-7 against the FP64 stream), the charges and transforms stay FP64.
+template <int N, typename NT = double>
 __global__ void __launch_bounds__(mv16_threads<N>()) k_mv16_pass1(const EventDev* __restrict__ ev,
                                                                   const int* __restrict__ slots, int slice,
                                                                   double2* __restrict__ P,
@@ -623,8 +625,11 @@ __global__ void __launch_bounds__(mv16_threads<N>()) k_mv16_pass1(const EventDev
     const EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     for (int y = threadIdx.x; y < N; y += blockDim.x) {
+        NT zt[8];
+        mv_normals<NT>(e.seed, (uint32_t)slice, (uint32_t)((long)x * N + y), zt);
         double z[8];
-        mv_normals<double>(e.seed, (uint32_t)slice, (uint32_t)((long)x * N + y), z);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z[k] = (double)zt[k];
 #pragma unroll
         for (int s = 0; s < 4; ++s)
             sm[pad16(s * N + y)] = make_double2(z[2 * s] * e.mv_sigma + 0.0, z[2 * s + 1] * e.mv_sigma + 0.0);
@@ -696,11 +701,11 @@ __global__ void __launch_bounds__(mv16_threads<N>()) k_mv16_pass3(EventDev* __re
             f[2 * s + 1] = u.y;
         }
         double2 m[9], v[9], r[9];
-        embed_lambda<double>(f, m);
-        expi_ch(m, 1.0);  // exp(+i f)
         const long site = (long)x * N + y;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];
+        for (int k = 0; k < 9; ++k) v[k] = e.V[k * vol + site];  // arrives while exp(+i f) is formed
+        embed_lambda<double>(f, m);
+        expi_ch(m, 1.0);  // exp(+i f)
         mul3(v, m, r);
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
