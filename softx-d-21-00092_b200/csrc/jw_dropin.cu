@@ -20,11 +20,15 @@ constexpr int kThreads = 256;
 inline unsigned blocks_for(long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 // ---- generate_gaussian (field.h:2116-2243) / _with_noise_coupling_constant (:2245-2365)
+// step_ptr, when set, holds the step index instead of `step` (a step captured
+// once in a CUDA graph and replayed reads its index there).
 __global__ void k_generate_gaussian(double2* __restrict__ xx, double2* __restrict__ xy, int N, uint64_t seed,
-                                    uint64_t step, int with_coupling) {
+                                    uint64_t step, const unsigned long long* __restrict__ step_ptr,
+                                    int with_coupling) {
     const long vol = (long)N * N;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= vol) return;
+    if (step_ptr) step = *step_ptr;
     double z[16];
     langevin_normals<double>(seed, step, (uint32_t)i, z);
     double f = 1.0;
@@ -315,6 +319,7 @@ JW_EXPORT jw_status jw_context_destroy(jw_context* c) {
     twiddles_destroy(&c->tw);
     if (c->d_flags) cudaFree(c->d_flags);
     if (c->d_tmp) cudaFree(c->d_tmp);
+    if (c->d_step) cudaFree(c->d_step);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return JW_OK;
@@ -459,10 +464,13 @@ JW_EXPORT jw_status jw_generate_gaussian(jw_context* c, jw_field* xx, jw_field* 
     JW_CHECK(c && same_ctx(xx, xy) && xx->ctx == c && xx->t == 9 && xy->t == 9 && xx != xy);
     const int N = c->N;
     k_generate_gaussian<<<blocks_for((long)N * N), kThreads, 0, c->stream>>>(xx->d, xy->d, N, c->cfg.seed,
-                                                                             step_index, with_coupling);
+                                                                             step_index, nullptr, with_coupling);
     JW_CUDA(cudaGetLastError());
     return JW_OK;
 }
+
+__global__ void k_set_counter(unsigned long long* p, unsigned long long v) { *p = v; }
+__global__ void k_advance_counter(unsigned long long* p) { *p += 1; }
 
 JW_EXPORT jw_status jw_set_mv_model(jw_context* c, jw_field* f, int slice, double g, double mu, int ny_slices) {
     JW_CHECK(c && f && f->ctx == c && f->t == 9 && ny_slices > 0 && slice >= 0);
@@ -598,22 +606,66 @@ JW_EXPORT jw_status jw_evolve_momentum(jw_context* c, jw_field* V, uint64_t step
              *ux = c->mom_work[4], *uy = c->mom_work[5];
     const int with_coupling = cfg.CouplingChoice == JW_NOISE_COUPLING_CONSTANT;
     const int kc = cfg.CouplingChoice == JW_FIXED_COUPLING_CONSTANT ? JW_NOISE_COUPLING_CONSTANT : cfg.CouplingChoice;
-    for (int k = 0; k < n && s == JW_OK; ++k) {
-        s = jw_generate_gaussian(c, xx, xy, step0 + (uint64_t)k, with_coupling);
-        if (!s) s = jw_execute2D(c, xx, 1);
-        if (!s) s = jw_execute2D(c, xy, 1);
-        if (!s) s = jw_prepare_A_local(c, A, xx, xy, kc, cfg.KernelChoice);
-        if (!s) s = jw_execute2D(c, A, 0);
-        if (!s) s = jw_execute2D(c, xx, 0);
-        if (!s) s = jw_execute2D(c, xy, 0);
-        if (!s) s = jw_uxiulocal(c, ux, uy, V, xx, xy);
-        if (!s) s = jw_execute2D(c, ux, 1);
-        if (!s) s = jw_execute2D(c, uy, 1);
-        if (!s) s = jw_prepare_A_local(c, B, ux, uy, kc, cfg.KernelChoice);
-        if (!s) s = jw_execute2D(c, B, 0);
-        if (!s) s = jw_update_uf(c, V, B, A, cfg.step);
+    // one step in the reference's call order; from_counter: the noise index is
+    // read from (and then advanced in) the context's device counter
+    auto step = [&](uint64_t k, bool from_counter) -> jw_status {
+        jw_status st = JW_OK;
+        if (from_counter) {
+            k_generate_gaussian<<<blocks_for((long)c->N * c->N), kThreads, 0, c->stream>>>(
+                xx->d, xy->d, c->N, cfg.seed, 0, c->d_step, with_coupling);
+            if (cudaGetLastError() != cudaSuccess) st = JW_ECUDA;
+        } else {
+            st = jw_generate_gaussian(c, xx, xy, step0 + k, with_coupling);
+        }
+        if (!st) st = jw_execute2D(c, xx, 1);
+        if (!st) st = jw_execute2D(c, xy, 1);
+        if (!st) st = jw_prepare_A_local(c, A, xx, xy, kc, cfg.KernelChoice);
+        if (!st) st = jw_execute2D(c, A, 0);
+        if (!st) st = jw_execute2D(c, xx, 0);
+        if (!st) st = jw_execute2D(c, xy, 0);
+        if (!st) st = jw_uxiulocal(c, ux, uy, V, xx, xy);
+        if (!st) st = jw_execute2D(c, ux, 1);
+        if (!st) st = jw_execute2D(c, uy, 1);
+        if (!st) st = jw_prepare_A_local(c, B, ux, uy, kc, cfg.KernelChoice);
+        if (!st) st = jw_execute2D(c, B, 0);
+        if (!st) st = jw_update_uf(c, V, B, A, cfg.step);
+        if (!st && from_counter) {
+            k_advance_counter<<<1, 1, 0, c->stream>>>(c->d_step);
+            if (cudaGetLastError() != cudaSuccess) st = JW_ECUDA;
+        }
+        return st;
+    };
+    // a short run (or no counter) goes call by call; a longer one runs its
+    // first step directly and replays the others from one captured step
+    if (n < 4) {
+        for (int k = 0; k < n && s == JW_OK; ++k) s = step((uint64_t)k, false);
+        return s;
     }
-    return s;
+    if (!c->d_step && cudaMalloc(&c->d_step, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        c->d_step = nullptr;
+    }
+    s = step(0, false);
+    if (s || !c->d_step) {
+        for (int k = 1; k < n && s == JW_OK; ++k) s = step((uint64_t)k, false);
+        return s;
+    }
+    k_set_counter<<<1, 1, 0, c->stream>>>(c->d_step, step0 + 1);
+    JW_CUDA(cudaGetLastError());
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    JW_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const jw_status captured = step(0, true);
+    const cudaError_t ended = cudaStreamEndCapture(c->stream, &graph);
+    cudaError_t ce = (captured == JW_OK && ended == cudaSuccess) ? cudaGraphInstantiate(&exec, graph, 0)
+                                                                  : cudaErrorUnknown;
+    for (int k = 1; k < n && ce == cudaSuccess; ++k) ce = cudaGraphLaunch(exec, c->stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (captured != JW_OK) return captured;
+    JW_CUDA(ended);
+    JW_CUDA(ce);
+    return JW_OK;
 }
 
 extern "C" jw_status jw_print_host(int N, int measurement, const double* sum, const double* err, double x,

@@ -57,6 +57,7 @@ struct jw_context {
     jw::Twiddles tw;
     int* d_flags = nullptr;       // device error flags
     double2* d_tmp = nullptr;     // one plane of scratch (average_and_symmetrize)
+    unsigned long long* d_step = nullptr;  // noise index of jw_evolve_momentum's replayed steps
     std::vector<jw_field*> fields;  // live fields, released by jw_context_destroy
     // position-space evolution (jw_position.cu), allocated on first use
     double2* d_pos_tab = nullptr;   // 2 planes: raw forward DFT of k_x(d), k_y(d)
