@@ -628,6 +628,12 @@ def main_arm(args):
             "what": "each request of the same mix alone, MV slices + steps through the call-for-call FP64 layer"}
         line["serve"]["vs_fp64_plain_mix"] = line["serve"]["site_steps_per_s"] / mix_rate
         line["uneven"] = uneven_leg(jw, local, 48)
+        # served and uneven throughput as a fraction of the HBM roofline, by the
+        # compulsory traffic of a mixed site-step (V read and written in FP64,
+        # A and B written and read in FP32: 576 B)
+        for leg in ("serve", "uneven"):
+            line[leg]["hbm_frac"] = line[leg]["site_steps_per_s"] * 576 / (peak * 1e9)
+            line[leg]["hbm_frac_basis"] = "576 B per site-step of compulsory traffic / measured HBM peak"
         line["position"] = position_leg(jw, local)
         line["c1"] = c1_leg(jw, local)
         # CPU baseline: the reference's own main on a bounded sample
