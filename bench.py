@@ -552,6 +552,15 @@ def main_arm(args):
 
     e2e_ms = timed_loop(lambda: eng.step_measure_ensemble(ids, 1, sum_h, err_h))
     two_ms = timed_loop(lambda: (eng.step(ids, 1), eng.measure_ensemble(ids, sum_h, err_h)))
+    # with several ranks, the ensemble of all ranks' events: one sum of the
+    # ranks' fields (the run's only collective), outside the timed loops
+    allreduce_ms = None
+    if world > 1:
+        from jimwlk.dist import allreduce_ensemble
+        barrier()
+        t0 = time.perf_counter()
+        allreduce_ensemble(sum_h, err_h)
+        allreduce_ms = max_over_ranks((time.perf_counter() - t0) * 1e3)
     e2e_value = world * sites * k_e2e / (e2e_ms / 1e3)
     h2d = 4 * events                   # the event id list
     d2h = 2 * n_side * n_side * 16     # sum and err, complex
@@ -588,7 +597,8 @@ def main_arm(args):
                 "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e,
                 "what": "jw_engine_step_measure_ensemble per step (one step + ensemble measurement to host arrays)",
                 "two_calls": {"value": world * sites * k_e2e / (two_ms / 1e3), "ms_per_step": two_ms / k_e2e,
-                              "what": "jw_engine_step + jw_engine_measure_ensemble per step"}},
+                              "what": "jw_engine_step + jw_engine_measure_ensemble per step"},
+                "ensemble_allreduce_ms": allreduce_ms},
         "gpu_launches": sum(cnt for _, cnt in launched.values()),
         "clocks": clocks,
         "roofline": roof,
