@@ -447,7 +447,10 @@ template <int N>
 void mix_configure() {
     static bool configured = false;
     if (configured) return;
-    cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
+    if constexpr (mx_groups<N>() == 2)
+        cudaFuncSetAttribute(k_mix_pass1_pair<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
+    else
+        cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
     for_each_p2_cols<N>([](auto c) {
         constexpr int C = decltype(c)::value;
         cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_s2_smem<N, C>());
@@ -473,8 +476,12 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
     if (tm) tm->start(kind);
     switch (kind) {
         case KIND_P1:
-            k_mix_pass1<N><<<dim3(N, mx_groups<N>(), nb), mx_p1_threads<N>(), mx_p1_smem<N>(), e->stream>>>(
-                g.d_ev, d_slots, P, g.tw.d32);
+            if constexpr (mx_groups<N>() == 2)
+                k_mix_pass1_pair<N><<<dim3(N, 2, nb), mx_p1_threads<N>(), mx_p1_smem<N>(), e->stream>>>(
+                    g.d_ev, d_slots, P, g.tw.d32);
+            else
+                k_mix_pass1<N><<<dim3(N, 1, nb), mx_p1_threads<N>(), mx_p1_smem<N>(), e->stream>>>(
+                    g.d_ev, d_slots, P, g.tw.d32);
             break;
         case KIND_P2:
             launch_pass2<N>(e, g, d_slots, nb, g.p2_cols, 1);

@@ -17,6 +17,8 @@
 // (128 B) and writes Q (64 B); pass 3 reads Q (64 B) and V and writes V (288 B).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "jw_engine_kernels.cuh"
 
 namespace jw {
@@ -25,7 +27,8 @@ namespace jw {
 // loads the V of its own sites straight into registers (a warp's loads of one
 // plane are contiguous), early enough that the noise or the exponentials of
 // the site cover the latency.  At N = 2048 the 8 pair rows of pass 1 take
-// 295 KB, so two CTAs (groups) share a row: noise rows and rotated rows.
+// 295 KB, so a cluster of two CTAs (groups) shares a row: noise rows and
+// rotated rows.
 template <int N> constexpr int mx_groups() { return 16 * padded_len16(8 * N) > 220 * 1024 ? 2 : 1; }
 template <int N> constexpr int mx_p1_threads() { return N >= 2048 ? 512 : 256; }
 template <int N> constexpr size_t mx_p1_smem() { return 16 * (size_t)padded_len16(8 / mx_groups<N>() * N); }
@@ -135,58 +138,108 @@ __device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int 
 }
 
 // ------------------------------------------------------------------ pass 1
+// One CTA per lattice row: noise and V xi V^dagger for every site into the 8
+// pair rows, then their forward row transforms (up to 1024^2; 2048^2 rows go
+// to k_mix_pass1_pair).
 template <int N>
 __global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_pass1(const EventDev* __restrict__ ev,
                                                                                      const int* __restrict__ slots,
                                                                                      float4* __restrict__ P,
                                                                                      const float2* __restrict__ tw) {
-    constexpr int G = mx_groups<N>();
-    constexpr int NP = 8 / G;  // pair rows per CTA
+    static_assert(mx_groups<N>() == 1, "one CTA holds all 8 pair rows");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
-    const int x = blockIdx.x, g = blockIdx.y, b = blockIdx.z;
+    const int x = blockIdx.x, b = blockIdx.z;
     const EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     const float* nf = e.nf32;
-    const bool want_noise = (G == 1) || g == 0;
-    const bool want_rot = (G == 1) || g == 1;
-    const int rot_base = (G == 1) ? 4 : 0;
     for (int y = threadIdx.x; y < N; y += blockDim.x) {
         const long site = (long)x * N + y;
         double2 dv[9];
-        if (want_rot) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) dv[k] = __ldg(&e.V[k * vol + site]);  // in flight during the noise
-        }
+        for (int k = 0; k < 9; ++k) dv[k] = __ldg(&e.V[k * vol + site]);  // in flight during the noise
         float z[16];
         langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
         const float f = nf ? nf[site] : 1.0f;
 #pragma unroll
         for (int k = 0; k < 16; ++k) z[k] *= f;
-        if (want_noise) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
-                sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+        for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+            sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+        float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            n[k] = z[2 * k];
+            m[k] = z[2 * k + 1];
         }
-        if (want_rot) {
-            float n[8], m[8], hx[8], hy[8];
+        float2 v[9];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                n[k] = z[2 * k];
-                m[k] = z[2 * k + 1];
-            }
-            float2 v[9];
+        for (int k = 0; k < 9; ++k) v[k] = make_float2((float)dv[k].x, (float)dv[k].y);
+        rotate_herm(v, n, hx);
+        rotate_herm(v, m, hy);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) v[k] = make_float2((float)dv[k].x, (float)dv[k].y);
-            rotate_herm(v, n, hx);
-            rotate_herm(v, m, hy);
-#pragma unroll
-            for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
-                sm[pad16((rot_base + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
-        }
+        for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+            sm[pad16((4 + j) * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
     }
     __syncthreads();
-    fft16_rows_store<float, N>(sm, NP, -1.0f, tw, P + ((long)b * 8 + NP * g) * vol + (long)x * N, vol);
+    fft16_rows_store<float, N>(sm, 8, -1.0f, tw, P + (long)b * 8 * vol + (long)x * N, vol);
+}
+
+// Pass 1 where the 8 pair rows of a lattice row do not fit one CTA (N = 2048):
+// a cluster of two CTAs shares the row through distributed shared memory.
+// Rank 0 holds the 4 noise rows (X_j, Y_j), rank 1 the 4 rotated rows
+// (BX_j, BY_j).  Each CTA draws the noise, loads V and rotates for half the
+// sites, and stores both pair elements of a site straight into the rows of
+// their owner (local or the partner's shared memory).  One cluster barrier
+// (release/acquire) orders those stores before each CTA transforms its rows;
+// nothing reads the partner's memory after it, so either CTA may finish first.
+template <int N>
+__global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p1_threads<N>(), 1)
+    k_mix_pass1_pair(const EventDev* __restrict__ ev, const int* __restrict__ slots, float4* __restrict__ P,
+                     const float2* __restrict__ tw) {
+    static_assert(mx_groups<N>() == 2, "two CTAs per lattice row");
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* sm = reinterpret_cast<float4*>(smem_raw);
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned rank = cluster.block_rank();  // = blockIdx.y
+    float4* noise_rows = cluster.map_shared_rank(sm, 0);
+    float4* rot_rows = cluster.map_shared_rank(sm, 1);
+    const int x = blockIdx.x, b = blockIdx.z;
+    const EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const float* nf = e.nf32;
+    constexpr int HALF = N / 2;
+    for (int y = (int)rank * HALF + threadIdx.x; y < ((int)rank + 1) * HALF; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        double2 dv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) dv[k] = __ldg(&e.V[k * vol + site]);  // in flight during the noise
+        float z[16];
+        langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+        const float f = nf ? nf[site] : 1.0f;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) z[k] *= f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+            noise_rows[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+        float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            n[k] = z[2 * k];
+            m[k] = z[2 * k + 1];
+        }
+        float2 v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = make_float2((float)dv[k].x, (float)dv[k].y);
+        rotate_herm(v, n, hx);
+        rotate_herm(v, m, hy);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+            rot_rows[pad16(j * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+    }
+    cluster.sync();
+    fft16_rows_store<float, N>(sm, 4, -1.0f, tw, P + ((long)b * 8 + 4 * rank) * vol + (long)x * N, vol);
 }
 
 // ------------------------------------------------------------------ pass 2
