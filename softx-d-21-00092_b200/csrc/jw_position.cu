@@ -53,8 +53,9 @@ constexpr int kThreads = 256;
 inline unsigned blocks_for(long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 // Cholesky apply tiling: 128 rows per CTA, 16 columns per staged tile, three
-// stages, 4096 columns per chunk; right-hand sides in multiples of 8 (at most 24).
-constexpr int kTR = 128, kKT = 16, kTC = 4096, kStages = 3, kMaxR = 24;
+// stages, 4096 columns per chunk; right-hand sides in multiples of 8 (at most 32:
+// the noise of two Langevin steps).
+constexpr int kTR = 128, kKT = 16, kTC = 4096, kStages = 3, kMaxR = 32;
 template <int NT> constexpr int apply_x_row_bytes() { return NT * 64 + 32; }  // padded: conflict-free B fragments
 template <int NT> constexpr int apply_stage_bytes() { return kTR * kKT * 16 + kKT * apply_x_row_bytes<NT>(); }
 constexpr int kDiagBlock = 128;
@@ -341,24 +342,29 @@ __global__ void k_chol_finish_field(const double2* __restrict__ P, double2* __re
 }
 
 // The 16 unit normals of each site in the reference's draw order
-// (field.h:2170-2173): X(i, a) = n_a (xi_x), X(i, 8 + a) = m_a (xi_y).
-__global__ void k_chol_noise_X(double* __restrict__ X, long n, uint64_t seed, uint64_t step) {
+// (field.h:2170-2173) for steps step .. step + nsteps - 1, 16 nsteps per site:
+// X(i, 16 s + a) = n_a (xi_x), X(i, 16 s + 8 + a) = m_a (xi_y) of step + s.
+__global__ void k_chol_noise_X(double* __restrict__ X, long n, uint64_t seed, uint64_t step, int nsteps) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double z[16];
-    langevin_normals<double>(seed, step, (uint32_t)i, z);
+    const int rp = 16 * nsteps;
+    for (int st = 0; st < nsteps; ++st) {
+        double z[16];
+        langevin_normals<double>(seed, step + (uint64_t)st, (uint32_t)i, z);
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        X[i * 16 + a] = z[2 * a];
-        X[i * 16 + 8 + a] = z[2 * a + 1];
+        for (int a = 0; a < 8; ++a) {
+            X[i * rp + 16 * st + a] = z[2 * a];
+            X[i * rp + 16 * st + 8 + a] = z[2 * a + 1];
+        }
     }
 }
 
 // xi_x = sum_a (L n_a) lambda_a, xi_y = sum_a (L m_a) lambda_a: the
 // correlated noise L (sum_a n_a lambda_a) of gfield::multiplyByCholesky,
 // with the (linear) embedding applied after L.
+// P holds rp right-hand sides per site; this step's 16 start at column off.
 __global__ void k_chol_finish_noise(const double2* __restrict__ P, double2* __restrict__ xx, double2* __restrict__ xy,
-                                    long n) {
+                                    long n, int rp, int off) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 y[16];
@@ -366,7 +372,7 @@ __global__ void k_chol_finish_noise(const double2* __restrict__ P, double2* __re
     for (int c = 0; c < 16; ++c) y[c] = make_double2(0.0, 0.0);
     const int nc = chunks_of_row(i, n);
     for (int ch = 0; ch < nc; ++ch) {
-        const double2* p = P + ((long)ch * n + i) * 16;
+        const double2* p = P + ((long)ch * n + i) * rp + off;
 #pragma unroll
         for (int c = 0; c < 16; ++c) y[c] = cadd(y[c], p[c]);
     }
@@ -457,14 +463,21 @@ void cholesky_free(jw_cholesky* L) {
     delete L;
 }
 
-// Correlated Langevin noise of one step into xi_x, xi_y.
-jw_status cholesky_noise(jw_context* c, const jw_cholesky* L, jw_field* xx, jw_field* xy, uint64_t step) {
+// L applied to the unit normals of nsteps (1 or 2) consecutive Langevin
+// steps from `step` in one pass over L (16 nsteps right-hand sides).
+jw_status cholesky_noise_apply(jw_context* c, const jw_cholesky* L, uint64_t step, int nsteps) {
     const long n = L->n;
-    k_chol_noise_X<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_X, n, c->cfg.seed, step);
+    k_chol_noise_X<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_X, n, c->cfg.seed, step, nsteps);
     JW_CUDA(cudaGetLastError());
-    jw_status s = launch_apply<2>(L, c->stream);
-    if (s) return s;
-    k_chol_finish_noise<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xx->d, xy->d, n);
+    return nsteps == 2 ? launch_apply<4>(L, c->stream) : launch_apply<2>(L, c->stream);
+}
+
+// The correlated noise of step `which` (< nsteps) of the last apply into xi_x, xi_y.
+jw_status cholesky_noise_finish(jw_context* c, const jw_cholesky* L, jw_field* xx, jw_field* xy, int nsteps,
+                                int which) {
+    const long n = L->n;
+    k_chol_finish_noise<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xx->d, xy->d, n, 16 * nsteps,
+                                                                   16 * which);
     JW_CUDA(cudaGetLastError());
     return JW_OK;
 }
@@ -673,10 +686,21 @@ JW_EXPORT jw_status jw_evolve_position(jw_context* c, jw_field* V, uint64_t step
         if (!c->pos_work[k]) s = jw_field_create(c, 9, &c->pos_work[k]);
     if (s) return s;
     jw_field *xx = c->pos_work[0], *xy = c->pos_work[1], *A = c->pos_work[2], *B = c->pos_work[3];
+    // correlated noise: one pass over L serves two steps (32 right-hand sides),
+    // halving the factor's HBM traffic per step; each column's sum is the one
+    // a single step would form, so the noise is the same bit for bit
+    int pair = 0;
     for (int k = 0; k < n && s == JW_OK; ++k) {
         const uint64_t step = step0 + (uint64_t)k;
-        if (correlated) s = cholesky_noise(c, L, xx, xy, step);
-        else s = jw_generate_gaussian(c, xx, xy, step, 0);
+        if (correlated) {
+            if (k % 2 == 0) {
+                pair = (k + 1 < n) ? 2 : 1;
+                s = cholesky_noise_apply(c, L, step, pair);
+            }
+            if (!s) s = cholesky_noise_finish(c, L, xx, xy, pair, k % 2);
+        } else {
+            s = jw_generate_gaussian(c, xx, xy, step, 0);
+        }
         if (!s) s = jw_prepare_A_and_B(c, A, B, xx, xy, V, rr, coupling, cfg.KernelChoice);
         if (!s) s = jw_update_uf(c, V, B, A, cfg.step);
     }
