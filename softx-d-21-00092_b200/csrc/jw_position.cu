@@ -45,6 +45,10 @@ struct jw_cholesky {
     int n_chunks = 0;
     double* d_X = nullptr;       // n x kMaxR real right-hand sides, site-major
     double2* d_P = nullptr;      // n_chunks x n x kMaxR partial products
+    // d_P holds the correlated noise of step `cached_step` (seed `cached_seed`)
+    // as the second half of the last two-step apply; any other use of d_P clears it
+    mutable bool cached = false;
+    mutable uint64_t cached_step = 0, cached_seed = 0;
 };
 
 namespace {
@@ -643,6 +647,7 @@ JW_EXPORT jw_status jw_cholesky_get(const jw_cholesky* L, double* host) {
 
 JW_EXPORT jw_status jw_multiply_by_cholesky(jw_context* c, jw_field* xi, const jw_cholesky* L) {
     JW_CHECK(c && xi && xi->ctx == c && L && L->ctx == c);
+    L->cached = false;  // d_P is about to hold this field's product
     const long n = L->n;
     const int RP = xi->t == 9 ? 24 : 8;
     k_chol_gather_field<<<blocks_for(n), kThreads, 0, c->stream>>>(xi->d, L->d_X, n, xi->t, RP);
@@ -687,17 +692,22 @@ JW_EXPORT jw_status jw_evolve_position(jw_context* c, jw_field* V, uint64_t step
     if (s) return s;
     jw_field *xx = c->pos_work[0], *xy = c->pos_work[1], *A = c->pos_work[2], *B = c->pos_work[3];
     // correlated noise: one pass over L serves two steps (32 right-hand sides),
-    // halving the factor's HBM traffic per step; each column's sum is the one
-    // a single step would form, so the noise is the same bit for bit
-    int pair = 0;
+    // halving the factor's HBM traffic per step.  The second step's noise stays
+    // in L's partial products for the next step, in this call or the next one
+    // (a driver that steps one at a time).  Each column's sum is the one a
+    // single step would form, so the noise is the same bit for bit.
     for (int k = 0; k < n && s == JW_OK; ++k) {
         const uint64_t step = step0 + (uint64_t)k;
         if (correlated) {
-            if (k % 2 == 0) {
-                pair = (k + 1 < n) ? 2 : 1;
-                s = cholesky_noise_apply(c, L, step, pair);
+            int which = 1;
+            if (!(L->cached && L->cached_step == step && L->cached_seed == cfg.seed)) {
+                s = cholesky_noise_apply(c, L, step, 2);
+                which = 0;
             }
-            if (!s) s = cholesky_noise_finish(c, L, xx, xy, pair, k % 2);
+            L->cached = which == 0 && !s;
+            L->cached_step = step + 1;
+            L->cached_seed = cfg.seed;
+            if (!s) s = cholesky_noise_finish(c, L, xx, xy, 2, which);
         } else {
             s = jw_generate_gaussian(c, xx, xy, step, 0);
         }
