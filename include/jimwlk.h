@@ -362,8 +362,8 @@ jw_status jw_engine_measure_ensemble(jw_engine* e, const int* ids, int n, double
 /* jw_engine_step(ids, nsteps) followed by jw_engine_measure_ensemble(ids):
  * the body of main_optimized.cpp's Langevin loop (evolution :234-304, then the
  * measurement :317-336) as one call, with the same results.  In mixed
- * precision up to 1024^2 the last step's third pass also row-transforms the new
- * V for the measurement, so V is not read again. */
+ * precision the last step's third pass also row-transforms the new V for the
+ * measurement, so V is not read again. */
 jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, int nsteps, double* sum,
                                           double* err);
 /* The column-tile width the autotuner chose for lattice size N (columns per

@@ -66,7 +66,7 @@ def test_ensemble_is_sum_of_event_measurements(jw, precision):
     ("mixed", 64, 5, 2),      # fused, three launch groups
     ("mixed", 512, 3, 0),     # fused
     ("mixed", 1024, 2, 0),    # fused
-    ("mixed", 2048, 1, 0),    # step, then the separate measurement kernels
+    ("mixed", 2048, 1, 0),    # fused, one CTA per SM; pass 1 as a two-CTA cluster
     ("fp64", 64, 3, 0),       # FP64 engine: step, then the FP64 measurement
 ])
 def test_step_measure_ensemble_same_as_two_calls(jw, precision, N, events, max_batch):
