@@ -447,10 +447,14 @@ template <int N>
 void mix_configure() {
     static bool configured = false;
     if (configured) return;
-    if constexpr (mx_groups<N>() == 2)
+    if constexpr (mx_pair<N>()) {
         cudaFuncSetAttribute(k_mix_pass1_pair<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
-    else
+        cudaFuncSetAttribute(k_mix_pass31_pair<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)mx_p31p_smem<N>());
+    } else {
         cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
+        cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
+    }
     for_each_p2_cols<N>([](auto c) {
         constexpr int C = decltype(c)::value;
         cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_s2_smem<N, C>());
@@ -459,8 +463,6 @@ void mix_configure() {
     if constexpr (mx_p3_meas_fits<N>())
         cudaFuncSetAttribute(k_mix_pass3<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)mx_p3_smem<N, true>());
-    if constexpr (mx_fuse31<N>())
-        cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
     cudaFuncSetAttribute(k_meas32_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p2_smem<N>());
     configured = true;
 }
@@ -476,7 +478,7 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
     if (tm) tm->start(kind);
     switch (kind) {
         case KIND_P1:
-            if constexpr (mx_groups<N>() == 2)
+            if constexpr (mx_pair<N>())
                 k_mix_pass1_pair<N><<<dim3(N, 2, nb), mx_p1_threads<N>(), mx_p1_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, P, g.tw.d32);
             else
@@ -499,7 +501,10 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
                                                                                             nullptr);
             break;
         case KIND_P31:
-            if constexpr (mx_fuse31<N>())
+            if constexpr (mx_pair<N>())
+                k_mix_pass31_pair<N><<<dim3(N, 2, nb), mx_p31_threads<N>(), mx_p31p_smem<N>(), e->stream>>>(
+                    g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
+            else
                 k_mix_pass31<N><<<dim3(N, nb), mx_p31_threads<N>(), mx_p31_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
             break;
@@ -510,8 +515,8 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
 }
 
 // nsteps >= 1 mixed steps of one launch group: pass 1, then nsteps - 1 times
-// (pass 2, pass 3 + next pass 1), then pass 2 and pass 3.  Where pass 1 splits
-// its rows over two CTAs (2048^2) the middle is (pass 2, pass 3, pass 1).
+// (pass 2, pass 3 + next pass 1), then pass 2 and pass 3.  From 1024^2 on,
+// passes 1 and 3 + 1 run as two-CTA clusters per lattice row.
 // With ens the last pass 3 also row-transforms the new V, and the column pass
 // and the ensemble reduction into ens follow (the same result as the steps
 // followed by launch_measure_ensemble).  The middle is captured once as a CUDA
@@ -563,12 +568,7 @@ cudaError_t launch_mix_run(jw_engine* e, Group& g, const int* d_slots, int nb, i
     }
     auto middle = [&]() {
         mix_launch<N>(e, g, d_slots, nb, KIND_P2, false, tm);
-        if constexpr (mx_fuse31<N>()) {
-            mix_launch<N>(e, g, d_slots, nb, KIND_P31, false, tm);
-        } else {
-            mix_launch<N>(e, g, d_slots, nb, KIND_P3, false, tm);
-            mix_launch<N>(e, g, d_slots, nb, KIND_P1, false, tm);
-        }
+        mix_launch<N>(e, g, d_slots, nb, KIND_P31, false, tm);
     };
     mix_launch<N>(e, g, d_slots, nb, KIND_P1, false, tm);
     const int reps = nsteps - 1;

@@ -26,10 +26,12 @@ namespace jw {
 // Passes 1 and 3 hold whole rows of pair planes in shared memory; each thread
 // loads the V of its own sites straight into registers (a warp's loads of one
 // plane are contiguous), early enough that the noise or the exponentials of
-// the site cover the latency.  At N = 2048 the 8 pair rows of pass 1 take
-// 295 KB, so a cluster of two CTAs (groups) shares a row: noise rows and
-// rotated rows.
-template <int N> constexpr int mx_groups() { return 16 * padded_len16(8 * N) > 220 * 1024 ? 2 : 1; }
+// the site cover the latency.  From N = 1024 on the 8 pair rows of pass 1
+// (147 KB at 1024^2) would leave one CTA per SM, so a cluster of two CTAs
+// shares each lattice row through distributed shared memory (mx_pair): rank 0
+// holds the noise rows, rank 1 the rotated rows.
+template <int N> constexpr bool mx_pair() { return 16 * padded_len16(8 * N) > 113 * 1024; }
+template <int N> constexpr int mx_groups() { return mx_pair<N>() ? 2 : 1; }
 template <int N> constexpr int mx_p1_threads() { return N >= 2048 ? 512 : 256; }
 template <int N> constexpr size_t mx_p1_smem() { return 16 * (size_t)padded_len16(8 / mx_groups<N>() * N); }
 template <int N> constexpr int mx_p1_blocks() { return mx_p1_threads<N>() <= 256 && mx_p1_smem<N>() <= 113 * 1024 ? 2 : 1; }
@@ -139,14 +141,14 @@ __device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int 
 
 // ------------------------------------------------------------------ pass 1
 // One CTA per lattice row: noise and V xi V^dagger for every site into the 8
-// pair rows, then their forward row transforms (up to 1024^2; 2048^2 rows go
-// to k_mix_pass1_pair).
+// pair rows, then their forward row transforms (up to 512^2; larger rows go to
+// k_mix_pass1_pair).
 template <int N>
 __global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_pass1(const EventDev* __restrict__ ev,
                                                                                      const int* __restrict__ slots,
                                                                                      float4* __restrict__ P,
                                                                                      const float2* __restrict__ tw) {
-    static_assert(mx_groups<N>() == 1, "one CTA holds all 8 pair rows");
+    static_assert(!mx_pair<N>(), "one CTA holds all 8 pair rows");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
     const int x = blockIdx.x, b = blockIdx.z;
@@ -185,8 +187,9 @@ __global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_p
     fft16_rows_store<float, N>(sm, 8, -1.0f, tw, P + (long)b * 8 * vol + (long)x * N, vol);
 }
 
-// Pass 1 where the 8 pair rows of a lattice row do not fit one CTA (N = 2048):
-// a cluster of two CTAs shares the row through distributed shared memory.
+// Pass 1 where the 8 pair rows of a lattice row would leave one CTA per SM or
+// do not fit one CTA (N >= 1024): a cluster of two CTAs shares the row through
+// distributed shared memory.
 // Rank 0 holds the 4 noise rows (X_j, Y_j), rank 1 the 4 rotated rows
 // (BX_j, BY_j).  Each CTA draws the noise, loads V and rotates for half the
 // sites, and stores both pair elements of a site straight into the rows of
@@ -194,10 +197,10 @@ __global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_p
 // (release/acquire) orders those stores before each CTA transforms its rows;
 // nothing reads the partner's memory after it, so either CTA may finish first.
 template <int N>
-__global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p1_threads<N>(), 1)
+__global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>())
     k_mix_pass1_pair(const EventDev* __restrict__ ev, const int* __restrict__ slots, float4* __restrict__ P,
                      const float2* __restrict__ tw) {
-    static_assert(mx_groups<N>() == 2, "two CTAs per lattice row");
+    static_assert(mx_pair<N>(), "two CTAs per lattice row");
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
@@ -310,16 +313,17 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // from the inverse row transforms in column y of the row buffer.  The old V is
 // loaded first and arrives while exp(+i sqrt(eps) B) is formed; one
 // exponential is held at a time.  Reports non-finite entries in fl.
-template <int N>
-__device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, int y, long site, long vol, double se,
-                                        double2 (&v)[9], int& fl) {
+// get_u(j) returns the element of inverse-transformed pair row j at the site.
+template <typename GetU>
+__device__ __forceinline__ void p3_site_g(const EventDev& e, GetU get_u, long site, long vol, double se,
+                                          double2 (&v)[9], int& fl) {
     double2 v0[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) v0[k] = e.V[k * vol + site];
     double a[8], bq[8];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float4 u = sm[pad16(j * N + y)];
+        const float4 u = get_u(j);
         a[2 * j] = (double)u.x * se;
         a[2 * j + 1] = (double)u.y * se;
         bq[2 * j] = (double)u.z * -se;
@@ -336,6 +340,12 @@ __device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, int
 #pragma unroll
     for (int k = 0; k < 9; ++k)
         if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+}
+
+template <int N>
+__device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, int y, long site, long vol, double se,
+                                        double2 (&v)[9], int& fl) {
+    p3_site_g(e, [&](int j) { return sm[pad16(j * N + y)]; }, site, vol, se, v, fl);
 }
 
 template <int N, bool MEAS = false>
@@ -391,15 +401,21 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 // site y overwrite column y of the inverse transforms, which the same thread
 // has just consumed, so the row buffer is pass 1's (8 rows).  Pass 2 has
 // advanced the step index, so e.step is the next step's noise index.
-template <int N> constexpr bool mx_fuse31() { return mx_groups<N>() == 1; }
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
 template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>(); }
+// the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
+template <int N> constexpr size_t mx_p31p_smem() {
+    return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
+}
+template <int N> constexpr int mx_p31p_blocks() {
+    return mx_p31_threads<N>() <= 256 && mx_p31p_smem<N>() <= 113 * 1024 ? 2 : 1;
+}
 
 template <int N>
 __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_pass31(
     EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q, float4* __restrict__ P,
     const float2* __restrict__ tw, int* __restrict__ flags) {
-    static_assert(mx_fuse31<N>(), "one CTA holds all 8 pair rows");
+    static_assert(!mx_pair<N>(), "one CTA holds all 8 pair rows");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
     const int x = blockIdx.x, b = blockIdx.y;
@@ -450,6 +466,81 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     if (fl) atomicOr(flags, fl);
     __syncthreads();
     fft16_rows_store<float, N>(sm, 8, -1.0f, tw, P + (long)b * 8 * vol + (long)x * N, vol);
+}
+
+// Pass 3 + next pass 1 where a lattice row needs a cluster of two CTAs
+// (mx_pair).  Rank r inverse-transforms Q rows 2r, 2r + 1 in its own shared
+// memory; after a cluster barrier each CTA updates half the row's sites,
+// reading the two other Q rows from its partner, and stores the next step's
+// noise pairs into rank 0's output rows and the rotated pairs into rank 1's.
+// A second barrier orders those stores before each CTA transforms its 4
+// output rows.  Nothing touches the partner's memory after it.
+template <int N>
+__global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p31_threads<N>(), mx_p31p_blocks<N>())
+    k_mix_pass31_pair(EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q,
+                      float4* __restrict__ P, const float2* __restrict__ tw, int* __restrict__ flags) {
+    static_assert(mx_pair<N>(), "two CTAs per lattice row");
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* qb = reinterpret_cast<float4*>(smem_raw);  // this CTA's 2 Q rows
+    float4* ob = qb + padded_len16(2 * N);               // this CTA's 4 output rows
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned rank = cluster.block_rank();  // = blockIdx.y
+    const float4* q_lo = cluster.map_shared_rank(qb, 0);  // Q rows 0, 1
+    const float4* q_hi = cluster.map_shared_rank(qb, 1);  // Q rows 2, 3
+    float4* noise_rows = cluster.map_shared_rank(ob, 0);
+    float4* rot_rows = cluster.map_shared_rank(ob, 1);
+    const int x = blockIdx.x, b = blockIdx.z;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const float4* in = Q + ((long)b * 4 + 2 * rank) * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x)
+        cp_async<16>(&qb[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    fft16_rows<N, 2>(qb, 1.0f, tw);
+    cluster.sync();
+    const double se = e.sqrt_eps;
+    const float* nf = e.nf32;
+    int fl = 0;
+    constexpr int HALF = N / 2;
+    for (int y = (int)rank * HALF + threadIdx.x; y < ((int)rank + 1) * HALF; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        float2 v32[9];
+        {
+            double2 v[9];
+            p3_site_g(e, [&](int j) { return j < 2 ? q_lo[pad16(j * N + y)] : q_hi[pad16((j - 2) * N + y)]; },
+                      site, vol, se, v, fl);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                e.V[k * vol + site] = v[k];
+                v32[k] = make_float2((float)v[k].x, (float)v[k].y);
+            }
+        }
+        float z[16];
+        langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+        const float f = nf ? nf[site] : 1.0f;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) z[k] *= f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+            noise_rows[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+        float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            n[k] = z[2 * k];
+            m[k] = z[2 * k + 1];
+        }
+        rotate_herm(v32, n, hx);
+        rotate_herm(v32, m, hy);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+            rot_rows[pad16(j * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+    }
+    if (fl) atomicOr(flags, fl);
+    cluster.sync();
+    fft16_rows_store<float, N>(ob, 4, -1.0f, tw, P + ((long)b * 8 + 4 * rank) * vol + (long)x * N, vol);
 }
 
 // ------------------------------------------------------------------ measurement (FP64)
