@@ -626,7 +626,6 @@ bool fused_measure_supported(int precision, int N) {
 
 template <typename T, int N>
 cudaError_t launch_step(jw_engine* e, Group& g, const int* d_slots, int nb, unsigned char* ws) {
-    if constexpr (sizeof(T) == 4) return launch_mix_run<N>(e, g, d_slots, nb, 1, nullptr, nullptr);
     using V2 = C2<T>;
     const long vol = (long)N * N;
     V2* P = reinterpret_cast<V2*>(ws);
@@ -750,10 +749,8 @@ cudaError_t launch_measure_ensemble(jw_engine* e, Group& g, const int* d_slots, 
         default: return cudaErrorInvalidValue;   \
     }
 
+// One FP64 step (mixed-precision steps go through launch_mix_run).
 cudaError_t dispatch_step(jw_engine* e, Group& g, const int* d_slots, int nb) {
-    if (e->opt.precision == JW_PRECISION_MIXED) {
-        JW_DISPATCH_N(g.N, (launch_step<float, NN>(e, g, d_slots, nb, g.ws)))
-    }
     switch (g.N) {
         case 8: return launch_step<double, 8>(e, g, d_slots, nb, g.ws);
         case 16: return launch_step<double, 16>(e, g, d_slots, nb, g.ws);
