@@ -577,9 +577,11 @@ JW_EXPORT jw_status jw_initial_condition(jw_context* c, jw_field* V) {
     const jw_config& cfg = c->cfg;
     JW_CHECK(cfg.elementaryWilsonLines > 0);
     const double g = 1.0, mu = cfg.mu / c->N;
-    jw_field* f = nullptr;
-    jw_status s = jw_field_create(c, 9, &f);
-    if (s) return s;
+    JW_CHECK(V != c->mv_work);
+    // the charge field is kept in the context: repeated calls allocate nothing
+    jw_status s = JW_OK;
+    if (!c->mv_work && (s = jw_field_create(c, 9, &c->mv_work))) return s;
+    jw_field* f = c->mv_work;
     s = jw_field_set_unit(V);
     for (int i = 0; i < cfg.elementaryWilsonLines && s == JW_OK; ++i) {
         s = jw_set_mv_model(c, f, i, g, mu, cfg.elementaryWilsonLines);
@@ -588,7 +590,6 @@ JW_EXPORT jw_status jw_initial_condition(jw_context* c, jw_field* V) {
         if (!s) s = jw_execute2D(c, f, 0);
         if (!s) s = jw_mul_exp(c, V, f);
     }
-    jw_field_destroy(f);
     return s;
 }
 

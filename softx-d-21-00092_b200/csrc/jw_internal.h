@@ -67,6 +67,7 @@ struct jw_context {
     std::vector<jw_cholesky*> choleskies;  // live factors, released by jw_context_destroy
     jw_field* pos_work[4] = {};     // xi_x, xi_y, A, B of jw_evolve_position (in `fields`)
     jw_field* mom_work[6] = {};     // xi_x, xi_y, A, B, ux, uy of jw_evolve_momentum (in `fields`)
+    jw_field* mv_work = nullptr;    // the charge field of jw_initial_condition (in `fields`)
 };
 
 namespace jw {
