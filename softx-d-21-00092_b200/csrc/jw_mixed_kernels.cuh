@@ -57,7 +57,7 @@ template <int N> constexpr size_t mx_p2_smem() { return 2 * 16 * (size_t)mx_tile
 // The step's pass 2 (k_mix_pass2) is built for every column-tile width C in
 // {1, 2, 4, 8} that fits (C N/8 <= 1024 threads, two tiles in 227 KB); the
 // engine's autotuner picks one per lattice size, mx_s2_cols is the default.
-template <int N> constexpr int mx_s2_cols() { return mx_cols<N>(); }
+template <int N> constexpr int mx_s2_cols() { return N == 256 ? 8 : mx_cols<N>(); }  // measured best
 template <int N, int C> constexpr int mx_s2_threads() { return C * (N / 8); }
 template <int N, int C> constexpr int mx_s2_tile_len() { return C >= 8 ? N * C : N * C + (N / 8) * C; }
 template <int N, int C> constexpr size_t mx_s2_smem() { return 2 * 16 * (size_t)mx_s2_tile_len<N, C>(); }
