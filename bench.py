@@ -3,17 +3,19 @@
 
 Workload (one "step" = one Langevin step of the whole batch): 64 independent
 events on 512 x 512 lattices, MV initial condition with g^2 mu a = 0.5,
-m a = 0.02 and 50 slices, fixed coupling alpha_s = 0.15 and ds = 1e-4
-(step = alpha_s ds / pi^2), SIN kernel, advanced by the batched engine in mixed
-precision (FP32 noise, rotation and transforms; FP64 exponentials, V and
-dipole sums).  Seeded synthetic inputs; no dataset is involved.  The
-per-event fields (V 144 B/site, workspaces 192 B/site) total ~5.6 GB, far above
-the 126 MB L2, so no flush is needed between steps.
+m a = 0.02 and 50 slices, running coupling (the reference's
+SQRT_COUPLING_CONSTANT, momentum evolution, SIN kernel) with ds = 1e-4
+(step = ds / pi^2), advanced by the batched engine in mixed precision (FP32
+noise, rotation and transforms; FP64 exponentials, V, per-step
+reunitarisation and dipole sums).  Seeded synthetic inputs; no dataset is
+involved.  The per-event fields (V 144 B/site, workspaces 192 B/site) total
+~5.6 GB, far above the 126 MB L2, so no flush is needed between steps.
 
 Arms
   default            the engine through the C ABI (softx-d-21-00092_b200/lib/libjimwlk.so)
   --impl reference   the reference's own main_optimized (oracle/_ref, OpenMP on all
-                     host cores, single-rank MPI and FFTW shims) on one 512^2 event
+                     host cores, single-rank MPI and FFTW shims) on one 512^2 event of
+                     the same configuration (the reference steps one event at a time)
 
 Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
 torchrun, one rank per GPU, each rank advancing its own 64 events (weak
@@ -46,7 +48,9 @@ NY_SLICES = 50
 MU = 0.5 * N          # g^2 mu a = 0.5 with g = 1 -> config mu = 0.5 N
 MASS = 0.04           # m a = 0.02 = mass * mu_MV
 ALPHA_S, DS = 0.15, 1e-4
-STEP = ALPHA_S * DS / math.pi ** 2
+FIXED_STEP = ALPHA_S * DS / math.pi ** 2  # fixed coupling: step = alpha_s ds / pi^2
+STEP = DS / math.pi ** 2                  # running (SQRT) coupling: alpha_s(k) sits in the kernel
+REUNITARIZE = True                        # the mixed form reunitarises V after every step
 METRIC = "lattice site-steps/s"
 # algorithmic HBM bytes per site of each kernel kind (mixed precision):
 #   pass 1: read V (9 complex FP64 = 144 B) + write 16 FP32 complex planes (128 B)
@@ -116,30 +120,74 @@ def profiled_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """SM clocks and throttle reasons while the timed region runs, read through
+    NVML every 5 ms on a host thread (the timed region lasts ~50-100 ms, too
+    short for nvidia-smi's 200 ms loop); nvidia-smi is the fallback when NVML
+    cannot be opened.  The GPU is found by its PCI bus id, so the sample is of
+    the device the run uses whatever CUDA_VISIBLE_DEVICES maps."""
 
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.005):
         self.device = device
+        self.period = period_s
+        self.rows = []
+        self.max_mhz = None
+        self.handle = None
+        self.thread = None
+        self.stop = None
         self.proc = None
         self.path = None
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.device)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+
+    def _poll(self):
+        import pynvml
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                self.rows.append((pynvml.nvmlDeviceGetClockInfo(self.handle, pynvml.NVML_CLOCK_SM),
+                                  get_reasons(self.handle)))
+            except Exception:
+                break
+            self.stop.wait(self.period)
+
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-        time.sleep(0.3)
+            import pynvml
+            self.handle = self._nvml_handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.handle = None
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            except OSError:
+                self.proc = None
+            time.sleep(0.3)
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.send_signal(signal.SIGTERM)
             try:
@@ -148,6 +196,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.handle is not None:
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "source": "nvml"}
+            reasons = sorted({name for _, r in self.rows for bit, name in self.REASONS.items() if r & bit})
+            return {"sm_mhz": statistics.median(m for m, _ in self.rows), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(self.rows), "source": "nvml, 5 ms"}
         rows = []
         if self.path and os.path.exists(self.path):
             for line in open(self.path):
@@ -161,7 +215,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]), "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 def parse_evolution_times(text: str):
@@ -170,7 +224,7 @@ def parse_evolution_times(text: str):
 
 def run_reference_main(steps: int, warmup: int, nthreads: int | None = None, n_side: int = N,
                        evolution: str = "MOMENTUM_EVOLUTION", coupling: str = "SQRT_COUPLING_CONSTANT",
-                       with_wall: bool = False):
+                       with_wall: bool = False, slices: int = 1, step: float = STEP):
     """The reference's main_optimized on one n_side^2 event: returns seconds per
     Langevin step (mean over the last `steps` of warmup + steps) and, with
     with_wall, the run's wall time outside the initial condition and the
@@ -181,10 +235,11 @@ def run_reference_main(steps: int, warmup: int, nthreads: int | None = None, n_s
     with tempfile.TemporaryDirectory() as d:
         cfg = os.path.join(d, "config")
         with open(cfg, "w") as fh:
-            # 1 MV slice: the initial condition is outside the per-step timing;
-            # SQRT coupling takes the reference's parallel generate_gaussian.
-            fh.write(f"stat = 1\nmu = {0.5 * n_side}\nmass = {MASS}\nelementaryWilsonLines = 1\n"
-                     f"file_name = bench\nlangevin_steps = {warmup + steps}\nmeasurements = 1\nstep = {STEP}\n"
+            # the initial condition is outside the per-step timing (1 MV slice
+            # unless asked); SQRT coupling takes the reference's parallel
+            # generate_gaussian
+            fh.write(f"stat = 1\nmu = {0.5 * n_side}\nmass = {MASS}\nelementaryWilsonLines = {slices}\n"
+                     f"file_name = bench\nlangevin_steps = {warmup + steps}\nmeasurements = 1\nstep = {step}\n"
                      f"EvolutionChoice = {evolution}\nCouplingChoice = {coupling}\nKernelChoice = SIN_KERNEL\n")
         env = dict(os.environ)
         env["OMP_NUM_THREADS"] = str(nthreads or os.cpu_count())
@@ -303,7 +358,8 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
         N = quantize_n(math.exp(rng.uniform(math.log(64), math.log(2048))))
         reqs.append(dict(N=N, ny_slices=int(rng.choice([50, 100])), steps=int(rng.integers(10, 2001)),
                          mu=float(rng.uniform(0.3, 0.8)) * N, seed=10_000 + i))
-    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=16, device=device, tick_sites=tick_sites)
+    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=16, device=device, tick_sites=tick_sites,
+                    reunitarize=REUNITARIZE)
     rids = [None] * n_requests
 
     def feeder():
@@ -312,8 +368,8 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
             dt = arrivals[i] - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            rids[i] = srv.submit(r["N"], r["steps"], ny_slices=r["ny_slices"], mu=r["mu"], mass=MASS, step=STEP,
-                                 coupling=jw.FIXED_COUPLING_CONSTANT, seed=r["seed"])
+            rids[i] = srv.submit(r["N"], r["steps"], ny_slices=r["ny_slices"], mu=r["mu"], mass=MASS,
+                                 step=FIXED_STEP, coupling=jw.FIXED_COUPLING_CONSTANT, seed=r["seed"])
 
     th = threading.Thread(target=feeder)
     th.start()
@@ -332,6 +388,9 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
     return {"requests": n_requests, "ok": ok, "rate_req_per_s": rate, "_mix": mix,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "site_steps_per_s": site_steps / (t_last - t_first), "wall_s": t_last - t_first,
+            "window": f"{n_requests} arrivals over {arrivals[-1]:.2f} s (Poisson, {rate:g}/s); latency and "
+                      f"throughput over the {t_last - t_first:.1f} s from the first submission to the last "
+                      "completion",
             "max_resident": stats.max_active,
             "offered_site_steps_per_s": site_steps / arrivals[-1],
             "tick_sites": tick_sites,
@@ -347,8 +406,8 @@ def plain_fp64_times(jw, device: int, sizes) -> dict:
     import torch
     out = {}
     for n in sizes:
-        cfg = jw.config_defaults(Nx=n, Ny=n, seed=3, mu=0.5 * n, mass=MASS, elementaryWilsonLines=2, step=STEP,
-                                 CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
+        cfg = jw.config_defaults(Nx=n, Ny=n, seed=3, mu=0.5 * n, mass=MASS, elementaryWilsonLines=2,
+                                 step=FIXED_STEP, CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
         ctx = jw.Context(cfg, device)
         s = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
         a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -373,12 +432,14 @@ def uneven_leg(jw, device: int, seed: int):
     fixed and running coupling mixed, all submitted at once to the server."""
     rng = np.random.default_rng(seed)
     sizes = [128] * 16 + [256] * 16 + [512] * 12 + [1024] * 4
-    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=32, device=device)
+    srv = jw.Server(precision=jw.PRECISION_MIXED, max_steps_per_tick=32, device=device, reunitarize=REUNITARIZE)
     reqs = [dict(N=n, steps=int(rng.integers(200, 2001)), coupling=[jw.FIXED_COUPLING_CONSTANT,
                                                                     jw.SQRT_COUPLING_CONSTANT][i % 2])
             for i, n in enumerate(sizes)]
     t0 = time.perf_counter()
-    rids = [srv.submit(r["N"], r["steps"], ny_slices=50, step=STEP, coupling=r["coupling"], seed=500 + i)
+    rids = [srv.submit(r["N"], r["steps"], ny_slices=50,
+                       step=FIXED_STEP if r["coupling"] == jw.FIXED_COUPLING_CONSTANT else STEP,
+                       coupling=r["coupling"], seed=500 + i)
             for i, r in enumerate(reqs)]
     ok = sum(srv.wait(rid, timeout=3600)[0] == jw.OK for rid in rids)
     wall = time.perf_counter() - t0
@@ -397,8 +458,8 @@ def c1_leg(jw, device: int):
     threads), per Langevin step."""
     import torch
     n = 64
-    cfg = jw.config_defaults(Nx=n, Ny=n, seed=1, mu=0.5 * n, mass=MASS, elementaryWilsonLines=NY_SLICES, step=STEP,
-                             CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
+    cfg = jw.config_defaults(Nx=n, Ny=n, seed=1, mu=0.5 * n, mass=MASS, elementaryWilsonLines=NY_SLICES,
+                             step=FIXED_STEP, CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
     ctx = jw.Context(cfg, device)
     s = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -425,12 +486,12 @@ def c1_leg(jw, device: int):
            "measure_ms": meas, "site_steps_per_s": n * n * 100 / (steps / 1e3), "Qs": qs}
     # the same event through the FP64 batched engine (fused kernels, graph replay)
     eng = jw.Engine(precision=jw.PRECISION_FP64, device=device)
-    warm = eng.add_event(n, ny_slices=NY_SLICES, mu=0.5 * n, mass=MASS, step=STEP,
+    warm = eng.add_event(n, ny_slices=NY_SLICES, mu=0.5 * n, mass=MASS, step=FIXED_STEP,
                          coupling=jw.FIXED_COUPLING_CONSTANT, seed=2)
     eng.init_mv([warm])
     eng.step([warm], 3)
     eng.measure([warm])
-    eid = eng.add_event(n, ny_slices=NY_SLICES, mu=0.5 * n, mass=MASS, step=STEP,
+    eid = eng.add_event(n, ny_slices=NY_SLICES, mu=0.5 * n, mass=MASS, step=FIXED_STEP,
                         coupling=jw.FIXED_COUPLING_CONSTANT, seed=1)
     es = torch.cuda.ExternalStream(eng.stream)
     torch.cuda.synchronize()
@@ -455,6 +516,74 @@ def c1_leg(jw, device: int):
     return out
 
 
+def fp64_engine_leg(jw, device: int, events: int, mixed_value: float, steps: int = 10) -> dict:
+    """The same workload through the FP64 batched engine (FP64 transforms,
+    k_step_pass1/2/3), timed with CUDA events over `steps` steps."""
+    import torch
+    eng = jw.Engine(precision=jw.PRECISION_FP64, device=device)
+    ids = [eng.add_event(N, ny_slices=NY_SLICES, mu=MU, mass=MASS, step=STEP, coupling=jw.SQRT_COUPLING_CONSTANT,
+                         seed=sd) for sd in event_seeds(0, events)]
+    eng.init_mv(ids)
+    eng.step(ids, 3)
+    s = torch.cuda.ExternalStream(eng.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(s)
+    eng.step(ids, steps)
+    b.record(s)
+    b.synchronize()
+    status = eng.sync()
+    eng.close()
+    ms = a.elapsed_time(b) / steps
+    v = events * N * N / (ms / 1e3)
+    return {"value": v, "unit": "site-steps/s", "ms_per_step": ms, "steps": steps, "status": status,
+            "mixed_over_fp64_batched": mixed_value / v,
+            "what": f"{events} events x {N}^2, FP64 batched engine (3 fused passes per step, graph replay)"}
+
+
+def mixed_error_leg(jw, device: int) -> dict:
+    """Mixed precision against the FP64 engine (pinned to the reference's V at
+    1e-12 by the parity tests) with the same seeds: max |dS(r)|, |dQ_s|/Q_s and
+    the unitarity drift, for the batched workload's size (4 of its events, 1000
+    steps), the uneven batch (one event per N, its step counts and couplings)
+    and a sample of the serving mix."""
+    from jimwlk.precision import compare_mixed_fp64
+
+    def sp(n, steps, seed, coupling, ny=NY_SLICES, g2mu=0.5):
+        fixed = coupling == jw.FIXED_COUPLING_CONSTANT
+        return dict(N=n, ny_slices=ny, mu=g2mu * n, mass=MASS, step=FIXED_STEP if fixed else STEP,
+                    coupling=coupling, seed=seed, steps=steps)
+
+    def summary(res, what):
+        return {"what": what, "dS_max": res["dS_max"], "Qs_rel_err_max": res["Qs_rel_err_max"],
+                "drift_mixed_max": res["drift_mixed_max"], "drift_fp64_max": res["drift_fp64_max"],
+                "ensembles": {str(k): v for k, v in res["ensembles"].items()}, "status": res["status"],
+                "per_event": [{k: e[k] for k in ("N", "steps", "dS_max", "Qs", "Qs_rel_err", "drift_mixed")}
+                              for e in res["per_event"]]}
+
+    t0 = time.perf_counter()
+    out = {"bars": {"dS_max": 1e-5, "Qs_rel_err": 1e-4}, "comparator": "FP64 batched engine, same seeds"}
+    out["C3"] = summary(compare_mixed_fp64(jw, [sp(N, 1000, 7000 + i, jw.SQRT_COUPLING_CONSTANT)
+                                                for i in range(4)], device),
+                        f"4 events x {N}^2, Ny = {NY_SLICES}, 1000 steps, running coupling (the benched workload)")
+    rng = np.random.default_rng(48)
+    c4 = [sp(n, int(rng.integers(200, 2001)), 600 + i,
+             [jw.FIXED_COUPLING_CONSTANT, jw.SQRT_COUPLING_CONSTANT][i % 2]) for i, n in enumerate((128, 256, 512, 1024))]
+    out["C4"] = summary(compare_mixed_fp64(jw, c4, device),
+                        "one event per N in {128, 256, 512, 1024}, steps U[200, 2000], fixed/running couplings")
+    rng = np.random.default_rng(2026)
+    c5 = []
+    for i in range(4):
+        n = quantize_n(math.exp(rng.uniform(math.log(64), math.log(2048))))
+        c5.append(sp(n, int(rng.integers(10, 2001)), 10_000 + i, jw.FIXED_COUPLING_CONSTANT,
+                     ny=int(rng.choice([50, 100])), g2mu=float(rng.uniform(0.3, 0.8))))
+    c5.append(sp(2048, 2000, 10_100, jw.FIXED_COUPLING_CONSTANT, ny=100, g2mu=0.8))
+    out["C5"] = summary(compare_mixed_fp64(jw, c5, device),
+                        "4 requests drawn from the serving mix + the largest one (2048^2, Ny = 100, 2000 steps)")
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -465,14 +594,26 @@ def cpu_model():
     return "unknown"
 
 
+def workload_config(events: int = EVENTS, n_side: int = N) -> dict:
+    """The benched workload, the same dictionary in both arms."""
+    return {"workload": f"{events} events x {n_side}^2 Langevin evolution, MV initial condition, running coupling",
+            "N": n_side, "events": events, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "ds": DS,
+            "step": STEP, "evolution": "momentum", "kernel": "SIN", "coupling": "running (SQRT_COUPLING_CONSTANT)",
+            "l2": "inputs ~5.6 GB per GPU > L2 (no flush needed)"}
+
+
 def reference_arm(args):
+    """The reference's main_optimized on one event of the benched configuration
+    (the reference steps one event at a time): the same N, MV slices, coupling,
+    kernel and step, K timed Langevin steps after W untimed ones (at most 100
+    and 10, a bounded sample of the 64-event workload)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     cores = os.cpu_count()
-    steps = max(1, min(args.steps, 10))
-    warm = max(1, min(args.warmup, 3))
-    t, why = run_reference_main(steps, warm)
+    steps = max(1, min(args.steps, 100))
+    warm = max(1, min(args.warmup, 10))
+    t, why = run_reference_main(steps, warm, slices=NY_SLICES)
     if t is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return
@@ -481,12 +622,11 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": 0,
         "steps": steps, "warmup": warm, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{EVENTS} events x {N}^2 Langevin evolution (reference: one event at a time)",
-                   "N": N, "events": EVENTS, "step": STEP, "kernel": "SIN", "coupling": "running (SQRT)"},
+        "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": "site-steps/s", "cores": cores, "kind": "reference",
-                         "sample": f"1 event {N}^2, {steps} Langevin steps after {warm} warm-up; main_optimized "
-                                   f"with OpenMP ({cores} threads, {cpu_model()}), FFTW replaced by the project "
-                                   "FFT shim"},
+                         "sample": f"1 of the {EVENTS} events ({N}^2, {NY_SLICES} MV slices), {steps} Langevin "
+                                   f"steps after {warm} warm-up; main_optimized with OpenMP ({cores} threads, "
+                                   f"{cpu_model()}), FFTW replaced by the project's radix-2 FFT shim"},
         "e2e": {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -505,9 +645,10 @@ def main_arm(args):
 
     events = args.events
     n_side = args.n
-    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch, autotune=True)
+    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch, autotune=True,
+                    reunitarize=REUNITARIZE)
     ids = [eng.add_event(n_side, ny_slices=NY_SLICES, mu=0.5 * n_side, mass=MASS, step=STEP,
-                         coupling=jw.FIXED_COUPLING_CONSTANT, seed=sd) for sd in event_seeds(rank, events)]
+                         coupling=jw.SQRT_COUPLING_CONSTANT, seed=sd) for sd in event_seeds(rank, events)]
     eng.init_mv(ids)
     eng.step(ids, args.warmup)
     if eng.sync() != jw.OK:
@@ -587,11 +728,9 @@ def main_arm(args):
         "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 transforms / f64 exponentials and V", "data": "synthetic",
-        "config": {"workload": f"{events} events x {n_side}^2, mixed precision, batched (per GPU)", "events": events,
-                   "max_batch": args.max_batch,
-                   "N": n_side, "ny_slices": NY_SLICES, "g2mu_a": 0.5, "m_a": 0.02, "alpha_s": ALPHA_S, "ds": DS,
-                   "step": STEP, "kernel": "SIN", "coupling": "fixed", "l2": "inputs ~5.6 GB per GPU > L2",
-                   "parallelism": f"events sharded, {world} rank(s)",
+        "config": workload_config(events, n_side),
+        "engine": {"precision": "mixed", "reunitarize": REUNITARIZE, "max_batch": args.max_batch,
+                   "parallelism": f"events sharded over {world} rank(s), {events} per rank",
                    "autotuned_column_tile": eng.tuning(n_side)},
         "e2e": {"value": e2e_value, "unit": "site-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e,
@@ -607,7 +746,7 @@ def main_arm(args):
     if rank == 0 and world == 1 and not args.no_extras and n_side == N:
         # plain FP64 form: the call-for-call layer (reference structure), one event at a time
         cfg = jw.config_defaults(Nx=N, Ny=N, seed=7, mu=MU, mass=MASS, elementaryWilsonLines=1, step=STEP,
-                                 CouplingChoice=jw.FIXED_COUPLING_CONSTANT)
+                                 CouplingChoice=jw.SQRT_COUPLING_CONSTANT)
         ctx = jw.Context(cfg)
         V = ctx.field()
         ctx.initial_condition(V)
@@ -615,16 +754,22 @@ def main_arm(args):
         ctx.sync()
         s0 = torch.cuda.ExternalStream(jw.lib().jw_context_stream(ctx._h))
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        kp = 5
+        kp = 10
         a0.record(s0)
         ctx.evolve_momentum(V, 2, kp)
         a1.record(s0)
         a1.synchronize()
         plain = N * N * kp / (a0.elapsed_time(a1) / 1e3)
-        line["fp64_plain"] = {"value": plain, "unit": "site-steps/s",
+        line["fp64_plain"] = {"value": plain, "unit": "site-steps/s", "steps": kp,
                               "what": "jw_evolve_momentum, reference call structure, FP64, one 512^2 event",
                               "mixed_batched_over_plain": value / plain}
         ctx.close()
+        # the FP64 batched engine on the same 64 events: what batching and fusion give
+        # without the FP32 transforms (the rest of the ratio above is precision)
+        line["fp64_engine"] = fp64_engine_leg(jw, local, events, value)
+        line["fp64_plain"]["fp64_batched_over_plain"] = line["fp64_engine"]["value"] / plain
+        # mixed-precision error against the FP64 engine at the quoted sizes and step counts
+        line["mixed_error"] = mixed_error_leg(jw, local)
         line["serve"] = serve_leg(jw, local, args.serve_requests, 200.0, 2026, tick_sites=SERVE_TICK_SITES)
         line["serve"]["vs_fp64_plain"] = line["serve"]["site_steps_per_s"] / plain
         # the plain FP64 form one request at a time on the same mix: MV slices and steps per request
@@ -674,7 +819,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64-plain and CPU-baseline legs")
     ap.add_argument("--events", type=int, default=EVENTS, help="events per GPU (profiling runs use fewer)")
     ap.add_argument("--max-batch", type=int, default=0, help="events per launch group (0 = engine default)")
-    ap.add_argument("--serve-requests", type=int, default=100, help="requests in the serving window")
+    ap.add_argument("--serve-requests", type=int, default=1000, help="requests in the serving window")
     ap.add_argument("--n", type=int, default=N, help="lattice side (profiling runs; the workload is 512)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "engine":

@@ -176,9 +176,15 @@ jw_status jw_average_and_symmetrize(jw_context* ctx, jw_field* corr);
  * 512*512 complex doubles (4 MiB) on every GPU that loads it, held until the
  * process exits; N > 512 returns JW_EINVAL.  All calls share that array and
  * each call overwrites what it reads, so calls that overlap on the GPU race
- * and must be ordered by the caller.  The first call on a device looks up the
- * array's device address with that device current; make it before any
- * stream capture begins.  Allocates nothing. */
+ * and must be ordered by the caller.  corr must be 16-byte aligned
+ * (JW_EINVAL otherwise).  CUDA loads the library's device code lazily, so the
+ * array is reserved on a device by the first call there, which also looks up
+ * its device address with that device current (again after the device's
+ * context was reset).  A caller whose pool allocator takes the device's free
+ * memory first calls jw_average_and_symmetrize_noalloc(NULL, 0, NULL) with
+ * the device current, before the pool reserves its memory: that set-up call
+ * launches nothing.  Make the first call before any stream capture begins.
+ * Calls no cudaMalloc or cudaFree. */
 jw_status jw_average_and_symmetrize_noalloc(double* corr, int N, void* stream);
 /* gfield::reduce(sum, err, mpi) (field.h:1521-1536): sum += corr, err += corr^2. */
 jw_status jw_reduce(jw_context* ctx, const jw_field* corr, jw_field* sum, jw_field* err);

@@ -228,6 +228,16 @@ __device__ __forceinline__ void mul3_adj(const V a[9], const V b[9], V c[9]) {
 // (arXiv:physics/0610206), restated here for double2 registers.  Only the
 // upper triangle and the real parts of the diagonal are read, except in the
 // Householder step, which reads the complex diagonal as the reference does.
+//
+// Licence notice.  The eigen-solver routines below (eig_cardano,
+// tridiag_householder, eig_ql, eigh3) follow, step for step, Kopp's
+// zheevh3 library (zheevc3.cpp, zheevq3.cpp, zhetrd3.cpp, zheevh3.cpp in the
+// reference's zheevh3-C-1.1 directory), Copyright (C) 2006 Joachim Kopp,
+// distributed under the GNU Lesser General Public License version 2.1 or
+// later.  The same operation order is kept so that the exponential matches the
+// reference's to 1e-13; these routines are therefore a work based on that
+// library and are covered by the LGPL 2.1 (or later) terms under which it is
+// distributed.
 struct Mat3d { double2 a[3][3]; };
 
 __device__ __forceinline__ double d_sqr(double x) { return x * x; }
