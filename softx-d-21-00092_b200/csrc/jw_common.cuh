@@ -10,6 +10,7 @@
 // Device-side error flags (bit mask in a device int, cleared by the syncs).
 #define JW_FLAG_NOCONV 1
 #define JW_FLAG_NAN 2
+#define JW_FLAG_TIMEOUT 4  // a bounded wait on a barrier or a tile load ran out
 
 namespace jw {
 

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -35,6 +36,7 @@ struct Group {
     double* nf64 = nullptr;          // noise factor (NOISE coupling)
     float* nf32 = nullptr;
     int p2_cols = 0;                 // mixed pass 2 column-tile width (0: the default)
+    int p31_form = 0;                // mixed pass 3 + 1: 0 one CTA per row, 1 persistent ring
     bool tuned = false;              // the autotuner has run for this size
 };
 
@@ -418,17 +420,85 @@ struct LaunchTimes {
     }
 };
 
-// f(std::integral_constant<int, C>) for every valid pass-2 tile width C.
+// The persistent column pass with tensor-memory-accelerator loads
+// (k_mix_pass2_tma, 8-column tiles) is tuning choice kP2Tma beside the tile
+// widths 1, 2, 4 and 8 of k_mix_pass2.
+constexpr int kP2Tma = 16;
+
+// cuTensorMapEncodeTiled through the runtime's driver entry points (no link
+// against libcuda); null when the driver does not provide it.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// f(std::integral_constant<int, C>) for every valid pass-2 tuning choice C.
 template <int N, typename F>
 void for_each_p2_cols(F&& f) {
     if constexpr (mx_s2_valid<N, 1>()) f(std::integral_constant<int, 1>{});
     if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, 2>{});
     if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, 4>{});
     if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, 8>{});
+    if constexpr (mx_t2_valid<N>())
+        if (encode_tiled()) f(std::integral_constant<int, kP2Tma>{});
 }
 
-// Pass 2 with tile width `cols` (0: the default); advance = 0 leaves the step
-// index alone (timing launches of the autotuner).
+// The pair planes P of a launch group ([8 nb N rows][4 N floats]) as a 2D
+// tensor with boxes of 8 float4 elements (128 bytes) by min(N, 256) rows.
+template <int N>
+bool p2_tensor_map(CUtensorMap* map, float4* P, int nb) {
+    const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)8 * nb * N};
+    const cuuint64_t strides[1] = {(cuuint64_t)4 * N * sizeof(float)};
+    const cuuint32_t box[2] = {32, (cuuint32_t)(N < 256 ? N : 256)};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, P, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// CTAs of the persistent column pass: every SM filled to its occupancy.
+template <int N>
+int p2_tma_grid() {
+    static int grid = 0;
+    if (grid == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass2_tma<N>, mx_t2_threads<N>(),
+                                                      mx_t2_smem<N>());
+        grid = std::max(1, sms * std::max(1, per_sm));
+    }
+    return grid;
+}
+
+// CTAs of the persistent pass 3 + next pass 1: every SM filled to its occupancy.
+template <int N>
+int p31_ring_grid() {
+    static int grid = 0;
+    if (grid == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass31_ring<N>, mx_p31_threads<N>(),
+                                                      mx_p31r_smem<N>());
+        grid = std::max(1, sms * std::max(1, per_sm));
+    }
+    return grid;
+}
+
+// Pass 2 with tuning choice `cols` (0: the default); advance = 0 leaves the
+// step index alone (timing launches of the autotuner).
 template <int N>
 void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, int advance) {
     const long vol = (long)N * N;
@@ -437,9 +507,17 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
     if (cols == 0) cols = mx_s2_cols<N>();
     for_each_p2_cols<N>([&](auto c) {
         constexpr int C = decltype(c)::value;
-        if (C == cols)
+        if (C != cols) return;
+        if constexpr (C == kP2Tma) {
+            CUtensorMap map;
+            if (!p2_tensor_map<N>(&map, P, nb)) return;
+            const int grid = std::min(p2_tma_grid<N>(), nb * 4 * (N / 8));
+            k_mix_pass2_tma<N><<<grid, mx_t2_threads<N>(), mx_t2_smem<N>(), e->stream>>>(
+                g.d_ev, d_slots, Q, g.tw.d32, nb, advance, e->d_flags, map);
+        } else {
             k_mix_pass2<N, C><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
                 g.d_ev, d_slots, P, Q, g.tw.d32, advance);
+        }
     });
 }
 
@@ -454,10 +532,18 @@ void mix_configure() {
     } else {
         cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
         cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
+        if constexpr (mx_p31r_valid<N>())
+            cudaFuncSetAttribute(k_mix_pass31_ring<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_p31r_smem<N>());
     }
     for_each_p2_cols<N>([](auto c) {
         constexpr int C = decltype(c)::value;
-        cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_s2_smem<N, C>());
+        if constexpr (C == kP2Tma)
+            cudaFuncSetAttribute(k_mix_pass2_tma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_t2_smem<N>());
+        else
+            cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_s2_smem<N, C>());
     });
     cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p3_smem<N>());
     if constexpr (mx_p3_meas_fits<N>())
@@ -504,6 +590,9 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
             if constexpr (mx_pair<N>())
                 k_mix_pass31_pair<N><<<dim3(N, 2, nb), mx_p31_threads<N>(), mx_p31p_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
+            else if (g.p31_form == 1 && mx_p31r_valid<N>())
+                k_mix_pass31_ring<N><<<std::min(p31_ring_grid<N>(), nb * N), mx_p31_threads<N>(), mx_p31r_smem<N>(),
+                                       e->stream>>>(g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags, nb);
             else
                 k_mix_pass31<N><<<dim3(N, nb), mx_p31_threads<N>(), mx_p31_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
@@ -1512,6 +1601,41 @@ JW_EXPORT jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols) {
     JW_CUDA(cudaStreamSynchronize(e->stream));  // launches already queued keep their width
     it->second->p2_cols = p2_cols;
     it->second->tuned = true;
+    return JW_OK;
+}
+
+namespace {
+bool row_form_valid(int N, int form) {
+    if (form == 0) return true;
+    if (form != 1) return false;
+    switch (N) {
+        case 8: return mx_p31r_valid<8>();
+        case 16: return mx_p31r_valid<16>();
+        case 32: return mx_p31r_valid<32>();
+        case 64: return mx_p31r_valid<64>();
+        case 128: return mx_p31r_valid<128>();
+        case 256: return mx_p31r_valid<256>();
+        case 512: return mx_p31r_valid<512>();
+        default: return false;
+    }
+}
+}  // namespace
+
+JW_EXPORT jw_status jw_engine_set_row_form(jw_engine* e, int N, int form) {
+    JW_CHECK(e);
+    auto it = e->groups.find(N);
+    if (it == e->groups.end()) return JW_ENOTFOUND;
+    if (!row_form_valid(N, form)) return JW_EINVAL;
+    JW_CUDA(cudaStreamSynchronize(e->stream));
+    it->second->p31_form = form;
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_engine_row_form(jw_engine* e, int N, int* form) {
+    JW_CHECK(e && form);
+    auto it = e->groups.find(N);
+    if (it == e->groups.end()) return JW_ENOTFOUND;
+    *form = it->second->p31_form;
     return JW_OK;
 }
 

@@ -44,6 +44,7 @@ bool supported_n(int N);
 inline jw_status flags_to_status(int flags) {
     if (flags & JW_FLAG_NOCONV) return JW_ENOCONV;
     if (flags & JW_FLAG_NAN) return JW_ENAN;
+    if (flags & JW_FLAG_TIMEOUT) return JW_ETIMEOUT;
     return JW_OK;
 }
 

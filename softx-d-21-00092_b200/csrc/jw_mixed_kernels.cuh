@@ -19,6 +19,7 @@
 
 #include <cooperative_groups.h>
 
+#include "jw_async.cuh"
 #include "jw_engine_kernels.cuh"
 
 namespace jw {
@@ -308,6 +309,140 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
     for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = reg_put(w, q);
 }
 
+// ------------------------------------------------------------------ pass 2, persistent with TMA
+// The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
+// rows, no padding needed), as a persistent kernel: each CTA walks the work
+// items (event, plane pair j, column tile) with stride gridDim.x, and the
+// tensor memory accelerator loads the next item's two planes while this one
+// is transformed.  Three tile buffers rotate: item k reads X (plane j) from
+// b0 and Y (plane 4 + j) from b1 and uses b1 for the inverse transform; the
+// next item's X goes to b2 when item k starts and its Y to b0 once X has been
+// transformed; the next item then finds (X, Y, free) in (b2, b0, b1).  Loads
+// are 2D tensor tiles {8 float4 elements, up to 256 rows} of P viewed as
+// [8 nb N rows][4 N floats], completion counted in bytes on one mbarrier per
+// buffer.  The arithmetic is k_mix_pass2's, element for element, so Q is
+// bit-identical.  Built for N <= 512 (three 64 KB tiles at 512^2).
+template <int N> constexpr int mx_t2_threads() { return 8 * (N / 8); }
+template <int N> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * 8 * N; }
+template <int N> constexpr size_t mx_t2_smem() { return 3 * mx_t2_tile_bytes<N>() + 1024; }
+template <int N> constexpr int mx_t2_blocks() {
+    return (int)((227 * 1024) / (mx_t2_smem<N>() + 1024)) < 1024 / mx_t2_threads<N>()
+               ? (int)((227 * 1024) / (mx_t2_smem<N>() + 1024))
+               : 1024 / mx_t2_threads<N>();
+}
+template <int N> constexpr bool mx_t2_valid() { return N >= 64 && N <= 512 && mx_t2_smem<N>() <= 227 * 1024; }
+
+template <int N>
+__global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_pass2_tma(
+    EventDev* __restrict__ ev, const int* __restrict__ slots, float4* __restrict__ Q, const float2* __restrict__ tw,
+    int nb, int advance, int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap) {
+    static_assert(mx_t2_valid<N>(), "three 8-column tiles per CTA");
+    constexpr int C = 8;
+    constexpr int PER = 8;
+    constexpr int RSTEP = N / 8;
+    constexpr int TILES = N / C;
+    constexpr int BOX = N < 256 ? N : 256;
+    constexpr unsigned TILE_BYTES = (unsigned)mx_t2_tile_bytes<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[3];
+    float4* base = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int tid = threadIdx.x;
+    const int cc = tid % C, r0 = tid / C;
+    const ColIdx16P<C> cidx{cc};
+    const long vol = (long)N * N;
+    const int items = nb * 4 * TILES;
+    if (tid == 0) {
+        tma_prefetch_map(&pmap);
+        for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // plane `half` (0: P[j], 1: P[4 + j]) of work item `it` into buffer bi (thread 0)
+    auto issue = [&](int it, int half, int bi) {
+        const int tile = it % TILES, j = (it / TILES) % 4, b = it / (TILES * 4);
+        const int y0 = (b * 8 + (half ? 4 + j : j)) * N;
+        float4* dst = base + (size_t)bi * N * C;
+        mbar_arrive_expect_tx(&bar[bi], TILE_BYTES);
+#pragma unroll
+        for (int r = 0; r < N; r += BOX) tma_load_2d(dst + (size_t)r * C, &pmap, tile * C * 4, y0 + r, &bar[bi]);
+    };
+    unsigned parity = 0;     // bit i: the parity buffer i's next completed phase has
+    unsigned pending = 0;    // bit i: a load into buffer i is in flight (same value in every thread)
+    int b0 = 0, b1 = 1, b2 = 2;
+    int it = blockIdx.x;
+    if (it < items) {
+        if (tid == 0) {
+            issue(it, 0, b0);
+            issue(it, 1, b1);
+        }
+        pending = (1u << b0) | (1u << b1);
+    }
+    bool timed_out = false;
+    for (; it < items; it += gridDim.x) {
+        const int next = it + (int)gridDim.x;
+        // the previous item's inverse transform is done with b2
+        if (__syncthreads_or(timed_out)) break;
+        if (next < items) {
+            if (tid == 0) {
+                fence_proxy_async_smem();
+                issue(next, 0, b2);
+            }
+            pending |= 1u << b2;
+        }
+        const int tile = it % TILES, j = (it / TILES) % 4, b = it / (TILES * 4);
+        const int c0 = tile * C;
+        if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
+        const EventDev& e = ev[slots[b]];
+        const float* kt = e.k32 + c0 + (long)r0 * N + cc;
+        float kx[PER], ky[PER];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            kx[q] = __ldg(kt + (long)q * RSTEP * N);
+            ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
+        }
+        float2 ra[2][8], w[2][8];
+        timed_out |= !mbar_wait_bounded(&bar[b0], (parity >> b0) & 1u);
+        parity ^= 1u << b0;
+        pending &= ~(1u << b0);
+        fft16x<float, N, false, true>(base + (size_t)b0 * N * C, cidx, r0, true, -1.0f, tw, ra);
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+            w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+        // every thread is done reading b0: the next item's Y may overwrite it
+        if (__syncthreads_or(timed_out)) break;
+        if (next < items) {
+            if (tid == 0) {
+                fence_proxy_async_smem();
+                issue(next, 1, b0);
+            }
+            pending |= 1u << b0;
+        }
+        timed_out |= !mbar_wait_bounded(&bar[b1], (parity >> b1) & 1u);
+        parity ^= 1u << b1;
+        pending &= ~(1u << b1);
+        fft16x<float, N, false, true>(base + (size_t)b1 * N * C, cidx, r0, true, -1.0f, tw, ra);
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+            w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+        // the inverse's first pass synchronises before it writes b1
+        fft16x<float, N, true, true>(base + (size_t)b1 * N * C, cidx, r0, true, 1.0f, tw, w);
+        float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = reg_put(w, q);
+        const int nb0 = b2, nb1 = b0, nb2 = b1;
+        b0 = nb0;
+        b1 = nb1;
+        b2 = nb2;
+    }
+    if (timed_out) {
+        if (tid == 0) atomicOr(flags, JW_FLAG_TIMEOUT);
+        // loads still in flight land in this CTA's shared memory: wait for them
+        // (bounded) before the CTA exits
+        for (int i = 0; i < 3; ++i)
+            if ((pending >> i) & 1u) mbar_wait_bounded(&bar[i], (parity >> i) & 1u);
+    }
+}
+
 // ------------------------------------------------------------------ pass 3
 // The update of site y: V <- exp(+i sqrt(eps) B) V exp(-i sqrt(eps) A), A and B
 // from the inverse row transforms in column y of the row buffer.  The old V is
@@ -466,6 +601,128 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     if (fl) atomicOr(flags, fl);
     __syncthreads();
     fft16_rows_store<float, N>(sm, 8, -1.0f, tw, P + (long)b * 8 * vol + (long)x * N, vol);
+}
+
+// Pass 3 + next pass 1 as a persistent kernel: each CTA walks the lattice
+// rows (event, x) with stride gridDim.x and copies the next row's 4 Q rows
+// (cp.async) while it works on this one.  Shared memory is three regions of
+// 4 padded pair rows.  Row k: Q in region k mod 3, transformed in place; the
+// next step's noise pairs overwrite it column by column (the thread that
+// consumed column y writes it), the rotated pairs go to region (k + 2) mod 3,
+// and the next row's Q arrives in region (k + 1) mod 3.  Row k + 1 then finds
+// its Q where it was copied and writes its rotated pairs where row k's Q was.
+// Per site the arithmetic is k_mix_pass31's, so V and P are bit-identical.
+template <int N> constexpr size_t mx_p31r_region() { return 16 * (size_t)padded_len16(4 * N); }
+template <int N> constexpr size_t mx_p31r_smem() { return 3 * mx_p31r_region<N>(); }
+template <int N> constexpr int mx_p31r_blocks() {
+    return mx_p31_threads<N>() <= 256 && mx_p31r_smem<N>() + 1024 <= 113 * 1024 ? 2 : 1;
+}
+template <int N> constexpr bool mx_p31r_valid() { return !mx_pair<N>() && mx_p31r_smem<N>() <= 112 * 1024; }
+
+// Copy the 4 Q rows of lattice row x of launch-group event b into region dst.
+template <int N>
+__device__ __forceinline__ void p31r_fetch(float4* dst, const float4* __restrict__ Q, int b, int x) {
+    const long vol = (long)N * N;
+    const float4* in = Q + (long)b * 4 * vol + (long)x * N;
+    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
+        cp_async<16>(&dst[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    cp_async_commit();
+}
+
+template <int N>
+__global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p31r_blocks<N>()) k_mix_pass31_ring(
+    EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q, float4* __restrict__ P,
+    const float2* __restrict__ tw, int* __restrict__ flags, int nb) {
+    static_assert(mx_p31r_valid<N>(), "three regions of 4 pair rows per CTA");
+    constexpr int RL = padded_len16(4 * N);  // elements per region
+    constexpr int TPS = N / 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* region = reinterpret_cast<float4*>(smem_raw);
+    const long vol = (long)N * N;
+    const int rows = nb * N;
+    int fl = 0;
+    int k = 0;
+    int item = blockIdx.x;
+    if (item < rows) p31r_fetch<N>(region, Q, item / N, item % N);
+#pragma unroll 1
+    for (; item < rows; item += gridDim.x, ++k) {
+        // fresh copies of the thread index and the twiddle pointer per row, so
+        // that the compiler does not keep the transforms' shared-memory
+        // indices and twiddles in registers across rows
+        const float2* twr = tw;
+        int tid = threadIdx.x;
+        asm volatile("" : "+l"(twr), "+r"(tid));
+        float4* rq = region + (size_t)(k % 3) * RL;        // Q, then the noise pairs
+        float4* rn = region + (size_t)((k + 1) % 3) * RL;  // the next row's Q
+        float4* ro = region + (size_t)((k + 2) % 3) * RL;  // the rotated pairs
+        const int b = item / N, x = item % N;
+        cp_async_wait<0>();
+        __syncthreads();  // this row's Q has landed; the previous row is done with rn and ro
+        const int next = item + (int)gridDim.x;
+        if (next < rows) p31r_fetch<N>(rn, Q, next / N, next % N);
+        {
+            const int r = tid / TPS;  // 4 rows in rounds of blockDim / TPS
+            for (int p0 = 0; p0 < 4; p0 += (int)blockDim.x / TPS)
+                fft16<float, N>(rq, RowIdx16{(p0 + r) * N}, tid % TPS, p0 + r < 4 && r < (int)blockDim.x / TPS,
+                                1.0f, twr);
+        }
+        EventDev& e = ev[slots[b]];
+        const double se = e.sqrt_eps;
+        const float* nf = e.nf32;
+        for (int y = tid; y < N; y += blockDim.x) {
+            const long site = (long)x * N + y;
+            float2 v32[9];
+            {
+                double2 v[9];
+                p3_site<N>(e, rq, y, site, vol, se, v, fl);
+#pragma unroll
+                for (int kk = 0; kk < 9; ++kk) {
+                    e.V[kk * vol + site] = v[kk];
+                    v32[kk] = make_float2((float)v[kk].x, (float)v[kk].y);
+                }
+            }
+            float z[16];
+            langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+            const float f = nf ? nf[site] : 1.0f;
+#pragma unroll
+            for (int kk = 0; kk < 16; ++kk) z[kk] *= f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+                rq[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+            float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                n[kk] = z[2 * kk];
+                m[kk] = z[2 * kk + 1];
+            }
+            rotate_herm(v32, n, hx);
+            rotate_herm(v32, m, hy);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+                ro[pad16(j * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+        }
+        __syncthreads();
+        // forward row transforms of the 8 pair rows (0..3 in rq, 4..7 in ro),
+        // the last pass storing straight to P
+        {
+            const int spr = blockDim.x / TPS;
+            const int r = tid / TPS, t = tid % TPS;
+            float4* out = P + (long)b * 8 * vol + (long)x * N;
+            for (int p0 = 0; p0 < 8; p0 += spr) {
+                const int p = p0 + r;
+                const bool act = r < spr && p < 8;
+                float2 rv[2][8];
+                fft16x<float, N, false, true>(p < 4 ? rq : ro, RowIdx16{(p & 3) * N}, t, act, -1.0f, twr, rv);
+                if (act) {
+                    float4* o = out + (long)p * vol + t;
+#pragma unroll
+                    for (int m = 0; m < 8; ++m) o[(long)m * TPS] = reg_put(rv, m);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+    if (fl) atomicOr(flags, fl);
 }
 
 // Pass 3 + next pass 1 where a lattice row needs a cluster of two CTAs

@@ -91,13 +91,15 @@ def test_autotuner_choice_does_not_change_results(jw, N):
     tuned.step(tids, 4)
     assert tuned.sync() == jw.OK
     chosen = tuned.tuning(N)
-    assert chosen in (1, 2, 4, 8)
+    assert chosen in (1, 2, 4, 8, 16)
     for a, i in zip(ref, tids):
         assert np.array_equal(a, tuned.get_V(i))
     assert all(tuned.steps_taken(i) == 4 for i in tids)
     tuned.close()
     widths = [c for c in (1, 2, 4, 8) if c <= N and c * (N // 8) <= 1024 and
               2 * 16 * (N * c + (0 if c >= 8 else (N // 8) * c)) <= 227 * 1024]
+    if 64 <= N <= 512:
+        widths.append(16)  # the persistent form with tensor-memory-accelerator tile loads
     assert chosen in widths
     for c in widths:
         eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
@@ -110,4 +112,32 @@ def test_autotuner_choice_does_not_change_results(jw, N):
     eng, ids = make(jw, N, 1, jw.PRECISION_MIXED)
     with pytest.raises(RuntimeError):
         eng.set_tuning(N, 3)
+    eng.close()
+
+
+@pytest.mark.parametrize("N,events", [(64, 3), (256, 2), (512, 3)])
+def test_kernel_forms_are_bitwise_identical(jw, N, events):
+    """The persistent forms (column pass with tensor-memory-accelerator tile
+    loads, row pass with the next row's input prefetched) give the default
+    forms' lattices bit for bit, over runs long enough for graph replay, with
+    more rows than persistent CTAs."""
+    eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+    eng.step(ids, 6)
+    ref = [eng.get_V(i) for i in ids]
+    eng.close()
+    for p2, row in ((16, 0), (0, 1), (16, 1)):
+        eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+        eng.set_tuning(N, p2)
+        eng.set_row_form(N, row)
+        assert eng.row_form(N) == row
+        eng.step(ids, 6)
+        assert eng.sync() == jw.OK
+        for a, i in zip(ref, ids):
+            assert np.array_equal(a, eng.get_V(i)), (p2, row)
+        eng.close()
+    eng, ids = make(jw, 1024, 1, jw.PRECISION_MIXED)
+    with pytest.raises(RuntimeError):
+        eng.set_row_form(1024, 1)
+    with pytest.raises(RuntimeError):
+        eng.set_tuning(1024, 16)
     eng.close()
