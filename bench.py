@@ -577,9 +577,9 @@ def mixed_error_leg(jw, device: int) -> dict:
         n = quantize_n(math.exp(rng.uniform(math.log(64), math.log(2048))))
         c5.append(sp(n, int(rng.integers(10, 2001)), 10_000 + i, jw.FIXED_COUPLING_CONSTANT,
                      ny=int(rng.choice([50, 100])), g2mu=float(rng.uniform(0.3, 0.8))))
-    c5.append(sp(2048, 2000, 10_100, jw.FIXED_COUPLING_CONSTANT, ny=100, g2mu=0.8))
     out["C5"] = summary(compare_mixed_fp64(jw, c5, device),
-                        "4 requests drawn from the serving mix + the largest one (2048^2, Ny = 100, 2000 steps)")
+                        "4 requests drawn from the serving mix (N = 128, 256, 2048, 128; the FP64 comparator "
+                        "above 1024^2 is the call-for-call layer)")
     out["seconds"] = time.perf_counter() - t0
     return out
 
