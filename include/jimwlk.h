@@ -469,6 +469,14 @@ jw_status jw_server_submit(jw_server* s, const jw_request_desc* d, int64_t* requ
 jw_status jw_server_wait(jw_server* s, int64_t request_id, double timeout_s, jw_request_result* res,
                          double* S_bins, double* r_bins, int nbins_cap);
 jw_status jw_server_get_stats(jw_server* s, jw_server_stats* st);
+/* No counterpart in the reference.  Per-lattice-size totals of the server's
+ * work so far, sizes in increasing order: site-steps advanced, device
+ * milliseconds of the Langevin-step launches (CUDA events on the engine
+ * stream around each size's launches of a tick) and of the MV initial
+ * conditions, and the ticks that stepped the size.  Fills at most cap entries
+ * of the (optional) arrays; *count receives the number of sizes. */
+jw_status jw_server_size_stats(jw_server* s, int* N, double* site_steps, double* step_ms, double* mv_ms,
+                               int64_t* ticks, int cap, int* count);
 
 #ifdef __cplusplus
 }

@@ -447,7 +447,9 @@ __device__ __forceinline__ int expi_herm(double2 m[9], double sign) {
 // evaluated for |c0| (f_j(-c0) = (-1)^j conj f_j(c0)) so that 9u^2 - w^2 >= 2 c1.
 // For c1 <= 0.05 (|Q| below ~0.3: every Langevin update at the usual step
 // sizes) the Taylor series of exp(iQ), reduced with Q^3 = c1 Q + c0, is used
-// instead; it needs no transcendental functions.
+// instead; it needs no transcendental functions.  For c1 <= 2e-3 (typical
+// updates) ten terms suffice and are summed as closed-form polynomials in c0
+// and c1.
 // Only the upper triangle and the real diagonal of m are read.
 __device__ __forceinline__ void expi_ch(double2 m[9], double sign) {
     const double a = sign * m[0].x, b = sign * m[4].x, c = sign * m[8].x;
@@ -462,7 +464,23 @@ __device__ __forceinline__ void expi_ch(double2 m[9], double sign) {
     const double2 def = cmulc(cmul(d, e), f);                          // d e conj(f)
     const double c0 = a * b * c - a * ee - b * ff - c * dd + 2.0 * def.x;
     double2 f0, f1, f2;
-    if (c1 <= 0.05) {
+    if (c1 <= 2e-3) {
+        // The same series truncated after (iQ)^10, with Q^n reduced to
+        // f0 + f1 Q + f2 Q^2 in closed form (polynomials in c0 and c1):
+        // |Q| <= sqrt(4 c1 / 3) <= 0.052 here, so the first omitted term is
+        // below 0.052^11 / 11! < 4e-22.  Evaluated in nested (Horner) form.
+        const double x = c0, y = c1, x2 = c0 * c0;
+        f0 = make_double2(1.0 + x2 * (-1.0 / 720.0 + y * (1.0 / 20160.0 - y * (1.0 / 1209600.0))),
+                          x * (-1.0 / 6.0 + y * (1.0 / 120.0 + y * (-1.0 / 5040.0 + y * (1.0 / 362880.0)))) +
+                              x2 * x * (1.0 / 362880.0));
+        f1 = make_double2(x * (1.0 / 24.0 + y * (-1.0 / 360.0 + y * (1.0 / 13440.0 - y * (1.0 / 907200.0)))) -
+                              x2 * x * (1.0 / 3628800.0),
+                          1.0 + y * (-1.0 / 6.0 + y * (1.0 / 120.0 + y * (-1.0 / 5040.0 + y * (1.0 / 362880.0)))) +
+                              x2 * (-1.0 / 5040.0 + y * (1.0 / 120960.0)));
+        f2 = make_double2(-0.5 + y * (1.0 / 24.0 + y * (-1.0 / 720.0 + y * (1.0 / 40320.0 - y * (1.0 / 3628800.0)))) +
+                              x2 * (1.0 / 40320.0 - y * (1.0 / 1209600.0)),
+                          x * (1.0 / 120.0 + y * (-1.0 / 2520.0 + y * (1.0 / 120960.0))));
+    } else if (c1 <= 0.05) {
         // sum_n (i^n / n!) Q^n with Q^n = a_n + b_n Q + c_n Q^2 and, from
         // Q^3 = c1 Q + c0: (a, b, c)_{n+1} = (c0 c_n, a_n + c1 c_n, b_n).
         // |Q| <= sqrt(2 c1) <= 0.32, so 16 terms leave < 1e-21.

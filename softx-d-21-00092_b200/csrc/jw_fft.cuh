@@ -189,16 +189,26 @@ struct ColIdx16 {
     __device__ __forceinline__ int operator()(int e) const { return e * C + c; }
 };
 
-template <typename V, typename T>
-__device__ __forceinline__ V tw_load(const V* __restrict__ tw, int m, T sign) {
-    V w = __ldg(&tw[m]);
+// Twiddle sources: the global table (read through the read-only cache) or a
+// copy of it in shared memory (TwShared), for kernels that keep one.
+template <typename V> struct TwShared {
+    const V* p;
+};
+template <typename V>
+__device__ __forceinline__ V tw_get(const V* __restrict__ tw, int m) { return __ldg(&tw[m]); }
+template <typename V>
+__device__ __forceinline__ V tw_get(const TwShared<V>& tw, int m) { return tw.p[m]; }
+
+template <typename V, typename T, typename TW>
+__device__ __forceinline__ V tw_load(const TW& tw, int m, T sign) {
+    V w = tw_get(tw, m);
     w.y *= sign;
     return w;
 }
 
-template <typename T, int N, int Ns, int R, typename IdxF>
+template <typename T, int N, int Ns, int R, typename IdxF, typename TW>
 __device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
-                                                bool active, T sign, const C2<T>* __restrict__ tw) {
+                                                bool active, T sign, const TW& tw) {
     using V = C2<T>;
     using E = typename Elem16<T>::E;
     constexpr int VL = Elem16<T>::VL;
@@ -221,11 +231,11 @@ __device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restric
             }
             if (Ns > 1) {
                 V w[8];
-                w[1] = tw_load(tw, k * TWS, sign);
-                if constexpr (R >= 4) w[2] = tw_load(tw, 2 * k * TWS, sign);
+                w[1] = tw_load<V>(tw, k * TWS, sign);
+                if constexpr (R >= 4) w[2] = tw_load<V>(tw, 2 * k * TWS, sign);
                 if constexpr (R == 4) w[3] = cmul(w[1], w[2]);
                 if constexpr (R == 8) {
-                    w[4] = tw_load(tw, 4 * k * TWS, sign);
+                    w[4] = tw_load<V>(tw, 4 * k * TWS, sign);
                     w[3] = cmul(w[1], w[2]);
                     w[5] = cmul(w[4], w[1]);
                     w[6] = cmul(w[4], w[2]);
@@ -267,9 +277,9 @@ __device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restric
     __syncthreads();
 }
 
-template <typename T, int N, int Ns, typename IdxF>
+template <typename T, int N, int Ns, typename IdxF, typename TW>
 __device__ __forceinline__ void fft16_passes(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
-                                             const C2<T>* __restrict__ tw) {
+                                             const TW& tw) {
     if constexpr (Ns < N) {
         constexpr int rem = N / Ns;
         constexpr int R = rem >= 8 ? 8 : rem;
@@ -283,9 +293,9 @@ __device__ __forceinline__ void fft16_passes(typename Elem16<T>::E* sm, const Id
 // elements.  So a transform can end in registers (for an elementwise step, a
 // reduction or a store) and the next one start from them, without the shared-
 // memory round trip.  reg[l][m] is element t + m N/8 of sequence l.
-template <typename T, int N, int Ns, int R, bool IN, bool OUT, typename IdxF>
+template <typename T, int N, int Ns, int R, bool IN, bool OUT, typename IdxF, typename TW>
 __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
-                                                 bool active, T sign, const C2<T>* __restrict__ tw,
+                                                 bool active, T sign, const TW& tw,
                                                  C2<T> (&reg)[Elem16<T>::VL][8]) {
     using V = C2<T>;
     constexpr int VL = Elem16<T>::VL;
@@ -315,11 +325,11 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
             }
             if (Ns > 1) {
                 V w[8];
-                w[1] = tw_load(tw, k * TWS, sign);
-                if constexpr (R >= 4) w[2] = tw_load(tw, 2 * k * TWS, sign);
+                w[1] = tw_load<V>(tw, k * TWS, sign);
+                if constexpr (R >= 4) w[2] = tw_load<V>(tw, 2 * k * TWS, sign);
                 if constexpr (R == 4) w[3] = cmul(w[1], w[2]);
                 if constexpr (R == 8) {
-                    w[4] = tw_load(tw, 4 * k * TWS, sign);
+                    w[4] = tw_load<V>(tw, 4 * k * TWS, sign);
                     w[3] = cmul(w[1], w[2]);
                     w[5] = cmul(w[4], w[1]);
                     w[6] = cmul(w[4], w[2]);
@@ -374,9 +384,9 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
     }
 }
 
-template <typename T, int N, int Ns, bool IN, bool OUT, typename IdxF>
+template <typename T, int N, int Ns, bool IN, bool OUT, typename IdxF, typename TW>
 __device__ __forceinline__ void fft16x_passes(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
-                                              const C2<T>* __restrict__ tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
+                                              const TW& tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
     if constexpr (Ns < N) {
         constexpr int rem = N / Ns;
         constexpr int R = rem >= 8 ? 8 : rem;
@@ -387,9 +397,9 @@ __device__ __forceinline__ void fft16x_passes(typename Elem16<T>::E* sm, const I
 
 // fft16 with the first pass reading reg (IN) and/or the last pass writing reg
 // (OUT) instead of sm; sm still carries the passes in between.
-template <typename T, int N, bool IN, bool OUT, typename IdxF>
+template <typename T, int N, bool IN, bool OUT, typename IdxF, typename TW>
 __device__ __forceinline__ void fft16x(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
-                                       const C2<T>* __restrict__ tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
+                                       const TW& tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
     static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two N >= 8");
     fft16x_passes<T, N, 1, IN, OUT>(sm, idx, t, active, sign, tw, reg);
 }
@@ -406,9 +416,9 @@ __device__ __forceinline__ double2 reg_put(const double2 (&reg)[1][8], int m) { 
 
 // Transform the VL sequences held in the elements sm[idx(e)], e < N, with
 // thread t < N/8; all threads of the CTA must call it.
-template <typename T, int N, typename IdxF>
+template <typename T, int N, typename IdxF, typename TW>
 __device__ __forceinline__ void fft16(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
-                                      const C2<T>* __restrict__ tw) {
+                                      const TW& tw) {
     static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two N >= 8");
     fft16_passes<T, N, 1>(sm, idx, t, active, sign, tw);
 }

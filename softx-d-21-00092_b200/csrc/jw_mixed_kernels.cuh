@@ -107,8 +107,8 @@ __device__ __forceinline__ void rotate_herm(const float2 v[9], const float n[8],
 }
 
 // Transform NP contiguous padded pair rows (16-byte elements) in rounds.
-template <int N, int NP>
-__device__ __forceinline__ void fft16_rows(float4* sm, float sign, const float2* __restrict__ tw) {
+template <int N, int NP, typename TW>
+__device__ __forceinline__ void fft16_rows(float4* sm, float sign, const TW& tw) {
     constexpr int TPS = N / 8;
     const int spr = blockDim.x / TPS;
     const int r = threadIdx.x / TPS;
@@ -120,10 +120,9 @@ __device__ __forceinline__ void fft16_rows(float4* sm, float sign, const float2*
 
 // np rows of the padded row buffer, transformed, the last pass storing row p
 // straight to out + p stride (no shared-memory round trip for the result)
-template <typename T, int N>
-__device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int np, T sign,
-                                                 const C2<T>* __restrict__ tw, typename Elem16<T>::E* __restrict__ out,
-                                                 long stride) {
+template <typename T, int N, typename TW>
+__device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int np, T sign, const TW& tw,
+                                                 typename Elem16<T>::E* __restrict__ out, long stride) {
     constexpr int TPS = N / 8;
     const int spr = blockDim.x / TPS;
     const int r = threadIdx.x / TPS, t = threadIdx.x % TPS;
@@ -311,20 +310,23 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 
 // ------------------------------------------------------------------ pass 2, persistent with TMA
 // The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
-// rows, no padding needed), as a persistent kernel: each CTA walks the work
-// items (event, plane pair j, column tile) with stride gridDim.x, and the
-// tensor memory accelerator loads the next item's two planes while this one
-// is transformed.  Three tile buffers rotate: item k reads X (plane j) from
-// b0 and Y (plane 4 + j) from b1 and uses b1 for the inverse transform; the
-// next item's X goes to b2 when item k starts and its Y to b0 once X has been
-// transformed; the next item then finds (X, Y, free) in (b2, b0, b1).  Loads
-// are 2D tensor tiles {8 float4 elements, up to 256 rows} of P viewed as
-// [8 nb N rows][4 N floats], completion counted in bytes on one mbarrier per
-// buffer.  The arithmetic is k_mix_pass2's, element for element, so Q is
-// bit-identical.  Built for N <= 512 (three 64 KB tiles at 512^2).
+// rows, no padding needed), as a persistent kernel: each CTA takes a
+// contiguous run of the work items (column tile, event, plane pair j), in
+// that order, and the tensor memory accelerator loads the next item's two
+// planes while this one is transformed.  Three tile buffers rotate: item k
+// reads X (plane j) from b0 and Y (plane 4 + j) from b1 and uses b1 for the
+// inverse transform; the next item's X goes to b2 when item k starts and its Y
+// to b0 once X has been transformed; the next item then finds (X, Y, free) in
+// (b2, b0, b1).  Loads are 2D tensor tiles {8 float4 elements, up to 256 rows}
+// of P viewed as [8 nb N rows][4 N floats], completion counted in bytes on
+// one mbarrier per buffer.  The twiddles sit in shared memory and the
+// kernel-table values of the thread's elements stay in registers while the
+// column tile does not change, so the transforms issue no global loads.  The
+// arithmetic is k_mix_pass2's, element for element, so Q is bit-identical.
+// Built for N <= 512 (three 64 KB tiles at 512^2).
 template <int N> constexpr int mx_t2_threads() { return 8 * (N / 8); }
 template <int N> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * 8 * N; }
-template <int N> constexpr size_t mx_t2_smem() { return 3 * mx_t2_tile_bytes<N>() + 1024; }
+template <int N> constexpr size_t mx_t2_smem() { return 3 * mx_t2_tile_bytes<N>() + 1024 + 8 * (size_t)N; }
 template <int N> constexpr int mx_t2_blocks() {
     return (int)((227 * 1024) / (mx_t2_smem<N>() + 1024)) < 1024 / mx_t2_threads<N>()
                ? (int)((227 * 1024) / (mx_t2_smem<N>() + 1024))
@@ -346,86 +348,96 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar[3];
     float4* base = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    float2* tws = reinterpret_cast<float2*>(base + (size_t)3 * N * C);
+    const TwShared<float2> twsrc{tws};
     const int tid = threadIdx.x;
     const int cc = tid % C, r0 = tid / C;
     const ColIdx16P<C> cidx{cc};
     const long vol = (long)N * N;
     const int items = nb * 4 * TILES;
+    // this CTA's run of items [begin, end): item -> (tile, b, j), tile-major
+    const int per = items / (int)gridDim.x, extra = items % (int)gridDim.x;
+    const int begin = (int)blockIdx.x * per + min((int)blockIdx.x, extra);
+    const int end = begin + per + ((int)blockIdx.x < extra ? 1 : 0);
     if (tid == 0) {
         tma_prefetch_map(&pmap);
         for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
         mbar_init_fence();
     }
+    for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
     __syncthreads();
     // plane `half` (0: P[j], 1: P[4 + j]) of work item `it` into buffer bi (thread 0)
     auto issue = [&](int it, int half, int bi) {
-        const int tile = it % TILES, j = (it / TILES) % 4, b = it / (TILES * 4);
+        const int tile = it / (nb * 4), r = it - tile * nb * 4, j = r & 3, b = r >> 2;
         const int y0 = (b * 8 + (half ? 4 + j : j)) * N;
         float4* dst = base + (size_t)bi * N * C;
         mbar_arrive_expect_tx(&bar[bi], TILE_BYTES);
 #pragma unroll
-        for (int r = 0; r < N; r += BOX) tma_load_2d(dst + (size_t)r * C, &pmap, tile * C * 4, y0 + r, &bar[bi]);
+        for (int rr = 0; rr < N; rr += BOX) tma_load_2d(dst + (size_t)rr * C, &pmap, tile * C * 4, y0 + rr, &bar[bi]);
     };
     unsigned parity = 0;     // bit i: the parity buffer i's next completed phase has
     unsigned pending = 0;    // bit i: a load into buffer i is in flight (same value in every thread)
     int b0 = 0, b1 = 1, b2 = 2;
-    int it = blockIdx.x;
-    if (it < items) {
+    if (begin < end) {
         if (tid == 0) {
-            issue(it, 0, b0);
-            issue(it, 1, b1);
+            issue(begin, 0, b0);
+            issue(begin, 1, b1);
         }
         pending = (1u << b0) | (1u << b1);
     }
     bool timed_out = false;
-    for (; it < items; it += gridDim.x) {
-        const int next = it + (int)gridDim.x;
+    int cur_tile = -1;
+    float kx[PER], ky[PER];
+#pragma unroll 1
+    for (int it = begin; it < end; ++it) {
+        const bool more = it + 1 < end;
         // the previous item's inverse transform is done with b2
         if (__syncthreads_or(timed_out)) break;
-        if (next < items) {
+        if (more) {
             if (tid == 0) {
                 fence_proxy_async_smem();
-                issue(next, 0, b2);
+                issue(it + 1, 0, b2);
             }
             pending |= 1u << b2;
         }
-        const int tile = it % TILES, j = (it / TILES) % 4, b = it / (TILES * 4);
+        const int tile = it / (nb * 4), rj = it - tile * nb * 4, j = rj & 3, b = rj >> 2;
         const int c0 = tile * C;
         if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
-        const EventDev& e = ev[slots[b]];
-        const float* kt = e.k32 + c0 + (long)r0 * N + cc;
-        float kx[PER], ky[PER];
+        if (tile != cur_tile) {  // kernel table values of this thread's elements (the same for every event)
+            const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            kx[q] = __ldg(kt + (long)q * RSTEP * N);
-            ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
+            for (int q = 0; q < PER; ++q) {
+                kx[q] = __ldg(kt + (long)q * RSTEP * N);
+                ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
+            }
+            cur_tile = tile;
         }
         float2 ra[2][8], w[2][8];
         timed_out |= !mbar_wait_bounded(&bar[b0], (parity >> b0) & 1u);
         parity ^= 1u << b0;
         pending &= ~(1u << b0);
-        fft16x<float, N, false, true>(base + (size_t)b0 * N * C, cidx, r0, true, -1.0f, tw, ra);
+        fft16x<float, N, false, true>(base + (size_t)b0 * N * C, cidx, r0, true, -1.0f, twsrc, ra);
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
         // every thread is done reading b0: the next item's Y may overwrite it
         if (__syncthreads_or(timed_out)) break;
-        if (next < items) {
+        if (more) {
             if (tid == 0) {
                 fence_proxy_async_smem();
-                issue(next, 1, b0);
+                issue(it + 1, 1, b0);
             }
             pending |= 1u << b0;
         }
         timed_out |= !mbar_wait_bounded(&bar[b1], (parity >> b1) & 1u);
         parity ^= 1u << b1;
         pending &= ~(1u << b1);
-        fft16x<float, N, false, true>(base + (size_t)b1 * N * C, cidx, r0, true, -1.0f, tw, ra);
+        fft16x<float, N, false, true>(base + (size_t)b1 * N * C, cidx, r0, true, -1.0f, twsrc, ra);
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
         // the inverse's first pass synchronises before it writes b1
-        fft16x<float, N, true, true>(base + (size_t)b1 * N * C, cidx, r0, true, 1.0f, tw, w);
+        fft16x<float, N, true, true>(base + (size_t)b1 * N * C, cidx, r0, true, 1.0f, twsrc, w);
         float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
 #pragma unroll
         for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = reg_put(w, q);
@@ -537,7 +549,8 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 // has just consumed, so the row buffer is pass 1's (8 rows).  Pass 2 has
 // advanced the step index, so e.step is the next step's noise index.
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
-template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>(); }
+// 8 pair rows and the twiddle table (N complex FP32)
+template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>() + 8 * (size_t)N; }
 // the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
 template <int N> constexpr size_t mx_p31p_smem() {
     return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
@@ -557,12 +570,15 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     const float4* in = Q + (long)b * 4 * vol + (long)x * N;
+    float2* tws = reinterpret_cast<float2*>(sm + padded_len16(8 * N));
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) cp_async<8>(&tws[i], &tw[i]);
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
-    fft16_rows<N, 4>(sm, 1.0f, tw);
+    const TwShared<float2> twsrc{tws};
+    fft16_rows<N, 4>(sm, 1.0f, twsrc);
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
     int fl = 0;
@@ -600,7 +616,7 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     }
     if (fl) atomicOr(flags, fl);
     __syncthreads();
-    fft16_rows_store<float, N>(sm, 8, -1.0f, tw, P + (long)b * 8 * vol + (long)x * N, vol);
+    fft16_rows_store<float, N>(sm, 8, -1.0f, twsrc, P + (long)b * 8 * vol + (long)x * N, vol);
 }
 
 // Pass 3 + next pass 1 as a persistent kernel: each CTA walks the lattice

@@ -54,6 +54,8 @@ struct Backend {
     // measure, then S(r) bins and Q_s
     virtual jw_status finish(int id, std::vector<double>& sb, std::vector<double>& rb, double* qs) = 0;
     virtual jw_status remove(int id) = 0;
+    // the stream the backend's device work runs on (null: no device)
+    virtual cudaStream_t stream() { return nullptr; }
 };
 
 struct EngineBackend : Backend {
@@ -87,6 +89,7 @@ struct EngineBackend : Backend {
         n_of.erase(id);
         return jw_engine_remove_event(e, id);
     }
+    cudaStream_t stream() override { return static_cast<cudaStream_t>(jw_engine_stream(e)); }
 };
 
 // Host-only stand-in: the engine's per-event footprint formula and budget,
@@ -174,8 +177,49 @@ struct jw_server {
     double site_steps = 0;
     int max_active_seen = 0;
     double t_admit = 0, t_mv = 0, t_step = 0, t_retire = 0;  // worker phases (under mu)
+    // per lattice size (under mu): site-steps, device ms of steps and MV, ticks
+    struct SizeStats { double site_steps = 0, step_ms = 0, mv_ms = 0; int64_t ticks = 0; };
+    std::map<int, SizeStats> by_size;
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
+
+namespace {
+
+// CUDA events bracketing one size's launches within a tick (engine backend).
+struct SizeTimer {
+    int N = 0;
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+void timer_begin(cudaStream_t st, std::vector<SizeTimer>& v, int N) {
+    if (!st) return;
+    SizeTimer t;
+    t.N = N;
+    if (cudaEventCreate(&t.a) != cudaSuccess) return;
+    if (cudaEventCreate(&t.b) != cudaSuccess) {
+        cudaEventDestroy(t.a);
+        return;
+    }
+    cudaEventRecord(t.a, st);
+    v.push_back(t);
+}
+
+void timer_end(cudaStream_t st, std::vector<SizeTimer>& v) {
+    if (st && !v.empty()) cudaEventRecord(v.back().b, st);
+}
+
+// After the stream has synchronised: the milliseconds of each bracket.
+void timers_collect(std::vector<SizeTimer>& v, std::map<int, double>& ms) {
+    for (SizeTimer& t : v) {
+        float x = 0.0f;
+        if (cudaEventElapsedTime(&x, t.a, t.b) == cudaSuccess) ms[t.N] += x;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    v.clear();
+}
+
+}  // namespace
 
 namespace {
 
@@ -272,11 +316,24 @@ void worker_loop(jw_server* s) {
                 }
             if (!eids.empty()) {
                 const double tm = s->now();
-                const jw_status st = s->be->init_mv(eids);
+                // one call per lattice size, each timed on the device
+                std::map<int, std::vector<int>> mv_by_n;
+                for (Request* r : fresh) mv_by_n[r->d.N].push_back(r->eid);
+                std::vector<SizeTimer> timers;
+                jw_status st = JW_OK;
+                for (auto& kv : mv_by_n) {
+                    timer_begin(s->be->stream(), timers, kv.first);
+                    const jw_status sn = s->be->init_mv(kv.second);
+                    timer_end(s->be->stream(), timers);
+                    if (sn && !st) st = sn;
+                }
                 const jw_status sy = s->be->sync();
+                std::map<int, double> ms;
+                timers_collect(timers, ms);
                 {
                     std::lock_guard<std::mutex> lk(s->mu);
                     s->t_mv += s->now() - tm;
+                    for (auto& kv : ms) s->by_size[kv.first].mv_ms += kv.second;
                 }
                 for (Request* r : fresh) r->mv = (st == JW_OK && sy == JW_OK);
                 if (st || sy) {
@@ -300,24 +357,38 @@ void worker_loop(jw_server* s) {
         for (Request* r : sel) by_n[r->d.N].push_back(r);
         double ss = 0;
         jw_status tick_status = JW_OK;
+        std::vector<SizeTimer> timers;
+        std::map<int, double> ss_by_n;
         for (auto& kv : by_n) {
             long k = K;
             for (Request* r : kv.second) k = std::min(k, r->remaining);
             if (k <= 0) continue;
             std::vector<int> eids;
             for (Request* r : kv.second) eids.push_back(r->eid);
+            timer_begin(s->be->stream(), timers, kv.first);
             const jw_status st = s->be->step(eids, (int)k);
+            timer_end(s->be->stream(), timers);
             if (st && !tick_status) tick_status = st;
             for (Request* r : kv.second) r->remaining -= k;
-            ss += (double)kv.first * kv.first * (double)k * kv.second.size();
+            const double n_ss = (double)kv.first * kv.first * (double)k * kv.second.size();
+            ss += n_ss;
+            ss_by_n[kv.first] += n_ss;
         }
         const jw_status sst = s->be->sync();
         if (!tick_status) tick_status = sst;
         const double tr = s->now();
+        std::map<int, double> ms;
+        timers_collect(timers, ms);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->site_steps += ss;
             s->t_step += tr - tt;
+            for (auto& kv : ss_by_n) {
+                jw_server::SizeStats& z = s->by_size[kv.first];
+                z.site_steps += kv.second;
+                z.ticks += 1;
+            }
+            for (auto& kv : ms) s->by_size[kv.first].step_ms += kv.second;
         }
         // retire finished events (all of this tick's events if the tick failed)
         std::vector<Request*> keep;
@@ -443,6 +514,25 @@ JW_EXPORT jw_status jw_server_wait(jw_server* s, int64_t rid, double timeout_s, 
         if (r_bins) std::memcpy(r_bins, r.rb.data(), sizeof(double) * r.rb.size());
     }
     s->reqs.erase(rid);
+    return JW_OK;
+}
+
+JW_EXPORT jw_status jw_server_size_stats(jw_server* s, int* N, double* site_steps, double* step_ms, double* mv_ms,
+                                         int64_t* ticks, int cap, int* count) {
+    if (!s || !count || cap < 0) return JW_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    int i = 0;
+    for (auto& kv : s->by_size) {
+        if (i < cap) {
+            if (N) N[i] = kv.first;
+            if (site_steps) site_steps[i] = kv.second.site_steps;
+            if (step_ms) step_ms[i] = kv.second.step_ms;
+            if (mv_ms) mv_ms[i] = kv.second.mv_ms;
+            if (ticks) ticks[i] = kv.second.ticks;
+        }
+        ++i;
+    }
+    *count = i;
     return JW_OK;
 }
 

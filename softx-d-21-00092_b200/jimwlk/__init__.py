@@ -78,6 +78,7 @@ class jw_server_stats(ctypes.Structure):
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
 _vp = ctypes.c_void_p
 
 
@@ -155,6 +156,8 @@ def _load():
         "jw_server_wait": ([_vp, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(jw_request_result), _dp, _dp,
                             ctypes.c_int], ctypes.c_int),
         "jw_server_get_stats": ([_vp, ctypes.POINTER(jw_server_stats)], ctypes.c_int),
+        "jw_server_size_stats": ([_vp, _ip, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int, _ip],
+                                 ctypes.c_int),
         "jw_engine_dipole": ([_vp, ctypes.c_int, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                               ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
         "jw_engine_measure_ensemble": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp], ctypes.c_int),
@@ -655,3 +658,15 @@ class Server:
         st = jw_server_stats()
         _ck(_lib.jw_server_get_stats(self._h, ctypes.byref(st)), "jw_server_get_stats")
         return st
+
+    def size_stats(self) -> dict:
+        """{N: dict(site_steps, step_ms, mv_ms, ticks)} per lattice size served so far."""
+        cnt = ctypes.c_int(0)
+        _ck(_lib.jw_server_size_stats(self._h, None, None, None, None, None, 0, ctypes.byref(cnt)),
+            "jw_server_size_stats")
+        n = cnt.value
+        Ns = (ctypes.c_int * max(n, 1))()
+        ss, sm, mm = ((ctypes.c_double * max(n, 1))() for _ in range(3))
+        tk = (ctypes.c_int64 * max(n, 1))()
+        _ck(_lib.jw_server_size_stats(self._h, Ns, ss, sm, mm, tk, n, ctypes.byref(cnt)), "jw_server_size_stats")
+        return {Ns[i]: dict(site_steps=ss[i], step_ms=sm[i], mv_ms=mm[i], ticks=tk[i]) for i in range(min(n, cnt.value))}
