@@ -454,11 +454,12 @@ void for_each_p2_cols(F&& f) {
         if (encode_tiled()) f(std::integral_constant<int, kP2Tma>{});
 }
 
-// The pair planes P of a launch group ([8 nb N rows][4 N floats]) as a 2D
-// tensor with boxes of 8 float4 elements (128 bytes) by min(N, 256) rows.
+// Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
+// planes per event, Q 4) as a 2D tensor with boxes of 8 float4 elements (128
+// bytes) by min(N, 256) rows.
 template <int N>
-bool p2_tensor_map(CUtensorMap* map, float4* P, int nb) {
-    const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)8 * nb * N};
+bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
+    const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)planes * nb * N};
     const cuuint64_t strides[1] = {(cuuint64_t)4 * N * sizeof(float)};
     const cuuint32_t box[2] = {32, (cuuint32_t)(N < 256 ? N : 256)};
     const cuuint32_t estr[2] = {1, 1};
@@ -509,11 +510,11 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
         constexpr int C = decltype(c)::value;
         if (C != cols) return;
         if constexpr (C == kP2Tma) {
-            CUtensorMap map;
-            if (!p2_tensor_map<N>(&map, P, nb)) return;
+            CUtensorMap pmap, qmap;
+            if (!p2_tensor_map<N>(&pmap, P, nb) || !p2_tensor_map<N>(&qmap, Q, nb, 4)) return;
             const int grid = std::min(p2_tma_grid<N>(), nb * 4 * (N / 8));
             k_mix_pass2_tma<N><<<grid, mx_t2_threads<N>(), mx_t2_smem<N>(), e->stream>>>(
-                g.d_ev, d_slots, Q, g.tw.d32, nb, advance, e->d_flags, map);
+                g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
         } else {
             k_mix_pass2<N, C><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
                 g.d_ev, d_slots, P, Q, g.tw.d32, advance);

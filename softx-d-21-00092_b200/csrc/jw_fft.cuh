@@ -206,6 +206,108 @@ __device__ __forceinline__ V tw_load(const TW& tw, int m, T sign) {
     return w;
 }
 
+__device__ __forceinline__ float2 tw_mul(float2 a, float2 b) {
+    return make_float2(__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)), __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ double2 tw_mul(double2 a, double2 b) {
+    return make_double2(__fma_rn(a.x, b.x, -__dmul_rn(a.y, b.y)), __fma_rn(a.x, b.y, __dmul_rn(a.y, b.x)));
+}
+
+// Per-pass twiddle table in shared memory (TwPass): for every pass with
+// sub-transform size Ns > 1, entry k < Ns holds w^0 .. w^7 of that pass's
+// butterfly (w = exp(+2 pi i k TWS / N)), 8 complex values, so a butterfly
+// reads its twiddles with four 128-bit loads of one 64-byte entry and forms
+// none of them by multiplication.  w, w^2 and w^4 come from the length-N table
+// and w^3, w^5, w^6, w^7 are formed by the same products tw_fill forms at run
+// time (conjugation commutes with them exactly), so every twiddle source gives
+// bit-identical transforms.  Entries of the pass with size Ns start at
+// tw_pass_offset<N, Ns>().
+template <typename V> struct TwPass {
+    const V* p;
+};
+template <int N, int Ns>
+__host__ __device__ constexpr int tw_pass_offset() {
+    // sum of the sizes Ns' of the earlier twiddled passes (1 < Ns' < Ns): 8, 64, 512, ...
+    int off = 0;
+    for (int n = 8; n < Ns && n < N; n *= 8) off += n;
+    return off;
+}
+template <int N>
+__host__ __device__ constexpr int tw_pass_entries() {
+    int off = 0;
+    for (int n = 8; n < N; n *= 8) off += n;
+    return off;
+}
+// Fill a TwPass table (tw_pass_entries<N>() * 8 values) from the length-N
+// table tw[m] = exp(+2 pi i m / N); all threads of the CTA call it.
+template <typename V, int N>
+__device__ __forceinline__ void tw_pass_fill(V* dst, const V* __restrict__ tw) {
+    constexpr int E = tw_pass_entries<N>();
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        int Ns = 8, base = 0;
+        while (e >= base + Ns) {
+            base += Ns;
+            Ns *= 8;
+        }
+        const int rem = N / Ns;
+        const int R = rem >= 8 ? 8 : rem;
+        const int k = e - base;
+        const int TWS = N / (Ns * R);
+        V w[8];
+        for (int r = 0; r < 8; ++r) w[r] = V{};
+        w[0].x = 1.0f;
+        w[1] = __ldg(&tw[k * TWS]);
+        if (R >= 4) w[2] = __ldg(&tw[2 * k * TWS]);
+        if (R == 4) w[3] = tw_mul(w[1], w[2]);
+        if (R == 8) {
+            w[4] = __ldg(&tw[4 * k * TWS]);
+            w[3] = tw_mul(w[1], w[2]);
+            w[5] = tw_mul(w[4], w[1]);
+            w[6] = tw_mul(w[4], w[2]);
+            w[7] = tw_mul(w[4], w[3]);
+        }
+        for (int r = 0; r < 8; ++r) dst[e * 8 + r] = w[r];
+    }
+}
+
+// The twiddles w^1 .. w^(R-1) of butterfly k of pass (Ns, R), conjugated for
+// sign = -1.  Products of twiddles use explicit fused multiply-adds, so that
+// the per-pass tables (formed from unconjugated values) and this run-time
+// derivation (from conjugated ones) agree bit for bit.
+template <typename V, typename T, int N, int Ns, int R, typename TW>
+__device__ __forceinline__ void tw_fill(const TW& tw, int k, T sign, V (&w)[8]) {
+    constexpr int TWS = N / (Ns * R);
+    w[1] = tw_load<V>(tw, k * TWS, sign);
+    if constexpr (R >= 4) w[2] = tw_load<V>(tw, 2 * k * TWS, sign);
+    if constexpr (R == 4) w[3] = tw_mul(w[1], w[2]);
+    if constexpr (R == 8) {
+        w[4] = tw_load<V>(tw, 4 * k * TWS, sign);
+        w[3] = tw_mul(w[1], w[2]);
+        w[5] = tw_mul(w[4], w[1]);
+        w[6] = tw_mul(w[4], w[2]);
+        w[7] = tw_mul(w[4], w[3]);
+    }
+}
+template <typename V, typename T, int N, int Ns, int R>
+__device__ __forceinline__ void tw_fill(const TwPass<V>& tw, int k, T sign, V (&w)[8]) {
+    static_assert(sizeof(V) == 8, "per-pass tables hold complex FP32");
+    const float4* e = reinterpret_cast<const float4*>(tw.p + (tw_pass_offset<N, Ns>() + k) * 8);
+    const float4 a = e[0];
+    w[1] = make_float2(a.z, a.w * sign);
+    if constexpr (R >= 4) {
+        const float4 b = e[1];
+        w[2] = make_float2(b.x, b.y * sign);
+        w[3] = make_float2(b.z, b.w * sign);
+    }
+    if constexpr (R == 8) {
+        const float4 c = e[2], d = e[3];
+        w[4] = make_float2(c.x, c.y * sign);
+        w[5] = make_float2(c.z, c.w * sign);
+        w[6] = make_float2(d.x, d.y * sign);
+        w[7] = make_float2(d.z, d.w * sign);
+    }
+}
+
 template <typename T, int N, int Ns, int R, typename IdxF, typename TW>
 __device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
                                                 bool active, T sign, const TW& tw) {
@@ -215,7 +317,6 @@ __device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restric
     constexpr int B = 8 / R;
     constexpr int NB = N / R;
     constexpr int TPS = N / 8;
-    constexpr int TWS = N / (Ns * R);
     V v[VL][8];
     if (active) {
 #pragma unroll
@@ -231,16 +332,7 @@ __device__ __forceinline__ void stockham_pass16(typename Elem16<T>::E* __restric
             }
             if (Ns > 1) {
                 V w[8];
-                w[1] = tw_load<V>(tw, k * TWS, sign);
-                if constexpr (R >= 4) w[2] = tw_load<V>(tw, 2 * k * TWS, sign);
-                if constexpr (R == 4) w[3] = cmul(w[1], w[2]);
-                if constexpr (R == 8) {
-                    w[4] = tw_load<V>(tw, 4 * k * TWS, sign);
-                    w[3] = cmul(w[1], w[2]);
-                    w[5] = cmul(w[4], w[1]);
-                    w[6] = cmul(w[4], w[2]);
-                    w[7] = cmul(w[4], w[3]);
-                }
+                tw_fill<V, T, N, Ns, R>(tw, k, sign, w);
 #pragma unroll
                 for (int r = 1; r < R; ++r)
 #pragma unroll
@@ -302,7 +394,6 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
     constexpr int B = 8 / R;
     constexpr int NB = N / R;
     constexpr int TPS = N / 8;
-    constexpr int TWS = N / (Ns * R);
     static_assert(!IN || Ns == 1, "register input feeds the first pass");
     static_assert(!OUT || Ns * R == N, "register output comes from the last pass");
     V v[VL][8];
@@ -325,16 +416,7 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
             }
             if (Ns > 1) {
                 V w[8];
-                w[1] = tw_load<V>(tw, k * TWS, sign);
-                if constexpr (R >= 4) w[2] = tw_load<V>(tw, 2 * k * TWS, sign);
-                if constexpr (R == 4) w[3] = cmul(w[1], w[2]);
-                if constexpr (R == 8) {
-                    w[4] = tw_load<V>(tw, 4 * k * TWS, sign);
-                    w[3] = cmul(w[1], w[2]);
-                    w[5] = cmul(w[4], w[1]);
-                    w[6] = cmul(w[4], w[2]);
-                    w[7] = cmul(w[4], w[3]);
-                }
+                tw_fill<V, T, N, Ns, R>(tw, k, sign, w);
 #pragma unroll
                 for (int r = 1; r < R; ++r)
 #pragma unroll

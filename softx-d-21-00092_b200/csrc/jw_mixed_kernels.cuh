@@ -312,21 +312,26 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
 // rows, no padding needed), as a persistent kernel: each CTA takes a
 // contiguous run of the work items (column tile, event, plane pair j), in
-// that order, and the tensor memory accelerator loads the next item's two
-// planes while this one is transformed.  Three tile buffers rotate: item k
-// reads X (plane j) from b0 and Y (plane 4 + j) from b1 and uses b1 for the
-// inverse transform; the next item's X goes to b2 when item k starts and its Y
-// to b0 once X has been transformed; the next item then finds (X, Y, free) in
-// (b2, b0, b1).  Loads are 2D tensor tiles {8 float4 elements, up to 256 rows}
-// of P viewed as [8 nb N rows][4 N floats], completion counted in bytes on
-// one mbarrier per buffer.  The twiddles sit in shared memory and the
-// kernel-table values of the thread's elements stay in registers while the
-// column tile does not change, so the transforms issue no global loads.  The
-// arithmetic is k_mix_pass2's, element for element, so Q is bit-identical.
-// Built for N <= 512 (three 64 KB tiles at 512^2).
+// that order.  The tensor memory accelerator moves every tile: loads of P
+// (2D boxes {8 float4 elements, up to 256 rows} of P viewed as
+// [8 nb N rows][4 N floats]) complete in bytes on one mbarrier per buffer,
+// and the result tile of Q leaves shared memory by a bulk tensor store, so
+// the threads issue no global loads or stores on the way.  Three tile
+// buffers rotate.  Item k finds X (plane j) in xb, Y (plane 4 + j) in yb,
+// and the third buffer fb still being read by item k - 1's store.  It
+// transforms X into registers, then (once that store has read fb) starts the
+// loads of item k + 1's X into fb and Y into xb, transforms Y, runs the
+// inverse transform in yb, writes the result tile into yb and stores it.  Item
+// k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
+// memory (per-pass table) and the kernel-table values of the thread's elements
+// stay in registers while the column tile does not change.  The arithmetic is
+// k_mix_pass2's, element for element, so Q is bit-identical.  Built for
+// N <= 512 (three 64 KB tiles at 512^2).
 template <int N> constexpr int mx_t2_threads() { return 8 * (N / 8); }
 template <int N> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * 8 * N; }
-template <int N> constexpr size_t mx_t2_smem() { return 3 * mx_t2_tile_bytes<N>() + 1024 + 8 * (size_t)N; }
+template <int N> constexpr size_t mx_t2_smem() {
+    return 3 * mx_t2_tile_bytes<N>() + 1024 + 64 * (size_t)tw_pass_entries<N>();
+}
 template <int N> constexpr int mx_t2_blocks() {
     return (int)((227 * 1024) / (mx_t2_smem<N>() + 1024)) < 1024 / mx_t2_threads<N>()
                ? (int)((227 * 1024) / (mx_t2_smem<N>() + 1024))
@@ -336,8 +341,8 @@ template <int N> constexpr bool mx_t2_valid() { return N >= 64 && N <= 512 && mx
 
 template <int N>
 __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_pass2_tma(
-    EventDev* __restrict__ ev, const int* __restrict__ slots, float4* __restrict__ Q, const float2* __restrict__ tw,
-    int nb, int advance, int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap) {
+    EventDev* __restrict__ ev, const int* __restrict__ slots, const float2* __restrict__ tw, int nb, int advance,
+    int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap qmap) {
     static_assert(mx_t2_valid<N>(), "three 8-column tiles per CTA");
     constexpr int C = 8;
     constexpr int PER = 8;
@@ -349,7 +354,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     __shared__ __align__(8) uint64_t bar[3];
     float4* base = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     float2* tws = reinterpret_cast<float2*>(base + (size_t)3 * N * C);
-    const TwShared<float2> twsrc{tws};
+    const TwPass<float2> twsrc{tws};
     const int tid = threadIdx.x;
     const int cc = tid % C, r0 = tid / C;
     const ColIdx16P<C> cidx{cc};
@@ -361,29 +366,30 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     const int end = begin + per + ((int)blockIdx.x < extra ? 1 : 0);
     if (tid == 0) {
         tma_prefetch_map(&pmap);
+        tma_prefetch_map(&qmap);
         for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
         mbar_init_fence();
     }
-    for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+    tw_pass_fill<float2, N>(tws, tw);
     __syncthreads();
+    auto buf = [&](int bi) { return base + (size_t)bi * N * C; };
     // plane `half` (0: P[j], 1: P[4 + j]) of work item `it` into buffer bi (thread 0)
     auto issue = [&](int it, int half, int bi) {
         const int tile = it / (nb * 4), r = it - tile * nb * 4, j = r & 3, b = r >> 2;
         const int y0 = (b * 8 + (half ? 4 + j : j)) * N;
-        float4* dst = base + (size_t)bi * N * C;
         mbar_arrive_expect_tx(&bar[bi], TILE_BYTES);
 #pragma unroll
-        for (int rr = 0; rr < N; rr += BOX) tma_load_2d(dst + (size_t)rr * C, &pmap, tile * C * 4, y0 + rr, &bar[bi]);
+        for (int rr = 0; rr < N; rr += BOX) tma_load_2d(buf(bi) + (size_t)rr * C, &pmap, tile * C * 4, y0 + rr, &bar[bi]);
     };
     unsigned parity = 0;     // bit i: the parity buffer i's next completed phase has
     unsigned pending = 0;    // bit i: a load into buffer i is in flight (same value in every thread)
-    int b0 = 0, b1 = 1, b2 = 2;
+    int xb = 0, yb = 1, fb = 2;
     if (begin < end) {
         if (tid == 0) {
-            issue(begin, 0, b0);
-            issue(begin, 1, b1);
+            issue(begin, 0, xb);
+            issue(begin, 1, yb);
         }
-        pending = (1u << b0) | (1u << b1);
+        pending = (1u << xb) | (1u << yb);
     }
     bool timed_out = false;
     int cur_tile = -1;
@@ -391,15 +397,6 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
 #pragma unroll 1
     for (int it = begin; it < end; ++it) {
         const bool more = it + 1 < end;
-        // the previous item's inverse transform is done with b2
-        if (__syncthreads_or(timed_out)) break;
-        if (more) {
-            if (tid == 0) {
-                fence_proxy_async_smem();
-                issue(it + 1, 0, b2);
-            }
-            pending |= 1u << b2;
-        }
         const int tile = it / (nb * 4), rj = it - tile * nb * 4, j = rj & 3, b = rj >> 2;
         const int c0 = tile * C;
         if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
@@ -413,39 +410,53 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
             cur_tile = tile;
         }
         float2 ra[2][8], w[2][8];
-        timed_out |= !mbar_wait_bounded(&bar[b0], (parity >> b0) & 1u);
-        parity ^= 1u << b0;
-        pending &= ~(1u << b0);
-        fft16x<float, N, false, true>(base + (size_t)b0 * N * C, cidx, r0, true, -1.0f, twsrc, ra);
+        timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
+        parity ^= 1u << xb;
+        pending &= ~(1u << xb);
+        fft16x<float, N, false, true>(buf(xb), cidx, r0, true, -1.0f, twsrc, ra);
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
-        // every thread is done reading b0: the next item's Y may overwrite it
+        // every thread is done reading xb; once the previous item's store has
+        // read fb, the next item's X goes to fb and its Y to xb
         if (__syncthreads_or(timed_out)) break;
         if (more) {
             if (tid == 0) {
+                tma_store_wait_read<0>();
                 fence_proxy_async_smem();
-                issue(it + 1, 1, b0);
+                issue(it + 1, 0, fb);
+                issue(it + 1, 1, xb);
             }
-            pending |= 1u << b0;
+            pending |= (1u << fb) | (1u << xb);
         }
-        timed_out |= !mbar_wait_bounded(&bar[b1], (parity >> b1) & 1u);
-        parity ^= 1u << b1;
-        pending &= ~(1u << b1);
-        fft16x<float, N, false, true>(base + (size_t)b1 * N * C, cidx, r0, true, -1.0f, twsrc, ra);
+        timed_out |= !mbar_wait_bounded(&bar[yb], (parity >> yb) & 1u);
+        parity ^= 1u << yb;
+        pending &= ~(1u << yb);
+        fft16x<float, N, false, true>(buf(yb), cidx, r0, true, -1.0f, twsrc, ra);
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
-        // the inverse's first pass synchronises before it writes b1
-        fft16x<float, N, true, true>(base + (size_t)b1 * N * C, cidx, r0, true, 1.0f, twsrc, w);
-        float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
+        // the inverse's first pass synchronises before it writes yb
+        fft16x<float, N, true, true>(buf(yb), cidx, r0, true, 1.0f, twsrc, w);
+        // the result tile into yb (dense [N][8] elements, the store box's layout)
+        __syncthreads();
+        float4* ot = buf(yb);
 #pragma unroll
-        for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = reg_put(w, q);
-        const int nb0 = b2, nb1 = b0, nb2 = b1;
-        b0 = nb0;
-        b1 = nb1;
-        b2 = nb2;
+        for (int q = 0; q < PER; ++q) ot[(r0 + q * RSTEP) * C + cc] = reg_put(w, q);
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const int y0 = (b * 4 + j) * N;
+#pragma unroll
+            for (int rr = 0; rr < N; rr += BOX) tma_store_2d(&qmap, c0 * 4, y0 + rr, ot + (size_t)rr * C);
+            tma_store_commit();
+        }
+        const int nx = fb, ny = xb, nf = yb;
+        xb = nx;
+        yb = ny;
+        fb = nf;
     }
+    if (tid == 0) tma_store_wait<0>();  // the last stores have completed before the CTA exits
     if (timed_out) {
         if (tid == 0) atomicOr(flags, JW_FLAG_TIMEOUT);
         // loads still in flight land in this CTA's shared memory: wait for them
@@ -549,8 +560,8 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 // has just consumed, so the row buffer is pass 1's (8 rows).  Pass 2 has
 // advanced the step index, so e.step is the next step's noise index.
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
-// 8 pair rows and the twiddle table (N complex FP32)
-template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>() + 8 * (size_t)N; }
+// 8 pair rows and the per-pass twiddle table
+template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>() + 64 * (size_t)tw_pass_entries<N>(); }
 // the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
 template <int N> constexpr size_t mx_p31p_smem() {
     return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
@@ -573,11 +584,11 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     float2* tws = reinterpret_cast<float2*>(sm + padded_len16(8 * N));
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) cp_async<8>(&tws[i], &tw[i]);
     cp_async_commit();
+    tw_pass_fill<float2, N>(tws, tw);
     cp_async_wait<0>();
     __syncthreads();
-    const TwShared<float2> twsrc{tws};
+    const TwPass<float2> twsrc{tws};
     fft16_rows<N, 4>(sm, 1.0f, twsrc);
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
