@@ -382,13 +382,6 @@ jw_status jw_engine_tuning(jw_engine* e, int N, int* p2_cols);
  * default), for example a width found once by the autotuner and kept; the
  * autotuner then skips that size.  Every choice gives bit-identical events. */
 jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols);
-/* No counterpart in the reference.  The form of size N's mixed-precision row
- * pass (pass 3 fused with the next step's pass 1): 0 = one CTA per lattice
- * row (the default), 1 = persistent CTAs that copy the next row's inverse-
- * transform input while they work on this one (N <= 512; JW_EINVAL
- * otherwise).  Both give bit-identical events.  jw_engine_row_form reads it. */
-jw_status jw_engine_set_row_form(jw_engine* e, int N, int form);
-jw_status jw_engine_row_form(jw_engine* e, int N, int* form);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
  * event around each kernel launch.  kernel_ms[4] receives the milliseconds
  * spent in each kernel kind and launches[4] its launch count: pass 1, pass 2,

@@ -92,14 +92,20 @@ __device__ __forceinline__ void box_muller(uint32_t r0, uint32_t r1, float& z0, 
 }
 
 // Box-Muller in FP32 with the hardware approximations: ln u0 from __logf
-// (absolute error <= 2^-21.4 near 1, relative ~2^-21 elsewhere) and
-// sin/cos of 2 pi u1 - pi from __sincosf (absolute error <= 2^-21.4 on
-// [-pi, pi]).  Each normal differs from the FP64 stream by at most ~3e-6
+// (absolute error <= 2^-21.4 near 1, relative ~2^-21 elsewhere), the square
+// root from sqrt.approx (relative error ~2^-23) and sin/cos of 2 pi u1 - pi
+// from __sincosf (absolute error <= 2^-21.4 on [-pi, pi]).  Each normal differs from the FP64 stream by at most ~3e-6
 // absolute; used by the mixed-precision engine.
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ void box_muller_fast(uint32_t r0, uint32_t r1, float& z0, float& z1) {
     const float u0 = __uint2float_rn(r0) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
     const float u1 = __uint2float_rn(r1) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
-    const float rad = sqrtf(-2.0f * __logf(u0));
+    const float rad = sqrt_approx(-2.0f * __logf(u0));
     float s, c;
     __sincosf(6.28318530717958648f * u1 - 3.14159265358979324f, &s, &c);
     z0 = -rad * c;  // cos(2 pi u1) = -cos(2 pi u1 - pi)

@@ -36,7 +36,6 @@ struct Group {
     double* nf64 = nullptr;          // noise factor (NOISE coupling)
     float* nf32 = nullptr;
     int p2_cols = 0;                 // mixed pass 2 column-tile width (0: the default)
-    int p31_form = 0;                // mixed pass 3 + 1: 0 one CTA per row, 1 persistent ring
     bool tuned = false;              // the autotuner has run for this size
 };
 
@@ -483,21 +482,6 @@ int p2_tma_grid() {
     return grid;
 }
 
-// CTAs of the persistent pass 3 + next pass 1: every SM filled to its occupancy.
-template <int N>
-int p31_ring_grid() {
-    static int grid = 0;
-    if (grid == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass31_ring<N>, mx_p31_threads<N>(),
-                                                      mx_p31r_smem<N>());
-        grid = std::max(1, sms * std::max(1, per_sm));
-    }
-    return grid;
-}
-
 // Pass 2 with tuning choice `cols` (0: the default); advance = 0 leaves the
 // step index alone (timing launches of the autotuner).
 template <int N>
@@ -533,9 +517,6 @@ void mix_configure() {
     } else {
         cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
         cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
-        if constexpr (mx_p31r_valid<N>())
-            cudaFuncSetAttribute(k_mix_pass31_ring<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)mx_p31r_smem<N>());
     }
     for_each_p2_cols<N>([](auto c) {
         constexpr int C = decltype(c)::value;
@@ -591,9 +572,6 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
             if constexpr (mx_pair<N>())
                 k_mix_pass31_pair<N><<<dim3(N, 2, nb), mx_p31_threads<N>(), mx_p31p_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
-            else if (g.p31_form == 1 && mx_p31r_valid<N>())
-                k_mix_pass31_ring<N><<<std::min(p31_ring_grid<N>(), nb * N), mx_p31_threads<N>(), mx_p31r_smem<N>(),
-                                       e->stream>>>(g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags, nb);
             else
                 k_mix_pass31<N><<<dim3(N, nb), mx_p31_threads<N>(), mx_p31_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
@@ -1602,41 +1580,6 @@ JW_EXPORT jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols) {
     JW_CUDA(cudaStreamSynchronize(e->stream));  // launches already queued keep their width
     it->second->p2_cols = p2_cols;
     it->second->tuned = true;
-    return JW_OK;
-}
-
-namespace {
-bool row_form_valid(int N, int form) {
-    if (form == 0) return true;
-    if (form != 1) return false;
-    switch (N) {
-        case 8: return mx_p31r_valid<8>();
-        case 16: return mx_p31r_valid<16>();
-        case 32: return mx_p31r_valid<32>();
-        case 64: return mx_p31r_valid<64>();
-        case 128: return mx_p31r_valid<128>();
-        case 256: return mx_p31r_valid<256>();
-        case 512: return mx_p31r_valid<512>();
-        default: return false;
-    }
-}
-}  // namespace
-
-JW_EXPORT jw_status jw_engine_set_row_form(jw_engine* e, int N, int form) {
-    JW_CHECK(e);
-    auto it = e->groups.find(N);
-    if (it == e->groups.end()) return JW_ENOTFOUND;
-    if (!row_form_valid(N, form)) return JW_EINVAL;
-    JW_CUDA(cudaStreamSynchronize(e->stream));
-    it->second->p31_form = form;
-    return JW_OK;
-}
-
-JW_EXPORT jw_status jw_engine_row_form(jw_engine* e, int N, int* form) {
-    JW_CHECK(e && form);
-    auto it = e->groups.find(N);
-    if (it == e->groups.end()) return JW_ENOTFOUND;
-    *form = it->second->p31_form;
     return JW_OK;
 }
 

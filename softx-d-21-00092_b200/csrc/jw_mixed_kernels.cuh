@@ -79,16 +79,32 @@ template <int N, bool MEAS = false> constexpr int mx_p3_blocks() {
 template <int N> constexpr bool mx_p3_meas_fits() { return mx_p3_smem<N, true>() <= 220 * 1024; }
 
 // Gell-Mann coefficients of R = V xi V^dagger, xi = sum_a n_a L_a: only the
-// upper triangle and the real diagonal of R are formed (R is Hermitian).
+// upper triangle and the real diagonal of R are formed (R is Hermitian), and
+// t = V xi uses xi's structure (real diagonal d, upper entries c, lower
+// entries conj(c)) instead of a general 3 x 3 product.
 __device__ __forceinline__ void rotate_herm(const float2 v[9], const float n[8], float h[8]) {
-    float2 xi[9], t[9];
-    embed_lambda<float>(n, xi);
-    mul3(v, xi, t);  // t = V xi
+    const float s = 0.57735026918962573f * n[7];  // n_7 / sqrt(3)
+    const float d0 = n[2] + s, d1 = -n[2] + s, d2 = -2.0f * s;
+    const float2 c01 = make_float2(n[0], n[1]), c02 = make_float2(n[3], n[4]), c12 = make_float2(n[5], n[6]);
+    float2 t[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float2 a = v[i * 3 + 0], b = v[i * 3 + 1], c = v[i * 3 + 2];
+        // t_i0 = a d0 + b conj(c01) + c conj(c02)
+        t[i * 3 + 0] = make_float2(a.x * d0 + (b.x * c01.x + b.y * c01.y) + (c.x * c02.x + c.y * c02.y),
+                                   a.y * d0 + (b.y * c01.x - b.x * c01.y) + (c.y * c02.x - c.x * c02.y));
+        // t_i1 = a c01 + b d1 + c conj(c12)
+        t[i * 3 + 1] = make_float2((a.x * c01.x - a.y * c01.y) + b.x * d1 + (c.x * c12.x + c.y * c12.y),
+                                   (a.x * c01.y + a.y * c01.x) + b.y * d1 + (c.y * c12.x - c.x * c12.y));
+        // t_i2 = a c02 + b c12 + c d2
+        t[i * 3 + 2] = make_float2((a.x * c02.x - a.y * c02.y) + (b.x * c12.x - b.y * c12.y) + c.x * d2,
+                                   (a.x * c02.y + a.y * c02.x) + (b.x * c12.y + b.y * c12.x) + c.y * d2);
+    }
     // R_ij = sum_k t_ik conj(V_jk)
     auto rij = [&](int i, int j) {
-        float2 s = cmulc(t[i * 3 + 0], v[j * 3 + 0]);
-        s = cadd(s, cmulc(t[i * 3 + 1], v[j * 3 + 1]));
-        return cadd(s, cmulc(t[i * 3 + 2], v[j * 3 + 2]));
+        float2 r = cmulc(t[i * 3 + 0], v[j * 3 + 0]);
+        r = cadd(r, cmulc(t[i * 3 + 1], v[j * 3 + 1]));
+        return cadd(r, cmulc(t[i * 3 + 2], v[j * 3 + 2]));
     };
     auto rii = [&](int i) {
         return t[i * 3 + 0].x * v[i * 3 + 0].x + t[i * 3 + 0].y * v[i * 3 + 0].y + t[i * 3 + 1].x * v[i * 3 + 1].x +
@@ -162,9 +178,11 @@ __global__ void __launch_bounds__(mx_p1_threads<N>(), mx_p1_blocks<N>()) k_mix_p
         for (int k = 0; k < 9; ++k) dv[k] = __ldg(&e.V[k * vol + site]);  // in flight during the noise
         float z[16];
         langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-        const float f = nf ? nf[site] : 1.0f;
+        if (nf) {  // NOISE coupling: the site-indexed factor (uniform over the event)
+            const float f = nf[site];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) z[k] *= f;
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
             sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
@@ -220,9 +238,11 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p1_threads<N>(), 
         for (int k = 0; k < 9; ++k) dv[k] = __ldg(&e.V[k * vol + site]);  // in flight during the noise
         float z[16];
         langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-        const float f = nf ? nf[site] : 1.0f;
+        if (nf) {  // NOISE coupling: the site-indexed factor (uniform over the event)
+            const float f = nf[site];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) z[k] *= f;
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
             noise_rows[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
@@ -310,9 +330,9 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 
 // ------------------------------------------------------------------ pass 2, persistent with TMA
 // The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
-// rows, no padding needed), as a persistent kernel: each CTA takes a
-// contiguous run of the work items (column tile, event, plane pair j), in
-// that order.  The tensor memory accelerator moves every tile: loads of P
+// rows, no padding needed), as a persistent kernel: CTA c takes the work
+// items c, c + gridDim.x, ... of the list (event, plane pair j, column tile)
+// with the tile fastest.  The tensor memory accelerator moves every tile: loads of P
 // (2D boxes {8 float4 elements, up to 256 rows} of P viewed as
 // [8 nb N rows][4 N floats]) complete in bytes on one mbarrier per buffer,
 // and the result tile of Q leaves shared memory by a bulk tensor store, so
@@ -323,8 +343,7 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // loads of item k + 1's X into fb and Y into xb, transforms Y, runs the
 // inverse transform in yb, writes the result tile into yb and stores it.  Item
 // k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
-// memory (per-pass table) and the kernel-table values of the thread's elements
-// stay in registers while the column tile does not change.  The arithmetic is
+// memory (per-pass table).  The arithmetic is
 // k_mix_pass2's, element for element, so Q is bit-identical.  Built for
 // N <= 512 (three 64 KB tiles at 512^2).
 template <int N> constexpr int mx_t2_threads() { return 8 * (N / 8); }
@@ -360,10 +379,10 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     const ColIdx16P<C> cidx{cc};
     const long vol = (long)N * N;
     const int items = nb * 4 * TILES;
-    // this CTA's run of items [begin, end): item -> (tile, b, j), tile-major
-    const int per = items / (int)gridDim.x, extra = items % (int)gridDim.x;
-    const int begin = (int)blockIdx.x * per + min((int)blockIdx.x, extra);
-    const int end = begin + per + ((int)blockIdx.x < extra ? 1 : 0);
+    // items it = blockIdx.x + k gridDim.x, the column tile fastest
+    // (it -> tile, j, b), so that the CTAs running at one time read adjacent
+    // tiles of the same planes (whole DRAM pages between them)
+    const int begin = blockIdx.x, stride = gridDim.x, end = items;
     if (tid == 0) {
         tma_prefetch_map(&pmap);
         tma_prefetch_map(&qmap);
@@ -375,7 +394,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     auto buf = [&](int bi) { return base + (size_t)bi * N * C; };
     // plane `half` (0: P[j], 1: P[4 + j]) of work item `it` into buffer bi (thread 0)
     auto issue = [&](int it, int half, int bi) {
-        const int tile = it / (nb * 4), r = it - tile * nb * 4, j = r & 3, b = r >> 2;
+        const int tile = it % TILES, j = (it / TILES) & 3, b = it / (TILES * 4);
         const int y0 = (b * 8 + (half ? 4 + j : j)) * N;
         mbar_arrive_expect_tx(&bar[bi], TILE_BYTES);
 #pragma unroll
@@ -392,22 +411,19 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
         pending = (1u << xb) | (1u << yb);
     }
     bool timed_out = false;
-    int cur_tile = -1;
-    float kx[PER], ky[PER];
 #pragma unroll 1
-    for (int it = begin; it < end; ++it) {
-        const bool more = it + 1 < end;
-        const int tile = it / (nb * 4), rj = it - tile * nb * 4, j = rj & 3, b = rj >> 2;
+    for (int it = begin; it < end; it += stride) {
+        const bool more = it + stride < end;
+        const int tile = it % TILES, j = (it / TILES) & 3, b = it / (TILES * 4);
         const int c0 = tile * C;
         if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
-        if (tile != cur_tile) {  // kernel table values of this thread's elements (the same for every event)
-            const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
+        // kernel table values of this thread's elements (the same for every event, L2-resident)
+        const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
+        float kx[PER], ky[PER];
 #pragma unroll
-            for (int q = 0; q < PER; ++q) {
-                kx[q] = __ldg(kt + (long)q * RSTEP * N);
-                ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
-            }
-            cur_tile = tile;
+        for (int q = 0; q < PER; ++q) {
+            kx[q] = __ldg(kt + (long)q * RSTEP * N);
+            ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
         }
         float2 ra[2][8], w[2][8];
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
@@ -424,8 +440,8 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
             if (tid == 0) {
                 tma_store_wait_read<0>();
                 fence_proxy_async_smem();
-                issue(it + 1, 0, fb);
-                issue(it + 1, 1, xb);
+                issue(it + stride, 0, fb);
+                issue(it + stride, 1, xb);
             }
             pending |= (1u << fb) | (1u << xb);
         }
@@ -560,8 +576,7 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 // has just consumed, so the row buffer is pass 1's (8 rows).  Pass 2 has
 // advanced the step index, so e.step is the next step's noise index.
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
-// 8 pair rows and the per-pass twiddle table
-template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>() + 64 * (size_t)tw_pass_entries<N>(); }
+template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>(); }
 // the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
 template <int N> constexpr size_t mx_p31p_smem() {
     return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
@@ -581,14 +596,12 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
     const float4* in = Q + (long)b * 4 * vol + (long)x * N;
-    float2* tws = reinterpret_cast<float2*>(sm + padded_len16(8 * N));
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    tw_pass_fill<float2, N>(tws, tw);
     cp_async_wait<0>();
     __syncthreads();
-    const TwPass<float2> twsrc{tws};
+    const float2* twsrc = tw;
     fft16_rows<N, 4>(sm, 1.0f, twsrc);
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
@@ -607,9 +620,11 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
         }
         float z[16];
         langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-        const float f = nf ? nf[site] : 1.0f;
+        if (nf) {  // NOISE coupling: the site-indexed factor (uniform over the event)
+            const float f = nf[site];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) z[k] *= f;
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
             sm[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
@@ -628,128 +643,6 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     if (fl) atomicOr(flags, fl);
     __syncthreads();
     fft16_rows_store<float, N>(sm, 8, -1.0f, twsrc, P + (long)b * 8 * vol + (long)x * N, vol);
-}
-
-// Pass 3 + next pass 1 as a persistent kernel: each CTA walks the lattice
-// rows (event, x) with stride gridDim.x and copies the next row's 4 Q rows
-// (cp.async) while it works on this one.  Shared memory is three regions of
-// 4 padded pair rows.  Row k: Q in region k mod 3, transformed in place; the
-// next step's noise pairs overwrite it column by column (the thread that
-// consumed column y writes it), the rotated pairs go to region (k + 2) mod 3,
-// and the next row's Q arrives in region (k + 1) mod 3.  Row k + 1 then finds
-// its Q where it was copied and writes its rotated pairs where row k's Q was.
-// Per site the arithmetic is k_mix_pass31's, so V and P are bit-identical.
-template <int N> constexpr size_t mx_p31r_region() { return 16 * (size_t)padded_len16(4 * N); }
-template <int N> constexpr size_t mx_p31r_smem() { return 3 * mx_p31r_region<N>(); }
-template <int N> constexpr int mx_p31r_blocks() {
-    return mx_p31_threads<N>() <= 256 && mx_p31r_smem<N>() + 1024 <= 113 * 1024 ? 2 : 1;
-}
-template <int N> constexpr bool mx_p31r_valid() { return !mx_pair<N>() && mx_p31r_smem<N>() <= 112 * 1024; }
-
-// Copy the 4 Q rows of lattice row x of launch-group event b into region dst.
-template <int N>
-__device__ __forceinline__ void p31r_fetch(float4* dst, const float4* __restrict__ Q, int b, int x) {
-    const long vol = (long)N * N;
-    const float4* in = Q + (long)b * 4 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
-        cp_async<16>(&dst[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
-    cp_async_commit();
-}
-
-template <int N>
-__global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p31r_blocks<N>()) k_mix_pass31_ring(
-    EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q, float4* __restrict__ P,
-    const float2* __restrict__ tw, int* __restrict__ flags, int nb) {
-    static_assert(mx_p31r_valid<N>(), "three regions of 4 pair rows per CTA");
-    constexpr int RL = padded_len16(4 * N);  // elements per region
-    constexpr int TPS = N / 8;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float4* region = reinterpret_cast<float4*>(smem_raw);
-    const long vol = (long)N * N;
-    const int rows = nb * N;
-    int fl = 0;
-    int k = 0;
-    int item = blockIdx.x;
-    if (item < rows) p31r_fetch<N>(region, Q, item / N, item % N);
-#pragma unroll 1
-    for (; item < rows; item += gridDim.x, ++k) {
-        // fresh copies of the thread index and the twiddle pointer per row, so
-        // that the compiler does not keep the transforms' shared-memory
-        // indices and twiddles in registers across rows
-        const float2* twr = tw;
-        int tid = threadIdx.x;
-        asm volatile("" : "+l"(twr), "+r"(tid));
-        float4* rq = region + (size_t)(k % 3) * RL;        // Q, then the noise pairs
-        float4* rn = region + (size_t)((k + 1) % 3) * RL;  // the next row's Q
-        float4* ro = region + (size_t)((k + 2) % 3) * RL;  // the rotated pairs
-        const int b = item / N, x = item % N;
-        cp_async_wait<0>();
-        __syncthreads();  // this row's Q has landed; the previous row is done with rn and ro
-        const int next = item + (int)gridDim.x;
-        if (next < rows) p31r_fetch<N>(rn, Q, next / N, next % N);
-        {
-            const int r = tid / TPS;  // 4 rows in rounds of blockDim / TPS
-            for (int p0 = 0; p0 < 4; p0 += (int)blockDim.x / TPS)
-                fft16<float, N>(rq, RowIdx16{(p0 + r) * N}, tid % TPS, p0 + r < 4 && r < (int)blockDim.x / TPS,
-                                1.0f, twr);
-        }
-        EventDev& e = ev[slots[b]];
-        const double se = e.sqrt_eps;
-        const float* nf = e.nf32;
-        for (int y = tid; y < N; y += blockDim.x) {
-            const long site = (long)x * N + y;
-            float2 v32[9];
-            {
-                double2 v[9];
-                p3_site<N>(e, rq, y, site, vol, se, v, fl);
-#pragma unroll
-                for (int kk = 0; kk < 9; ++kk) {
-                    e.V[kk * vol + site] = v[kk];
-                    v32[kk] = make_float2((float)v[kk].x, (float)v[kk].y);
-                }
-            }
-            float z[16];
-            langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-            const float f = nf ? nf[site] : 1.0f;
-#pragma unroll
-            for (int kk = 0; kk < 16; ++kk) z[kk] *= f;
-#pragma unroll
-            for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
-                rq[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
-            float n[8], m[8], hx[8], hy[8];
-#pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
-                n[kk] = z[2 * kk];
-                m[kk] = z[2 * kk + 1];
-            }
-            rotate_herm(v32, n, hx);
-            rotate_herm(v32, m, hy);
-#pragma unroll
-            for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
-                ro[pad16(j * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
-        }
-        __syncthreads();
-        // forward row transforms of the 8 pair rows (0..3 in rq, 4..7 in ro),
-        // the last pass storing straight to P
-        {
-            const int spr = blockDim.x / TPS;
-            const int r = tid / TPS, t = tid % TPS;
-            float4* out = P + (long)b * 8 * vol + (long)x * N;
-            for (int p0 = 0; p0 < 8; p0 += spr) {
-                const int p = p0 + r;
-                const bool act = r < spr && p < 8;
-                float2 rv[2][8];
-                fft16x<float, N, false, true>(p < 4 ? rq : ro, RowIdx16{(p & 3) * N}, t, act, -1.0f, twr, rv);
-                if (act) {
-                    float4* o = out + (long)p * vol + t;
-#pragma unroll
-                    for (int m = 0; m < 8; ++m) o[(long)m * TPS] = reg_put(rv, m);
-                }
-            }
-        }
-    }
-    cp_async_wait<0>();
-    if (fl) atomicOr(flags, fl);
 }
 
 // Pass 3 + next pass 1 where a lattice row needs a cluster of two CTAs
@@ -804,9 +697,11 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p31_threads<N>(),
         }
         float z[16];
         langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
-        const float f = nf ? nf[site] : 1.0f;
+        if (nf) {  // NOISE coupling: the site-indexed factor (uniform over the event)
+            const float f = nf[site];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) z[k] *= f;
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
             noise_rows[pad16(j * N + y)] = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);

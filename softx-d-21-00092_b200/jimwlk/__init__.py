@@ -165,8 +165,6 @@ def _load():
                                             ctypes.c_int),
         "jw_engine_tuning": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "jw_engine_set_tuning": ([_vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
-        "jw_engine_set_row_form": ([_vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
-        "jw_engine_row_form": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "jw_engine_step_timed": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, _dp,
                                   ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     }
@@ -567,14 +565,6 @@ class Engine:
     def set_tuning(self, N: int, p2_cols: int) -> None:
         _ck(_lib.jw_engine_set_tuning(self._h, int(N), int(p2_cols)), "jw_engine_set_tuning")
 
-    def set_row_form(self, N: int, form: int) -> None:
-        """Pass 3 + next pass 1 for size N: 0 one CTA per row, 1 persistent with prefetch."""
-        _ck(_lib.jw_engine_set_row_form(self._h, int(N), int(form)), "jw_engine_set_row_form")
-
-    def row_form(self, N: int) -> int:
-        c = ctypes.c_int(0)
-        _ck(_lib.jw_engine_row_form(self._h, int(N), ctypes.byref(c)), "jw_engine_row_form")
-        return c.value
 
     def step_timed(self, ids, nsteps: int):
         """nsteps steps with every kernel timed: ({kind: (total ms, launches)}, total ms)."""

@@ -116,28 +116,23 @@ def test_autotuner_choice_does_not_change_results(jw, N):
 
 
 @pytest.mark.parametrize("N,events", [(64, 3), (256, 2), (512, 3)])
-def test_kernel_forms_are_bitwise_identical(jw, N, events):
-    """The persistent forms (column pass with tensor-memory-accelerator tile
-    loads, row pass with the next row's input prefetched) give the default
-    forms' lattices bit for bit, over runs long enough for graph replay, with
-    more rows than persistent CTAs."""
+def test_persistent_column_pass_is_bitwise_identical(jw, N, events):
+    """The persistent column pass (tuning choice 16: tensor-memory-accelerator
+    tile loads and stores, per-pass twiddle table) gives the default column
+    pass's lattices bit for bit, over runs long enough for graph replay, with
+    more work items than persistent CTAs."""
     eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
     eng.step(ids, 6)
     ref = [eng.get_V(i) for i in ids]
     eng.close()
-    for p2, row in ((16, 0), (0, 1), (16, 1)):
-        eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
-        eng.set_tuning(N, p2)
-        eng.set_row_form(N, row)
-        assert eng.row_form(N) == row
-        eng.step(ids, 6)
-        assert eng.sync() == jw.OK
-        for a, i in zip(ref, ids):
-            assert np.array_equal(a, eng.get_V(i)), (p2, row)
-        eng.close()
+    eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+    eng.set_tuning(N, 16)
+    eng.step(ids, 6)
+    assert eng.sync() == jw.OK
+    for a, i in zip(ref, ids):
+        assert np.array_equal(a, eng.get_V(i))
+    eng.close()
     eng, ids = make(jw, 1024, 1, jw.PRECISION_MIXED)
-    with pytest.raises(RuntimeError):
-        eng.set_row_form(1024, 1)
     with pytest.raises(RuntimeError):
         eng.set_tuning(1024, 16)
     eng.close()
