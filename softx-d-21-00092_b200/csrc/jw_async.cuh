@@ -54,13 +54,18 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 // Wait until the barrier's phase with this parity has completed, for at most
 // ~limit_ns of wall time.  Returns false if the wait ran out.
+// The clock is read only after 1024 unsuccessful tries, so that waits that end
+// soon issue nothing but the tries.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
                                                   uint64_t limit_ns = 2000000000ull) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
+    uint64_t t0 = 0;
     for (unsigned it = 0; it < (1u << 26); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 255u && global_ns() - t0 > limit_ns) return false;
+        if ((it & 1023u) == 1023u) {
+            const uint64_t t = global_ns();
+            if (it == 1023u) t0 = t;
+            else if (t - t0 > limit_ns) return false;
+        }
     }
     return false;
 }

@@ -330,9 +330,9 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 
 // ------------------------------------------------------------------ pass 2, persistent with TMA
 // The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
-// rows, no padding needed), as a persistent kernel: CTA c takes the work
-// items c, c + gridDim.x, ... of the list (event, plane pair j, column tile)
-// with the tile fastest.  The tensor memory accelerator moves every tile: loads of P
+// rows, no padding needed), as a persistent kernel: each CTA takes a
+// contiguous run of the work items (column tile, event, plane pair j), in
+// that order.  The tensor memory accelerator moves every tile: loads of P
 // (2D boxes {8 float4 elements, up to 256 rows} of P viewed as
 // [8 nb N rows][4 N floats]) complete in bytes on one mbarrier per buffer,
 // and the result tile of Q leaves shared memory by a bulk tensor store, so
@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // loads of item k + 1's X into fb and Y into xb, transforms Y, runs the
 // inverse transform in yb, writes the result tile into yb and stores it.  Item
 // k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
-// memory (per-pass table).  The arithmetic is
+// memory (per-pass table) and the kernel-table values of the thread's elements
+// stay in registers while the column tile does not change.  The arithmetic is
 // k_mix_pass2's, element for element, so Q is bit-identical.  Built for
 // N <= 512 (three 64 KB tiles at 512^2).
 template <int N> constexpr int mx_t2_threads() { return 8 * (N / 8); }
@@ -379,10 +380,12 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     const ColIdx16P<C> cidx{cc};
     const long vol = (long)N * N;
     const int items = nb * 4 * TILES;
-    // items it = blockIdx.x + k gridDim.x, the column tile fastest
-    // (it -> tile, j, b), so that the CTAs running at one time read adjacent
-    // tiles of the same planes (whole DRAM pages between them)
-    const int begin = blockIdx.x, stride = gridDim.x, end = items;
+    // this CTA's run of items [begin, end): item -> (tile, b, j), tile-major
+    // (measured faster than a round-robin over tile-fastest items)
+    const int per = items / (int)gridDim.x, extra = items % (int)gridDim.x;
+    const int begin = (int)blockIdx.x * per + min((int)blockIdx.x, extra);
+    const int end = begin + per + ((int)blockIdx.x < extra ? 1 : 0);
+    const int stride = 1;
     if (tid == 0) {
         tma_prefetch_map(&pmap);
         tma_prefetch_map(&qmap);
@@ -394,7 +397,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     auto buf = [&](int bi) { return base + (size_t)bi * N * C; };
     // plane `half` (0: P[j], 1: P[4 + j]) of work item `it` into buffer bi (thread 0)
     auto issue = [&](int it, int half, int bi) {
-        const int tile = it % TILES, j = (it / TILES) & 3, b = it / (TILES * 4);
+        const int tile = it / (nb * 4), r = it - tile * nb * 4, j = r & 3, b = r >> 2;
         const int y0 = (b * 8 + (half ? 4 + j : j)) * N;
         mbar_arrive_expect_tx(&bar[bi], TILE_BYTES);
 #pragma unroll
@@ -411,19 +414,22 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
         pending = (1u << xb) | (1u << yb);
     }
     bool timed_out = false;
+    int cur_tile = -1;
+    float kx[PER], ky[PER];
 #pragma unroll 1
     for (int it = begin; it < end; it += stride) {
         const bool more = it + stride < end;
-        const int tile = it % TILES, j = (it / TILES) & 3, b = it / (TILES * 4);
+        const int tile = it / (nb * 4), rj = it - tile * nb * 4, j = rj & 3, b = rj >> 2;
         const int c0 = tile * C;
         if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
-        // kernel table values of this thread's elements (the same for every event, L2-resident)
-        const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
-        float kx[PER], ky[PER];
+        if (tile != cur_tile) {  // kernel table values of this thread's elements (the same for every event)
+            const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            kx[q] = __ldg(kt + (long)q * RSTEP * N);
-            ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
+            for (int q = 0; q < PER; ++q) {
+                kx[q] = __ldg(kt + (long)q * RSTEP * N);
+                ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
+            }
+            cur_tile = tile;
         }
         float2 ra[2][8], w[2][8];
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
@@ -488,12 +494,13 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
 // loaded first and arrives while exp(+i sqrt(eps) B) is formed; one
 // exponential is held at a time.  Reports non-finite entries in fl.
 // get_u(j) returns the element of inverse-transformed pair row j at the site.
-template <typename GetU>
-__device__ __forceinline__ void p3_site_g(const EventDev& e, GetU get_u, long site, long vol, double se,
-                                          double2 (&v)[9], int& fl) {
+// get_v(k) returns entry k of the site's old V (by default loaded from e.V).
+template <typename GetU, typename GetV>
+__device__ __forceinline__ void p3_site_gv(const EventDev& e, GetU get_u, GetV get_v, double se, double2 (&v)[9],
+                                           int& fl) {
     double2 v0[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) v0[k] = e.V[k * vol + site];
+    for (int k = 0; k < 9; ++k) v0[k] = get_v(k);
     double a[8], bq[8];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -514,6 +521,12 @@ __device__ __forceinline__ void p3_site_g(const EventDev& e, GetU get_u, long si
 #pragma unroll
     for (int k = 0; k < 9; ++k)
         if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+}
+
+template <typename GetU>
+__device__ __forceinline__ void p3_site_g(const EventDev& e, GetU get_u, long site, long vol, double se,
+                                          double2 (&v)[9], int& fl) {
+    p3_site_gv(e, get_u, [&](int k) { return e.V[k * vol + site]; }, se, v, fl);
 }
 
 template <int N>
@@ -576,7 +589,11 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 // has just consumed, so the row buffer is pass 1's (8 rows).  Pass 2 has
 // advanced the step index, so e.step is the next step's noise index.
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
-template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>(); }
+// 8 pair rows, then the old V of one site per thread ([9][threads] double2),
+// copied ahead with cp.async
+template <int N> constexpr size_t mx_p31_smem() {
+    return mx_p1_smem<N>() + (size_t)9 * 16 * mx_p31_threads<N>();
+}
 // the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
 template <int N> constexpr size_t mx_p31p_smem() {
     return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
@@ -595,23 +612,43 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     const int x = blockIdx.x, b = blockIdx.y;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
+    constexpr int TH = mx_p31_threads<N>();
+    const int tid = threadIdx.x;
     const float4* in = Q + (long)b * 4 * vol + (long)x * N;
-    for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
-        cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
+    // the old V of this thread's site tid + k TH sits in slot vs[k'][tid], k' < 9,
+    // copied ahead: the first site while the inverse transforms run, the next
+    // one while this one is updated
+    double2* vs = reinterpret_cast<double2*>(sm + padded_len16(8 * N));
+    const double2* vrow = e.V + (long)x * N;
+    for (int i = tid; i < 4 * N; i += TH) cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    cp_async_wait<0>();
+    if (tid < N) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) cp_async<16>(&vs[k * TH + tid], &vrow[k * vol + tid]);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();  // Q has landed (V may still be in flight)
     __syncthreads();
     const float2* twsrc = tw;
     fft16_rows<N, 4>(sm, 1.0f, twsrc);
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
     int fl = 0;
-    for (int y = threadIdx.x; y < N; y += blockDim.x) {
+    for (int y = tid; y < N; y += TH) {
         const long site = (long)x * N + y;
         float2 v32[9];
         {
+            cp_async_wait<0>();  // this thread's copy of the site's V
+            double2 vold[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) vold[k] = vs[k * TH + tid];
+            if (y + TH < N) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) cp_async<16>(&vs[k * TH + tid], &vrow[k * vol + y + TH]);
+                cp_async_commit();
+            }
             double2 v[9];
-            p3_site<N>(e, sm, y, site, vol, se, v, fl);
+            p3_site_gv(e, [&](int j) { return sm[pad16(j * N + y)]; }, [&](int k) { return vold[k]; }, se, v, fl);
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
                 e.V[k * vol + site] = v[k];
