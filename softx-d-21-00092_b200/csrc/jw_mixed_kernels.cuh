@@ -70,8 +70,10 @@ template <int N, int C> constexpr bool mx_s2_valid() {
 // memory.  MEAS: pass 3 also leaves the row-transformed measurement planes of
 // the new V (5 FP32 pair planes, as k_meas32_rows writes them) in a fifth row.
 template <int N> constexpr int mx_p3_threads() { return row_threads<N>(); }
+template <int N> constexpr bool mx_pair();
 template <int N, bool MEAS = false> constexpr size_t mx_p3_smem() {
-    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N);
+    // the row buffer, then (one-CTA sizes) the old V of one site per thread
+    return 16 * (size_t)padded_len16((MEAS ? 5 : 4) * N) + (mx_pair<N>() ? 0 : (size_t)9 * 16 * row_threads<N>());
 }
 template <int N, bool MEAS = false> constexpr int mx_p3_blocks() {
     return mx_p3_threads<N>() <= 256 && mx_p3_smem<N, MEAS>() <= 113 * 1024 ? 2 : 1;
@@ -535,6 +537,40 @@ __device__ __forceinline__ void p3_site(const EventDev& e, const float4* sm, int
     p3_site_g(e, [&](int j) { return sm[pad16(j * N + y)]; }, site, vol, se, v, fl);
 }
 
+// The old V of the sites a thread updates in a row pass, copied ahead into
+// shared memory with cp.async: slot vs[k * TH + tid] holds entry k of site
+// tid + i TH.  start() copies the first site (the caller commits it as the
+// last group before the row's transform input is awaited with
+// cp_async_wait<1>); take() waits for the current site, reads it and starts
+// the copy of the thread's next site into the same slots.  Passes 3 and 3 + 1
+// both read V this way, so that their updates compile to the same arithmetic.
+template <int N, int TH>
+struct VAhead {
+    double2* vs;
+    const double2* __restrict__ vrow;  // row x of the event's V
+    long vol;
+    int tid;
+    __device__ __forceinline__ void start() const {
+        if (tid < N) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) cp_async<16>(&vs[k * TH + tid], &vrow[k * vol + tid]);
+        }
+        cp_async_commit();
+    }
+    __device__ __forceinline__ void take(int y, double2 (&vold)[9]) const {
+        cp_async_wait<0>();
+#pragma unroll
+        for (int k = 0; k < 9; ++k) vold[k] = vs[k * TH + tid];
+        if (y + TH < N) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) cp_async<16>(&vs[k * TH + tid], &vrow[k * vol + y + TH]);
+            cp_async_commit();
+        }
+    }
+};
+// the V slots of the one-CTA row passes (up to 512^2): [9][threads] double2
+template <int N> constexpr size_t v_ahead_bytes(int threads) { return mx_pair<N>() ? 0 : (size_t)9 * 16 * threads; }
+
 template <int N, bool MEAS = false>
 __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k_mix_pass3(EventDev* __restrict__ ev,
                                                                                          const int* __restrict__ slots,
@@ -547,11 +583,17 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
     const int x = blockIdx.x, b = blockIdx.y;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
+    constexpr int TH = mx_p3_threads<N>();
+    constexpr bool AHEAD = !mx_pair<N>();  // one-CTA sizes copy V ahead, like pass 3 + 1
     const float4* in = Q + (long)b * 4 * vol + (long)x * N;
+    const VAhead<N, TH> va{reinterpret_cast<double2*>(sm + padded_len16((MEAS ? 5 : 4) * N)), e.V + (long)x * N, vol,
+                           (int)threadIdx.x};
     for (int i = threadIdx.x; i < 4 * N; i += blockDim.x)
         cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    cp_async_wait<0>();
+    if constexpr (AHEAD) va.start();
+    else cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
     fft16_rows<N, 4>(sm, 1.0f, tw);
     const double se = e.sqrt_eps;
@@ -559,7 +601,13 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
     for (int y = threadIdx.x; y < N; y += blockDim.x) {
         const long site = (long)x * N + y;
         double2 v[9];
-        p3_site<N>(e, sm, y, site, vol, se, v, fl);
+        if constexpr (AHEAD) {
+            double2 vold[9];
+            va.take(y, vold);
+            p3_site_gv(e, [&](int j) { return sm[pad16(j * N + y)]; }, [&](int k) { return vold[k]; }, se, v, fl);
+        } else {
+            p3_site<N>(e, sm, y, site, vol, se, v, fl);
+        }
 #pragma unroll
         for (int k = 0; k < 9; ++k) e.V[k * vol + site] = v[k];
         if constexpr (MEAS) {
@@ -591,9 +639,7 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
 // 8 pair rows, then the old V of one site per thread ([9][threads] double2),
 // copied ahead with cp.async
-template <int N> constexpr size_t mx_p31_smem() {
-    return mx_p1_smem<N>() + (size_t)9 * 16 * mx_p31_threads<N>();
-}
+template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>() + v_ahead_bytes<N>(mx_p31_threads<N>()); }
 // the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
 template <int N> constexpr size_t mx_p31p_smem() {
     return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
@@ -615,18 +661,12 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     constexpr int TH = mx_p31_threads<N>();
     const int tid = threadIdx.x;
     const float4* in = Q + (long)b * 4 * vol + (long)x * N;
-    // the old V of this thread's site tid + k TH sits in slot vs[k'][tid], k' < 9,
-    // copied ahead: the first site while the inverse transforms run, the next
-    // one while this one is updated
-    double2* vs = reinterpret_cast<double2*>(sm + padded_len16(8 * N));
-    const double2* vrow = e.V + (long)x * N;
+    // the old V of this thread's sites, copied ahead: the first site while the
+    // inverse transforms run, the next one while this one is updated
+    const VAhead<N, TH> va{reinterpret_cast<double2*>(sm + padded_len16(8 * N)), e.V + (long)x * N, vol, tid};
     for (int i = tid; i < 4 * N; i += TH) cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    if (tid < N) {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) cp_async<16>(&vs[k * TH + tid], &vrow[k * vol + tid]);
-    }
-    cp_async_commit();
+    va.start();
     cp_async_wait<1>();  // Q has landed (V may still be in flight)
     __syncthreads();
     const float2* twsrc = tw;
@@ -638,15 +678,8 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
         const long site = (long)x * N + y;
         float2 v32[9];
         {
-            cp_async_wait<0>();  // this thread's copy of the site's V
             double2 vold[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) vold[k] = vs[k * TH + tid];
-            if (y + TH < N) {
-#pragma unroll
-                for (int k = 0; k < 9; ++k) cp_async<16>(&vs[k * TH + tid], &vrow[k * vol + y + TH]);
-                cp_async_commit();
-            }
+            va.take(y, vold);
             double2 v[9];
             p3_site_gv(e, [&](int j) { return sm[pad16(j * N + y)]; }, [&](int k) { return vold[k]; }, se, v, fl);
 #pragma unroll
