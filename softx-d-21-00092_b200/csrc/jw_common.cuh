@@ -102,14 +102,16 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
+// Every operation is explicitly rounded, so the kernels that draw the noise
+// (pass 1 and pass 3 + 1) give the same bits.
 __device__ __forceinline__ void box_muller_fast(uint32_t r0, uint32_t r1, float& z0, float& z1) {
-    const float u0 = __uint2float_rn(r0) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
-    const float u1 = __uint2float_rn(r1) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
-    const float rad = sqrt_approx(-2.0f * __logf(u0));
+    const float u0 = __fmaf_rn(__uint2float_rn(r0), 2.3283064365386963e-10f, 1.1641532182693481e-10f);
+    const float u1 = __fmaf_rn(__uint2float_rn(r1), 2.3283064365386963e-10f, 1.1641532182693481e-10f);
+    const float rad = sqrt_approx(__fmul_rn(-2.0f, __logf(u0)));
     float s, c;
-    __sincosf(6.28318530717958648f * u1 - 3.14159265358979324f, &s, &c);
-    z0 = -rad * c;  // cos(2 pi u1) = -cos(2 pi u1 - pi)
-    z1 = -rad * s;
+    __sincosf(__fmaf_rn(6.28318530717958648f, u1, -3.14159265358979324f), &s, &c);
+    z0 = __fmul_rn(-rad, c);  // cos(2 pi u1) = -cos(2 pi u1 - pi)
+    z1 = __fmul_rn(-rad, s);
 }
 
 __device__ __forceinline__ void langevin_normals_fast(uint64_t seed, uint64_t step, uint32_t site, float z[16]) {
@@ -166,6 +168,21 @@ __device__ __forceinline__ void embed_lambda(const T n[8], V m[9]) {
     m[6] = mk<T>(n[3], -n[4]);
     m[7] = mk<T>(n[5], -n[6]);
     m[8] = mk<T>((T)-2 * d8, 0);
+}
+
+// embed_lambda for FP64 with explicitly rounded arithmetic (the mixed
+// engine's update; see namespace xr below)
+__device__ __forceinline__ void embed_lambda_x(const double n[8], double2 m[9]) {
+    const double d8 = __dmul_rn(n[7], 0.57735026918962573);
+    m[0] = make_double2(__dadd_rn(n[2], d8), 0.0);
+    m[1] = make_double2(n[0], n[1]);
+    m[2] = make_double2(n[3], n[4]);
+    m[3] = make_double2(n[0], -n[1]);
+    m[4] = make_double2(__dsub_rn(d8, n[2]), 0.0);
+    m[5] = make_double2(n[5], n[6]);
+    m[6] = make_double2(n[3], -n[4]);
+    m[7] = make_double2(n[5], -n[6]);
+    m[8] = make_double2(__dmul_rn(-2.0, d8), 0.0);
 }
 
 // The reference's exact sequence of accumulations for one site (used by the
@@ -566,6 +583,161 @@ __device__ __forceinline__ void reunitarize(double2 m[9]) {
     m[7] = cconj(csub(cmul(m[2], m[3]), cmul(m[0], m[5])));
     m[8] = cconj(csub(cmul(m[0], m[4]), cmul(m[1], m[3])));
 }
+
+// ------------------------------------------------------------------ explicitly rounded FP64 update
+// The mixed-precision engine updates V in two kernels (pass 3, and pass 3
+// fused with the next pass 1).  The exponentials, products and
+// reunitarisation below spell every operation as a rounded intrinsic, so that
+// the compiler cannot fuse them differently in the two kernels: a run of K
+// steps gives the same bits however its steps are split into calls.  The
+// mathematics is expi_ch / mul3 / reunitarize's.
+namespace xr {
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -mul(a.y, b.y)), fma(a.x, b.y, mul(a.y, b.x)));
+}
+// a * conj(b)
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, mul(a.y, b.y)), fma(a.y, b.x, -mul(a.x, b.y)));
+}
+// c + a * b
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(add(a.x, b.x), add(a.y, b.y)); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(mul(a.x, s), mul(a.y, s)); }
+__device__ __forceinline__ double cabs2(double2 a) { return fma(a.x, a.x, mul(a.y, a.y)); }
+
+// c = a b (3 x 3 complex)
+__device__ __forceinline__ void mul3(const double2 a[9], const double2 b[9], double2 c[9]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double2 t = cmul(a[i * 3 + 0], b[0 * 3 + j]);
+            t = cfma(a[i * 3 + 1], b[1 * 3 + j], t);
+            c[i * 3 + j] = cfma(a[i * 3 + 2], b[2 * 3 + j], t);
+        }
+}
+
+// m <- exp(i sign Q) for the Hermitian Q given by m's upper triangle and real
+// diagonal (expi_ch's three branches).
+__device__ __forceinline__ void expi_ch(double2 m[9], double sign) {
+    const double a = sign * m[0].x, b = sign * m[4].x, c = sign * m[8].x;
+    const double2 d = make_double2(sign * m[1].x, sign * m[1].y), f = make_double2(sign * m[2].x, sign * m[2].y),
+                  e = make_double2(sign * m[5].x, sign * m[5].y);
+    const double dd = cabs2(d), ee = cabs2(e), ff = cabs2(f);
+    const double q00 = add(fma(a, a, dd), ff), q11 = add(fma(b, b, dd), ee), q22 = fma(c, c, add(ff, ee));
+    const double2 q01 = cadd(cscale(d, add(a, b)), cmulc(f, e));  // a d + d b + f conj(e)
+    const double2 q02 = cadd(cscale(f, add(a, c)), cmul(d, e));   // a f + d e + f c
+    const double2 q12 = cadd(cmulc(f, d), cscale(e, add(b, c)));   // conj(d) f + b e + e c
+    const double c1 = mul(0.5, add(add(q00, q11), q22));
+    const double2 de = cmul(d, e);
+    const double def = fma(de.x, f.x, mul(de.y, f.y));  // Re(d e conj(f))
+    const double c0 = fma(2.0, def, sub(sub(sub(mul(mul(a, b), c), mul(a, ee)), mul(b, ff)), mul(c, dd)));
+    double2 f0, f1, f2;
+    if (c1 <= 2e-3) {
+        const double x = c0, y = c1, x2 = mul(c0, c0);
+        f0 = make_double2(
+            fma(x2, fma(y, fma(y, -1.0 / 1209600.0, 1.0 / 20160.0), -1.0 / 720.0), 1.0),
+            fma(mul(x2, x), 1.0 / 362880.0,
+                mul(x, fma(y, fma(y, fma(y, 1.0 / 362880.0, -1.0 / 5040.0), 1.0 / 120.0), -1.0 / 6.0))));
+        f1 = make_double2(
+            fma(mul(x2, x), -1.0 / 3628800.0,
+                mul(x, fma(y, fma(y, fma(y, -1.0 / 907200.0, 1.0 / 13440.0), -1.0 / 360.0), 1.0 / 24.0))),
+            fma(x2, fma(y, 1.0 / 120960.0, -1.0 / 5040.0),
+                fma(y, fma(y, fma(y, fma(y, 1.0 / 362880.0, -1.0 / 5040.0), 1.0 / 120.0), -1.0 / 6.0), 1.0)));
+        f2 = make_double2(
+            fma(x2, fma(y, -1.0 / 1209600.0, 1.0 / 40320.0),
+                fma(y, fma(y, fma(y, fma(y, -1.0 / 3628800.0, 1.0 / 40320.0), -1.0 / 720.0), 1.0 / 24.0), -0.5)),
+            mul(x, fma(y, fma(y, 1.0 / 120960.0, -1.0 / 2520.0), 1.0 / 120.0)));
+    } else if (c1 <= 0.05) {
+        double an = 1.0, bn = 0.0, cn = 0.0, fac = 1.0;
+        double r0 = 0.0, i0 = 0.0, r1 = 0.0, i1 = 0.0, r2 = 0.0, i2 = 0.0;
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            const double sg = (n & 2) ? -fac : fac;
+            if (n & 1) { i0 = fma(sg, an, i0); i1 = fma(sg, bn, i1); i2 = fma(sg, cn, i2); }
+            else { r0 = fma(sg, an, r0); r1 = fma(sg, bn, r1); r2 = fma(sg, cn, r2); }
+            const double a2 = mul(c0, cn), b2 = fma(c1, cn, an);
+            cn = bn; an = a2; bn = b2;
+            fac /= (double)(n + 1);
+        }
+        f0 = make_double2(r0, i0);
+        f1 = make_double2(r1, i1);
+        f2 = make_double2(r2, i2);
+    } else {
+        const bool neg = c0 < 0.0;
+        const double c0a = fabs(c0);
+        const double s13 = sqrt(c1 / 3.0);
+        const double c0max = mul(mul(2.0, s13), mul(s13, s13));
+        const double r = fmin(c0a / c0max, 1.0);
+        const double theta = acos(r);
+        double st, ct;
+        sincos(theta / 3.0, &st, &ct);
+        const double u = mul(s13, ct), w = mul(sqrt(c1), st);
+        const double u2 = mul(u, u), w2 = mul(w, w);
+        double su, cu, sw, cw;
+        sincos(u, &su, &cu);
+        sincos(w, &sw, &cw);
+        const double xi0 = (fabs(w) < 0.05)
+                               ? sub(1.0, mul(w2 / 6.0, sub(1.0, mul(w2 / 20.0, sub(1.0, w2 / 42.0)))))
+                               : sw / w;
+        const double2 e2 = make_double2(sub(1.0, mul(2.0, mul(su, su))), mul(2.0, mul(su, cu)));
+        const double2 em = make_double2(cu, -su);
+        const double2 h0 = cadd(cscale(e2, sub(u2, w2)),
+                                cmul(em, make_double2(mul(8.0, mul(u2, cw)), mul(mul(2.0, u), mul(fma(3.0, u2, w2), xi0)))));
+        const double2 h1 = cadd(cscale(e2, mul(2.0, u)),
+                                cscale(cmul(em, make_double2(mul(mul(2.0, u), cw), -mul(fma(3.0, u2, -w2), xi0))), -1.0));
+        const double2 h2 = cadd(e2, cscale(cmul(em, make_double2(cw, mul(mul(3.0, u), xi0))), -1.0));
+        const double inv = 1.0 / fma(9.0, u2, -w2);
+        f0 = cscale(h0, inv);
+        f1 = cscale(h1, inv);
+        f2 = cscale(h2, inv);
+        if (neg) {
+            f0 = make_double2(f0.x, -f0.y);
+            f1 = make_double2(-f1.x, f1.y);
+            f2 = make_double2(f2.x, -f2.y);
+        }
+    }
+    // exp(iQ) = f0 I + f1 Q + f2 Q^2
+    const double2 Qm[9] = {make_double2(a, 0.0), d, f, make_double2(d.x, -d.y), make_double2(b, 0.0), e,
+                           make_double2(f.x, -f.y), make_double2(e.x, -e.y), make_double2(c, 0.0)};
+    const double2 Q2[9] = {make_double2(q00, 0.0), q01, q02, make_double2(q01.x, -q01.y), make_double2(q11, 0.0),
+                           q12, make_double2(q02.x, -q02.y), make_double2(q12.x, -q12.y), make_double2(q22, 0.0)};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        if (k == 0 || k == 4 || k == 8)
+            m[k] = make_double2(fma(f2.x, Q2[k].x, fma(f1.x, Qm[k].x, f0.x)), fma(f2.y, Q2[k].x, fma(f1.y, Qm[k].x, f0.y)));
+        else
+            m[k] = cfma(f2, Q2[k], cmul(f1, Qm[k]));
+    }
+}
+
+// Gram-Schmidt on rows 0 and 1, row 2 = conj(row0 x row1) (reunitarize)
+__device__ __forceinline__ void reunitarize(double2 m[9]) {
+    const double n0 = rsqrt(add(add(cabs2(m[0]), cabs2(m[1])), cabs2(m[2])));
+    m[0] = cscale(m[0], n0); m[1] = cscale(m[1], n0); m[2] = cscale(m[2], n0);
+    // <r0, r1> = sum conj(r0) r1
+    const double2 d = cadd(cadd(cmulc(m[3], m[0]), cmulc(m[4], m[1])), cmulc(m[5], m[2]));
+    const double2 md = make_double2(-d.x, -d.y);
+    m[3] = cfma(md, m[0], m[3]);
+    m[4] = cfma(md, m[1], m[4]);
+    m[5] = cfma(md, m[2], m[5]);
+    const double n1 = rsqrt(add(add(cabs2(m[3]), cabs2(m[4])), cabs2(m[5])));
+    m[3] = cscale(m[3], n1); m[4] = cscale(m[4], n1); m[5] = cscale(m[5], n1);
+    auto cross = [](double2 p, double2 q, double2 r, double2 t) {  // conj(p q - r t)
+        const double2 u = cfma(make_double2(-r.x, -r.y), t, cmul(p, q));
+        return make_double2(u.x, -u.y);
+    };
+    m[6] = cross(m[1], m[5], m[2], m[4]);
+    m[7] = cross(m[2], m[3], m[0], m[5]);
+    m[8] = cross(m[0], m[4], m[1], m[3]);
+}
+}  // namespace xr
 
 // ------------------------------------------------------------------ lattice momenta
 // momenta::set (momenta.h:90-124): phat2 = 4 sin^2(pi kx/N) + 4 sin^2(pi ky/N),

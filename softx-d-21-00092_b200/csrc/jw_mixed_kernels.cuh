@@ -83,45 +83,62 @@ template <int N> constexpr bool mx_p3_meas_fits() { return mx_p3_smem<N, true>()
 // Gell-Mann coefficients of R = V xi V^dagger, xi = sum_a n_a L_a: only the
 // upper triangle and the real diagonal of R are formed (R is Hermitian), and
 // t = V xi uses xi's structure (real diagonal d, upper entries c, lower
-// entries conj(c)) instead of a general 3 x 3 product.
+// entries conj(c)) instead of a general 3 x 3 product.  Passes 1 and 3 + 1
+// both rotate; every operation is an explicitly rounded intrinsic, so the two
+// kernels give the same bits whatever the compiler would fuse around them.
+__device__ __forceinline__ float fm(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ void rotate_herm(const float2 v[9], const float n[8], float h[8]) {
-    const float s = 0.57735026918962573f * n[7];  // n_7 / sqrt(3)
-    const float d0 = n[2] + s, d1 = -n[2] + s, d2 = -2.0f * s;
+    const float s = __fmul_rn(0.57735026918962573f, n[7]);  // n_7 / sqrt(3)
+    const float d0 = __fadd_rn(n[2], s), d1 = __fsub_rn(s, n[2]), d2 = __fmul_rn(-2.0f, s);
     const float2 c01 = make_float2(n[0], n[1]), c02 = make_float2(n[3], n[4]), c12 = make_float2(n[5], n[6]);
     float2 t[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const float2 a = v[i * 3 + 0], b = v[i * 3 + 1], c = v[i * 3 + 2];
         // t_i0 = a d0 + b conj(c01) + c conj(c02)
-        t[i * 3 + 0] = make_float2(a.x * d0 + (b.x * c01.x + b.y * c01.y) + (c.x * c02.x + c.y * c02.y),
-                                   a.y * d0 + (b.y * c01.x - b.x * c01.y) + (c.y * c02.x - c.x * c02.y));
+        t[i * 3 + 0] = make_float2(fm(c.y, c02.y, fm(c.x, c02.x, fm(b.y, c01.y, fm(b.x, c01.x, __fmul_rn(a.x, d0))))),
+                                   fm(-c.x, c02.y, fm(c.y, c02.x, fm(-b.x, c01.y, fm(b.y, c01.x, __fmul_rn(a.y, d0))))));
         // t_i1 = a c01 + b d1 + c conj(c12)
-        t[i * 3 + 1] = make_float2((a.x * c01.x - a.y * c01.y) + b.x * d1 + (c.x * c12.x + c.y * c12.y),
-                                   (a.x * c01.y + a.y * c01.x) + b.y * d1 + (c.y * c12.x - c.x * c12.y));
+        t[i * 3 + 1] = make_float2(fm(c.y, c12.y, fm(c.x, c12.x, fm(b.x, d1, fm(-a.y, c01.y, __fmul_rn(a.x, c01.x))))),
+                                   fm(-c.x, c12.y, fm(c.y, c12.x, fm(b.y, d1, fm(a.y, c01.x, __fmul_rn(a.x, c01.y))))));
         // t_i2 = a c02 + b c12 + c d2
-        t[i * 3 + 2] = make_float2((a.x * c02.x - a.y * c02.y) + (b.x * c12.x - b.y * c12.y) + c.x * d2,
-                                   (a.x * c02.y + a.y * c02.x) + (b.x * c12.y + b.y * c12.x) + c.y * d2);
+        t[i * 3 + 2] = make_float2(fm(c.x, d2, fm(-b.y, c12.y, fm(b.x, c12.x, fm(-a.y, c02.y, __fmul_rn(a.x, c02.x))))),
+                                   fm(c.y, d2, fm(b.y, c12.x, fm(b.x, c12.y, fm(a.y, c02.x, __fmul_rn(a.x, c02.y))))));
     }
-    // R_ij = sum_k t_ik conj(V_jk)
+    // R_ij = sum_k t_ik conj(V_jk): real part sum t.x v.x + t.y v.y, imaginary sum t.y v.x - t.x v.y
     auto rij = [&](int i, int j) {
-        float2 r = cmulc(t[i * 3 + 0], v[j * 3 + 0]);
-        r = cadd(r, cmulc(t[i * 3 + 1], v[j * 3 + 1]));
-        return cadd(r, cmulc(t[i * 3 + 2], v[j * 3 + 2]));
+        float re = __fmul_rn(t[i * 3].x, v[j * 3].x), im = __fmul_rn(t[i * 3].y, v[j * 3].x);
+        re = fm(t[i * 3].y, v[j * 3].y, re);
+        im = fm(-t[i * 3].x, v[j * 3].y, im);
+#pragma unroll
+        for (int k = 1; k < 3; ++k) {
+            re = fm(t[i * 3 + k].x, v[j * 3 + k].x, re);
+            re = fm(t[i * 3 + k].y, v[j * 3 + k].y, re);
+            im = fm(t[i * 3 + k].y, v[j * 3 + k].x, im);
+            im = fm(-t[i * 3 + k].x, v[j * 3 + k].y, im);
+        }
+        return make_float2(re, im);
     };
     auto rii = [&](int i) {
-        return t[i * 3 + 0].x * v[i * 3 + 0].x + t[i * 3 + 0].y * v[i * 3 + 0].y + t[i * 3 + 1].x * v[i * 3 + 1].x +
-               t[i * 3 + 1].y * v[i * 3 + 1].y + t[i * 3 + 2].x * v[i * 3 + 2].x + t[i * 3 + 2].y * v[i * 3 + 2].y;
+        float re = __fmul_rn(t[i * 3].x, v[i * 3].x);
+        re = fm(t[i * 3].y, v[i * 3].y, re);
+#pragma unroll
+        for (int k = 1; k < 3; ++k) {
+            re = fm(t[i * 3 + k].x, v[i * 3 + k].x, re);
+            re = fm(t[i * 3 + k].y, v[i * 3 + k].y, re);
+        }
+        return re;
     };
     const float2 r01 = rij(0, 1), r02 = rij(0, 2), r12 = rij(1, 2);
     const float r00 = rii(0), r11 = rii(1), r22 = rii(2);
     h[0] = r01.x;
     h[1] = r01.y;
-    h[2] = 0.5f * (r00 - r11);
+    h[2] = __fmul_rn(0.5f, __fsub_rn(r00, r11));
     h[3] = r02.x;
     h[4] = r02.y;
     h[5] = r12.x;
     h[6] = r12.y;
-    h[7] = (r00 + r11 - 2.0f * r22) / (2.0f * 1.7320508075688772f);
+    h[7] = __fmul_rn(fm(-2.0f, r22, __fadd_rn(r00, r11)), 0.28867513459481287f);  // / (2 sqrt 3)
 }
 
 // Transform NP contiguous padded pair rows (16-byte elements) in rounds.
@@ -507,19 +524,20 @@ __device__ __forceinline__ void p3_site_gv(const EventDev& e, GetU get_u, GetV g
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const float4 u = get_u(j);
-        a[2 * j] = (double)u.x * se;
-        a[2 * j + 1] = (double)u.y * se;
-        bq[2 * j] = (double)u.z * -se;
-        bq[2 * j + 1] = (double)u.w * -se;
+        a[2 * j] = __dmul_rn((double)u.x, se);
+        a[2 * j + 1] = __dmul_rn((double)u.y, se);
+        bq[2 * j] = __dmul_rn((double)u.z, -se);
+        bq[2 * j + 1] = __dmul_rn((double)u.w, -se);
     }
+    // the explicitly rounded forms (xr): passes 3 and 3 + 1 give the same bits
     double2 m[9], tmp[9];
-    embed_lambda<double>(bq, m);
-    expi_ch(m, -1.0);  // exp(+i sqrt(eps) B), formed while V arrives
-    mul3(m, v0, tmp);
-    embed_lambda<double>(a, m);
-    expi_ch(m, -1.0);  // exp(-i sqrt(eps) A)
-    mul3(tmp, m, v);
-    if (e.reunit) reunitarize(v);
+    embed_lambda_x(bq, m);
+    xr::expi_ch(m, -1.0);  // exp(+i sqrt(eps) B)
+    xr::mul3(m, v0, tmp);
+    embed_lambda_x(a, m);
+    xr::expi_ch(m, -1.0);  // exp(-i sqrt(eps) A)
+    xr::mul3(tmp, m, v);
+    if (e.reunit) xr::reunitarize(v);
 #pragma unroll
     for (int k = 0; k < 9; ++k)
         if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
