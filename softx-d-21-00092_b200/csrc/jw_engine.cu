@@ -455,7 +455,10 @@ void for_each_p2_cols(F&& f) {
 
 // Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
 // planes per event, Q 4) as a 2D tensor with boxes of 8 float4 elements (128
-// bytes) by min(N, 256) rows.
+// bytes) by min(N, 256) rows.  L2 promotion stays at the box row's 128 bytes:
+// with 256-byte promotion every row fetched the neighbouring tile's half line
+// too, which the column pass reads much later (measured 1.5x the algorithmic
+// DRAM reads).
 template <int N>
 bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
     const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)planes * nb * N};
@@ -464,7 +467,7 @@ bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
     const cuuint32_t estr[2] = {1, 1};
     return encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, P, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // CTAs of the persistent column pass: every SM filled to its occupancy.
