@@ -419,9 +419,9 @@ struct LaunchTimes {
     }
 };
 
-// The persistent column pass with tensor-memory-accelerator loads
-// (k_mix_pass2_tma, 8-column tiles) is tuning choice kP2Tma beside the tile
-// widths 1, 2, 4 and 8 of k_mix_pass2.
+// The persistent column pass with tensor-memory-accelerator tile moves
+// (k_mix_pass2_tma) is tuning choice kP2Tma + C (C = 8 or 4 columns per tile)
+// beside the tile widths 1, 2, 4 and 8 of k_mix_pass2; 16 stands for 24.
 constexpr int kP2Tma = 16;
 
 // cuTensorMapEncodeTiled through the runtime's driver entry points (no link
@@ -449,21 +449,23 @@ void for_each_p2_cols(F&& f) {
     if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, 2>{});
     if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, 4>{});
     if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, 8>{});
-    if constexpr (mx_t2_valid<N>())
-        if (encode_tiled()) f(std::integral_constant<int, kP2Tma>{});
+    if constexpr (mx_t2_valid<N, 4>())
+        if (encode_tiled()) f(std::integral_constant<int, kP2Tma + 4>{});
+    if constexpr (mx_t2_valid<N, 8>())
+        if (encode_tiled()) f(std::integral_constant<int, kP2Tma + 8>{});
 }
 
 // Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
-// planes per event, Q 4) as a 2D tensor with boxes of 8 float4 elements (128
-// bytes) by min(N, 256) rows.  L2 promotion stays at the box row's 128 bytes:
-// with 256-byte promotion every row fetched the neighbouring tile's half line
-// too, which the column pass reads much later (measured 1.5x the algorithmic
-// DRAM reads).
-template <int N>
+// planes per event, Q 4) as a 2D tensor with boxes of C float4 elements (C = 8:
+// 128 bytes) by min(N, 256) rows.  L2 promotion stays at 128 bytes: with
+// 256-byte promotion every row fetched the neighbouring tile's half line too,
+// which the column pass reads much later (measured 1.5x the algorithmic DRAM
+// reads).
+template <int N, int C>
 bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
     const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)planes * nb * N};
     const cuuint64_t strides[1] = {(cuuint64_t)4 * N * sizeof(float)};
-    const cuuint32_t box[2] = {32, (cuuint32_t)(N < 256 ? N : 256)};
+    const cuuint32_t box[2] = {(cuuint32_t)(4 * C), (cuuint32_t)(N < 256 ? N : 256)};
     const cuuint32_t estr[2] = {1, 1};
     return encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, P, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -471,15 +473,15 @@ bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
 }
 
 // CTAs of the persistent column pass: every SM filled to its occupancy.
-template <int N>
+template <int N, int C>
 int p2_tma_grid() {
     static int grid = 0;
     if (grid == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass2_tma<N>, mx_t2_threads<N>(),
-                                                      mx_t2_smem<N>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass2_tma<N, C>, mx_t2_threads<N, C>(),
+                                                      mx_t2_smem<N, C>());
         grid = std::max(1, sms * std::max(1, per_sm));
     }
     return grid;
@@ -493,14 +495,16 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
     float4* P = reinterpret_cast<float4*>(g.ws);
     float4* Q = P + (size_t)8 * vol * nb;
     if (cols == 0) cols = mx_s2_cols<N>();
+    if (cols == kP2Tma) cols = kP2Tma + 8;
     for_each_p2_cols<N>([&](auto c) {
         constexpr int C = decltype(c)::value;
         if (C != cols) return;
-        if constexpr (C == kP2Tma) {
+        if constexpr (C > kP2Tma) {
+            constexpr int TC = C - kP2Tma;
             CUtensorMap pmap, qmap;
-            if (!p2_tensor_map<N>(&pmap, P, nb) || !p2_tensor_map<N>(&qmap, Q, nb, 4)) return;
-            const int grid = std::min(p2_tma_grid<N>(), nb * 4 * (N / 8));
-            k_mix_pass2_tma<N><<<grid, mx_t2_threads<N>(), mx_t2_smem<N>(), e->stream>>>(
+            if (!p2_tensor_map<N, TC>(&pmap, P, nb) || !p2_tensor_map<N, TC>(&qmap, Q, nb, 4)) return;
+            const int grid = std::min(p2_tma_grid<N, TC>(), nb * 4 * (N / TC));
+            k_mix_pass2_tma<N, TC><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC>(), e->stream>>>(
                 g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
         } else {
             k_mix_pass2<N, C><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
@@ -523,9 +527,9 @@ void mix_configure() {
     }
     for_each_p2_cols<N>([](auto c) {
         constexpr int C = decltype(c)::value;
-        if constexpr (C == kP2Tma)
-            cudaFuncSetAttribute(k_mix_pass2_tma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)mx_t2_smem<N>());
+        if constexpr (C > kP2Tma)
+            cudaFuncSetAttribute(k_mix_pass2_tma<N, C - kP2Tma>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_t2_smem<N, C - kP2Tma>());
         else
             cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)mx_s2_smem<N, C>());
@@ -1555,6 +1559,7 @@ JW_EXPORT jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids
 namespace {
 template <int N>
 bool p2_cols_valid_n(int cols) {
+    if (cols == kP2Tma) cols = kP2Tma + 8;
     bool ok = false;
     for_each_p2_cols<N>([&](auto c) { ok = ok || decltype(c)::value == cols; });
     return ok;

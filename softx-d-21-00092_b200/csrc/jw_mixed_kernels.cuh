@@ -348,8 +348,10 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 }
 
 // ------------------------------------------------------------------ pass 2, persistent with TMA
-// The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
-// rows, no padding needed), as a persistent kernel: each CTA takes a
+// The same column pass as k_mix_pass2 with C-column tiles (C = 8: 128-byte
+// tile rows, one CTA of 512 threads per SM at 512^2; C = 4: 64-byte rows, two
+// CTAs of 256 threads per SM, whose first-pass stores meet two-way bank
+// conflicts in the unpadded box layout), as a persistent kernel: each CTA takes a
 // contiguous run of the work items (column tile, event, plane pair j), in
 // that order.  The tensor memory accelerator moves every tile: loads of P
 // (2D boxes {8 float4 elements, up to 256 rows} of P viewed as
@@ -365,30 +367,31 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // memory (per-pass table) and the kernel-table values of the thread's elements
 // stay in registers while the column tile does not change.  The arithmetic is
 // k_mix_pass2's, element for element, so Q is bit-identical.  Built for
-// N <= 512 (three 64 KB tiles at 512^2).
-template <int N> constexpr int mx_t2_threads() { return 8 * (N / 8); }
-template <int N> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * 8 * N; }
-template <int N> constexpr size_t mx_t2_smem() {
-    return 3 * mx_t2_tile_bytes<N>() + 1024 + 64 * (size_t)tw_pass_entries<N>();
+// N <= 512 (three 64 KB or 32 KB tiles at 512^2).
+template <int N, int C> constexpr int mx_t2_threads() { return C * (N / 8); }
+template <int N, int C> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * C * N; }
+template <int N, int C> constexpr size_t mx_t2_smem() {
+    return 3 * mx_t2_tile_bytes<N, C>() + 1024 + 64 * (size_t)tw_pass_entries<N>();
 }
-template <int N> constexpr int mx_t2_blocks() {
-    return (int)((227 * 1024) / (mx_t2_smem<N>() + 1024)) < 1024 / mx_t2_threads<N>()
-               ? (int)((227 * 1024) / (mx_t2_smem<N>() + 1024))
-               : 1024 / mx_t2_threads<N>();
+template <int N, int C> constexpr int mx_t2_blocks() {
+    return (int)((227 * 1024) / (mx_t2_smem<N, C>() + 1024)) < 1024 / mx_t2_threads<N, C>()
+               ? (int)((227 * 1024) / (mx_t2_smem<N, C>() + 1024))
+               : 1024 / mx_t2_threads<N, C>();
 }
-template <int N> constexpr bool mx_t2_valid() { return N >= 64 && N <= 512 && mx_t2_smem<N>() <= 227 * 1024; }
+template <int N, int C> constexpr bool mx_t2_valid() {
+    return (C == 4 || C == 8) && N >= 64 && N <= 512 && mx_t2_smem<N, C>() <= 227 * 1024;
+}
 
-template <int N>
-__global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_pass2_tma(
+template <int N, int C>
+__global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k_mix_pass2_tma(
     EventDev* __restrict__ ev, const int* __restrict__ slots, const float2* __restrict__ tw, int nb, int advance,
     int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap qmap) {
-    static_assert(mx_t2_valid<N>(), "three 8-column tiles per CTA");
-    constexpr int C = 8;
+    static_assert(mx_t2_valid<N, C>(), "three C-column tiles per CTA");
     constexpr int PER = 8;
     constexpr int RSTEP = N / 8;
     constexpr int TILES = N / C;
     constexpr int BOX = N < 256 ? N : 256;
-    constexpr unsigned TILE_BYTES = (unsigned)mx_t2_tile_bytes<N>();
+    constexpr unsigned TILE_BYTES = (unsigned)mx_t2_tile_bytes<N, C>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar[3];
     float4* base = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -396,7 +399,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N>(), mx_t2_blocks<N>()) k_mix_p
     const TwPass<float2> twsrc{tws};
     const int tid = threadIdx.x;
     const int cc = tid % C, r0 = tid / C;
-    const ColIdx16P<C> cidx{cc};
+    const ColIdx16<C> cidx{cc};  // dense [N][C] tile, the TMA box layout
     const long vol = (long)N * N;
     const int items = nb * 4 * TILES;
     // this CTA's run of items [begin, end): item -> (tile, b, j), tile-major
