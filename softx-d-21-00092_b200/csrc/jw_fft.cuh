@@ -380,15 +380,31 @@ __device__ __forceinline__ void fft16_passes(typename Elem16<T>::E* sm, const Id
     }
 }
 
+// Synchronisation of the threads that share a transform: the whole CTA
+// (SyncCTA), or a named barrier of a group of `count` threads (SyncBar;
+// count a multiple of 32, id 1..15, every thread of the group takes part).
+struct SyncCTA {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct SyncBar {
+    int id, count;
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+    }
+};
+
 // Register hand-off.  After the last pass thread t holds the elements
 // t + m N/8 (m = 0..7) of its sequences, and the first pass reads exactly those
 // elements.  So a transform can end in registers (for an elementwise step, a
 // reduction or a store) and the next one start from them, without the shared-
 // memory round trip.  reg[l][m] is element t + m N/8 of sequence l.
-template <typename T, int N, int Ns, int R, bool IN, bool OUT, typename IdxF, typename TW>
-__device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
-                                                 bool active, T sign, const TW& tw,
-                                                 C2<T> (&reg)[Elem16<T>::VL][8]) {
+// The general pass loads with idxL and stores with idxS (a transform may read
+// its input in one layout and continue in another) and synchronises with sync.
+template <typename T, int N, int Ns, int R, bool IN, bool OUT, typename IdxL, typename IdxS, typename TW,
+          typename Sync>
+__device__ __forceinline__ void stockham_pass16g(typename Elem16<T>::E* __restrict__ sm, const IdxL& idxL,
+                                                 const IdxS& idxS, int t, bool active, T sign, const TW& tw,
+                                                 C2<T> (&reg)[Elem16<T>::VL][8], const Sync& sync) {
     using V = C2<T>;
     constexpr int VL = Elem16<T>::VL;
     constexpr int B = 8 / R;
@@ -409,7 +425,7 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
                     for (int l = 0; l < VL; ++l) v[l][q * R + r] = reg[l][q + r * B];  // element b + r NB
                 } else {
                     V u[VL];
-                    unpack16(sm[idx(b + r * NB)], u);
+                    unpack16(sm[idxL(b + r * NB)], u);
 #pragma unroll
                     for (int l = 0; l < VL; ++l) v[l][q * R + r] = u[l];
                 }
@@ -446,7 +462,7 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
                     for (int l = 0; l < VL; ++l) reg[l][q + r * B] = v[l][q * R + r];
         }
     } else {
-        __syncthreads();
+        sync();
         if (active) {
 #pragma unroll
             for (int q = 0; q < B; ++q) {
@@ -458,12 +474,47 @@ __device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restri
                     V u[VL];
 #pragma unroll
                     for (int l = 0; l < VL; ++l) u[l] = v[l][q * R + r];
-                    sm[idx(base + r * Ns)] = pack16(u);
+                    sm[idxS(base + r * Ns)] = pack16(u);
                 }
             }
         }
-        __syncthreads();
+        sync();
     }
+}
+
+template <typename T, int N, int Ns, int R, bool IN, bool OUT, typename IdxF, typename TW>
+__device__ __forceinline__ void stockham_pass16x(typename Elem16<T>::E* __restrict__ sm, const IdxF& idx, int t,
+                                                 bool active, T sign, const TW& tw,
+                                                 C2<T> (&reg)[Elem16<T>::VL][8]) {
+    stockham_pass16g<T, N, Ns, R, IN, OUT>(sm, idx, idx, t, active, sign, tw, reg, SyncCTA{});
+}
+
+template <typename T, int N, int Ns, bool IN, bool OUT, typename IdxL0, typename IdxF, typename TW, typename Sync0,
+          typename Sync>
+__device__ __forceinline__ void fft16g_passes(typename Elem16<T>::E* sm, const IdxL0& idxL0, const IdxF& idx, int t,
+                                              bool active, T sign, const TW& tw, C2<T> (&reg)[Elem16<T>::VL][8],
+                                              const Sync0& sync0, const Sync& sync) {
+    if constexpr (Ns < N) {
+        constexpr int rem = N / Ns;
+        constexpr int R = rem >= 8 ? 8 : rem;
+        if constexpr (Ns == 1)
+            stockham_pass16g<T, N, Ns, R, IN, OUT && Ns * R == N>(sm, idxL0, idx, t, active, sign, tw, reg, sync0);
+        else
+            stockham_pass16g<T, N, Ns, R, false, OUT && Ns * R == N>(sm, idx, idx, t, active, sign, tw, reg, sync);
+        fft16g_passes<T, N, Ns * R, IN, OUT>(sm, idxL0, idx, t, active, sign, tw, reg, sync0, sync);
+    }
+}
+
+// fft16x with the first pass loading through idxL0 (its input layout) and
+// synchronising with sync0, every later access through idx and every later
+// pass synchronising with sync.
+template <typename T, int N, bool IN, bool OUT, typename IdxL0, typename IdxF, typename TW, typename Sync0,
+          typename Sync>
+__device__ __forceinline__ void fft16g(typename Elem16<T>::E* sm, const IdxL0& idxL0, const IdxF& idx, int t,
+                                       bool active, T sign, const TW& tw, C2<T> (&reg)[Elem16<T>::VL][8],
+                                       const Sync0& sync0, const Sync& sync) {
+    static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two N >= 8");
+    fft16g_passes<T, N, 1, IN, OUT>(sm, idxL0, idx, t, active, sign, tw, reg, sync0, sync);
 }
 
 template <typename T, int N, int Ns, bool IN, bool OUT, typename IdxF, typename TW>
