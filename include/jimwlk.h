@@ -377,11 +377,11 @@ jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, i
  * JW_ENOTFOUND if the engine holds no event of that size. */
 jw_status jw_engine_tuning(jw_engine* e, int N, int* p2_cols);
 /* Fix the column-tile width of size N's column pass (1, 2, 4 or 8 where it
- * fits; 16 + C = the persistent form with C-column tiles, C = 4 or 8, whose
- * tiles move through the tensor memory accelerator, N <= 512, with 16 meaning
- * 24; JW_EINVAL otherwise; 0 = the built-in default), for example a width
- * found once by the autotuner and kept; the autotuner then skips that size.
- * Every choice gives bit-identical events. */
+ * fits; 24 = the persistent form with 8-column tiles that move through the
+ * tensor memory accelerator, N <= 512, 16 meaning the same; JW_EINVAL
+ * otherwise; 0 = the built-in default), for example a width found once by the
+ * autotuner and kept; the autotuner then skips that size.  Every choice gives
+ * bit-identical events. */
 jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
  * event around each kernel launch.  kernel_ms[4] receives the milliseconds

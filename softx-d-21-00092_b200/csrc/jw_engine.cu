@@ -420,12 +420,10 @@ struct LaunchTimes {
 };
 
 // The persistent column pass with tensor-memory-accelerator tile moves
-// (k_mix_pass2_tma) is tuning choice kP2Tma + C (C = 8 or 4 columns per tile)
-// beside the tile widths 1, 2, 4 and 8 of k_mix_pass2; 16 stands for 24.
+// (k_mix_pass2_tma, 8-column tiles) is tuning choice kP2Tma + 8 beside the
+// tile widths 1, 2, 4 and 8 of k_mix_pass2; 16 stands for 24.
 constexpr int kP2Tma = 16;
-// ... and the same with the 8 columns transformed by independent thread groups
-// (k_mix_pass2_cg), tuning choice kP2ColGroups
-constexpr int kP2ColGroups = 32;
+
 
 // cuTensorMapEncodeTiled through the runtime's driver entry points (no link
 // against libcuda); null when the driver does not provide it.
@@ -452,12 +450,8 @@ void for_each_p2_cols(F&& f) {
     if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, 2>{});
     if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, 4>{});
     if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, 8>{});
-    if constexpr (mx_t2_valid<N, 4>())
-        if (encode_tiled()) f(std::integral_constant<int, kP2Tma + 4>{});
     if constexpr (mx_t2_valid<N, 8>())
         if (encode_tiled()) f(std::integral_constant<int, kP2Tma + 8>{});
-    if constexpr (mx_cg_valid<N>())
-        if (encode_tiled()) f(std::integral_constant<int, kP2ColGroups>{});
 }
 
 // Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
@@ -467,14 +461,13 @@ void for_each_p2_cols(F&& f) {
 // which the column pass reads much later (measured 1.5x the algorithmic DRAM
 // reads).
 template <int N, int C>
-bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8, bool swizzle128 = false) {
+bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
     const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)planes * nb * N};
     const cuuint64_t strides[1] = {(cuuint64_t)4 * N * sizeof(float)};
     const cuuint32_t box[2] = {(cuuint32_t)(4 * C), (cuuint32_t)(N < 256 ? N : 256)};
     const cuuint32_t estr[2] = {1, 1};
     return encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, P, dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -493,20 +486,6 @@ int p2_tma_grid() {
     return grid;
 }
 
-template <int N>
-int p2_cg_grid() {
-    static int grid = 0;
-    if (grid == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass2_cg<N>, mx_t2_threads<N, 8>(),
-                                                      mx_t2_smem<N, 8>());
-        grid = std::max(1, sms * std::max(1, per_sm));
-    }
-    return grid;
-}
-
 // Pass 2 with tuning choice `cols` (0: the default); advance = 0 leaves the
 // step index alone (timing launches of the autotuner).
 template <int N>
@@ -519,13 +498,7 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
     for_each_p2_cols<N>([&](auto c) {
         constexpr int C = decltype(c)::value;
         if (C != cols) return;
-        if constexpr (C == kP2ColGroups) {
-            CUtensorMap pmap, qmap;
-            if (!p2_tensor_map<N, 8>(&pmap, P, nb, 8, true) || !p2_tensor_map<N, 8>(&qmap, Q, nb, 4, true)) return;
-            const int grid = std::min(p2_cg_grid<N>(), nb * 4 * (N / 8));
-            k_mix_pass2_cg<N><<<grid, mx_t2_threads<N, 8>(), mx_t2_smem<N, 8>(), e->stream>>>(
-                g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
-        } else if constexpr (C > kP2Tma) {
+        if constexpr (C > kP2Tma) {
             constexpr int TC = C - kP2Tma;
             CUtensorMap pmap, qmap;
             if (!p2_tensor_map<N, TC>(&pmap, P, nb) || !p2_tensor_map<N, TC>(&qmap, Q, nb, 4)) return;
@@ -553,10 +526,7 @@ void mix_configure() {
     }
     for_each_p2_cols<N>([](auto c) {
         constexpr int C = decltype(c)::value;
-        if constexpr (C == kP2ColGroups)
-            cudaFuncSetAttribute(k_mix_pass2_cg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)mx_t2_smem<N, 8>());
-        else if constexpr (C > kP2Tma)
+        if constexpr (C > kP2Tma)
             cudaFuncSetAttribute(k_mix_pass2_tma<N, C - kP2Tma>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)mx_t2_smem<N, C - kP2Tma>());
         else

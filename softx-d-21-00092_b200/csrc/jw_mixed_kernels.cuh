@@ -348,10 +348,9 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 }
 
 // ------------------------------------------------------------------ pass 2, persistent with TMA
-// The same column pass as k_mix_pass2 with C-column tiles (C = 8: 128-byte
-// tile rows, one CTA of 512 threads per SM at 512^2; C = 4: 64-byte rows, two
-// CTAs of 256 threads per SM, whose first-pass stores meet two-way bank
-// conflicts in the unpadded box layout), as a persistent kernel: each CTA takes a
+// The same column pass as k_mix_pass2 with 8-column tiles (128-byte tile
+// rows, no padding needed; one CTA of 512 threads per SM at 512^2), as a
+// persistent kernel: each CTA takes a
 // contiguous run of the work items (column tile, event, plane pair j), in
 // that order.  The tensor memory accelerator moves every tile: loads of P
 // (2D boxes {8 float4 elements, up to 256 rows} of P viewed as
@@ -359,15 +358,15 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // and the result tile of Q leaves shared memory by a bulk tensor store, so
 // the threads issue no global loads or stores on the way.  Three tile
 // buffers rotate.  Item k finds X (plane j) in xb, Y (plane 4 + j) in yb,
-// and the third buffer fb still being read by item k - 1's store.  It
-// transforms X into registers, then (once that store has read fb) starts the
-// loads of item k + 1's X into fb and Y into xb, transforms Y, runs the
-// inverse transform in yb, writes the result tile into yb and stores it.  Item
-// k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
+// and the third buffer fb still being read by item k - 1's store.  Once that
+// store has read fb it starts the load of item k + 1's X into fb, transforms X
+// into registers, starts the load of item k + 1's Y into xb, transforms Y,
+// runs the inverse transform in yb, writes the result tile into yb and stores
+// it.  Item k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
 // memory (per-pass table) and the kernel-table values of the thread's elements
 // stay in registers while the column tile does not change.  The arithmetic is
 // k_mix_pass2's, element for element, so Q is bit-identical.  Built for
-// N <= 512 (three 64 KB or 32 KB tiles at 512^2).
+// N <= 512 (three 64 KB tiles at 512^2).
 template <int N, int C> constexpr int mx_t2_threads() { return C * (N / 8); }
 template <int N, int C> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * C * N; }
 template <int N, int C> constexpr size_t mx_t2_smem() {
@@ -379,7 +378,7 @@ template <int N, int C> constexpr int mx_t2_blocks() {
                : 1024 / mx_t2_threads<N, C>();
 }
 template <int N, int C> constexpr bool mx_t2_valid() {
-    return (C == 4 || C == 8) && N >= 64 && N <= 512 && mx_t2_smem<N, C>() <= 227 * 1024;
+    return C == 8 && N >= 64 && N <= 512 && mx_t2_smem<N, C>() <= 227 * 1024;
 }
 
 template <int N, int C>
@@ -454,6 +453,16 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
             cur_tile = tile;
         }
         float2 ra[2][8], w[2][8];
+        // the next item's X goes to fb as soon as the previous item's store
+        // has read it
+        if (more) {
+            if (tid == 0) {
+                tma_store_wait_read<0>();
+                fence_proxy_async_smem();
+                issue(it + stride, 0, fb);
+            }
+            pending |= 1u << fb;
+        }
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
         parity ^= 1u << xb;
         pending &= ~(1u << xb);
@@ -461,17 +470,14 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
-        // every thread is done reading xb; once the previous item's store has
-        // read fb, the next item's X goes to fb and its Y to xb
+        // every thread is done reading xb: the next item's Y goes there
         if (__syncthreads_or(timed_out)) break;
         if (more) {
             if (tid == 0) {
-                tma_store_wait_read<0>();
                 fence_proxy_async_smem();
-                issue(it + stride, 0, fb);
                 issue(it + stride, 1, xb);
             }
-            pending |= (1u << fb) | (1u << xb);
+            pending |= 1u << xb;
         }
         timed_out |= !mbar_wait_bounded(&bar[yb], (parity >> yb) & 1u);
         parity ^= 1u << yb;
@@ -505,154 +511,6 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         if (tid == 0) atomicOr(flags, JW_FLAG_TIMEOUT);
         // loads still in flight land in this CTA's shared memory: wait for them
         // (bounded) before the CTA exits
-        for (int i = 0; i < 3; ++i)
-            if ((pending >> i) & 1u) mbar_wait_bounded(&bar[i], (parity >> i) & 1u);
-    }
-}
-
-// ------------------------------------------------------------------ pass 2, persistent, column groups
-// k_mix_pass2_tma's schedule (persistent CTAs, contiguous tile-major item runs,
-// three TMA tile buffers, Q by TMA bulk stores) with each of the tile's 8
-// columns transformed by its own group of N/8 consecutive threads that
-// synchronise through a named barrier, so the 8 column transforms proceed
-// independently instead of in lock step across the CTA.  The tiles arrive in
-// the TMA 128-byte swizzle (element (e, c) in chunk c ^ (e mod 8) of row e),
-// which a group reads conflict-free along its column; the transforms continue
-// in the layout chunk c ^ ((e ^ e/8) mod 8), conflict-free for every later
-// access.  Both layouts give each column its own chunks of every row, but the
-// two differ, so the forward transforms' first pass (which reads one and
-// writes the other) and the write of the result tile (back into the TMA
-// layout for the store) synchronise the whole CTA.  The arithmetic is
-// k_mix_pass2's, element for element, so Q is bit-identical.  N = 256, 512.
-struct IdxSw128 {  // TMA 128-byte swizzle of an [N][8] tile of 16-byte elements
-    int c;
-    __device__ __forceinline__ int operator()(int e) const { return e * 8 + (c ^ (e & 7)); }
-};
-struct IdxSwCol {  // the transforms' working layout
-    int c;
-    __device__ __forceinline__ int operator()(int e) const { return e * 8 + (c ^ ((e ^ (e >> 3)) & 7)); }
-};
-template <int N> constexpr bool mx_cg_valid() { return N == 256 || N == 512; }
-
-template <int N>
-__global__ void __launch_bounds__(mx_t2_threads<N, 8>(), mx_t2_blocks<N, 8>()) k_mix_pass2_cg(
-    EventDev* __restrict__ ev, const int* __restrict__ slots, const float2* __restrict__ tw, int nb, int advance,
-    int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap qmap) {
-    static_assert(mx_cg_valid<N>(), "column groups of whole warps");
-    constexpr int C = 8;
-    constexpr int PER = 8;
-    constexpr int TPS = N / 8;  // threads per column group
-    constexpr int TILES = N / C;
-    constexpr int BOX = N < 256 ? N : 256;
-    constexpr unsigned TILE_BYTES = (unsigned)mx_t2_tile_bytes<N, C>();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar[3];
-    float4* base = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    float2* tws = reinterpret_cast<float2*>(base + (size_t)3 * N * C);
-    const TwPass<float2> twsrc{tws};
-    const int tid = threadIdx.x;
-    const int cc = tid / TPS, r0 = tid % TPS;
-    const IdxSw128 tma_idx{cc};
-    const IdxSwCol col_idx{cc};
-    const SyncBar gsync{1 + cc, TPS};
-    const SyncCTA csync{};
-    const long vol = (long)N * N;
-    const int items = nb * 4 * TILES;
-    const int per = items / (int)gridDim.x, extra = items % (int)gridDim.x;
-    const int begin = (int)blockIdx.x * per + min((int)blockIdx.x, extra);
-    const int end = begin + per + ((int)blockIdx.x < extra ? 1 : 0);
-    if (tid == 0) {
-        tma_prefetch_map(&pmap);
-        tma_prefetch_map(&qmap);
-        for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
-        mbar_init_fence();
-    }
-    tw_pass_fill<float2, N>(tws, tw);
-    __syncthreads();
-    auto buf = [&](int bi) { return base + (size_t)bi * N * C; };
-    auto issue = [&](int it, int half, int bi) {
-        const int tile = it / (nb * 4), r = it - tile * nb * 4, j = r & 3, b = r >> 2;
-        const int y0 = (b * 8 + (half ? 4 + j : j)) * N;
-        mbar_arrive_expect_tx(&bar[bi], TILE_BYTES);
-#pragma unroll
-        for (int rr = 0; rr < N; rr += BOX) tma_load_2d(buf(bi) + (size_t)rr * C, &pmap, tile * C * 4, y0 + rr, &bar[bi]);
-    };
-    unsigned parity = 0, pending = 0;
-    int xb = 0, yb = 1, fb = 2;
-    if (begin < end) {
-        if (tid == 0) {
-            issue(begin, 0, xb);
-            issue(begin, 1, yb);
-        }
-        pending = (1u << xb) | (1u << yb);
-    }
-    bool timed_out = false;
-    int cur_tile = -1;
-    float kx[PER], ky[PER];
-#pragma unroll 1
-    for (int it = begin; it < end; ++it) {
-        const bool more = it + 1 < end;
-        const int tile = it / (nb * 4), rj = it - tile * nb * 4, j = rj & 3, b = rj >> 2;
-        const int c0 = tile * C;
-        if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
-        if (tile != cur_tile) {
-            const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
-#pragma unroll
-            for (int q = 0; q < PER; ++q) {
-                kx[q] = __ldg(kt + (long)q * TPS * N);
-                ky[q] = __ldg(kt + vol + (long)q * TPS * N);
-            }
-            cur_tile = tile;
-        }
-        float2 ra[2][8], w[2][8];
-        timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
-        parity ^= 1u << xb;
-        pending &= ~(1u << xb);
-        fft16g<float, N, false, true>(buf(xb), tma_idx, col_idx, r0, true, -1.0f, twsrc, ra, csync, gsync);
-#pragma unroll
-        for (int q = 0; q < PER; ++q)
-            w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
-        if (__syncthreads_or(timed_out)) break;
-        if (more) {
-            if (tid == 0) {
-                tma_store_wait_read<0>();
-                fence_proxy_async_smem();
-                issue(it + 1, 0, fb);
-                issue(it + 1, 1, xb);
-            }
-            pending |= (1u << fb) | (1u << xb);
-        }
-        timed_out |= !mbar_wait_bounded(&bar[yb], (parity >> yb) & 1u);
-        parity ^= 1u << yb;
-        pending &= ~(1u << yb);
-        fft16g<float, N, false, true>(buf(yb), tma_idx, col_idx, r0, true, -1.0f, twsrc, ra, csync, gsync);
-#pragma unroll
-        for (int q = 0; q < PER; ++q)
-            w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
-        // the inverse works in this column's own chunks of yb
-        fft16g<float, N, true, true>(buf(yb), col_idx, col_idx, r0, true, 1.0f, twsrc, w, gsync, gsync);
-        // every column's inverse is done with yb before the result tile goes in
-        // (TMA layout, chunks shared between the two layouts' columns)
-        __syncthreads();
-        float4* ot = buf(yb);
-#pragma unroll
-        for (int q = 0; q < PER; ++q) ot[tma_idx(r0 + q * TPS)] = reg_put(w, q);
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            const int y0 = (b * 4 + j) * N;
-#pragma unroll
-            for (int rr = 0; rr < N; rr += BOX) tma_store_2d(&qmap, c0 * 4, y0 + rr, ot + (size_t)rr * C);
-            tma_store_commit();
-        }
-        const int nx = fb, ny = xb, nf = yb;
-        xb = nx;
-        yb = ny;
-        fb = nf;
-    }
-    if (tid == 0) tma_store_wait<0>();
-    if (timed_out) {
-        if (tid == 0) atomicOr(flags, JW_FLAG_TIMEOUT);
         for (int i = 0; i < 3; ++i)
             if ((pending >> i) & 1u) mbar_wait_bounded(&bar[i], (parity >> i) & 1u);
     }
