@@ -358,11 +358,11 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // and the result tile of Q leaves shared memory by a bulk tensor store, so
 // the threads issue no global loads or stores on the way.  Three tile
 // buffers rotate.  Item k finds X (plane j) in xb, Y (plane 4 + j) in yb,
-// and the third buffer fb still being read by item k - 1's store.  Once that
-// store has read fb it starts the load of item k + 1's X into fb, transforms X
-// into registers, starts the load of item k + 1's Y into xb, transforms Y,
-// runs the inverse transform in yb, writes the result tile into yb and stores
-// it.  Item k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
+// and the third buffer fb still being read by item k - 1's store.  It
+// transforms X into registers, then (once that store has read fb) starts the
+// loads of item k + 1's X into fb and Y into xb, transforms Y, runs the
+// inverse transform in yb, writes the result tile into yb and stores it.  Item
+// k + 1 then finds (X, Y, store) in (fb, xb, yb).  The twiddles sit in shared
 // memory (per-pass table) and the kernel-table values of the thread's elements
 // stay in registers while the column tile does not change.  The arithmetic is
 // k_mix_pass2's, element for element, so Q is bit-identical.  Built for
@@ -453,16 +453,6 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
             cur_tile = tile;
         }
         float2 ra[2][8], w[2][8];
-        // the next item's X goes to fb as soon as the previous item's store
-        // has read it
-        if (more) {
-            if (tid == 0) {
-                tma_store_wait_read<0>();
-                fence_proxy_async_smem();
-                issue(it + stride, 0, fb);
-            }
-            pending |= 1u << fb;
-        }
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
         parity ^= 1u << xb;
         pending &= ~(1u << xb);
@@ -470,14 +460,18 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
-        // every thread is done reading xb: the next item's Y goes there
+        // every thread is done reading xb; once the previous item's store has
+        // read fb, the next item's X goes to fb and its Y to xb (issuing X at
+        // the item's start, waiting for that store there, measured slower)
         if (__syncthreads_or(timed_out)) break;
         if (more) {
             if (tid == 0) {
+                tma_store_wait_read<0>();
                 fence_proxy_async_smem();
+                issue(it + stride, 0, fb);
                 issue(it + stride, 1, xb);
             }
-            pending |= 1u << xb;
+            pending |= (1u << fb) | (1u << xb);
         }
         timed_out |= !mbar_wait_bounded(&bar[yb], (parity >> yb) & 1u);
         parity ^= 1u << yb;
