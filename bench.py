@@ -313,13 +313,22 @@ def position_leg(jw, device: int, steps: int = POS_STEPS, every: int = POS_EVERY
     n = POS_N * POS_N
     lbytes = 16.0 * n * (n + 1) / 2
     step_ms = evo_ms / steps
+    # one apply streams L's lower triangle once for the noise of two steps:
+    # 32 real right-hand sides, 2 real FMAs per complex entry and right-hand side
+    apply_flops = 2.0 * 2 * 32 * n * (n + 1) / 2
     out = {"workload": f"1 event {POS_N}^2, POSITION_EVOLUTION + NOISE_COUPLING_CONSTANT (Cholesky-correlated "
                        f"noise), SIN kernel, FP64, Ny = {POS_SLICES}, {steps} steps, measured every {every}",
            "status": status, "initial_condition_ms": ic_ms, "cholesky_decompose_s": dec_s,
-           "cholesky_tflops_fp64": 4.0 * n ** 3 / 3.0 / dec_s / 1e12, "cholesky_bytes": 16.0 * n * n,
+           "cholesky_tflops_fp64": 4.0 * n ** 3 / 3.0 / dec_s / 1e12,
+           "cholesky_decompose_note": "own kernels: diagonal blocks, warp-per-row panel solves, FP64 tensor-core "
+                                      "(mma.sync m8n8k4) trailing updates; 4 n^3 / 3 real flops",
+           "cholesky_bytes": 16.0 * n * n,
            "step_ms": step_ms, "site_steps_per_s": n / (step_ms / 1e3),
-           "factor_stream_gbs": lbytes / (step_ms / 1e3) / 1e9,
-           "factor_stream_note": "lower triangle of L per step / whole-step time (the apply is ~96% of a step)",
+           "factor_stream_gbs": lbytes / (2 * step_ms / 1e3) / 1e9,
+           "factor_apply_tflops_fp64": apply_flops / (2 * step_ms / 1e3) / 1e12,
+           "factor_stream_note": "the apply reads L's lower triangle once per two steps (both steps' noise): "
+                                 "bytes and FP64 tensor flops of one apply / two whole steps' time; the FP64 "
+                                 "tensor pipe, not HBM, bounds it (nominal B200 FP64 tensor peak 40 TFLOP/s)",
            "Qs_every_50": qs, "unitarity_drift": drift}
     # the reference's own position path on a bounded sample (32^2), extrapolated by V^2 per step and V^3
     # for the decomposition; 256^2 itself is out of reach on the CPU

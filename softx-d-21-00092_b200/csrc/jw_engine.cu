@@ -493,7 +493,9 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
     const long vol = (long)N * N;
     float4* P = reinterpret_cast<float4*>(g.ws);
     float4* Q = P + (size_t)8 * vol * nb;
-    if (cols == 0) cols = mx_s2_cols<N>();
+    // the default: the persistent TMA form where it is built (measured fastest
+    // at 256^2 and 512^2), else the tile width mx_s2_cols
+    if (cols == 0) cols = (mx_t2_valid<N, 8>() && encode_tiled()) ? kP2Tma + 8 : mx_s2_cols<N>();
     if (cols == kP2Tma) cols = kP2Tma + 8;
     for_each_p2_cols<N>([&](auto c) {
         constexpr int C = decltype(c)::value;

@@ -64,7 +64,6 @@ struct jw_context {
     double2* d_pos_tab = nullptr;   // 2 planes: raw forward DFT of k_x(d), k_y(d)
     int pos_key[3] = {-1, -1, -1};  // (rr, coupling, kernel) of d_pos_tab
     double2* d_pos_scratch = nullptr;  // 18 planes
-    void* cublas = nullptr;         // cublasHandle_t (Cholesky decomposition)
     std::vector<jw_cholesky*> choleskies;  // live factors, released by jw_context_destroy
     jw_field* pos_work[4] = {};     // xi_x, xi_y, A, B of jw_evolve_position (in `fields`)
     jw_field* mom_work[6] = {};     // xi_x, xi_y, A, B, ux, uy of jw_evolve_momentum (in `fields`)

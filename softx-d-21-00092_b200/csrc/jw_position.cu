@@ -14,10 +14,11 @@
 // The Cholesky factor L of the V x V site-site correlation (68.7 GB of
 // complex doubles at 256^2) is stored row-major lower, the reference's own
 // layout, which column-major BLAS sees as the upper factor U = L^T of
-// S = U^T U.  The decomposition is right-looking and blocked: a one-CTA
-// kernel factors each 128 x 128 diagonal block, and cuBLAS ZTRSM / ZSYRK (the
-// complex-symmetric, non-conjugating rank-k update) handle the panel and the
-// trailing matrix.  Applying L streams its lower triangle once per call
+// S = U^T U.  The decomposition is right-looking and blocked (b = 128): a
+// one-CTA kernel factors each diagonal block, a warp per row solves the panel
+// below it (k_chol_trsm), and the FP64 tensor cores update the trailing lower
+// triangle by the complex-symmetric, non-conjugating rank-b product
+// (k_chol_syrk).  Applying L streams its lower triangle once per call
 // on the FP64 tensor cores (k_chol_apply, mma.sync m8n8k4): each CTA owns 128
 // rows and one 4096-column chunk, stages 128 x 16 tiles of L with cp.async,
 // and multiplies them with 8, 16 or 24 real right-hand sides.  For the
@@ -26,8 +27,6 @@
 // does 32 FP64 FMAs per 16 B of L: HBM-bound when the tensor pipe runs above
 // about 70% of its peak.  Partial products of the chunks are summed in a
 // fixed order, so results are deterministic.
-#include <cublas_v2.h>
-
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -215,6 +214,153 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }
+
+
+// ---- panel solve (the TRSM step of the blocked factorisation): every row a of
+// the panel below the diagonal block becomes x with x L_kk^T = a, i.e. for
+// j = 0..b-1: x_j = a_j / L_kk[j][j], then a_m -= x_j L_kk[m][j] for m > j
+// (right-looking forward substitution).  One warp per panel row, lane l
+// holding a_m for m = l + 32 s; the diagonal block's lower triangle sits in
+// shared memory packed by columns, so the lanes read column j contiguously.
+constexpr int kTrsmThreads = 1024;
+__host__ __device__ constexpr int trsm_col_off(int j) { return kDiagBlock * j - j * (j - 1) / 2; }
+constexpr size_t trsm_smem_bytes() { return sizeof(double2) * (size_t)trsm_col_off(kDiagBlock); }
+
+__global__ void __launch_bounds__(kTrsmThreads) k_chol_trsm(double2* __restrict__ L, long ld, long k0, long rest) {
+    static_assert(kDiagBlock == 128, "four slots of 32 per lane");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* Lc = reinterpret_cast<double2*>(smem_raw);  // column j, rows j..b-1 at trsm_col_off(j) + (m - j)
+    const double2* Lkk = L + k0 * ld + k0;
+    for (int idx = threadIdx.x; idx < kDiagBlock * kDiagBlock; idx += blockDim.x) {
+        const int m = idx / kDiagBlock, jj = idx % kDiagBlock;
+        if (jj <= m) Lc[trsm_col_off(jj) + (m - jj)] = Lkk[(long)m * ld + jj];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (long r = (long)blockIdx.x * warps + warp; r < rest; r += (long)gridDim.x * warps) {
+        double2* row = L + (k0 + kDiagBlock + r) * ld + k0;
+        double2 a[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) a[s] = row[lane + 32 * s];
+#pragma unroll
+        for (int sj = 0; sj < 4; ++sj) {
+#pragma unroll 1
+            for (int jl = 0; jl < 32; ++jl) {
+                const int j = 32 * sj + jl;
+                double2 x = a[sj];
+                if (lane == jl) x = cdiv_smith(a[sj], Lc[trsm_col_off(j)]);
+                x.x = __shfl_sync(0xffffffffu, x.x, jl);
+                x.y = __shfl_sync(0xffffffffu, x.y, jl);
+                if (lane == jl) a[sj] = x;
+                const double2* col = Lc + trsm_col_off(j) - j;  // col[m] = L_kk[m][j], m >= j
+#pragma unroll
+                for (int s = sj; s < 4; ++s) {
+                    const int m = lane + 32 * s;
+                    if (m > j) a[s] = csub(a[s], cmul(x, col[m]));
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) row[lane + 32 * s] = a[s];
+    }
+}
+
+// ---- trailing update (the SYRK step): S(i, l) -= sum_m P(i, m) P(l, m) for
+// the lower triangle of the trailing matrix, P the b = 128 columns of the
+// solved panel (complex symmetric: no conjugation), on the FP64 tensor cores.
+// One CTA (4 warps) per 64 x 64 tile of the lower triangle, grid-strided; a
+// warp owns a 32 x 32 quarter as 4 x 4 complex 8 x 8 blocks, each the four real
+// products (re re, -im im, re im, im re) of m8n8k4 fragments that share one
+// 16-byte load of the real and imaginary parts.  Stages of 16 complex columns
+// of both tiles' panel rows (16 KB each, 16-byte chunks XOR-swizzled by the row
+// so that the fragment loads hit every bank once per four lanes) come three
+// deep through cp.async.  Diagonal tiles leave their upper part (zero) alone.
+constexpr int kSyT = 64, kSyK = 16, kSyStages = 3, kSyThreads = 128;
+constexpr size_t kSyStageBytes = 2 * (size_t)kSyT * kSyK * 16;
+constexpr size_t syrk_smem_bytes() { return kSyStages * kSyStageBytes; }
+
+__global__ void __launch_bounds__(kSyThreads, 2) k_chol_syrk(double2* __restrict__ L, long ld, long k0, long t0,
+                                                             int nt) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int g = lane >> 2, q = lane & 3, wi = w >> 1, wj = w & 1;
+    constexpr int chunks = kDiagBlock / kSyK;
+    const long ntiles = (long)nt * (nt + 1) / 2;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        long I = (long)((sqrt(8.0 * (double)tile + 1.0) - 1.0) * 0.5);
+        while ((I + 1) * (I + 2) / 2 <= tile) ++I;
+        while (I * (I + 1) / 2 > tile) --I;
+        const long J = tile - I * (I + 1) / 2;
+        const long r0 = t0 + I * kSyT, c0 = t0 + J * kSyT;
+        auto stage = [&](int t) {
+            unsigned char* sb = smem + (t % kSyStages) * kSyStageBytes;
+            const long kb = k0 + (long)t * kSyK;
+#pragma unroll
+            for (int c = tid; c < 2 * kSyT * kSyK; c += kSyThreads) {
+                const int half = c / (kSyT * kSyK), rr = (c % (kSyT * kSyK)) / kSyK, e = c % kSyK;
+                const double2* src = L + ((half ? c0 : r0) + rr) * ld + kb + e;
+                cpa16(sb + half * (kSyT * kSyK * 16) + rr * (kSyK * 16) + ((e ^ (rr & 7)) << 4), src);
+            }
+            cpa_commit();
+        };
+        double acc[4][4][2][2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) acc[a][b][c][0] = acc[a][b][c][1] = 0.0;
+        stage(0);
+        stage(1);
+#pragma unroll 1
+        for (int t = 0; t < chunks; ++t) {
+            if (t + 2 < chunks) stage(t + 2);
+            else cpa_commit();
+            cpa_wait<2>();
+            __syncthreads();
+            const unsigned char* sa = smem + (t % kSyStages) * kSyStageBytes;
+            const unsigned char* sbb = sa + kSyT * kSyK * 16;
+#pragma unroll
+            for (int ks = 0; ks < kSyK / 4; ++ks) {
+                const int e = 4 * ks + q;
+                double2 af[4], bf[4];
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi) {
+                    const int row = 32 * wi + 8 * mi + g;
+                    af[mi] = *reinterpret_cast<const double2*>(sa + row * (kSyK * 16) + ((e ^ (row & 7)) << 4));
+                }
+#pragma unroll
+                for (int nj = 0; nj < 4; ++nj) {
+                    const int row = 32 * wj + 8 * nj + g;
+                    bf[nj] = *reinterpret_cast<const double2*>(sbb + row * (kSyK * 16) + ((e ^ (row & 7)) << 4));
+                }
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                    for (int nj = 0; nj < 4; ++nj) {
+                        dmma(acc[mi][nj][0][0], acc[mi][nj][0][1], af[mi].x, bf[nj].x);   // re re
+                        dmma(acc[mi][nj][0][0], acc[mi][nj][0][1], af[mi].y, -bf[nj].y);  // - im im
+                        dmma(acc[mi][nj][1][0], acc[mi][nj][1][1], af[mi].x, bf[nj].y);   // re im
+                        dmma(acc[mi][nj][1][0], acc[mi][nj][1][1], af[mi].y, bf[nj].x);   // im re
+                    }
+            }
+            __syncthreads();  // the stage is read by every warp before it is refilled
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int nj = 0; nj < 4; ++nj) {
+                const long row = r0 + 32 * wi + 8 * mi + g;
+                const long col = c0 + 32 * wj + 8 * nj + 2 * q;
+                double2* p = L + row * ld + col;
+#pragma unroll
+                for (int d = 0; d < 2; ++d)
+                    if (I != J || col + d <= row)
+                        p[d] = make_double2(p[d].x - acc[mi][nj][0][d], p[d].y - acc[mi][nj][1][d]);
+            }
+    }
+}
+
 
 // P[chunk][row][c] = sum over the chunk's columns k of L(row, k) X(k, c):
 // complex L times RP = 8 NT real right-hand sides on the FP64 tensor cores.
@@ -494,10 +640,9 @@ void position_release(jw_context* c) {
     c->choleskies.clear();
     if (c->d_pos_tab) cudaFree(c->d_pos_tab);
     if (c->d_pos_scratch) cudaFree(c->d_pos_scratch);
-    if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
+
     c->d_pos_tab = nullptr;
     c->d_pos_scratch = nullptr;
-    c->cublas = nullptr;
 }
 }  // namespace jw
 
@@ -564,13 +709,16 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     size_t free_b = 0, total_b = 0;
     JW_CUDA(cudaMemGetInfo(&free_b, &total_b));
     if (bytesL + bytesX + bytesP + ((size_t)1 << 30) > free_b) return JW_ENOMEM;
-    if (!c->cublas) {
-        cublasHandle_t h = nullptr;
-        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return JW_ECUDA;
-        c->cublas = h;
+    if (n > kDiagBlock && n % kDiagBlock != 0) return JW_EUNSUPPORTED;  // N^2 for power-of-two N >= 16 always divides
+    static bool configured = false;
+    if (!configured) {
+        JW_CUDA(cudaFuncSetAttribute(k_chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem_bytes()));
+        JW_CUDA(cudaFuncSetAttribute(k_chol_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)syrk_smem_bytes()));
+        configured = true;
     }
-    cublasHandle_t h = static_cast<cublasHandle_t>(c->cublas);
-    if (cublasSetStream(h, c->stream) != CUBLAS_STATUS_SUCCESS) return JW_ECUDA;
+    int dev = 0, sms = 0;
+    JW_CUDA(cudaGetDevice(&dev));
+    JW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     jw_cholesky* L = new jw_cholesky();
     L->ctx = c;
     L->n = n;
@@ -603,7 +751,8 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
         return fail(JW_ECUDA);
     k_chol_fill<<<148 * 16, kThreads, 0, c->stream>>>(L->d_L, corr->d, N, n);
     if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
-    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), minus_one = make_cuDoubleComplex(-1.0, 0.0);
+    // right-looking blocked factorisation, b = 128: factor the diagonal block,
+    // solve the panel below it, update the trailing lower triangle
     for (long k0 = 0; k0 < n; k0 += kDiagBlock) {
         const long b = std::min((long)kDiagBlock, n - k0);
         double2* Akk = L->d_L + k0 * n + k0;
@@ -611,17 +760,14 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
         if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
         const long rest = n - k0 - b;
         if (rest == 0) break;
-        // column-major view: U = L^T is upper; panel U(k0:k0+b, k0+b:n) <- U_kk^-T panel
-        cuDoubleComplex* Ukk = reinterpret_cast<cuDoubleComplex*>(Akk);
-        cuDoubleComplex* Upan = reinterpret_cast<cuDoubleComplex*>(L->d_L + (k0 + b) * n + k0);
-        cuDoubleComplex* Utr = reinterpret_cast<cuDoubleComplex*>(L->d_L + (k0 + b) * n + (k0 + b));
-        if (cublasZtrsm_64(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, b, rest, &one,
-                           Ukk, n, Upan, n) != CUBLAS_STATUS_SUCCESS)
-            return fail(JW_ECUDA);
-        // trailing S(k0+b:, k0+b:) -= panel^T panel (upper, complex symmetric)
-        if (cublasZsyrk_64(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, rest, b, &minus_one, Upan, n, &one, Utr, n) !=
-            CUBLAS_STATUS_SUCCESS)
-            return fail(JW_ECUDA);
+        const long warps = kTrsmThreads / 32;
+        k_chol_trsm<<<(unsigned)std::min((rest + warps - 1) / warps, (long)sms), kTrsmThreads, trsm_smem_bytes(),
+                      c->stream>>>(L->d_L, n, k0, rest);
+        const int nt = (int)(rest / kSyT);
+        const long ntiles = (long)nt * (nt + 1) / 2;
+        k_chol_syrk<<<(unsigned)std::min(ntiles, 2L * sms), kSyThreads, syrk_smem_bytes(), c->stream>>>(
+            L->d_L, n, k0, k0 + b, nt);
+        if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(JW_ECUDA);
     c->choleskies.push_back(L);

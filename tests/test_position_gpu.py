@@ -149,8 +149,11 @@ def test_cholesky_factor_reproduces_correlation(jw, N):
     assert ctx.sync() == jw.OK
 
 
-def test_cholesky_matches_oracle_N16(jw, oracle):
-    N = 16
+@pytest.mark.parametrize("N", [16, 32])
+def test_cholesky_matches_oracle(jw, oracle, N):
+    """The blocked factorisation (diagonal blocks, panel solves, tensor-core
+    trailing updates: one panel at 16^2, eight at 32^2) against the oracle's
+    column-by-column recurrence (matrix.h:151-200)."""
     ctx = ctx_for(jw, N, 3, 0.0004, 1, 1)
     corr = ctx.field(1)
     ctx.set_correlations_for_coupling_constant(corr)
