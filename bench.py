@@ -391,9 +391,19 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
         t_first = res.t_submit if t_first is None else min(t_first, res.t_submit)
         t_last = max(t_last, res.t_done)
     stats = srv.stats()
+    sizes = srv.size_stats()
     srv.close()
     site_steps = sum(r["N"] ** 2 * r["steps"] for r in reqs)
     mix = [(r["N"], r["ny_slices"], r["steps"]) for r in reqs]
+    # where the device time goes: per lattice size, the site-steps it advanced,
+    # the device time of its step launches and MV slices (CUDA events on the
+    # engine stream), and its own rate
+    dev_ms = sum(v["step_ms"] + v["mv_ms"] for v in sizes.values())
+    per_n = {str(n): {"requests": sum(1 for r in reqs if r["N"] == n), "site_steps": v["site_steps"],
+                      "step_ms": v["step_ms"], "mv_ms": v["mv_ms"], "ticks": v["ticks"],
+                      "share_of_device_time": (v["step_ms"] + v["mv_ms"]) / dev_ms if dev_ms else None,
+                      "site_steps_per_s_while_stepping": v["site_steps"] / (v["step_ms"] / 1e3) if v["step_ms"] else None}
+             for n, v in sorted(sizes.items())}
     return {"requests": n_requests, "ok": ok, "rate_req_per_s": rate, "_mix": mix,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "site_steps_per_s": site_steps / (t_last - t_first), "wall_s": t_last - t_first,
@@ -401,6 +411,9 @@ def serve_leg(jw, device: int, n_requests: int, rate: float, seed: int, tick_sit
                       f"throughput over the {t_last - t_first:.1f} s from the first submission to the last "
                       "completion",
             "max_resident": stats.max_active,
+            "per_n": per_n,
+            "phases_s": {"admit": stats.t_admit, "mv": stats.t_mv, "step": stats.t_step, "retire": stats.t_retire},
+            "device_busy_fraction": dev_ms / 1e3 / (t_last - t_first),
             "offered_site_steps_per_s": site_steps / arrivals[-1],
             "tick_sites": tick_sites,
             "what": "Poisson arrivals, N log-uniform 64..2048 rounded to powers of two, steps U[10,2000], "
@@ -452,9 +465,14 @@ def uneven_leg(jw, device: int, seed: int):
             for i, r in enumerate(reqs)]
     ok = sum(srv.wait(rid, timeout=3600)[0] == jw.OK for rid in rids)
     wall = time.perf_counter() - t0
+    sizes = srv.size_stats()
     srv.close()
     ss = sum(r["N"] ** 2 * r["steps"] for r in reqs)
+    per_n = {str(n): {"site_steps": v["site_steps"], "step_ms": v["step_ms"], "mv_ms": v["mv_ms"],
+                      "site_steps_per_s_while_stepping": v["site_steps"] / (v["step_ms"] / 1e3) if v["step_ms"] else None}
+             for n, v in sorted(sizes.items())}
     return {"events": len(reqs), "ok": ok, "site_steps": ss, "wall_s": wall, "site_steps_per_s": ss / wall,
+            "per_n": per_n,
             "what": "48 events N in {128,256,512,1024} (16/16/12/4), steps U[200,2000], mixed couplings, "
                     "one server, MV initial conditions included"}
 

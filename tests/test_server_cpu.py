@@ -27,6 +27,13 @@ def test_fake_server_completes_everything(jw):
     s = srv.stats()
     assert s.completed == 4 and s.failed == 0 and s.queued == 0
     assert s.site_steps == sum(N * N * k for N, k in [(64, 40), (128, 10), (32, 100), (256, 5)])
+    # per-size totals: every size served, site-steps split exactly, no device
+    # time on the host-only backend
+    sizes = srv.size_stats()
+    assert sorted(sizes) == [32, 64, 128, 256]
+    for N, k in [(64, 40), (128, 10), (32, 100), (256, 5)]:
+        assert sizes[N]["site_steps"] == N * N * k and sizes[N]["ticks"] >= 1
+        assert sizes[N]["step_ms"] == 0.0 and sizes[N]["mv_ms"] == 0.0
     srv.close()
 
 
