@@ -191,20 +191,35 @@ __global__ void k_chol_fill(double2* __restrict__ M, const double2* __restrict__
 // the columns to its left are already applied: L_jj = sqrt(a_jj),
 // L_ij = a_ij / L_jj, a_il -= L_ij L_lj.  One CTA; the block stays in L2.
 __global__ void __launch_bounds__(1024) k_chol_diag(double2* __restrict__ a, long ld, int b) {
+    // the block's lower triangle in shared memory, packed by rows: row i
+    // starts at i (i + 1) / 2
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* s = reinterpret_cast<double2*>(smem_raw);
+    auto at = [](int i, int j) { return i * (i + 1) / 2 + j; };
+    for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+        const int i = idx / b, j = idx % b;
+        if (j <= i) s[at(i, j)] = a[(long)i * ld + j];
+    }
+    __syncthreads();
     for (int j = 0; j < b; ++j) {
-        if (threadIdx.x == 0) a[(long)j * ld + j] = csqrt_p(a[(long)j * ld + j]);
+        if (threadIdx.x == 0) s[at(j, j)] = csqrt_p(s[at(j, j)]);
         __syncthreads();
-        const double2 d = a[(long)j * ld + j];
-        for (int i = j + 1 + threadIdx.x; i < b; i += blockDim.x) a[(long)i * ld + j] = cdiv_smith(a[(long)i * ld + j], d);
+        const double2 d = s[at(j, j)];
+        for (int i = j + 1 + threadIdx.x; i < b; i += blockDim.x) s[at(i, j)] = cdiv_smith(s[at(i, j)], d);
         __syncthreads();
         const int m = b - j - 1;
         for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
             const int i = j + 1 + q / m, l = j + 1 + q % m;
-            if (l <= i) a[(long)i * ld + l] = csub(a[(long)i * ld + l], cmul(a[(long)i * ld + j], a[(long)l * ld + j]));
+            if (l <= i) s[at(i, l)] = csub(s[at(i, l)], cmul(s[at(i, j)], s[at(l, j)]));
         }
         __syncthreads();
     }
+    for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+        const int i = idx / b, j = idx % b;
+        if (j <= i) a[(long)i * ld + j] = s[at(i, j)];
+    }
 }
+constexpr size_t diag_smem_bytes() { return sizeof(double2) * (size_t)kDiagBlock * (kDiagBlock + 1) / 2; }
 
 // One FP64 tensor-core product D(8x8) += A(8x4) B(4x8) (mma.sync m8n8k4):
 // lane (g = lane/4, q = lane%4) supplies A[g][q] and B[q][g] and holds
@@ -334,15 +349,28 @@ __global__ void __launch_bounds__(kSyThreads, 2) k_chol_syrk(double2* __restrict
                     const int row = 32 * wj + 8 * nj + g;
                     bf[nj] = *reinterpret_cast<const double2*>(sbb + row * (kSyK * 16) + ((e ^ (row & 7)) << 4));
                 }
+                // the four real products in four sweeps over the 16 blocks, so
+                // that products into one accumulator are 32 instructions apart
 #pragma unroll
                 for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-                    for (int nj = 0; nj < 4; ++nj) {
-                        dmma(acc[mi][nj][0][0], acc[mi][nj][0][1], af[mi].x, bf[nj].x);   // re re
+                    for (int nj = 0; nj < 4; ++nj)
+                        dmma(acc[mi][nj][0][0], acc[mi][nj][0][1], af[mi].x, bf[nj].x);  // re re
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                    for (int nj = 0; nj < 4; ++nj)
+                        dmma(acc[mi][nj][1][0], acc[mi][nj][1][1], af[mi].x, bf[nj].y);  // re im
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                    for (int nj = 0; nj < 4; ++nj)
                         dmma(acc[mi][nj][0][0], acc[mi][nj][0][1], af[mi].y, -bf[nj].y);  // - im im
-                        dmma(acc[mi][nj][1][0], acc[mi][nj][1][1], af[mi].x, bf[nj].y);   // re im
-                        dmma(acc[mi][nj][1][0], acc[mi][nj][1][1], af[mi].y, bf[nj].x);   // im re
-                    }
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                    for (int nj = 0; nj < 4; ++nj)
+                        dmma(acc[mi][nj][1][0], acc[mi][nj][1][1], af[mi].y, bf[nj].x);  // im re
             }
             __syncthreads();  // the stage is read by every warp before it is refilled
         }
@@ -712,6 +740,7 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     if (n > kDiagBlock && n % kDiagBlock != 0) return JW_EUNSUPPORTED;  // N^2 for power-of-two N >= 16 always divides
     static bool configured = false;
     if (!configured) {
+        JW_CUDA(cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem_bytes()));
         JW_CUDA(cudaFuncSetAttribute(k_chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem_bytes()));
         JW_CUDA(cudaFuncSetAttribute(k_chol_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)syrk_smem_bytes()));
         configured = true;
@@ -756,7 +785,7 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     for (long k0 = 0; k0 < n; k0 += kDiagBlock) {
         const long b = std::min((long)kDiagBlock, n - k0);
         double2* Akk = L->d_L + k0 * n + k0;
-        k_chol_diag<<<1, 1024, 0, c->stream>>>(Akk, n, (int)b);
+        k_chol_diag<<<1, 1024, diag_smem_bytes(), c->stream>>>(Akk, n, (int)b);
         if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
         const long rest = n - k0 - b;
         if (rest == 0) break;
