@@ -301,23 +301,44 @@ __global__ void __launch_bounds__(kSyThreads, 2) k_chol_syrk(double2* __restrict
     const int g = lane >> 2, q = lane & 3, wi = w >> 1, wj = w & 1;
     constexpr int chunks = kDiagBlock / kSyK;
     const long ntiles = (long)nt * (nt + 1) / 2;
-    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // tile index -> (I, J), I >= J, and its first rows / columns
+    auto corner = [&](long tile, long& r0, long& c0, bool& diag) {
         long I = (long)((sqrt(8.0 * (double)tile + 1.0) - 1.0) * 0.5);
         while ((I + 1) * (I + 2) / 2 <= tile) ++I;
         while (I * (I + 1) / 2 > tile) --I;
         const long J = tile - I * (I + 1) / 2;
-        const long r0 = t0 + I * kSyT, c0 = t0 + J * kSyT;
-        auto stage = [&](int t) {
-            unsigned char* sb = smem + (t % kSyStages) * kSyStageBytes;
-            const long kb = k0 + (long)t * kSyK;
+        r0 = t0 + I * kSyT;
+        c0 = t0 + J * kSyT;
+        diag = I == J;
+    };
+    // chunk t of the tile at (r0, c0) into the stage buffer of the n-th chunk
+    // this CTA stages (chunks are consumed in the order they are staged)
+    int staged = 0;
+    auto stage = [&](long r0, long c0, int t) {
+        unsigned char* sb = smem + (staged++ % kSyStages) * kSyStageBytes;
+        const long kb = k0 + (long)t * kSyK;
 #pragma unroll
-            for (int c = tid; c < 2 * kSyT * kSyK; c += kSyThreads) {
-                const int half = c / (kSyT * kSyK), rr = (c % (kSyT * kSyK)) / kSyK, e = c % kSyK;
-                const double2* src = L + ((half ? c0 : r0) + rr) * ld + kb + e;
-                cpa16(sb + half * (kSyT * kSyK * 16) + rr * (kSyK * 16) + ((e ^ (rr & 7)) << 4), src);
-            }
-            cpa_commit();
-        };
+        for (int c = tid; c < 2 * kSyT * kSyK; c += kSyThreads) {
+            const int half = c / (kSyT * kSyK), rr = (c % (kSyT * kSyK)) / kSyK, e = c % kSyK;
+            const double2* src = L + ((half ? c0 : r0) + rr) * ld + kb + e;
+            cpa16(sb + half * (kSyT * kSyK * 16) + rr * (kSyK * 16) + ((e ^ (rr & 7)) << 4), src);
+        }
+        cpa_commit();
+    };
+    long tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    long r0, c0;
+    bool diag;
+    corner(tile, r0, c0, diag);
+    stage(r0, c0, 0);
+    stage(r0, c0, 1);
+    int consumed = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        // the next tile's first chunks are staged during this tile's last ones
+        const long next = tile + gridDim.x;
+        long nr0 = 0, nc0 = 0;
+        bool ndiag = false;
+        if (next < ntiles) corner(next, nr0, nc0, ndiag);
         double acc[4][4][2][2];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
@@ -325,15 +346,14 @@ __global__ void __launch_bounds__(kSyThreads, 2) k_chol_syrk(double2* __restrict
             for (int b = 0; b < 4; ++b)
 #pragma unroll
                 for (int c = 0; c < 2; ++c) acc[a][b][c][0] = acc[a][b][c][1] = 0.0;
-        stage(0);
-        stage(1);
 #pragma unroll 1
         for (int t = 0; t < chunks; ++t) {
-            if (t + 2 < chunks) stage(t + 2);
+            if (t + 2 < chunks) stage(r0, c0, t + 2);
+            else if (next < ntiles) stage(nr0, nc0, t + 2 - chunks);
             else cpa_commit();
             cpa_wait<2>();
             __syncthreads();
-            const unsigned char* sa = smem + (t % kSyStages) * kSyStageBytes;
+            const unsigned char* sa = smem + (consumed++ % kSyStages) * kSyStageBytes;
             const unsigned char* sbb = sa + kSyT * kSyK * 16;
 #pragma unroll
             for (int ks = 0; ks < kSyK / 4; ++ks) {
@@ -383,9 +403,12 @@ __global__ void __launch_bounds__(kSyThreads, 2) k_chol_syrk(double2* __restrict
                 double2* p = L + row * ld + col;
 #pragma unroll
                 for (int d = 0; d < 2; ++d)
-                    if (I != J || col + d <= row)
+                    if (!diag || col + d <= row)
                         p[d] = make_double2(p[d].x - acc[mi][nj][0][d], p[d].y - acc[mi][nj][1][d]);
             }
+        r0 = nr0;
+        c0 = nc0;
+        diag = ndiag;
     }
 }
 
