@@ -672,10 +672,12 @@ def main_arm(args):
 
     events = args.events
     n_side = args.n
-    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch, autotune=True,
-                    reunitarize=REUNITARIZE)
+    eng = jw.Engine(precision=jw.PRECISION_MIXED, device=local, max_batch=args.max_batch,
+                    autotune=args.column_form == 0, reunitarize=REUNITARIZE)
     ids = [eng.add_event(n_side, ny_slices=NY_SLICES, mu=0.5 * n_side, mass=MASS, step=STEP,
                          coupling=jw.SQRT_COUPLING_CONSTANT, seed=sd) for sd in event_seeds(rank, events)]
+    if args.column_form:
+        eng.set_tuning(n_side, args.column_form)
     eng.init_mv(ids)
     eng.step(ids, args.warmup)
     if eng.sync() != jw.OK:
@@ -737,18 +739,27 @@ def main_arm(args):
     peak, peak_kind = measured_peaks()
     launched = {k: v for k, v in kernels.items() if v[1] > 0}
     dom = max(launched, key=lambda k: launched[k][0])
-    name = f"{KIND_KERNEL[dom]}<{n_side}>"
+    tuned = eng.tuning(n_side)
+    kernel_of = dict(KIND_KERNEL)
+    if tuned in (16, 24) or (tuned == 0 and n_side <= 512):  # the persistent TMA column pass
+        kernel_of["pass2"] = "k_mix_pass2_tma"
+    name = f"{kernel_of[dom]}<{n_side}>"
     per_launch = {k: ms / cnt for k, (ms, cnt) in launched.items()}
     alg_bytes = KIND_BYTES[dom] * sites
     achieved = alg_bytes / (per_launch[dom] / 1e3) / 1e9
-    traffic = profiled_traffic().get(name)
+    measured = profiled_traffic()
+    traffic = measured.get(name)
     kernel_time = sum(ms for ms, _ in launched.values())
     roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic * sites if traffic else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per site at 16 events x 512^2 "
+                              "(working set >> L2), times this launch's sites (profiles/step_kernels_512x64.md)",
             "algorithmic_bytes": alg_bytes,
-            "kernels": {f"{KIND_KERNEL[k]}<{n_side}>": {
+            "traffic_over_algorithmic": traffic * sites / alg_bytes if traffic else None,
+            "kernels": {f"{kernel_of[k]}<{n_side}>": {
                 "launches": cnt, "ms_per_launch": per_launch[k], "share": ms / kernel_time,
-                "hbm_frac": KIND_BYTES[k] * sites / (per_launch[k] / 1e3) / 1e9 / peak}
+                "hbm_frac": KIND_BYTES[k] * sites / (per_launch[k] / 1e3) / 1e9 / peak,
+                "traffic_bytes_per_site": measured.get(f"{kernel_of[k]}<{n_side}>")}
                 for k, (ms, cnt) in launched.items()}}
 
     line = {
@@ -848,6 +859,8 @@ def main():
     ap.add_argument("--max-batch", type=int, default=0, help="events per launch group (0 = engine default)")
     ap.add_argument("--serve-requests", type=int, default=1000, help="requests in the serving window")
     ap.add_argument("--n", type=int, default=N, help="lattice side (profiling runs; the workload is 512)")
+    ap.add_argument("--column-form", type=int, default=0,
+                    help="fix the column pass's tuning choice instead of autotuning (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "engine":
         args.warmup = 3
