@@ -393,7 +393,12 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
     constexpr unsigned TILE_BYTES = (unsigned)mx_t2_tile_bytes<N, C>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar[3];
-    float4* base = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    // the tiles start on a 1024-byte boundary; the offset is added to the
+    // shared array itself (not to an integer copy of its address), so that
+    // every tile access compiles to a shared-memory instruction rather than a
+    // generic one
+    const unsigned align_pad = (1024u - (smem_addr(smem_raw) & 1023u)) & 1023u;
+    float4* base = reinterpret_cast<float4*>(smem_raw + align_pad);
     float2* tws = reinterpret_cast<float2*>(base + (size_t)3 * N * C);
     const TwPass<float2> twsrc{tws};
     const int tid = threadIdx.x;
