@@ -270,6 +270,50 @@ __device__ __forceinline__ void tw_pass_fill(V* dst, const V* __restrict__ tw) {
     }
 }
 
+// The same per-pass table in the layout the row transforms want (TwRows):
+// the Ns entries of a pass are stored as 4 blocks of Ns float4 values, block j
+// holding (w^2j, w^2j+1) of every butterfly k.  Threads of a row transform read
+// consecutive k, so their 128-bit loads are conflict-free; the entry-major
+// TwPass layout puts consecutive k 64 bytes apart (a 4-way bank conflict) and
+// suits the column transforms, whose quarter-warps share one k.  The values
+// are TwPass's, so both give bit-identical transforms.
+template <typename V> struct TwRows {
+    const V* p;
+};
+template <typename V, int N>
+__device__ __forceinline__ void tw_rows_fill(V* dst, const V* __restrict__ tw) {
+    constexpr int E = tw_pass_entries<N>();
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        int Ns = 8, base = 0;
+        while (e >= base + Ns) {
+            base += Ns;
+            Ns *= 8;
+        }
+        const int rem = N / Ns;
+        const int R = rem >= 8 ? 8 : rem;
+        const int k = e - base;
+        const int TWS = N / (Ns * R);
+        V w[8];
+        for (int r = 0; r < 8; ++r) w[r] = V{};
+        w[0].x = 1.0f;
+        w[1] = __ldg(&tw[k * TWS]);
+        if (R >= 4) w[2] = __ldg(&tw[2 * k * TWS]);
+        if (R == 4) w[3] = tw_mul(w[1], w[2]);
+        if (R == 8) {
+            w[4] = __ldg(&tw[4 * k * TWS]);
+            w[3] = tw_mul(w[1], w[2]);
+            w[5] = tw_mul(w[4], w[1]);
+            w[6] = tw_mul(w[4], w[2]);
+            w[7] = tw_mul(w[4], w[3]);
+        }
+        for (int j = 0; j < 4; ++j) {
+            V* d = dst + 2 * (4 * base + j * Ns + k);
+            d[0] = w[2 * j];
+            d[1] = w[2 * j + 1];
+        }
+    }
+}
+
 // The twiddles w^1 .. w^(R-1) of butterfly k of pass (Ns, R), conjugated for
 // sign = -1.  Products of twiddles use explicit fused multiply-adds, so that
 // the per-pass tables (formed from unconjugated values) and this run-time
@@ -301,6 +345,26 @@ __device__ __forceinline__ void tw_fill(const TwPass<V>& tw, int k, T sign, V (&
     }
     if constexpr (R == 8) {
         const float4 c = e[2], d = e[3];
+        w[4] = make_float2(c.x, c.y * sign);
+        w[5] = make_float2(c.z, c.w * sign);
+        w[6] = make_float2(d.x, d.y * sign);
+        w[7] = make_float2(d.z, d.w * sign);
+    }
+}
+
+template <typename V, typename T, int N, int Ns, int R>
+__device__ __forceinline__ void tw_fill(const TwRows<V>& tw, int k, T sign, V (&w)[8]) {
+    static_assert(sizeof(V) == 8, "per-pass tables hold complex FP32");
+    const float4* e = reinterpret_cast<const float4*>(tw.p) + 4 * tw_pass_offset<N, Ns>() + k;
+    const float4 a = e[0];
+    w[1] = make_float2(a.z, a.w * sign);
+    if constexpr (R >= 4) {
+        const float4 b = e[Ns];
+        w[2] = make_float2(b.x, b.y * sign);
+        w[3] = make_float2(b.z, b.w * sign);
+    }
+    if constexpr (R == 8) {
+        const float4 c = e[2 * Ns], d = e[3 * Ns];
         w[4] = make_float2(c.x, c.y * sign);
         w[5] = make_float2(c.z, c.w * sign);
         w[6] = make_float2(d.x, d.y * sign);

@@ -174,6 +174,113 @@ __device__ __forceinline__ void fft16_rows_store(typename Elem16<T>::E* sm, int 
     }
 }
 
+// One Stockham pass over two rows per thread: rows at sm and sm + off1 (the
+// same padded layout), the arithmetic of stockham_pass16g element for
+// element, so the transforms are bit-identical to one row per thread.  The
+// two rows share butterfly index k, hence one twiddle set per butterfly, and
+// a CTA needs half as many rounds (and barriers) for the same rows.
+template <int N, int Ns, int R, bool OUT, typename TW>
+__device__ __forceinline__ void stockham_pass16_rows2(float4* __restrict__ sm, int off1, int base, int t, float sign,
+                                                      const TW& tw, float2 (&reg)[2][2][8]) {
+    using V = float2;
+    constexpr int B = 8 / R;
+    constexpr int NB = N / R;
+    constexpr int TPS = N / 8;
+    V v[2][2][8];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+        const int b = t + q * TPS;
+        const int k = b & (Ns - 1);
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                V u[2];
+                unpack16(sm[s * off1 + pad16(base + b + r * NB)], u);
+                v[s][0][q * R + r] = u[0];
+                v[s][1][q * R + r] = u[1];
+            }
+        if (Ns > 1) {
+            V w[8];
+            tw_fill<V, float, N, Ns, R>(tw, k, sign, w);
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+#pragma unroll
+                for (int r = 1; r < R; ++r)
+#pragma unroll
+                    for (int l = 0; l < 2; ++l) v[s][l][q * R + r] = cmul(v[s][l][q * R + r], w[r]);
+        }
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                if constexpr (R == 8) {
+                    bfly8<V, float>(v[s][l], sign);
+                } else if constexpr (R == 4) {
+                    bfly4<V, float>(v[s][l][q * 4 + 0], v[s][l][q * 4 + 1], v[s][l][q * 4 + 2], v[s][l][q * 4 + 3],
+                                    sign);
+                } else {
+                    bfly2<V, float>(v[s][l][q * 2 + 0], v[s][l][q * 2 + 1]);
+                }
+            }
+    }
+    if constexpr (OUT) {
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+            for (int q = 0; q < B; ++q)
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int l = 0; l < 2; ++l) reg[s][l][q + r * B] = v[s][l][q * R + r];
+    } else {
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const int b = t + q * TPS;
+            const int k = b & (Ns - 1);
+            const int base2 = (b / Ns) * Ns * R + k;
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const V u[2] = {v[s][0][q * R + r], v[s][1][q * R + r]};
+                    sm[s * off1 + pad16(base + base2 + r * Ns)] = pack16(u);
+                }
+        }
+        __syncthreads();
+    }
+}
+template <int N, int Ns, typename TW>
+__device__ __forceinline__ void fft16_rows2_passes(float4* sm, int off1, int base, int t, float sign, const TW& tw,
+                                                   float2 (&reg)[2][2][8]) {
+    if constexpr (Ns < N) {
+        constexpr int rem = N / Ns;
+        constexpr int R = rem >= 8 ? 8 : rem;
+        stockham_pass16_rows2<N, Ns, R, Ns * R == N>(sm, off1, base, t, sign, tw, reg);
+        fft16_rows2_passes<N, Ns * R>(sm, off1, base, t, sign, tw, reg);
+    }
+}
+// The 2 spr rows of the padded row buffer (spr = blockDim / (N/8), every thread
+// active), thread (r, t) transforming rows r and r + spr in one round, the last
+// pass storing row p straight to out + p stride.
+template <int N, typename TW>
+__device__ __forceinline__ void fft16_rows2_store(float4* sm, float sign, const TW& tw, float4* __restrict__ out,
+                                                  long stride) {
+    constexpr int TPS = N / 8;
+    const int spr = blockDim.x / TPS;
+    const int r = threadIdx.x / TPS, t = threadIdx.x % TPS;
+    const int off1 = padded_len16(spr * N);
+    float2 rv[2][2][8];
+    fft16_rows2_passes<N, 1>(sm, off1, r * N, t, sign, tw, rv);
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        float4* o = out + (long)(r + s * spr) * stride + t;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) o[(long)m * TPS] = reg_put(rv[s], m);
+    }
+}
+
 // ------------------------------------------------------------------ pass 1
 // One CTA per lattice row: noise and V xi V^dagger for every site into the 8
 // pair rows, then their forward row transforms (up to 512^2; larger rows go to
@@ -522,7 +629,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
 // exponential is held at a time.  Reports non-finite entries in fl.
 // get_u(j) returns the element of inverse-transformed pair row j at the site.
 // get_v(k) returns entry k of the site's old V (by default loaded from e.V).
-template <typename GetU, typename GetV>
+template <bool CHECK = true, typename GetU, typename GetV>
 __device__ __forceinline__ void p3_site_gv(const EventDev& e, GetU get_u, GetV get_v, double se, double2 (&v)[9],
                                            int& fl) {
     double2 v0[9];
@@ -546,9 +653,11 @@ __device__ __forceinline__ void p3_site_gv(const EventDev& e, GetU get_u, GetV g
     xr::expi_ch(m, -1.0);  // exp(-i sqrt(eps) A)
     xr::mul3(tmp, m, v);
     if (e.reunit) xr::reunitarize(v);
+    if constexpr (CHECK) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k)
-        if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+        for (int k = 0; k < 9; ++k)
+            if (!isfinite(v[k].x) || !isfinite(v[k].y)) fl |= JW_FLAG_NAN;
+    }
 }
 
 template <typename GetU>
@@ -664,8 +773,9 @@ __global__ void __launch_bounds__(mx_p3_threads<N>(), mx_p3_blocks<N, MEAS>()) k
 // advanced the step index, so e.step is the next step's noise index.
 template <int N> constexpr int mx_p31_threads() { return mx_p1_threads<N>(); }
 // 8 pair rows, then the old V of one site per thread ([9][threads] double2),
-// copied ahead with cp.async
-template <int N> constexpr size_t mx_p31_smem() { return mx_p1_smem<N>() + v_ahead_bytes<N>(mx_p31_threads<N>()); }
+// copied ahead with cp.async, then the per-pass twiddle table (TwRows)
+template <int N> constexpr size_t mx_p31_tw_offset() { return mx_p1_smem<N>() + v_ahead_bytes<N>(mx_p31_threads<N>()); }
+template <int N> constexpr size_t mx_p31_smem() { return mx_p31_tw_offset<N>() + 64 * (size_t)tw_pass_entries<N>(); }
 // the cluster form (mx_pair): 2 inverse-transformed Q rows and 4 output rows per CTA
 template <int N> constexpr size_t mx_p31p_smem() {
     return 16 * ((size_t)padded_len16(2 * N) + (size_t)padded_len16(4 * N));
@@ -679,6 +789,7 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q, float4* __restrict__ P,
     const float2* __restrict__ tw, int* __restrict__ flags) {
     static_assert(!mx_pair<N>(), "one CTA holds all 8 pair rows");
+    static_assert(mx_p1_blocks<N>() < 2 || mx_p31_smem<N>() <= 113 * 1024, "two CTAs per SM");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sm = reinterpret_cast<float4*>(smem_raw);
     const int x = blockIdx.x, b = blockIdx.y;
@@ -693,9 +804,14 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     for (int i = tid; i < 4 * N; i += TH) cp_async<16>(&sm[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
     va.start();
+    // the per-pass twiddle table (bit-identical to the run-time derivation
+    // from tw), filled while the copies are in flight: the transforms then
+    // read their twiddles from shared memory and form none of them
+    float2* tws = reinterpret_cast<float2*>(smem_raw + mx_p31_tw_offset<N>());
+    tw_rows_fill<float2, N>(tws, tw);
+    const TwRows<float2> twsrc{tws};
     cp_async_wait<1>();  // Q has landed (V may still be in flight)
     __syncthreads();
-    const float2* twsrc = tw;
     fft16_rows<N, 4>(sm, 1.0f, twsrc);
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
@@ -707,12 +823,16 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
             double2 vold[9];
             va.take(y, vold);
             double2 v[9];
-            p3_site_gv(e, [&](int j) { return sm[pad16(j * N + y)]; }, [&](int k) { return vold[k]; }, se, v, fl);
+            p3_site_gv<false>(e, [&](int j) { return sm[pad16(j * N + y)]; }, [&](int k) { return vold[k]; }, se, v,
+                              fl);
+            float fin = 0.0f;  // non-finite iff an entry of the new V is (or exceeds the FP32 range)
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
                 e.V[k * vol + site] = v[k];
                 v32[k] = make_float2((float)v[k].x, (float)v[k].y);
+                fin += v32[k].x + v32[k].y;
             }
+            if (!isfinite(fin)) fl |= JW_FLAG_NAN;
         }
         float z[16];
         langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
@@ -738,7 +858,10 @@ __global__ void __launch_bounds__(mx_p31_threads<N>(), mx_p1_blocks<N>()) k_mix_
     }
     if (fl) atomicOr(flags, fl);
     __syncthreads();
-    fft16_rows_store<float, N>(sm, 8, -1.0f, twsrc, P + (long)b * 8 * vol + (long)x * N, vol);
+    if constexpr (TH == 4 * (N / 8))  // 8 rows, 4 per round: two rows per thread in one round
+        fft16_rows2_store<N>(sm, -1.0f, twsrc, P + (long)b * 8 * vol + (long)x * N, vol);
+    else
+        fft16_rows_store<float, N>(sm, 8, -1.0f, twsrc, P + (long)b * 8 * vol + (long)x * N, vol);
 }
 
 // Pass 3 + next pass 1 where a lattice row needs a cluster of two CTAs
