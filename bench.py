@@ -477,6 +477,58 @@ def uneven_leg(jw, device: int, seed: int):
                     "one server, MV initial conditions included"}
 
 
+def uneven_streams_leg(jw, device: int, steps: int = 40) -> dict:
+    """The C4 batch's kernels without the server: 48 events N in {128, 256,
+    512, 1024} (16/16/12/4), K steps each, (a) as per-size runs back to back on
+    one stream (one engine), (b) the four size groups on four concurrent
+    streams (one engine per size), (c) each size alone.  Whether one launch
+    over mixed sizes could gain: only if a size's own launches leave the GPU
+    idle, which (a) against (b) and the sum of (c) measure."""
+    import torch
+    sizes = [128] * 16 + [256] * 16 + [512] * 12 + [1024] * 4
+
+    def add(eng, i, n):
+        c = [jw.FIXED_COUPLING_CONSTANT, jw.SQRT_COUPLING_CONSTANT][i % 2]
+        return eng.add_event(n, ny_slices=2, mu=0.5 * n, mass=MASS, coupling=c, seed=500 + i,
+                             step=FIXED_STEP if c == jw.FIXED_COUPLING_CONSTANT else STEP)
+
+    def timed(runs):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for eng, ids in runs:
+            eng.step(ids, steps)
+        for eng, _ in runs:
+            if eng.sync() != jw.OK:
+                raise RuntimeError("device error in the uneven-streams leg")
+        torch.cuda.synchronize(device)
+        return time.perf_counter() - t0
+
+    ss = sum(n * n for n in sizes) * steps
+    one = jw.Engine(precision=jw.PRECISION_MIXED, device=device, reunitarize=REUNITARIZE, autotune=True)
+    ids = [add(one, i, n) for i, n in enumerate(sizes)]
+    one.init_mv(ids)
+    one.step(ids, 3)
+    t_one = min(timed([(one, ids)]) for _ in range(3))
+    one.close()
+    per = {}
+    for n in (128, 256, 512, 1024):
+        e = jw.Engine(precision=jw.PRECISION_MIXED, device=device, reunitarize=REUNITARIZE, autotune=True)
+        per[n] = (e, [add(e, i, m) for i, m in enumerate(sizes) if m == n])
+        per[n][0].init_mv(per[n][1])
+        per[n][0].step(per[n][1], 3)
+    t_streams = min(timed(list(per.values())) for _ in range(3))
+    alone = {n: min(timed([per[n]]) for _ in range(3)) for n in per}
+    for e, _ in per.values():
+        e.close()
+    return {"steps": steps, "site_steps": ss,
+            "one_stream_s": t_one, "one_stream_site_steps_per_s": ss / t_one,
+            "concurrent_streams_s": t_streams, "concurrent_streams_site_steps_per_s": ss / t_streams,
+            "alone_s": {str(n): t for n, t in alone.items()}, "sum_alone_s": sum(alone.values()),
+            "alone_site_steps_per_s": {str(n): len(per[n][1]) * n * n * steps / t for n, t in alone.items()},
+            "what": "C4's 48 events without the server: per-size runs on one stream, the size groups on four "
+                    "concurrent streams, each size alone (wall time, device synchronised)"}
+
+
 def c1_leg(jw, device: int):
     """C1, the reference's CPU-runnable case: one FP64 event at 64^2, MV initial
     condition (g^2 mu a = 0.5, m a = 0.02, Ny = 50), 100 fixed-coupling steps
@@ -741,7 +793,7 @@ def main_arm(args):
     dom = max(launched, key=lambda k: launched[k][0])
     tuned = eng.tuning(n_side)
     kernel_of = dict(KIND_KERNEL)
-    if tuned in (16, 24) or (tuned == 0 and n_side <= 512):  # the persistent TMA column pass
+    if tuned in (16, 20, 24) or (tuned == 0 and 64 <= n_side <= 1024):  # the persistent TMA column pass
         kernel_of["pass2"] = "k_mix_pass2_tma"
     name = f"{kernel_of[dom]}<{n_side}>"
     per_launch = {k: ms / cnt for k, (ms, cnt) in launched.items()}
@@ -821,6 +873,7 @@ def main_arm(args):
             "what": "each request of the same mix alone, MV slices + steps through the call-for-call FP64 layer"}
         line["serve"]["vs_fp64_plain_mix"] = line["serve"]["site_steps_per_s"] / mix_rate
         line["uneven"] = uneven_leg(jw, local, 48)
+        line["uneven"]["streams"] = uneven_streams_leg(jw, local)
         # served and uneven throughput as a fraction of the HBM roofline, by the
         # compulsory traffic of a mixed site-step (V read and written in FP64,
         # A and B written and read in FP32: 576 B)

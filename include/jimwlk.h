@@ -378,10 +378,10 @@ jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids, int n, i
 jw_status jw_engine_tuning(jw_engine* e, int N, int* p2_cols);
 /* Fix the column-tile width of size N's column pass (1, 2, 4 or 8 where it
  * fits; 24 = the persistent form with 8-column tiles that move through the
- * tensor memory accelerator, N <= 512, 16 meaning the same; JW_EINVAL
- * otherwise; 0 = the built-in default), for example a width found once by the
- * autotuner and kept; the autotuner then skips that size.  Every choice gives
- * bit-identical events. */
+ * tensor memory accelerator, 64 <= N <= 512, and 20 its 4-column form at
+ * N = 1024, 16 meaning whichever of the two N has; JW_EINVAL otherwise; 0 = the
+ * built-in default), for example a width found once by the autotuner and kept;
+ * the autotuner then skips that size.  Every choice gives bit-identical events. */
 jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
  * event around each kernel launch.  kernel_ms[4] receives the milliseconds

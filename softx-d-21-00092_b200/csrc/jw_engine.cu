@@ -420,8 +420,9 @@ struct LaunchTimes {
 };
 
 // The persistent column pass with tensor-memory-accelerator tile moves
-// (k_mix_pass2_tma, 8-column tiles) is tuning choice kP2Tma + 8 beside the
-// tile widths 1, 2, 4 and 8 of k_mix_pass2; 16 stands for 24.
+// (k_mix_pass2_tma, mx_t2_cols<N>() columns per tile: 8 up to 512^2, 4 at
+// 1024^2) is tuning choice kP2Tma + that width (24 or 20) beside the tile
+// widths 1, 2, 4 and 8 of k_mix_pass2; 16 stands for it.
 constexpr int kP2Tma = 16;
 
 
@@ -450,16 +451,16 @@ void for_each_p2_cols(F&& f) {
     if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, 2>{});
     if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, 4>{});
     if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, 8>{});
-    if constexpr (mx_t2_valid<N, 8>())
-        if (encode_tiled()) f(std::integral_constant<int, kP2Tma + 8>{});
+    if constexpr (mx_t2_valid<N, mx_t2_cols<N>()>())
+        if (encode_tiled()) f(std::integral_constant<int, kP2Tma + mx_t2_cols<N>()>{});
 }
 
 // Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
 // planes per event, Q 4) as a 2D tensor with boxes of C float4 elements (C = 8:
-// 128 bytes) by min(N, 256) rows.  L2 promotion stays at 128 bytes: with
-// 256-byte promotion every row fetched the neighbouring tile's half line too,
-// which the column pass reads much later (measured 1.5x the algorithmic DRAM
-// reads).
+// 128 bytes; 4 columns at 1024^2) by min(N, 256) rows, no swizzle (dense
+// boxes).  L2 promotion stays at 128 bytes: with 256-byte
+// promotion every row fetched the neighbouring tile's half line too, which the
+// column pass reads much later (measured 1.5x the algorithmic DRAM reads).
 template <int N, int C>
 bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
     const cuuint64_t dims[2] = {(cuuint64_t)4 * N, (cuuint64_t)planes * nb * N};
@@ -494,16 +495,23 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
     float4* P = reinterpret_cast<float4*>(g.ws);
     float4* Q = P + (size_t)8 * vol * nb;
     // the default: the persistent TMA form where it is built (measured fastest
-    // at 256^2 and 512^2), else the tile width mx_s2_cols
-    if (cols == 0) cols = (mx_t2_valid<N, 8>() && encode_tiled()) ? kP2Tma + 8 : mx_s2_cols<N>();
-    if (cols == kP2Tma) cols = kP2Tma + 8;
+    // at 256^2, 512^2 and 1024^2), else the tile width mx_s2_cols
+    constexpr int kTma = kP2Tma + mx_t2_cols<N>();
+    if (cols == 0) cols = (mx_t2_valid<N, mx_t2_cols<N>()>() && encode_tiled()) ? kTma : mx_s2_cols<N>();
+    if (cols == kP2Tma) cols = kTma;
     for_each_p2_cols<N>([&](auto c) {
         constexpr int C = decltype(c)::value;
         if (C != cols) return;
         if constexpr (C > kP2Tma) {
             constexpr int TC = C - kP2Tma;
             CUtensorMap pmap, qmap;
-            if (!p2_tensor_map<N, TC>(&pmap, P, nb) || !p2_tensor_map<N, TC>(&qmap, Q, nb, 4)) return;
+            if (!p2_tensor_map<N, TC>(&pmap, P, nb) || !p2_tensor_map<N, TC>(&qmap, Q, nb, 4)) {
+                // no tensor map for these planes: the classic form of the default width
+                constexpr int CC = mx_s2_cols<N>();
+                k_mix_pass2<N, CC><<<dim3(N / CC, 4, nb), mx_s2_threads<N, CC>(), mx_s2_smem<N, CC>(), e->stream>>>(
+                    g.d_ev, d_slots, P, Q, g.tw.d32, advance);
+                return;
+            }
             const int grid = std::min(p2_tma_grid<N, TC>(), nb * 4 * (N / TC));
             k_mix_pass2_tma<N, TC><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC>(), e->stream>>>(
                 g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
@@ -1560,7 +1568,7 @@ JW_EXPORT jw_status jw_engine_step_measure_ensemble(jw_engine* e, const int* ids
 namespace {
 template <int N>
 bool p2_cols_valid_n(int cols) {
-    if (cols == kP2Tma) cols = kP2Tma + 8;
+    if (cols == kP2Tma) cols = kP2Tma + mx_t2_cols<N>();
     bool ok = false;
     for_each_p2_cols<N>([&](auto c) { ok = ok || decltype(c)::value == cols; });
     return ok;

@@ -214,14 +214,14 @@ __device__ __forceinline__ double2 tw_mul(double2 a, double2 b) {
 }
 
 // Per-pass twiddle table in shared memory (TwPass): for every pass with
-// sub-transform size Ns > 1, entry k < Ns holds w^0 .. w^7 of that pass's
-// butterfly (w = exp(+2 pi i k TWS / N)), 8 complex values, so a butterfly
-// reads its twiddles with four 128-bit loads of one 64-byte entry and forms
+// sub-transform size Ns > 1 and radix R, entry k < Ns holds w^0 .. w^(R-1) of
+// that pass's butterfly (w = exp(+2 pi i k TWS / N)), R complex values, so a
+// butterfly reads its twiddles with R/2 128-bit loads of one entry and forms
 // none of them by multiplication.  w, w^2 and w^4 come from the length-N table
 // and w^3, w^5, w^6, w^7 are formed by the same products tw_fill forms at run
 // time (conjugation commutes with them exactly), so every twiddle source gives
-// bit-identical transforms.  Entries of the pass with size Ns start at
-// tw_pass_offset<N, Ns>().
+// bit-identical transforms.  Entries of the pass with size Ns start at value
+// tw_pass_voffset<N, Ns>(); the table holds tw_pass_values<N>() values.
 template <typename V> struct TwPass {
     const V* p;
 };
@@ -238,8 +238,25 @@ __host__ __device__ constexpr int tw_pass_entries() {
     for (int n = 8; n < N; n *= 8) off += n;
     return off;
 }
-// Fill a TwPass table (tw_pass_entries<N>() * 8 values) from the length-N
-// table tw[m] = exp(+2 pi i m / N); all threads of the CTA call it.
+// radix of the pass after sub-transforms of size Ns (8, then the remaining 4 or 2)
+template <int N>
+__host__ __device__ constexpr int tw_radix(int Ns) {
+    return N / Ns >= 8 ? 8 : N / Ns;
+}
+template <int N, int Ns>
+__host__ __device__ constexpr int tw_pass_voffset() {
+    int off = 0;
+    for (int n = 8; n < Ns && n < N; n *= 8) off += n * tw_radix<N>(n);
+    return off;
+}
+template <int N>
+__host__ __device__ constexpr int tw_pass_values() {
+    int off = 0;
+    for (int n = 8; n < N; n *= 8) off += n * tw_radix<N>(n);
+    return off;
+}
+// Fill a TwPass table (tw_pass_values<N>() values) from the length-N table
+// tw[m] = exp(+2 pi i m / N); all threads of the CTA call it.
 template <typename V, int N>
 __device__ __forceinline__ void tw_pass_fill(V* dst, const V* __restrict__ tw) {
     constexpr int E = tw_pass_entries<N>();
@@ -266,7 +283,12 @@ __device__ __forceinline__ void tw_pass_fill(V* dst, const V* __restrict__ tw) {
             w[6] = tw_mul(w[4], w[2]);
             w[7] = tw_mul(w[4], w[3]);
         }
-        for (int r = 0; r < 8; ++r) dst[e * 8 + r] = w[r];
+        // entries before this one: the earlier passes' values, then k entries of R
+        int voff = 0;
+        for (int n = 8; n < Ns; n *= 8) voff += n * (N / n >= 8 ? 8 : N / n);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if (r < R) dst[voff + k * R + r] = w[r];
     }
 }
 
@@ -335,7 +357,7 @@ __device__ __forceinline__ void tw_fill(const TW& tw, int k, T sign, V (&w)[8]) 
 template <typename V, typename T, int N, int Ns, int R>
 __device__ __forceinline__ void tw_fill(const TwPass<V>& tw, int k, T sign, V (&w)[8]) {
     static_assert(sizeof(V) == 8, "per-pass tables hold complex FP32");
-    const float4* e = reinterpret_cast<const float4*>(tw.p + (tw_pass_offset<N, Ns>() + k) * 8);
+    const float4* e = reinterpret_cast<const float4*>(tw.p + tw_pass_voffset<N, Ns>() + k * R);
     const float4 a = e[0];
     w[1] = make_float2(a.z, a.w * sign);
     if constexpr (R >= 4) {

@@ -473,19 +473,28 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // memory (per-pass table) and the kernel-table values of the thread's elements
 // stay in registers while the column tile does not change.  The arithmetic is
 // k_mix_pass2's, element for element, so Q is bit-identical.  Built for
-// N <= 512 (three 64 KB tiles at 512^2).
+// 64 <= N <= 1024: 8-column tiles up to 512^2 (64 KB at 512^2), then 64 KB
+// tiles of 4 columns at 1024^2.
 template <int N, int C> constexpr int mx_t2_threads() { return C * (N / 8); }
 template <int N, int C> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * C * N; }
 template <int N, int C> constexpr size_t mx_t2_smem() {
-    return 3 * mx_t2_tile_bytes<N, C>() + 1024 + 64 * (size_t)tw_pass_entries<N>();
+    return 3 * mx_t2_tile_bytes<N, C>() + 1024 + 8 * (size_t)tw_pass_values<N>();
 }
+// tile width of the persistent form: 8 columns up to 512^2, then 4 at 1024^2
+// (64 KB tiles, so that three still fit).  Every tile is the dense [N][C] box
+// layout of the tensor map (no swizzle).  4-column rows are 64 bytes, so the
+// first pass's stores of rows 8 b + r and 8 (b + 1) + r meet in one bank
+// (2-way conflict); measured 1.33 ms per 16 x 1024^2 launch against 1.47 ms
+// for the best classic width.  At 2048^2 the 2-column form (4-way conflicts)
+// measured 2.68 ms against 1.77 ms classic and is not built.
+template <int N> constexpr int mx_t2_cols() { return N <= 512 ? 8 : 4096 / N; }
 template <int N, int C> constexpr int mx_t2_blocks() {
     return (int)((227 * 1024) / (mx_t2_smem<N, C>() + 1024)) < 1024 / mx_t2_threads<N, C>()
                ? (int)((227 * 1024) / (mx_t2_smem<N, C>() + 1024))
                : 1024 / mx_t2_threads<N, C>();
 }
 template <int N, int C> constexpr bool mx_t2_valid() {
-    return C == 8 && N >= 64 && N <= 512 && mx_t2_smem<N, C>() <= 227 * 1024;
+    return C == mx_t2_cols<N>() && N >= 64 && N <= 1024 && mx_t2_smem<N, C>() <= 227 * 1024;
 }
 
 template <int N, int C>
@@ -598,7 +607,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         __syncthreads();
         float4* ot = buf(yb);
 #pragma unroll
-        for (int q = 0; q < PER; ++q) ot[(r0 + q * RSTEP) * C + cc] = reg_put(w, q);
+        for (int q = 0; q < PER; ++q) ot[cidx(r0 + q * RSTEP)] = reg_put(w, q);
         fence_proxy_async_smem();
         __syncthreads();
         if (tid == 0) {

@@ -74,11 +74,12 @@ def test_chunked_launch_groups_match_one_group(jw):
     b.close()
 
 
-@pytest.mark.parametrize("N", [64, 512, 2048])
+@pytest.mark.parametrize("N", [64, 512, 1024, 2048])
 def test_autotuner_choice_does_not_change_results(jw, N):
     """The autotuner picks a valid column-tile width on the first run of a size,
     and every width gives the same lattice bit for bit."""
-    events = {64: 3, 512: 2, 2048: 1}[N]
+    events = {64: 3, 512: 2, 1024: 1, 2048: 1}[N]
+    tma = 16 + (8 if N <= 512 else 4)  # the persistent form with tensor-memory-accelerator tile moves
     eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
     eng.step(ids, 4)
     ref = [eng.get_V(i) for i in ids]
@@ -91,15 +92,15 @@ def test_autotuner_choice_does_not_change_results(jw, N):
     tuned.step(tids, 4)
     assert tuned.sync() == jw.OK
     chosen = tuned.tuning(N)
-    assert chosen in (1, 2, 4, 8, 24)
+    assert chosen in (1, 2, 4, 8, tma)
     for a, i in zip(ref, tids):
         assert np.array_equal(a, tuned.get_V(i))
     assert all(tuned.steps_taken(i) == 4 for i in tids)
     tuned.close()
     widths = [c for c in (1, 2, 4, 8) if c <= N and c * (N // 8) <= 1024 and
               2 * 16 * (N * c + (0 if c >= 8 else (N // 8) * c)) <= 227 * 1024]
-    if 64 <= N <= 512:
-        widths.append(24)  # the persistent form with tensor-memory-accelerator tile moves
+    if 64 <= N <= 1024:
+        widths.append(tma)
     assert chosen in widths
     for c in widths:
         eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
@@ -115,17 +116,19 @@ def test_autotuner_choice_does_not_change_results(jw, N):
     eng.close()
 
 
-@pytest.mark.parametrize("N,events", [(64, 3), (256, 2), (512, 3)])
+@pytest.mark.parametrize("N,events", [(64, 3), (256, 2), (512, 3), (1024, 1)])
 def test_persistent_column_pass_is_bitwise_identical(jw, N, events):
-    """The persistent column pass (tuning choice 24, or 16: tensor-memory-
-    accelerator tile loads and stores, per-pass twiddle table) gives the default column
-    pass's lattices bit for bit, over runs long enough for graph replay, with
-    more work items than persistent CTAs."""
+    """The persistent column pass (tuning choice 24, or 20 with 4-column tiles at
+    1024^2, or 16 for either: tensor-memory-accelerator tile loads and stores,
+    per-pass twiddle table) gives the classic column pass's lattices bit for
+    bit, over runs long enough for graph replay, with more work items than
+    persistent CTAs."""
     eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+    eng.set_tuning(N, 4 if N >= 1024 else 8)  # a classic width
     eng.step(ids, 6)
     ref = [eng.get_V(i) for i in ids]
     eng.close()
-    for choice in (16, 24):
+    for choice in (16, 24 if N <= 512 else 20):
         eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
         eng.set_tuning(N, choice)
         eng.step(ids, 6)
@@ -133,7 +136,7 @@ def test_persistent_column_pass_is_bitwise_identical(jw, N, events):
         for a, i in zip(ref, ids):
             assert np.array_equal(a, eng.get_V(i)), choice
         eng.close()
-    eng, ids = make(jw, 1024, 1, jw.PRECISION_MIXED)
-    with pytest.raises(RuntimeError):
-        eng.set_tuning(1024, 16)
+    eng, ids = make(jw, 2048, 1, jw.PRECISION_MIXED)
+    with pytest.raises(RuntimeError):  # not built at 2048^2
+        eng.set_tuning(2048, 16)
     eng.close()
