@@ -272,10 +272,13 @@ typedef struct jw_engine_options {
     int max_batch;        /* events advanced per launch group (0 = all) */
     size_t max_batch_sites; /* and at most this many lattice sites per launch group (0 = no limit;
                                at least one event), which also bounds each size's workspace */
-    int autotune;         /* nonzero: the first mixed-precision run of each lattice size times
+    int autotune;         /* 1: the first mixed-precision run of each lattice size times
                              every compiled column-tile width of the column pass on its own
                              workspace and keeps the fastest (jw_engine_tuning); results do
-                             not depend on the choice.  0: the built-in default */
+                             not depend on the choice.  2: the column transforms' radix
+                             schedules compete as well (radix-2/4 pass first or last, for N
+                             that has one); a schedule rounds differently, so results then
+                             depend on the recorded choice.  0: the built-in default */
 } jw_engine_options;
 
 typedef struct jw_event_desc {
@@ -381,7 +384,11 @@ jw_status jw_engine_tuning(jw_engine* e, int N, int* p2_cols);
  * tensor memory accelerator, 64 <= N <= 512, and 20 its 4-column form at
  * N = 1024, 16 meaning whichever of the two N has; JW_EINVAL otherwise; 0 = the
  * built-in default), for example a width found once by the autotuner and kept;
- * the autotuner then skips that size.  Every choice gives bit-identical events. */
+ * the autotuner then skips that size.  Every such choice gives bit-identical
+ * events.  Adding 32 to a choice selects the radix-first schedule of the column
+ * transforms (N = 16, 32, 128, 256, 1024, 2048 only): its events are
+ * bit-identical among its own widths, and differ from the default schedule's
+ * by FP32 rounding. */
 jw_status jw_engine_set_tuning(jw_engine* e, int N, int p2_cols);
 /* nsteps Langevin steps of the listed events (one lattice size) with a CUDA
  * event around each kernel launch.  kernel_ms[4] receives the milliseconds

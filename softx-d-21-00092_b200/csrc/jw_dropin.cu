@@ -296,8 +296,8 @@ JW_EXPORT jw_status jw_context_create(const jw_config* cfg, int device, jw_conte
     c->device = device;
     c->N = cfg->Nx;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        twiddles_create(c->N, &c->tw) != cudaSuccess || cudaMalloc(&c->d_flags, sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->d_flags, 0, sizeof(int)) != cudaSuccess ||
+        twiddles_create(c->N, &c->tw, c->stream) != cudaSuccess || cudaMalloc(&c->d_flags, sizeof(int)) != cudaSuccess ||
+        cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream) != cudaSuccess ||
         cudaMalloc(&c->d_tmp, sizeof(double2) * (size_t)c->N * c->N) != cudaSuccess) {
         jw_context_destroy(c);
         return JW_ENOMEM;
@@ -330,7 +330,8 @@ JW_EXPORT jw_status jw_context_sync(jw_context* c) {
     JW_CUDA(cudaStreamSynchronize(c->stream));
     int flags = 0;
     JW_CUDA(cudaMemcpy(&flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flags) JW_CUDA(cudaMemset(c->d_flags, 0, sizeof(int)));
+    // on the stream: a legacy-stream memset is not ordered with later kernels
+    if (flags) JW_CUDA(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
     return flags_to_status(flags);
 }
 

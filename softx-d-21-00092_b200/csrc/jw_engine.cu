@@ -357,7 +357,7 @@ jw_status group_get(jw_engine* e, int N, Group** out) {
     }
     auto g = std::make_unique<Group>();
     g->N = N;
-    JW_CUDA(twiddles_create(N, &g->tw));
+    JW_CUDA(twiddles_create(N, &g->tw, e->stream));
     *out = g.get();
     e->groups[N] = std::move(g);
     return JW_OK;
@@ -444,15 +444,29 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
+// The radix schedule of the column transforms is part of the choice: choice
+// c + kRadixFirst (c one of the above) runs the column transforms with the
+// radix-2 or radix-4 pass first (fft_radix, schedule 1), for the sizes that
+// have one (N = 16, 32, 128, 256, 1024, 2048).  Schedule 1 rounds differently,
+// so it is tuned only with jw_engine_options.autotune = 2 and a run's lattices
+// depend on the recorded choice (jw_engine_tuning / jw_engine_set_tuning).
+constexpr int kRadixFirst = 32;
+
 // f(std::integral_constant<int, C>) for every valid pass-2 tuning choice C.
+template <int N, int S, typename F>
+void for_each_p2_cols_s(F&& f) {
+    constexpr int B = S * kRadixFirst;
+    if constexpr (mx_s2_valid<N, 1>()) f(std::integral_constant<int, B + 1>{});
+    if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, B + 2>{});
+    if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, B + 4>{});
+    if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, B + 8>{});
+    if constexpr (mx_t2_valid<N, mx_t2_cols<N>()>())
+        if (encode_tiled()) f(std::integral_constant<int, B + kP2Tma + mx_t2_cols<N>()>{});
+}
 template <int N, typename F>
 void for_each_p2_cols(F&& f) {
-    if constexpr (mx_s2_valid<N, 1>()) f(std::integral_constant<int, 1>{});
-    if constexpr (mx_s2_valid<N, 2>()) f(std::integral_constant<int, 2>{});
-    if constexpr (mx_s2_valid<N, 4>()) f(std::integral_constant<int, 4>{});
-    if constexpr (mx_s2_valid<N, 8>()) f(std::integral_constant<int, 8>{});
-    if constexpr (mx_t2_valid<N, mx_t2_cols<N>()>())
-        if (encode_tiled()) f(std::integral_constant<int, kP2Tma + mx_t2_cols<N>()>{});
+    for_each_p2_cols_s<N, 0>(f);
+    if constexpr (fft_has_rem<N>()) for_each_p2_cols_s<N, 1>(f);
 }
 
 // Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
@@ -473,15 +487,15 @@ bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
 }
 
 // CTAs of the persistent column pass: every SM filled to its occupancy.
-template <int N, int C>
+template <int N, int C, int S>
 int p2_tma_grid() {
     static int grid = 0;
     if (grid == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass2_tma<N, C>, mx_t2_threads<N, C>(),
-                                                      mx_t2_smem<N, C>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix_pass2_tma<N, C, S>, mx_t2_threads<N, C>(),
+                                                      mx_t2_smem<N, C, S>());
         grid = std::max(1, sms * std::max(1, per_sm));
     }
     return grid;
@@ -499,24 +513,27 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
     constexpr int kTma = kP2Tma + mx_t2_cols<N>();
     if (cols == 0) cols = (mx_t2_valid<N, mx_t2_cols<N>()>() && encode_tiled()) ? kTma : mx_s2_cols<N>();
     if (cols == kP2Tma) cols = kTma;
+    if (cols == kRadixFirst + kP2Tma) cols = kRadixFirst + kTma;
     for_each_p2_cols<N>([&](auto c) {
-        constexpr int C = decltype(c)::value;
-        if (C != cols) return;
+        constexpr int CS = decltype(c)::value;
+        if (CS != cols) return;
+        constexpr int S = CS >= kRadixFirst ? 1 : 0;
+        constexpr int C = CS - S * kRadixFirst;
         if constexpr (C > kP2Tma) {
             constexpr int TC = C - kP2Tma;
             CUtensorMap pmap, qmap;
             if (!p2_tensor_map<N, TC>(&pmap, P, nb) || !p2_tensor_map<N, TC>(&qmap, Q, nb, 4)) {
                 // no tensor map for these planes: the classic form of the default width
                 constexpr int CC = mx_s2_cols<N>();
-                k_mix_pass2<N, CC><<<dim3(N / CC, 4, nb), mx_s2_threads<N, CC>(), mx_s2_smem<N, CC>(), e->stream>>>(
-                    g.d_ev, d_slots, P, Q, g.tw.d32, advance);
+                k_mix_pass2<N, CC, S><<<dim3(N / CC, 4, nb), mx_s2_threads<N, CC>(), mx_s2_smem<N, CC>(),
+                                        e->stream>>>(g.d_ev, d_slots, P, Q, g.tw.d32, advance);
                 return;
             }
-            const int grid = std::min(p2_tma_grid<N, TC>(), nb * 4 * (N / TC));
-            k_mix_pass2_tma<N, TC><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC>(), e->stream>>>(
+            const int grid = std::min(p2_tma_grid<N, TC, S>(), nb * 4 * (N / TC));
+            k_mix_pass2_tma<N, TC, S><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC, S>(), e->stream>>>(
                 g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
         } else {
-            k_mix_pass2<N, C><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
+            k_mix_pass2<N, C, S><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
                 g.d_ev, d_slots, P, Q, g.tw.d32, advance);
         }
     });
@@ -535,12 +552,14 @@ void mix_configure() {
         cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
     }
     for_each_p2_cols<N>([](auto c) {
-        constexpr int C = decltype(c)::value;
+        constexpr int CS = decltype(c)::value;
+        constexpr int S = CS >= kRadixFirst ? 1 : 0;
+        constexpr int C = CS - S * kRadixFirst;
         if constexpr (C > kP2Tma)
-            cudaFuncSetAttribute(k_mix_pass2_tma<N, C - kP2Tma>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)mx_t2_smem<N, C - kP2Tma>());
+            cudaFuncSetAttribute(k_mix_pass2_tma<N, C - kP2Tma, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_t2_smem<N, C - kP2Tma, S>());
         else
-            cudaFuncSetAttribute(k_mix_pass2<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_mix_pass2<N, C, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)mx_s2_smem<N, C>());
     });
     cudaFuncSetAttribute(k_mix_pass3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p3_smem<N>());
@@ -609,6 +628,7 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
 // The autotuner: every valid pass-2 tile width runs 1 + 3 times on this launch
 // group's workspace (the step index frozen; pass 2 only maps P to Q, which the
 // run then recomputes), and the fastest by CUDA events is kept for the size.
+// With autotune = 2 the radix-first schedules (kRadixFirst) compete too.
 template <int N>
 cudaError_t tune_mix(jw_engine* e, Group& g, const int* d_slots, int nb) {
     float best = 0.0f;
@@ -617,6 +637,7 @@ cudaError_t tune_mix(jw_engine* e, Group& g, const int* d_slots, int nb) {
     for_each_p2_cols<N>([&](auto c) {
         constexpr int C = decltype(c)::value;
         if (ce != cudaSuccess) return;
+        if (C >= kRadixFirst && e->opt.autotune < 2) return;  // results must not depend on the choice
         cudaEvent_t a = nullptr, b = nullptr;
         cudaEventCreate(&a);
         cudaEventCreate(&b);
@@ -1012,7 +1033,8 @@ JW_EXPORT jw_status jw_engine_create(const jw_engine_options* opt, int device, j
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess ||
         cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&e->d_flags, sizeof(int)) != cudaSuccess || cudaMemset(e->d_flags, 0, sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&e->d_flags, sizeof(int)) != cudaSuccess ||
+        cudaMemsetAsync(e->d_flags, 0, sizeof(int), e->stream) != cudaSuccess) {
         jw_engine_destroy(e);
         return JW_ECUDA;
     }
@@ -1046,7 +1068,8 @@ JW_EXPORT jw_status jw_engine_sync(jw_engine* e) {
     JW_CUDA(cudaStreamSynchronize(e->stream));
     int flags = 0;
     JW_CUDA(cudaMemcpy(&flags, e->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flags) JW_CUDA(cudaMemset(e->d_flags, 0, sizeof(int)));
+    // on the stream: a legacy-stream memset is not ordered with later kernels
+    if (flags) JW_CUDA(cudaMemsetAsync(e->d_flags, 0, sizeof(int), e->stream));
     return flags_to_status(flags);
 }
 
@@ -1569,6 +1592,7 @@ namespace {
 template <int N>
 bool p2_cols_valid_n(int cols) {
     if (cols == kP2Tma) cols = kP2Tma + mx_t2_cols<N>();
+    if (cols == kRadixFirst + kP2Tma) cols = kRadixFirst + kP2Tma + mx_t2_cols<N>();
     bool ok = false;
     for_each_p2_cols<N>([&](auto c) { ok = ok || decltype(c)::value == cols; });
     return ok;

@@ -13,7 +13,11 @@ namespace jw {
 
 bool supported_n(int N) { return N >= 8 && N <= 2048 && (N & (N - 1)) == 0; }
 
-cudaError_t twiddles_create(int N, Twiddles* tw) {
+// The tables are copied on stream s (stream-ordered: a kernel queued on s
+// after this call reads the finished tables; a synchronous cudaMemcpy from
+// pageable memory may return before its DMA lands, unordered with a
+// non-blocking stream).
+cudaError_t twiddles_create(int N, Twiddles* tw, cudaStream_t s) {
     std::vector<double2> h64(N);
     std::vector<float2> h32(N);
     for (int m = 0; m < N; ++m) {
@@ -26,9 +30,11 @@ cudaError_t twiddles_create(int N, Twiddles* tw) {
     if (e != cudaSuccess) return e;
     e = cudaMalloc(&tw->d32, sizeof(float2) * N);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpy(tw->d64, h64.data(), sizeof(double2) * N, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(tw->d64, h64.data(), sizeof(double2) * N, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return e;
-    return cudaMemcpy(tw->d32, h32.data(), sizeof(float2) * N, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(tw->d32, h32.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);  // the host tables go out of scope
 }
 
 void twiddles_destroy(Twiddles* tw) {

@@ -221,8 +221,22 @@ __device__ __forceinline__ double2 tw_mul(double2 a, double2 b) {
 // and w^3, w^5, w^6, w^7 are formed by the same products tw_fill forms at run
 // time (conjugation commutes with them exactly), so every twiddle source gives
 // bit-identical transforms.  Entries of the pass with size Ns start at value
-// tw_pass_voffset<N, Ns>(); the table holds tw_pass_values<N>() values.
-template <typename V> struct TwPass {
+// tw_pass_voffset<N, Ns, S>(); the table holds tw_pass_values<N, S>() values
+// (S: the radix schedule, below).
+// Radix schedules.  A transform of N = 8^a r points (r = 1, 2 or 4) takes
+// a radix-8 passes and one radix-r pass.  Schedule 0 runs the radix-8 passes
+// first and the radix-r pass last (the default of every transform); schedule
+// 1 runs the radix-r pass first.  The two round differently, so a schedule is
+// a tuning choice that must be recorded with the results.
+__host__ __device__ constexpr int lg2c(int n) { return n <= 1 ? 0 : 1 + lg2c(n / 2); }
+template <int N, int S>
+__host__ __device__ constexpr int fft_radix(int Ns) {
+    return (S == 1 && Ns == 1 && lg2c(N) % 3 != 0 && N > 8) ? (1 << (lg2c(N) % 3)) : (N / Ns >= 8 ? 8 : N / Ns);
+}
+// N has a radix-r pass (r = 2 or 4), so schedule 1 differs from schedule 0
+template <int N> constexpr bool fft_has_rem() { return N > 8 && lg2c(N) % 3 != 0; }
+
+template <typename V, int S = 0> struct TwPass {
     const V* p;
 };
 template <int N, int Ns>
@@ -238,36 +252,39 @@ __host__ __device__ constexpr int tw_pass_entries() {
     for (int n = 8; n < N; n *= 8) off += n;
     return off;
 }
-// radix of the pass after sub-transforms of size Ns (8, then the remaining 4 or 2)
-template <int N>
-__host__ __device__ constexpr int tw_radix(int Ns) {
-    return N / Ns >= 8 ? 8 : N / Ns;
-}
-template <int N, int Ns>
+// Offsets of the compact table of schedule S: the twiddled passes (Ns > 1) in
+// order, each with Ns entries of R values.
+template <int N, int Ns, int S = 0>
 __host__ __device__ constexpr int tw_pass_voffset() {
     int off = 0;
-    for (int n = 8; n < Ns && n < N; n *= 8) off += n * tw_radix<N>(n);
+    for (int n = fft_radix<N, S>(1); n < Ns && n < N; n *= fft_radix<N, S>(n)) off += n * fft_radix<N, S>(n);
     return off;
 }
-template <int N>
+template <int N, int S = 0>
 __host__ __device__ constexpr int tw_pass_values() {
     int off = 0;
-    for (int n = 8; n < N; n *= 8) off += n * tw_radix<N>(n);
+    for (int n = fft_radix<N, S>(1); n < N; n *= fft_radix<N, S>(n)) off += n * fft_radix<N, S>(n);
     return off;
 }
-// Fill a TwPass table (tw_pass_values<N>() values) from the length-N table
+template <int N, int S = 0>
+__host__ __device__ constexpr int tw_pass_entries_s() {
+    int off = 0;
+    for (int n = fft_radix<N, S>(1); n < N; n *= fft_radix<N, S>(n)) off += n;
+    return off;
+}
+// Fill a TwPass table (tw_pass_values<N, S>() values) from the length-N table
 // tw[m] = exp(+2 pi i m / N); all threads of the CTA call it.
-template <typename V, int N>
+template <typename V, int N, int S = 0>
 __device__ __forceinline__ void tw_pass_fill(V* dst, const V* __restrict__ tw) {
-    constexpr int E = tw_pass_entries<N>();
+    constexpr int E = tw_pass_entries_s<N, S>();
     for (int e = threadIdx.x; e < E; e += blockDim.x) {
-        int Ns = 8, base = 0;
+        int Ns = fft_radix<N, S>(1), base = 0, voff = 0;
         while (e >= base + Ns) {
             base += Ns;
-            Ns *= 8;
+            voff += Ns * fft_radix<N, S>(Ns);
+            Ns *= fft_radix<N, S>(Ns);
         }
-        const int rem = N / Ns;
-        const int R = rem >= 8 ? 8 : rem;
+        const int R = fft_radix<N, S>(Ns);
         const int k = e - base;
         const int TWS = N / (Ns * R);
         V w[8];
@@ -283,9 +300,7 @@ __device__ __forceinline__ void tw_pass_fill(V* dst, const V* __restrict__ tw) {
             w[6] = tw_mul(w[4], w[2]);
             w[7] = tw_mul(w[4], w[3]);
         }
-        // entries before this one: the earlier passes' values, then k entries of R
-        int voff = 0;
-        for (int n = 8; n < Ns; n *= 8) voff += n * (N / n >= 8 ? 8 : N / n);
+        // entries before this one: the earlier passes' values (voff), then k entries of R
 #pragma unroll
         for (int r = 0; r < 8; ++r)
             if (r < R) dst[voff + k * R + r] = w[r];
@@ -354,10 +369,10 @@ __device__ __forceinline__ void tw_fill(const TW& tw, int k, T sign, V (&w)[8]) 
         w[7] = tw_mul(w[4], w[3]);
     }
 }
-template <typename V, typename T, int N, int Ns, int R>
-__device__ __forceinline__ void tw_fill(const TwPass<V>& tw, int k, T sign, V (&w)[8]) {
+template <typename V, typename T, int N, int Ns, int R, int S>
+__device__ __forceinline__ void tw_fill(const TwPass<V, S>& tw, int k, T sign, V (&w)[8]) {
     static_assert(sizeof(V) == 8, "per-pass tables hold complex FP32");
-    const float4* e = reinterpret_cast<const float4*>(tw.p + tw_pass_voffset<N, Ns>() + k * R);
+    const float4* e = reinterpret_cast<const float4*>(tw.p + tw_pass_voffset<N, Ns, S>() + k * R);
     const float4 a = e[0];
     w[1] = make_float2(a.z, a.w * sign);
     if constexpr (R >= 4) {
@@ -603,24 +618,25 @@ __device__ __forceinline__ void fft16g(typename Elem16<T>::E* sm, const IdxL0& i
     fft16g_passes<T, N, 1, IN, OUT>(sm, idxL0, idx, t, active, sign, tw, reg, sync0, sync);
 }
 
-template <typename T, int N, int Ns, bool IN, bool OUT, typename IdxF, typename TW>
+template <typename T, int N, int Ns, bool IN, bool OUT, int S, typename IdxF, typename TW>
 __device__ __forceinline__ void fft16x_passes(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
                                               const TW& tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
     if constexpr (Ns < N) {
-        constexpr int rem = N / Ns;
-        constexpr int R = rem >= 8 ? 8 : rem;
+        constexpr int R = fft_radix<N, S>(Ns);
         stockham_pass16x<T, N, Ns, R, IN && Ns == 1, OUT && Ns * R == N>(sm, idx, t, active, sign, tw, reg);
-        fft16x_passes<T, N, Ns * R, IN, OUT>(sm, idx, t, active, sign, tw, reg);
+        fft16x_passes<T, N, Ns * R, IN, OUT, S>(sm, idx, t, active, sign, tw, reg);
     }
 }
 
 // fft16 with the first pass reading reg (IN) and/or the last pass writing reg
-// (OUT) instead of sm; sm still carries the passes in between.
-template <typename T, int N, bool IN, bool OUT, typename IdxF, typename TW>
+// (OUT) instead of sm; sm still carries the passes in between.  S is the
+// radix schedule (fft_radix).  Whatever the last radix, thread t ends holding
+// elements t + m N/8, so the hand-off works for both schedules.
+template <typename T, int N, bool IN, bool OUT, int S = 0, typename IdxF, typename TW>
 __device__ __forceinline__ void fft16x(typename Elem16<T>::E* sm, const IdxF& idx, int t, bool active, T sign,
                                        const TW& tw, C2<T> (&reg)[Elem16<T>::VL][8]) {
     static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two N >= 8");
-    fft16x_passes<T, N, 1, IN, OUT>(sm, idx, t, active, sign, tw, reg);
+    fft16x_passes<T, N, 1, IN, OUT, S>(sm, idx, t, active, sign, tw, reg);
 }
 
 __device__ __forceinline__ void reg_get(const float4& e, float2 (&reg)[2][8], int m) {

@@ -35,7 +35,7 @@ struct Twiddles {
     double2* d64 = nullptr;
     float2* d32 = nullptr;
 };
-cudaError_t twiddles_create(int N, Twiddles* tw);
+cudaError_t twiddles_create(int N, Twiddles* tw, cudaStream_t s);
 void twiddles_destroy(Twiddles* tw);
 
 bool supported_n(int N);

@@ -397,7 +397,7 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p1_threads<N>(), 
 // holds rows r0 + m N/8 of column cc between the transforms (fft16x), so the
 // plane-j transform starts from global loads, the kernel product and the
 // inverse start from registers and the inverse ends in the store.
-template <int N, int C>
+template <int N, int C, int S = 0>
 __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k_mix_pass2(EventDev* __restrict__ ev,
                                                                    const int* __restrict__ slots,
                                                                    const float4* __restrict__ P,
@@ -436,19 +436,19 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
         ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
     }
     // (i kx) X + (i ky) Y, X and Y the two halves of a plane element
-    fft16x<float, N, true, true>(ta, cidx, r0, true, -1.0f, tw, ra);
+    fft16x<float, N, true, true, S>(ta, cidx, r0, true, -1.0f, tw, ra);
     float2 w[2][8];
 #pragma unroll
     for (int q = 0; q < PER; ++q)
         w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
     cp_async_wait<0>();
     __syncthreads();
-    fft16x<float, N, false, true>(tb, cidx, r0, true, -1.0f, tw, ra);
+    fft16x<float, N, false, true, S>(tb, cidx, r0, true, -1.0f, tw, ra);
 #pragma unroll
     for (int q = 0; q < PER; ++q)
         w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
     // every thread has passed a barrier since its last read of ta
-    fft16x<float, N, true, true>(ta, cidx, r0, true, 1.0f, tw, w);
+    fft16x<float, N, true, true, S>(ta, cidx, r0, true, 1.0f, tw, w);
     float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
 #pragma unroll
     for (int q = 0; q < PER; ++q) out[(long)q * RSTEP * N] = reg_put(w, q);
@@ -477,8 +477,8 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
 // tiles of 4 columns at 1024^2.
 template <int N, int C> constexpr int mx_t2_threads() { return C * (N / 8); }
 template <int N, int C> constexpr size_t mx_t2_tile_bytes() { return (size_t)16 * C * N; }
-template <int N, int C> constexpr size_t mx_t2_smem() {
-    return 3 * mx_t2_tile_bytes<N, C>() + 1024 + 8 * (size_t)tw_pass_values<N>();
+template <int N, int C, int S = 0> constexpr size_t mx_t2_smem() {
+    return 3 * mx_t2_tile_bytes<N, C>() + 1024 + 8 * (size_t)tw_pass_values<N, S>();
 }
 // tile width of the persistent form: 8 columns up to 512^2, then 4 at 1024^2
 // (64 KB tiles, so that three still fit).  Every tile is the dense [N][C] box
@@ -497,7 +497,7 @@ template <int N, int C> constexpr bool mx_t2_valid() {
     return C == mx_t2_cols<N>() && N >= 64 && N <= 1024 && mx_t2_smem<N, C>() <= 227 * 1024;
 }
 
-template <int N, int C>
+template <int N, int C, int S = 0>
 __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k_mix_pass2_tma(
     EventDev* __restrict__ ev, const int* __restrict__ slots, const float2* __restrict__ tw, int nb, int advance,
     int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap qmap) {
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
     const unsigned align_pad = (1024u - (smem_addr(smem_raw) & 1023u)) & 1023u;
     float4* base = reinterpret_cast<float4*>(smem_raw + align_pad);
     float2* tws = reinterpret_cast<float2*>(base + (size_t)3 * N * C);
-    const TwPass<float2> twsrc{tws};
+    const TwPass<float2, S> twsrc{tws};
     const int tid = threadIdx.x;
     const int cc = tid % C, r0 = tid / C;
     const ColIdx16<C> cidx{cc};  // dense [N][C] tile, the TMA box layout
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
         mbar_init_fence();
     }
-    tw_pass_fill<float2, N>(tws, tw);
+    tw_pass_fill<float2, N, S>(tws, tw);
     __syncthreads();
     auto buf = [&](int bi) { return base + (size_t)bi * N * C; };
     // plane `half` (0: P[j], 1: P[4 + j]) of work item `it` into buffer bi (thread 0)
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
         parity ^= 1u << xb;
         pending &= ~(1u << xb);
-        fft16x<float, N, false, true>(buf(xb), cidx, r0, true, -1.0f, twsrc, ra);
+        fft16x<float, N, false, true, S>(buf(xb), cidx, r0, true, -1.0f, twsrc, ra);
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
@@ -597,12 +597,12 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         timed_out |= !mbar_wait_bounded(&bar[yb], (parity >> yb) & 1u);
         parity ^= 1u << yb;
         pending &= ~(1u << yb);
-        fft16x<float, N, false, true>(buf(yb), cidx, r0, true, -1.0f, twsrc, ra);
+        fft16x<float, N, false, true, S>(buf(yb), cidx, r0, true, -1.0f, twsrc, ra);
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
         // the inverse's first pass synchronises before it writes yb
-        fft16x<float, N, true, true>(buf(yb), cidx, r0, true, 1.0f, twsrc, w);
+        fft16x<float, N, true, true, S>(buf(yb), cidx, r0, true, 1.0f, twsrc, w);
         // the result tile into yb (dense [N][8] elements, the store box's layout)
         __syncthreads();
         float4* ot = buf(yb);

@@ -625,7 +625,10 @@ jw_status ensure_table(jw_context* c, int rr, int coupling, int kernel) {
     // the previous table may still be read by work queued on the stream
     JW_CUDA(cudaStreamSynchronize(c->stream));
     c->pos_key[0] = c->pos_key[1] = c->pos_key[2] = -1;
-    JW_CUDA(cudaMemcpy(c->d_pos_tab, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice));
+    // on the context's stream: a synchronous cudaMemcpy from pageable memory can
+    // return before its DMA lands and is not ordered with the (non-blocking)
+    // stream, so the transform below could read a partly copied table
+    JW_CUDA(cudaMemcpyAsync(c->d_pos_tab, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice, c->stream));
     JW_CUDA(fft2d_planes<double>(c->d_pos_tab, 2, N, 1, 1.0, c->tw, c->stream));
     c->pos_key[0] = rr;
     c->pos_key[1] = coupling;
@@ -743,8 +746,8 @@ JW_EXPORT jw_status jw_set_correlations_for_coupling_constant(jw_context* c, jw_
             const double cc = f / std::log(std::pow(w + std::pow((ph2 * N * N) / 6.0 / 6.0, 1.0 / 0.2), 0.2));
             h[(long)x * N + y] = make_double2(cc / std::sqrt((double)(N * N)), 0.0);
         }
-    JW_CUDA(cudaStreamSynchronize(c->stream));
-    JW_CUDA(cudaMemcpy(corr->d, h.data(), sizeof(double2) * vol, cudaMemcpyHostToDevice));
+    // stream-ordered, like every later use of corr on the context's stream
+    JW_CUDA(cudaMemcpyAsync(corr->d, h.data(), sizeof(double2) * vol, cudaMemcpyHostToDevice, c->stream));
     return JW_OK;
 }
 
@@ -799,7 +802,8 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
         cholesky_free(L);
         return s;
     };
-    if (cudaMemcpy(L->d_units, units.data(), sizeof(int2) * units.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(L->d_units, units.data(), sizeof(int2) * units.size(), cudaMemcpyHostToDevice, c->stream) !=
+        cudaSuccess)
         return fail(JW_ECUDA);
     k_chol_fill<<<148 * 16, kThreads, 0, c->stream>>>(L->d_L, corr->d, N, n);
     if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);

@@ -407,7 +407,7 @@ class Engine:
     """The batched engine (jw_engine): resident events advanced by fused kernels."""
 
     def __init__(self, precision: int = PRECISION_MIXED, reunitarize: bool = False, max_bytes: int = 0,
-                 max_batch: int = 0, device: int = 0, max_batch_sites: int = 0, autotune: bool = False):
+                 max_batch: int = 0, device: int = 0, max_batch_sites: int = 0, autotune: int = 0):
         self.opt = jw_engine_options(precision, int(reunitarize), max_bytes, max_batch, max_batch_sites,
                                      int(autotune))
         self._h = _vp()

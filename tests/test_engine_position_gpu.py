@@ -36,6 +36,34 @@ def test_fp64_position_engine_matches_reference(jw, gold):
     assert eng.sync() == jw.OK
 
 
+@pytest.mark.parametrize("coupling,rr", [(SQRT, 0), (HATTA, 40)])
+def test_fp64_position_engine_matches_call_for_call_at_256(jw, coupling, rr):
+    """At C2's lattice size (256^2), where the CPU oracle cannot run, the FP64
+    position engine against the call-for-call position path (jw_evolve_position,
+    prepare_A_and_B + update_uf in the reference's call order), which the
+    reference's own fixtures pin at 16^2: the same MV initial condition and
+    steps give the same V to 1e-12."""
+    N, seed, steps, step = 256, 29, 4, 0.0004
+    eng = jw.Engine(precision=jw.PRECISION_FP64)
+    eid = pos_event(eng, N, seed, coupling, rr=rr, step=step, slices=2)
+    eng.init_mv([eid])
+    V0 = eng.get_V(eid)
+    eng.step([eid], steps)
+    got = eng.get_V(eid)
+    assert eng.sync() == jw.OK
+    eng.close()
+    ctx = jw.Context(jw.config_defaults(Nx=N, Ny=N, seed=seed, mu=0.5 * N, mass=0.04, elementaryWilsonLines=2,
+                                        step=step, CouplingChoice=coupling, KernelChoice=jw.SIN_KERNEL))
+    V = ctx.field()
+    V.set(V0)
+    ctx.evolve_position(V, 0, steps, rr=rr)
+    want = V.get()
+    assert ctx.sync() == jw.OK
+    ctx.close()
+    assert np.abs(want - V0).max() > 1e-6  # the steps moved V
+    assert np.abs(got - want).max() < TOL_V64
+
+
 @pytest.mark.parametrize("coupling,rr", [(FIXED, 0), (HATTA, 5), (HATTA, 0), (SQRT, 0)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_position_engine_matches_oracle(jw, oracle, coupling, rr, precision):

@@ -140,3 +140,50 @@ def test_persistent_column_pass_is_bitwise_identical(jw, N, events):
     with pytest.raises(RuntimeError):  # not built at 2048^2
         eng.set_tuning(2048, 16)
     eng.close()
+
+
+@pytest.mark.parametrize("N,events", [(128, 2), (256, 2), (1024, 1), (2048, 1)])
+def test_radix_first_schedule(jw, N, events):
+    """The column transforms' radix-first schedule (tuning choices + 32): bit-
+    identical among its own tile widths, within FP32 rounding of the default
+    schedule, offered to the autotuner only with autotune = 2, and a recorded
+    choice replays its lattices bit for bit."""
+    widths = [c for c in (1, 2, 4, 8) if c <= N and c * (N // 8) <= 1024 and
+              2 * 16 * (N * c + (0 if c >= 8 else (N // 8) * c)) <= 227 * 1024]
+    if 64 <= N <= 1024:
+        widths.append(16 + (8 if N <= 512 else 4))
+    eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+    eng.step(ids, 4)
+    ref0 = [eng.get_V(i) for i in ids]
+    eng.close()
+    ref1 = None
+    for c in widths:
+        eng, ids = make(jw, N, events, jw.PRECISION_MIXED)
+        eng.set_tuning(N, c + 32)
+        eng.step(ids, 4)
+        assert eng.sync() == jw.OK
+        got = [eng.get_V(i) for i in ids]
+        eng.close()
+        if ref1 is None:
+            ref1 = got
+            moved = max(float(np.abs(a - b).max()) for a, b in zip(got, ref0))
+            # another rounding: within the mixed form's V tolerance (2e-5) of the default schedule
+            assert 0.0 < moved < 2e-5, moved
+        for a, b in zip(ref1, got):
+            assert np.array_equal(a, b), c
+    tuned = jw.Engine(precision=jw.PRECISION_MIXED, autotune=2)
+    tids = [tuned.add_event(N, ny_slices=2, mu=0.5 * N, mass=0.04, step=2e-3, coupling=jw.FIXED_COUPLING_CONSTANT,
+                            seed=11 + i) for i in range(events)]
+    tuned.init_mv(tids)
+    tuned.step(tids, 4)
+    assert tuned.sync() == jw.OK
+    chosen = tuned.tuning(N)
+    assert chosen in widths + [c + 32 for c in widths]
+    want = ref1 if chosen >= 32 else ref0
+    for a, i in zip(want, tids):
+        assert np.array_equal(a, tuned.get_V(i))
+    tuned.close()
+    eng, ids = make(jw, 512, 1, jw.PRECISION_MIXED)  # 512 = 8^3 has no radix-first schedule
+    with pytest.raises(RuntimeError):
+        eng.set_tuning(512, 8 + 32)
+    eng.close()
