@@ -472,7 +472,8 @@ void for_each_p2_cols(F&& f) {
 // Pair planes of a launch group ([planes nb N rows][4 N floats]: P has 8
 // planes per event, Q 4) as a 2D tensor with boxes of C float4 elements (C = 8:
 // 128 bytes; 4 columns at 1024^2) by min(N, 256) rows, no swizzle (dense
-// boxes).  L2 promotion stays at 128 bytes: with 256-byte
+// boxes).  L2 promotion is the box row (128 bytes, or 64 bytes for 4-column
+// tiles, which at 128 bytes read 2.1x the algorithmic bytes): with 256-byte
 // promotion every row fetched the neighbouring tile's half line too, which the
 // column pass reads much later (measured 1.5x the algorithmic DRAM reads).
 template <int N, int C>
@@ -483,7 +484,8 @@ bool p2_tensor_map(CUtensorMap* map, float4* P, int nb, int planes = 8) {
     const cuuint32_t estr[2] = {1, 1};
     return encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, P, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+                          C >= 8 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B : CU_TENSOR_MAP_L2_PROMOTION_L2_64B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // CTAs of the persistent column pass: every SM filled to its occupancy.
