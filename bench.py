@@ -121,7 +121,7 @@ def profiled_traffic():
 
 class ClockSampler:
     """SM clocks and throttle reasons while the timed region runs, read through
-    NVML every 5 ms on a host thread (the timed region lasts ~50-100 ms, too
+    NVML every 2 ms on a host thread (the timed region lasts ~50-100 ms, too
     short for nvidia-smi's 200 ms loop); nvidia-smi is the fallback when NVML
     cannot be opened.  The GPU is found by its PCI bus id, so the sample is of
     the device the run uses whatever CUDA_VISIBLE_DEVICES maps."""
@@ -131,7 +131,7 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int, period_s: float = 0.005):
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device = device
         self.period = period_s
         self.rows = []
@@ -201,7 +201,7 @@ class ClockSampler:
                 return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "source": "nvml"}
             reasons = sorted({name for _, r in self.rows for bit, name in self.REASONS.items() if r & bit})
             return {"sm_mhz": statistics.median(m for m, _ in self.rows), "sm_max_mhz": self.max_mhz,
-                    "reasons": reasons, "samples": len(self.rows), "source": "nvml, 5 ms"}
+                    "reasons": reasons, "samples": len(self.rows), "source": "nvml, 2 ms"}
         rows = []
         if self.path and os.path.exists(self.path):
             for line in open(self.path):
