@@ -947,7 +947,10 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p31_threads<N>(),
     }
     if (fl) atomicOr(flags, fl);
     cluster.sync();
-    fft16_rows_store<float, N>(ob, 4, -1.0f, tw, P + ((long)b * 8 + 4 * rank) * vol + (long)x * N, vol);
+    if constexpr (mx_p31_threads<N>() == 2 * (N / 8))  // 4 rows, 2 per round: two rows per thread in one round
+        fft16_rows2_store<N>(ob, -1.0f, tw, P + ((long)b * 8 + 4 * rank) * vol + (long)x * N, vol);
+    else
+        fft16_rows_store<float, N>(ob, 4, -1.0f, tw, P + ((long)b * 8 + 4 * rank) * vol + (long)x * N, vol);
 }
 
 // ------------------------------------------------------------------ measurement (FP64)
