@@ -288,7 +288,10 @@ typedef struct jw_event_desc {
     double mass;          /* config mass (Poisson mass = mass * mu_MV) */
     double step;          /* Langevin step (config step) */
     int coupling;         /* JW_SQRT_, JW_NOISE_, JW_FIXED_ (and, in position space, JW_HATTA_) COUPLING_CONSTANT */
-    int kernel;           /* JW_SIN_KERNEL (the engine's only kernel) */
+    int kernel;           /* JW_SIN_KERNEL; JW_LINEAR_KERNEL in position space only (in momentum
+                             space its multiplier is not Hermitian-symmetric at the Nyquist
+                             lines, which the engine's packed coefficients cannot represent:
+                             JW_EUNSUPPORTED, use the call-for-call layer) */
     uint64_t seed;        /* noise stream key of this event */
     /* 0: momentum-space steps (main_optimized.cpp:249-269).  Nonzero:
      * position-space steps (:271-302, jw_prepare_A_and_B) with plain noise;

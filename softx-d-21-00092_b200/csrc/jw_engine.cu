@@ -50,8 +50,9 @@ struct Event {
     float* k32 = nullptr;
 };
 
-// Per-event table bytes of a position-space event: [2][N*N] in FP64 and FP32.
-size_t position_table_bytes(int N) { return (sizeof(double) + sizeof(float)) * 2 * (size_t)N * N; }
+// Per-event table bytes of a position-space event: [4][N*N] in FP64 and FP32
+// (imaginary parts of the x and y tables, then their real parts).
+size_t position_table_bytes(int N) { return (sizeof(double) + sizeof(float)) * 4 * (size_t)N * N; }
 
 template <typename T> size_t step_ws_bytes(int N) { return sizeof(C2<T>) * 24 * (size_t)N * N; }
 size_t meas_ws_bytes(int N) { return (sizeof(double2) * 9 + 2 * sizeof(double)) * (size_t)N * N; }
@@ -158,9 +159,12 @@ __global__ void k_position_table(const double2* __restrict__ dft, double* __rest
                                  long n2, double inv) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n2) return;
-    const double v = dft[i].y * inv;
+    const double v = dft[i].y * inv, r = dft[i].x * inv;
     k64[i] = v;
     k32[i] = (float)v;
+    // real parts after the imaginary ones (read only for kernels that have them)
+    k64[n2 + i] = r;
+    k32[n2 + i] = (float)r;
 }
 
 // One accumulator site of an event: acc[site] and the plane stride.
@@ -1088,7 +1092,9 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     JW_CHECK(e && d && event_id);
     *event_id = -1;
     if (!engine_supported(e->opt.precision, d->N)) return JW_EUNSUPPORTED;
-    if (d->kernel != JW_SIN_KERNEL) return JW_EUNSUPPORTED;
+    // the LINEAR kernel in position space only: its momentum-space multiplier
+    // is not Hermitian-symmetric at the Nyquist lines (below)
+    if (d->kernel != JW_SIN_KERNEL && !(d->position_space && d->kernel == JW_LINEAR_KERNEL)) return JW_EUNSUPPORTED;
     if (d->position_space) {
         if (d->coupling != JW_SQRT_COUPLING_CONSTANT && d->coupling != JW_HATTA_COUPLING_CONSTANT &&
             d->coupling != JW_FIXED_COUPLING_CONSTANT)
@@ -1124,7 +1130,7 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     ev.slot = slot;
     ev.desc = *d;
     const size_t bV = sizeof(double2) * 9 * vol, bA = sizeof(double) * 4 * vol;
-    const size_t b64 = sizeof(double) * 2 * vol, b32 = sizeof(float) * 2 * vol, bT = sizeof(double2) * 2 * vol;
+    const size_t b64 = sizeof(double) * 4 * vol, b32 = sizeof(float) * 4 * vol, bT = sizeof(double2) * 2 * vol;
     ev.V = static_cast<double2*>(ev_alloc(e, bV));
     ev.acc = static_cast<double*>(ev_alloc(e, bA));
     if (!ev.V || !ev.acc) {
@@ -1173,6 +1179,11 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
     const int cp = d->coupling;
     h.k64 = d->position_space ? ev.k64 : g->k64[cp];
     h.k32 = d->position_space ? ev.k32 : g->k32[cp];
+    // the LINEAR position kernel k_i(d) is not odd at d_i = -N/2, so its DFT has a
+    // real part; the SIN kernel's and the momentum kernels' tables are imaginary
+    const bool re = d->position_space && d->kernel == JW_LINEAR_KERNEL;
+    h.kre64 = re ? ev.k64 + 2 * vol : nullptr;
+    h.kre32 = re ? ev.k32 + 2 * vol : nullptr;
     // the site-indexed noise factor belongs to momentum-space NOISE coupling only
     const bool nf = !d->position_space && cp == JW_NOISE_COUPLING_CONSTANT;
     h.nf64 = nf ? g->nf64 : nullptr;
@@ -1222,8 +1233,8 @@ JW_EXPORT jw_status jw_engine_remove_event(jw_engine* e, int id) {
                        (ev.desc.position_space ? position_table_bytes(ev.N) : 0);
     ev_free(e, ev.V, sizeof(double2) * 9 * vol);
     ev_free(e, ev.acc, sizeof(double) * 4 * vol);
-    ev_free(e, ev.k64, sizeof(double) * 2 * vol);
-    ev_free(e, ev.k32, sizeof(float) * 2 * vol);
+    ev_free(e, ev.k64, sizeof(double) * 4 * vol);
+    ev_free(e, ev.k32, sizeof(float) * 4 * vol);
     e->events.erase(it);
     return JW_OK;
 }

@@ -44,6 +44,8 @@ struct EventDev {
     double* acc;                // 4 planes of N*N: sum, sum compensation, err, err compensation
     const double* k64;          // kernel tables: [2][N*N] imag(K_x), imag(K_y), scaled by 1/N^2
     const float* k32;
+    const double* kre64;        // real parts of the tables, same layout (a position-space kernel whose
+    const float* kre32;         //   DFT has one: LINEAR), or null
     const double* nf64;         // per-site noise factor (NOISE coupling) or null
     const float* nf32;
     unsigned long long seed;
@@ -113,6 +115,20 @@ __device__ __forceinline__ void fft_rows_smem(C2<T>* sm, T sign, const C2<T>* __
 template <typename T> __device__ __forceinline__ const T* ktab(const EventDev& e);
 template <> __device__ __forceinline__ const double* ktab<double>(const EventDev& e) { return e.k64; }
 template <> __device__ __forceinline__ const float* ktab<float>(const EventDev& e) { return e.k32; }
+template <typename T> __device__ __forceinline__ const T* kretab(const EventDev& e);
+template <> __device__ __forceinline__ const double* kretab<double>(const EventDev& e) { return e.kre64; }
+template <> __device__ __forceinline__ const float* kretab<float>(const EventDev& e) { return e.kre32; }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// w + re(K_x) X + re(K_y) Y: the real parts of a kernel table (null for the
+// momentum kernels and the SIN position kernel, whose tables are imaginary)
+template <typename V, typename T>
+__device__ __forceinline__ V kmul_re(V w, T rx, T ry, V X, V Y) {
+    V r;
+    r.x = fma_t(ry, Y.x, fma_t(rx, X.x, w.x));
+    r.y = fma_t(ry, Y.y, fma_t(rx, X.y, w.y));
+    return r;
+}
 template <typename T> __device__ __forceinline__ const T* nftab(const EventDev& e);
 template <> __device__ __forceinline__ const double* nftab<double>(const EventDev& e) { return e.nf64; }
 template <> __device__ __forceinline__ const float* nftab<float>(const EventDev& e) { return e.nf32; }
@@ -250,6 +266,7 @@ __global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8), p2_cols<T, N>() * (
     T* kxs = reinterpret_cast<T*>(t1 + TILE);
     T* kys = kxs + N * C;
     const T* kt = ktab<T>(e) + c0 + (long)r0 * N + cc;
+    const T* kre = kretab<T>(e) ? kretab<T>(e) + c0 + (long)r0 * N + cc : nullptr;
 #pragma unroll 1
     for (int q = 0; q < PER; ++q) {
         const int i = threadIdx.x + q * TH;
@@ -271,7 +288,9 @@ __global__ void __launch_bounds__(p2_cols<T, N>() * (N / 8), p2_cols<T, N>() * (
         const V2 a = t0[pad(i)], bb = t1[pad(i)];
         const T kx = kxs[i], ky = kys[i];
         // (i kx) a + (i ky) b
-        t0[pad(i)] = mk<T>(-kx * a.y - ky * bb.y, kx * a.x + ky * bb.x);
+        V2 w = mk<T>(-kx * a.y - ky * bb.y, kx * a.x + ky * bb.x);
+        if (kre) w = kmul_re(w, __ldg(kre + q * RSTEP * N), __ldg(kre + vol + q * RSTEP * N), a, bb);
+        t0[pad(i)] = w;
     }
     __syncthreads();
     fft_smem<T, N>(t0, ColIdx<C>{c}, t, true, (T)1, tw);

@@ -438,15 +438,28 @@ __global__ void __launch_bounds__(mx_s2_threads<N, C>(), mx_s2_blocks<N, C>()) k
     // (i kx) X + (i ky) Y, X and Y the two halves of a plane element
     fft16x<float, N, true, true, S>(ta, cidx, r0, true, -1.0f, tw, ra);
     float2 w[2][8];
+    const float* kr = e.kre32 ? e.kre32 + c0 + (long)r0 * N + cc : nullptr;
 #pragma unroll
     for (int q = 0; q < PER; ++q)
         w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+    if (kr) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+            w[0][q] = kmul_re(w[0][q], __ldg(kr + (long)q * RSTEP * N), __ldg(kr + vol + (long)q * RSTEP * N), ra[0][q],
+                              ra[1][q]);
+    }
     cp_async_wait<0>();
     __syncthreads();
     fft16x<float, N, false, true, S>(tb, cidx, r0, true, -1.0f, tw, ra);
 #pragma unroll
     for (int q = 0; q < PER; ++q)
         w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+    if (kr) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+            w[1][q] = kmul_re(w[1][q], __ldg(kr + (long)q * RSTEP * N), __ldg(kr + vol + (long)q * RSTEP * N), ra[0][q],
+                              ra[1][q]);
+    }
     // every thread has passed a barrier since its last read of ta
     fft16x<float, N, true, true, S>(ta, cidx, r0, true, 1.0f, tw, w);
     float4* out = Q + ((long)b * 4 + j) * vol + c0 + (long)r0 * N + cc;
@@ -557,6 +570,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
     }
     bool timed_out = false;
     int cur_tile = -1;
+    const float* cur_tab = nullptr;
     float kx[PER], ky[PER];
 #pragma unroll 1
     for (int it = begin; it < end; it += stride) {
@@ -564,15 +578,22 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         const int tile = it / (nb * 4), rj = it - tile * nb * 4, j = rj & 3, b = rj >> 2;
         const int c0 = tile * C;
         if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
-        if (tile != cur_tile) {  // kernel table values of this thread's elements (the same for every event)
-            const float* kt = ev[slots[b]].k32 + c0 + (long)r0 * N + cc;
+        // kernel-table values of this thread's elements, kept while the tile and
+        // the table stay the same (events of one size and coupling share a table;
+        // position-space events have their own)
+        const float* tab = ev[slots[b]].k32;
+        if (tile != cur_tile || tab != cur_tab) {
+            const float* kt = tab + c0 + (long)r0 * N + cc;
 #pragma unroll
             for (int q = 0; q < PER; ++q) {
                 kx[q] = __ldg(kt + (long)q * RSTEP * N);
                 ky[q] = __ldg(kt + vol + (long)q * RSTEP * N);
             }
             cur_tile = tile;
+            cur_tab = tab;
         }
+        const float* kr0 = ev[slots[b]].kre32;
+        const float* kr = kr0 ? kr0 + c0 + (long)r0 * N + cc : nullptr;
         float2 ra[2][8], w[2][8];
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
         parity ^= 1u << xb;
@@ -581,6 +602,12 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[0][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+        if (kr) {
+#pragma unroll
+            for (int q = 0; q < PER; ++q)
+                w[0][q] = kmul_re(w[0][q], __ldg(kr + (long)q * RSTEP * N), __ldg(kr + vol + (long)q * RSTEP * N),
+                                  ra[0][q], ra[1][q]);
+        }
         // every thread is done reading xb; once the previous item's store has
         // read fb, the next item's X goes to fb and its Y to xb (issuing X at
         // the item's start, waiting for that store there, measured slower)
@@ -601,6 +628,12 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
 #pragma unroll
         for (int q = 0; q < PER; ++q)
             w[1][q] = make_float2(-kx[q] * ra[0][q].y - ky[q] * ra[1][q].y, kx[q] * ra[0][q].x + ky[q] * ra[1][q].x);
+        if (kr) {
+#pragma unroll
+            for (int q = 0; q < PER; ++q)
+                w[1][q] = kmul_re(w[1][q], __ldg(kr + (long)q * RSTEP * N), __ldg(kr + vol + (long)q * RSTEP * N),
+                                  ra[0][q], ra[1][q]);
+        }
         // the inverse's first pass synchronises before it writes yb
         fft16x<float, N, true, true, S>(buf(yb), cidx, r0, true, 1.0f, twsrc, w);
         // the result tile into yb (dense [N][8] elements, the store box's layout)

@@ -19,9 +19,9 @@ def jw():
     return jimwlk
 
 
-def pos_event(eng, N, seed, coupling, rr=0, step=0.0004, slices=6, step0=0):
+def pos_event(eng, N, seed, coupling, rr=0, step=0.0004, slices=6, step0=0, kernel=1):
     return eng.add_event(N, ny_slices=slices, mu=0.5 * N, mass=0.04, step=step, coupling=coupling, seed=seed,
-                         position_space=True, rr=rr, step0=step0)
+                         position_space=True, rr=rr, step0=step0, kernel=kernel)
 
 
 def test_fp64_position_engine_matches_reference(jw, gold):
@@ -80,6 +80,26 @@ def test_position_engine_matches_oracle(jw, oracle, coupling, rr, precision):
     assert eng.sync() == jw.OK
 
 
+@pytest.mark.parametrize("coupling,rr", [(SQRT, 0), (HATTA, 5), (FIXED, 0)])
+@pytest.mark.parametrize("precision,N", [("fp64", 32), ("mixed", 32), ("mixed", 64)])
+def test_linear_kernel_position_engine_matches_oracle(jw, oracle, coupling, rr, precision, N):
+    """The LINEAR position kernel (positions.h:105-150 with the unwrapped
+    distance) in the engine: its DFT has a real part (k_i(d) is not odd at
+    d_i = -N/2), carried in the event's real-part tables, against the oracle's
+    direct sum (field.h:2368-2519).  At 64^2 the mixed engine's column pass is
+    the persistent TMA form."""
+    seed, steps, step = 19, 5, 0.0004
+    eng = jw.Engine(precision=jw.PRECISION_FP64 if precision == "fp64" else jw.PRECISION_MIXED)
+    eid = pos_event(eng, N, seed, coupling, rr=rr, step=step, step0=2, kernel=0)
+    eng.init_mv([eid])
+    V0 = eng.get_V(eid)
+    eng.step([eid], steps)
+    want = oracle.evolve_position(V0, steps, 2, step, coupling, 0, rr, None, seed)
+    tol = TOL_V64 if precision == "fp64" else TOL_V32
+    assert np.abs(eng.get_V(eid) - want).max() < tol
+    assert eng.sync() == jw.OK
+
+
 def test_hatta_branches_batched(jw, oracle):
     """The Hatta loop's branches (main_optimized.cpp:200-216): one event per
     (ix, iy), each with its own rr and noise offset, stepped in one batch, then
@@ -121,7 +141,7 @@ def test_position_engine_rejects_what_it_cannot_do(jw):
     eng = jw.Engine(precision=jw.PRECISION_MIXED)
     st, _ = eng.try_add_event(N=16, coupling=NOISE, position_space=True)   # needs the Cholesky factor
     assert st == jw.EUNSUPPORTED
-    st, _ = eng.try_add_event(N=16, coupling=SQRT, kernel=0, position_space=True)  # LINEAR kernel
+    st, _ = eng.try_add_event(N=16, coupling=SQRT, kernel=0)               # LINEAR kernel in momentum space
     assert st == jw.EUNSUPPORTED
     st, _ = eng.try_add_event(N=16, coupling=HATTA)                        # HATTA in momentum space
     assert st == jw.EUNSUPPORTED

@@ -187,3 +187,37 @@ def test_radix_first_schedule(jw, N, events):
     with pytest.raises(RuntimeError):
         eng.set_tuning(512, 8 + 32)
     eng.close()
+
+
+@pytest.mark.parametrize("N", [64, 256])
+def test_events_with_different_tables_share_a_launch(jw, N):
+    """Events of one size with different kernel tables in one launch group --
+    momentum-space couplings (one table per coupling) and position-space events
+    (a table per event, HATTA with different rr, SIN and LINEAR kernels) -- give
+    each event's lattice bit for bit as when it runs alone.  The persistent
+    column pass keeps a tile's table values across the work items of one table
+    only."""
+    descs = [dict(coupling=jw.SQRT_COUPLING_CONSTANT), dict(coupling=jw.FIXED_COUPLING_CONSTANT),
+             dict(coupling=jw.SQRT_COUPLING_CONSTANT), dict(coupling=jw.FIXED_COUPLING_CONSTANT),
+             dict(coupling=jw.HATTA_COUPLING_CONSTANT, position_space=True, rr=3),
+             dict(coupling=jw.HATTA_COUPLING_CONSTANT, position_space=True, rr=40),
+             dict(coupling=jw.SQRT_COUPLING_CONSTANT, position_space=True, kernel=jw.LINEAR_KERNEL)]
+
+    def add(eng, i, d):
+        return eng.add_event(N, ny_slices=2, mu=0.5 * N, mass=0.04, step=4e-4, seed=31 + i, **d)
+
+    eng = jw.Engine(precision=jw.PRECISION_MIXED)
+    ids = [add(eng, i, d) for i, d in enumerate(descs)]
+    eng.init_mv(ids)
+    eng.step(ids, 5)
+    assert eng.sync() == jw.OK
+    together = [eng.get_V(i) for i in ids]
+    eng.close()
+    for i, d in enumerate(descs):
+        one = jw.Engine(precision=jw.PRECISION_MIXED)
+        eid = add(one, i, d)
+        one.init_mv([eid])
+        one.step([eid], 5)
+        assert one.sync() == jw.OK
+        assert np.array_equal(one.get_V(eid), together[i]), d
+        one.close()
