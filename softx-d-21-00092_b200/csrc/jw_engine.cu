@@ -37,6 +37,7 @@ struct Group {
     float* nf32 = nullptr;
     int p2_cols = 0;                 // mixed pass 2 column-tile width (0: the default)
     bool tuned = false;              // the autotuner has run for this size
+    int n_re = 0;                    // resident events whose kernel tables have real parts (LINEAR, position)
 };
 
 struct Event {
@@ -536,8 +537,13 @@ void launch_pass2(jw_engine* e, Group& g, const int* d_slots, int nb, int cols, 
                 return;
             }
             const int grid = std::min(p2_tma_grid<N, TC, S>(), nb * 4 * (N / TC));
-            k_mix_pass2_tma<N, TC, S><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC, S>(), e->stream>>>(
-                g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
+            // the form that reads real table parts only for groups holding such events
+            if (g.n_re > 0)
+                k_mix_pass2_tma<N, TC, S, true><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC, S>(), e->stream>>>(
+                    g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
+            else
+                k_mix_pass2_tma<N, TC, S><<<grid, mx_t2_threads<N, TC>(), mx_t2_smem<N, TC, S>(), e->stream>>>(
+                    g.d_ev, d_slots, g.tw.d32, nb, advance, e->d_flags, pmap, qmap);
         } else {
             k_mix_pass2<N, C, S><<<dim3(N / C, 4, nb), mx_s2_threads<N, C>(), mx_s2_smem<N, C>(), e->stream>>>(
                 g.d_ev, d_slots, P, Q, g.tw.d32, advance);
@@ -561,10 +567,12 @@ void mix_configure() {
         constexpr int CS = decltype(c)::value;
         constexpr int S = CS >= kRadixFirst ? 1 : 0;
         constexpr int C = CS - S * kRadixFirst;
-        if constexpr (C > kP2Tma)
+        if constexpr (C > kP2Tma) {
             cudaFuncSetAttribute(k_mix_pass2_tma<N, C - kP2Tma, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)mx_t2_smem<N, C - kP2Tma, S>());
-        else
+            cudaFuncSetAttribute(k_mix_pass2_tma<N, C - kP2Tma, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_t2_smem<N, C - kP2Tma, S>());
+        } else
             cudaFuncSetAttribute(k_mix_pass2<N, C, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)mx_s2_smem<N, C>());
     });
@@ -1215,6 +1223,7 @@ JW_EXPORT jw_status jw_engine_add_event(jw_engine* e, const jw_event_desc* d, in
         ev_free(e, ev.k32, b32);
         return s;
     }
+    if (h.kre32) g->n_re += 1;
     e->events[ev.id] = ev;
     *event_id = ev.id;
     return JW_OK;
@@ -1228,6 +1237,7 @@ JW_EXPORT jw_status jw_engine_remove_event(jw_engine* e, int id) {
     Event& ev = it->second;
     Group& g = *e->groups[ev.N];
     g.owner[ev.slot] = -1;
+    if (ev.desc.position_space && ev.desc.kernel == JW_LINEAR_KERNEL) g.n_re -= 1;
     const size_t vol = (size_t)ev.N * ev.N;
     e->bytes_in_use -= vol * (sizeof(double2) * 9 + sizeof(double) * 4) +
                        (ev.desc.position_space ? position_table_bytes(ev.N) : 0);

@@ -510,7 +510,7 @@ template <int N, int C> constexpr bool mx_t2_valid() {
     return C == mx_t2_cols<N>() && N >= 64 && N <= 1024 && mx_t2_smem<N, C>() <= 227 * 1024;
 }
 
-template <int N, int C, int S = 0>
+template <int N, int C, int S = 0, bool RE = false>
 __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k_mix_pass2_tma(
     EventDev* __restrict__ ev, const int* __restrict__ slots, const float2* __restrict__ tw, int nb, int advance,
     int* __restrict__ flags, const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap qmap) {
@@ -571,6 +571,11 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
     bool timed_out = false;
     int cur_tile = -1;
     const float* cur_tab = nullptr;
+    auto item_tab = [&](int i2) {
+        const int t2 = i2 / (nb * 4);
+        return ev[slots[(i2 - t2 * nb * 4) >> 2]].k32;
+    };
+    const float* tab_next = begin < end ? item_tab(begin) : nullptr;
     float kx[PER], ky[PER];
 #pragma unroll 1
     for (int it = begin; it < end; it += stride) {
@@ -580,8 +585,10 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
         if (advance && tile == 0 && j == 0 && tid == 0) ev[slots[b]].step += 1;
         // kernel-table values of this thread's elements, kept while the tile and
         // the table stay the same (events of one size and coupling share a table;
-        // position-space events have their own)
-        const float* tab = ev[slots[b]].k32;
+        // position-space events have their own).  The next item's table pointer
+        // is loaded here, an item ahead of its use.
+        const float* tab = tab_next;
+        if (more) tab_next = item_tab(it + stride);
         if (tile != cur_tile || tab != cur_tab) {
             const float* kt = tab + c0 + (long)r0 * N + cc;
 #pragma unroll
@@ -592,7 +599,7 @@ __global__ void __launch_bounds__(mx_t2_threads<N, C>(), mx_t2_blocks<N, C>()) k
             cur_tile = tile;
             cur_tab = tab;
         }
-        const float* kr0 = ev[slots[b]].kre32;
+        const float* kr0 = RE ? ev[slots[b]].kre32 : nullptr;  // real table parts (RE launches only)
         const float* kr = kr0 ? kr0 + c0 + (long)r0 * N + cc : nullptr;
         float2 ra[2][8], w[2][8];
         timed_out |= !mbar_wait_bounded(&bar[xb], (parity >> xb) & 1u);
