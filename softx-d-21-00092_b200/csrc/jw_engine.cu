@@ -559,6 +559,9 @@ void mix_configure() {
         cudaFuncSetAttribute(k_mix_pass1_pair<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
         cudaFuncSetAttribute(k_mix_pass31_pair<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)mx_p31p_smem<N>());
+        if constexpr (N == 2048)
+            cudaFuncSetAttribute(k_mix_pass31_quad<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mx_p31q_smem<N>());
     } else {
         cudaFuncSetAttribute(k_mix_pass1<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p1_smem<N>());
         cudaFuncSetAttribute(k_mix_pass31<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_p31_smem<N>());
@@ -618,7 +621,10 @@ void mix_launch(jw_engine* e, Group& g, const int* d_slots, int nb, int kind, bo
                                                                                             nullptr);
             break;
         case KIND_P31:
-            if constexpr (mx_pair<N>())
+            if constexpr (N == 2048)  // four-CTA clusters, two CTAs per SM
+                k_mix_pass31_quad<N><<<dim3(N, 4, nb), kQuadThreads, mx_p31q_smem<N>(), e->stream>>>(
+                    g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
+            else if constexpr (mx_pair<N>())
                 k_mix_pass31_pair<N><<<dim3(N, 2, nb), mx_p31_threads<N>(), mx_p31p_smem<N>(), e->stream>>>(
                     g.d_ev, d_slots, Q, P, g.tw.d32, e->d_flags);
             else

@@ -993,6 +993,86 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p31_threads<N>(),
         fft16_rows_store<float, N>(ob, 4, -1.0f, tw, P + ((long)b * 8 + 4 * rank) * vol + (long)x * N, vol);
 }
 
+// Pass 3 + next pass 1 at 2048^2 as a cluster of four CTAs of 256 threads (two
+// CTAs per SM, the configuration of the two-CTA form at 1024^2).  Rank r
+// inverse-transforms Q row r; after a cluster barrier it updates the sites
+// [r N/4, (r + 1) N/4), reading the four Q rows from their owners, and stores
+// the next step's pair elements into their owners' rows: pair row p (noise
+// rows 0-3, rotated rows 4-7) belongs to rank p / 2 as its local row p % 2.
+// A second barrier orders those stores before each CTA transforms its 2
+// output rows.  The per-site arithmetic is the two-CTA form's, so lattices are
+// bit-identical.
+constexpr int kQuadThreads = 256;
+template <int N> constexpr size_t mx_p31q_smem() {
+    return 16 * ((size_t)padded_len16(N) + (size_t)padded_len16(2 * N));
+}
+template <int N>
+__global__ void __cluster_dims__(1, 4, 1) __launch_bounds__(kQuadThreads, 2)
+    k_mix_pass31_quad(EventDev* __restrict__ ev, const int* __restrict__ slots, const float4* __restrict__ Q,
+                      float4* __restrict__ P, const float2* __restrict__ tw, int* __restrict__ flags) {
+    static_assert(N / 8 == kQuadThreads, "one row transform per CTA round");
+    static_assert(mx_p31q_smem<N>() <= 113 * 1024, "two CTAs per SM");
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* qb = reinterpret_cast<float4*>(smem_raw);  // Q row `rank`
+    float4* ob = qb + padded_len16(N);                   // pair rows 2 rank, 2 rank + 1
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned rank = cluster.block_rank();  // = blockIdx.y
+    const int x = blockIdx.x, b = blockIdx.z;
+    EventDev& e = ev[slots[b]];
+    const long vol = (long)N * N;
+    const float4* in = Q + ((long)b * 4 + rank) * vol + (long)x * N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) cp_async<16>(&qb[pad16(i)], &in[i]);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    fft16_rows<N, 1>(qb, 1.0f, tw);
+    cluster.sync();
+    const double se = e.sqrt_eps;
+    const float* nf = e.nf32;
+    int fl = 0;
+    constexpr int QUARTER = N / 4;
+    // element y of pair row p (0..7) in its owner's shared memory
+    auto orow = [&](int p, int y) -> float4* { return cluster.map_shared_rank(ob, p >> 1) + pad16((p & 1) * N + y); };
+    for (int y = (int)rank * QUARTER + threadIdx.x; y < ((int)rank + 1) * QUARTER; y += blockDim.x) {
+        const long site = (long)x * N + y;
+        float2 v32[9];
+        {
+            double2 v[9];
+            p3_site_g(e, [&](int j) { return *(cluster.map_shared_rank(qb, j) + pad16(y)); }, site, vol, se, v, fl);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                e.V[k * vol + site] = v[k];
+                v32[k] = make_float2((float)v[k].x, (float)v[k].y);
+            }
+        }
+        float z[16];
+        langevin_normals_fast(e.seed, e.step, (uint32_t)site, z);
+        if (nf) {  // NOISE coupling: the site-indexed factor (uniform over the event)
+            const float f = nf[site];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) z[k] *= f;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (X_j, Y_j)
+            *orow(j, y) = make_float4(z[4 * j], z[4 * j + 2], z[4 * j + 1], z[4 * j + 3]);
+        float n[8], m[8], hx[8], hy[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            n[k] = z[2 * k];
+            m[k] = z[2 * k + 1];
+        }
+        rotate_herm(v32, n, hx);
+        rotate_herm(v32, m, hy);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
+            *orow(4 + j, y) = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
+    }
+    if (fl) atomicOr(flags, fl);
+    cluster.sync();
+    fft16_rows2_store<N>(ob, -1.0f, tw, P + ((long)b * 8 + 2 * rank) * vol + (long)x * N, vol);
+}
+
 // ------------------------------------------------------------------ measurement (FP64)
 // C(k) = sum over the 9 entries of |FFT(V_ij)(k)|^2 / N^6 (lfield::trace,
 // field.h:1375-1432, after the unitary forward transform), with the 16-byte

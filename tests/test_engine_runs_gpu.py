@@ -26,7 +26,8 @@ def make(jw, N, events, precision, max_batch=0):
 @pytest.mark.parametrize("precision,N,events", [
     ("mixed", 64, 3),      # fused pass 3 + 1
     ("mixed", 512, 2),     # fused, two CTAs per SM
-    ("mixed", 1024, 1),    # fused, one CTA per SM
+    ("mixed", 1024, 1),    # fused, two-CTA clusters
+    ("mixed", 2048, 1),    # fused, four-CTA clusters against the two-CTA pass 1 and pass 3
     ("fp64", 64, 2),       # FP64 engine: per-step graph replay
 ])
 def test_split_of_steps_into_calls_is_bitwise_invariant(jw, precision, N, events):
