@@ -105,7 +105,10 @@ typedef struct jw_field jw_field;
 
 /* Replaces the set-up of main_optimized.cpp:68-92 (mpi_class, momenta,
  * positions, fftw2D::init2D): binds device `device`, creates a stream and the
- * FFT twiddle tables for cfg->Nx. */
+ * FFT twiddle tables for cfg->Nx.  Nx = Ny, any size from 2 to 2048 (the
+ * reference plans FFTW for any size, mpi_fftw_class.h:165-186); sizes that
+ * are not powers of two transform by the chirp-z form.  JW_EUNSUPPORTED
+ * otherwise.  The batched engine and the server take powers of two only. */
 jw_status jw_context_create(const jw_config* cfg, int device, jw_context** out);
 /* Also releases every field still open in the context; those handles are
  * invalid afterwards. */

@@ -289,7 +289,7 @@ JW_EXPORT const char* jw_status_string(jw_status s) {
 JW_EXPORT jw_status jw_context_create(const jw_config* cfg, int device, jw_context** out) {
     JW_CHECK(cfg && out);
     *out = nullptr;
-    if (cfg->Nx != cfg->Ny || !supported_n(cfg->Nx)) return JW_EUNSUPPORTED;
+    if (cfg->Nx != cfg->Ny || !supported_n_fp64(cfg->Nx)) return JW_EUNSUPPORTED;
     JW_CUDA(cudaSetDevice(device));
     jw_context* c = new jw_context();
     c->cfg = *cfg;

@@ -30,15 +30,26 @@
 namespace jw {
 
 // FP64-accurate twiddle tables exp(+2 pi i m / N), m < N, for one N.
+// For an N that is not a power of two in [8, 2048] the FP64 transform runs
+// as Bluestein's chirp-z transform over a power-of-two length M >= 2N - 1,
+// and the tables are those of the chirp-z form instead (d64 = d32 = null).
 struct Twiddles {
     int N = 0;
     double2* d64 = nullptr;
     float2* d32 = nullptr;
+    int M = 0;                    // chirp-z length (0: N is a power of two)
+    double2* chirp = nullptr;     // w[n] = exp(-i pi n^2 / N), n < N
+    double2* bhat = nullptr;      // [2][M]: DFT_M of the wrapped chirp kernel / M, forward then backward
+    double2* twM = nullptr;       // exp(+2 pi i m / M), m < M
 };
 cudaError_t twiddles_create(int N, Twiddles* tw, cudaStream_t s);
 void twiddles_destroy(Twiddles* tw);
 
+// Power-of-two N in [8, 2048]: every layer (the engine's fused kernels included).
 bool supported_n(int N);
+// Any N in [2, 2048]: the call-for-call FP64 layer, whose transform falls back
+// to the chirp-z form for N that supported_n rejects.
+bool supported_n_fp64(int N);
 
 // Converts a device error-flag word to a status (and clears nothing).
 inline jw_status flags_to_status(int flags) {

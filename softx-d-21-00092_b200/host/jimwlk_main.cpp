@@ -12,7 +12,8 @@
 // call (jw_evolve_momentum / jw_evolve_position), and the Hatta branches
 // (HATTA coupling, main_optimized.cpp:200-216) run together as events of the
 // batched engine, one per (ix, iy), stepped in one launch sequence (FP64, or
-// mixed precision with --mixed).  --call-for-call runs the body of
+// mixed precision with --mixed; at sizes that are not powers of two the
+// branches run one after another).  --call-for-call runs the body of
 // main_optimized.cpp:232-304 literally, one adapter call per reference call,
 // branch after branch.  All modes draw the same noise: Langevin step n of the
 // run (branches in the reference's order) uses stream index n, MV slice n
@@ -201,7 +202,9 @@ int main(int argc, char* argv[]) {
             dev.sync();
             std::printf("Initial condition time: %g\n", ti.seconds());
 
-            if (cp == HATTA_COUPLING_CONSTANT && !call_for_call) {
+            // the batched engine takes power-of-two lattices; other sizes run the branches one by one
+            const bool engine_size = Nx >= 8 && Nx <= 2048 && (Nx & (Nx - 1)) == 0;
+            if (cp == HATTA_COUPLING_CONSTANT && !call_for_call && engine_size) {
                 run_hatta_batched(dev, cnfg, uf, sum, err, device_id, mixed);
                 dev.sync();
                 std::printf("Statistics time: %g\n", ts.seconds());

@@ -3,7 +3,7 @@
 Run in a container that has the reference tree (for oracle/_ref/libref_<N>.so,
 built by `make -C oracle ref`):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]   # all fixtures when none is named
 
 Every output array below is produced by the reference's functions (field.h,
 su3_matrix.h, zheevh3, mpi_fftw_class.h with the project FFT shim) fed with the
@@ -123,6 +123,10 @@ DRIVER_RUNS = {
     "driver_position_cholesky_N16": (16, 44, dict(stat=1, mu=8.0, mass=0.04, wilson_lines=6, langevin_steps=4,
                                                   measurements=2, step=0.0004, evolution="POSITION_EVOLUTION",
                                                   coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL")),
+    # a size that is not a power of two (the reference compiles any Nx = Ny)
+    "driver_sqrt_sin_N24": (24, 45, dict(stat=1, mu=12.0, mass=0.04, wilson_lines=6, langevin_steps=8,
+                                         measurements=2, step=0.0004, evolution="MOMENTUM_EVOLUTION",
+                                         coupling="SQRT_COUPLING_CONSTANT", kernel="SIN_KERNEL")),
 }
 
 
@@ -178,10 +182,19 @@ def check_oracle(o: Oracle, fx: dict) -> float:
                np.abs(corr - fx["corr"]).max() / np.abs(fx["corr"]).max())
 
 
-def main() -> None:
+def main(only: list[str]) -> None:
+    """Writes every fixture, or only those named on the command line."""
     o = Oracle()
-    fns = fixture_functions(o, 16, 101)
-    np.savez_compressed(os.path.join(HERE, "functions_N16.npz"), **{k: np.asarray(v) for k, v in fns.items()})
+
+    def wanted(name: str) -> bool:
+        return not only or name in only
+
+    # lattice sizes that are not powers of two: the reference plans FFTW for
+    # any N (mpi_fftw_class.h:165-186); 15 is odd, 24 = 2^3 3
+    for name, N, seed in (("functions_N16", 16, 101), ("functions_N24", 24, 102), ("functions_N15", 15, 103)):
+        if wanted(name):
+            fns = fixture_functions(o, N, seed)
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fns.items()})
     runs = {
         # reference default main path: MOMENTUM + NOISE coupling (site-indexed noise factor), SIN kernel
         "evolve_noise_N16": dict(N=16, seed=7, coupling="NOISE_COUPLING_CONSTANT", steps=20, step=f32(0.0004),
@@ -199,8 +212,15 @@ def main() -> None:
         # the reference's default step at 32^2 for a visible evolution
         "evolve_fixed_N32": dict(N=32, seed=3, coupling="FIXED", steps=50, step=f32(0.0004), slices=20, mu=16.0,
                                  mass=f32(0.04)),
+        # sizes that are not powers of two
+        "evolve_sqrt_N24": dict(N=24, seed=10, coupling="SQRT_COUPLING_CONSTANT", steps=12, step=f32(0.0004),
+                                slices=6, mu=12.0, mass=f32(0.04)),
+        "evolve_noise_N15": dict(N=15, seed=11, coupling="NOISE_COUPLING_CONSTANT", steps=12, step=f32(0.0004),
+                                 slices=6, mu=7.5, mass=f32(0.04)),
     }
     for name, kw in runs.items():
+        if not wanted(name):
+            continue
         fx = fixture_evolution(o, **kw)
         d = check_oracle(o, fx)
         print(f"{name}: oracle vs reference max deviation {d:.3e}")
@@ -216,8 +236,12 @@ def main() -> None:
                                      slices=6),
         "position_cholesky_N16": dict(N=16, seed=24, coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL",
                                       steps=3, slices=6),
+        "position_sqrt_sin_N15": dict(N=15, seed=25, coupling="SQRT_COUPLING_CONSTANT", kernel="SIN_KERNEL", steps=3,
+                                      slices=6),
     }
     for name, kw in pos.items():
+        if not wanted(name):
+            continue
         fx = fixture_position(o, **kw)
         d = check_oracle_position(o, fx)
         print(f"{name}: oracle vs reference max deviation {d:.3e}")
@@ -225,10 +249,12 @@ def main() -> None:
             raise SystemExit(f"oracle disagrees with the reference on {name}")
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fx.items()})
     for name, (N, seed, cfg) in DRIVER_RUNS.items():
+        if not wanted(name):
+            continue
         fx = fixture_driver(o, N, seed, cfg)
         print(f"{name}: {len(fx['dat'].splitlines())} output lines")
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **{k: np.asarray(v) for k, v in fx.items()})
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

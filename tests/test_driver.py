@@ -15,7 +15,8 @@ from jwref import f32
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(REPO, "softx-d-21-00092_b200", "bin", "jimwlk_main")
-NAMES = ["driver_sqrt_sin_N16", "driver_noise_sin_N16", "driver_sqrt_linear_N16", "driver_position_cholesky_N16"]
+NAMES = ["driver_sqrt_sin_N16", "driver_noise_sin_N16", "driver_sqrt_linear_N16", "driver_position_cholesky_N16",
+         "driver_sqrt_sin_N24"]
 COUPLING = {"SQRT_COUPLING_CONSTANT": 0, "NOISE_COUPLING_CONSTANT": 1, "HATTA_COUPLING_CONSTANT": 2}
 
 

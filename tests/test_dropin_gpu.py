@@ -42,8 +42,39 @@ def test_execute2D_matches_dft(jw, N):
     assert ctx.sync() == jw.OK
 
 
-def test_functions_match_reference(jw, gold):
-    fx = gold("functions_N16")
+@pytest.mark.parametrize("N", [2, 3, 12, 15, 24, 100, 384, 1000, 1536, 2047])
+def test_execute2D_general_n_matches_dft(jw, N):
+    """Sizes that are not powers of two: the chirp-z transform (power-of-two
+    convolution length M >= 2N - 1) against numpy's DFT, forward and back."""
+    ctx = make_ctx(jw, N)
+    rng = np.random.default_rng(N)
+    t = 9 if N <= 384 else 1
+    a = rng.standard_normal((N, N, t)) + 1j * rng.standard_normal((N, N, t))
+    f = ctx.field(t).set(a)
+    ctx.execute2D(f, 1)
+    M = 8
+    while M < 2 * N - 1:
+        M *= 2
+    tol = 1e-14 * np.log2(M)
+    assert rel(f.get(), np.fft.fft2(a, axes=(0, 1)) / N) < tol
+    ctx.execute2D(f, 0)
+    assert np.abs(f.get() - a).max() < 4 * tol
+    assert ctx.sync() == jw.OK
+
+
+def test_context_rejects_unsupported_sizes(jw):
+    for N in (1, 2049, 4096):
+        with pytest.raises(jw.JimwlkError):
+            make_ctx(jw, N)
+    with pytest.raises(jw.JimwlkError):
+        jw.Context(jw.config_defaults(Nx=24, Ny=16))
+
+
+@pytest.mark.parametrize("name", ["functions_N16", "functions_N24", "functions_N15"])
+def test_functions_match_reference(jw, gold, name):
+    """One call of each function against the reference; 24 and 15 are not
+    powers of two, so their transforms take the chirp-z form."""
+    fx = gold(name)
     N, seed = int(fx["N"]), int(fx["seed"])
     ctx = make_ctx(jw, N, seed=seed)
     f = ctx.field().set(fx["fft_in"])
@@ -95,7 +126,7 @@ COUPLING = {"FIXED": 3, "NOISE_COUPLING_CONSTANT": 1, "SQRT_COUPLING_CONSTANT": 
 
 
 @pytest.mark.parametrize("name", ["evolve_noise_N16", "evolve_sqrt_N16", "evolve_linear_N16", "evolve_fixed_N32",
-                                  "c1_N64"])
+                                  "c1_N64", "evolve_sqrt_N24", "evolve_noise_N15"])
 def test_evolution_matches_reference(jw, gold, name):
     """MV initial condition + Langevin steps + one measurement, V element-wise <= 1e-12."""
     fx = gold(name)
@@ -155,4 +186,4 @@ def test_bad_arguments_are_rejected(jw):
     with pytest.raises(jw.JimwlkError):
         ctx.prepare_A_local(a, ctx.field(), ctx.field(), 2, 1)  # HATTA is undefined in momentum space
     with pytest.raises(jw.JimwlkError):
-        make_ctx(jw, 24)  # not a power of two
+        make_ctx(jw, 4096)  # above the largest lattice

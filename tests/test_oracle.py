@@ -13,7 +13,7 @@ COUPLING = {"FIXED": FIXED_COUPLING, "NOISE_COUPLING_CONSTANT": 1, "SQRT_COUPLIN
 
 
 @pytest.mark.parametrize("name", ["evolve_noise_N16", "evolve_sqrt_N16", "evolve_linear_N16", "evolve_fixed_N32",
-                                  "c1_N64"])
+                                  "c1_N64", "evolve_sqrt_N24", "evolve_noise_N15"])
 def test_oracle_matches_golden_evolution(oracle, gold, name):
     fx = gold(name)
     N, seed = int(fx["N"]), int(fx["seed"])
@@ -27,8 +27,11 @@ def test_oracle_matches_golden_evolution(oracle, gold, name):
     assert np.abs(e - fx["err"]).max() <= 1e-13 * np.abs(fx["err"]).max()
 
 
-def test_oracle_matches_golden_functions(oracle, gold):
-    fx = gold("functions_N16")
+@pytest.mark.parametrize("name", ["functions_N16", "functions_N24", "functions_N15"])
+def test_oracle_matches_golden_functions(oracle, gold, name):
+    """One application of each hot-path function; 24 and 15 are sizes that
+    are not powers of two (the reference plans FFTW for any N)."""
+    fx = gold(name)
     N, seed = int(fx["N"]), int(fx["seed"])
     assert np.abs(oracle.execute2D(fx["fft_in"], 1) - fx["fft_fwd"]).max() <= 1e-13
     assert np.abs(oracle.execute2D(fx["fft_in"], 0) - fx["fft_bwd"]).max() <= 1e-13
@@ -49,7 +52,7 @@ def test_oracle_matches_golden_functions(oracle, gold):
 
 
 @pytest.mark.parametrize("name", ["position_sqrt_sin_N16", "position_sqrt_linear_N8", "position_cholesky_N8",
-                                  "position_cholesky_N16"])
+                                  "position_cholesky_N16", "position_sqrt_sin_N15"])
 def test_oracle_matches_golden_position(oracle, gold, name):
     """Position-space evolution (main_optimized.cpp:271-304) with Cholesky-
     correlated noise for NOISE coupling (main_optimized.cpp:145-157)."""

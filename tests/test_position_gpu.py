@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 COUPLING = {"SQRT_COUPLING_CONSTANT": 0, "NOISE_COUPLING_CONSTANT": 1}
 HATTA = 2
 POSITION_FIXTURES = ["position_sqrt_sin_N16", "position_sqrt_linear_N8", "position_cholesky_N8",
-                     "position_cholesky_N16"]
+                     "position_cholesky_N16", "position_sqrt_sin_N15"]
 
 
 @pytest.fixture(scope="module")
