@@ -938,25 +938,39 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p31_threads<N>(),
     const int x = blockIdx.x, b = blockIdx.z;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
+    constexpr int HALF = N / 2, TH = mx_p31_threads<N>();
+    static_assert(TH <= HALF && 9 * TH <= padded_len16(4 * N), "first-site V stage fits the output rows");
     const float4* in = Q + ((long)b * 4 + 2 * rank) * vol + (long)x * N;
     for (int i = threadIdx.x; i < 2 * N; i += blockDim.x)
         cp_async<16>(&qb[pad16(i)], &in[(long)(i / N) * vol + (i % N)]);
     cp_async_commit();
-    cp_async_wait<0>();
+    // the old V of this thread's first site, staged in the output rows (unused
+    // until the cluster barrier) while the Q rows transform
+    const int y0 = (int)rank * HALF + threadIdx.x;
+    double2* vstage = reinterpret_cast<double2*>(ob);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) cp_async<16>(&vstage[k * TH + threadIdx.x], &e.V[k * vol + (long)x * N + y0]);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
     fft16_rows<N, 2>(qb, 1.0f, tw);
+    cp_async_wait<0>();
+    double2 vfirst[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) vfirst[k] = vstage[k * TH + threadIdx.x];
+    // the partner writes into this CTA's output rows only after this barrier
     cluster.sync();
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
     int fl = 0;
-    constexpr int HALF = N / 2;
-    for (int y = (int)rank * HALF + threadIdx.x; y < ((int)rank + 1) * HALF; y += blockDim.x) {
+    // one site: the update from get_v's old V, then the next step's noise and rotation
+    auto site_step = [&](int y, auto get_v) {
         const long site = (long)x * N + y;
         float2 v32[9];
         {
             double2 v[9];
-            p3_site_g(e, [&](int j) { return j < 2 ? q_lo[pad16(j * N + y)] : q_hi[pad16((j - 2) * N + y)]; },
-                      site, vol, se, v, fl);
+            p3_site_gv(e, [&](int j) { return j < 2 ? q_lo[pad16(j * N + y)] : q_hi[pad16((j - 2) * N + y)]; },
+                       get_v, se, v, fl);
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
                 e.V[k * vol + site] = v[k];
@@ -984,7 +998,11 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(mx_p31_threads<N>(),
 #pragma unroll
         for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
             rot_rows[pad16(j * N + y)] = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
-    }
+    };
+    site_step(y0, [&](int k) { return vfirst[k]; });
+#pragma unroll 1
+    for (int y = y0 + TH; y < ((int)rank + 1) * HALF; y += TH)
+        site_step(y, [&](int k) { return e.V[k * vol + (long)x * N + y]; });
     if (fl) atomicOr(flags, fl);
     cluster.sync();
     if constexpr (mx_p31_threads<N>() == 2 * (N / 8))  // 4 rows, 2 per round: two rows per thread in one round
@@ -1021,25 +1039,39 @@ __global__ void __cluster_dims__(1, 4, 1) __launch_bounds__(kQuadThreads, 2)
     const int x = blockIdx.x, b = blockIdx.z;
     EventDev& e = ev[slots[b]];
     const long vol = (long)N * N;
+    constexpr int QUARTER = N / 4, TH = kQuadThreads;
+    static_assert(TH <= QUARTER && 9 * TH <= padded_len16(2 * N), "first-site V stage fits the output rows");
     const float4* in = Q + ((long)b * 4 + rank) * vol + (long)x * N;
     for (int i = threadIdx.x; i < N; i += blockDim.x) cp_async<16>(&qb[pad16(i)], &in[i]);
     cp_async_commit();
-    cp_async_wait<0>();
+    // the old V of this thread's first site, staged in the output rows (unused
+    // until the cluster barrier) while the Q row transforms
+    const int y0 = (int)rank * QUARTER + threadIdx.x;
+    double2* vstage = reinterpret_cast<double2*>(ob);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) cp_async<16>(&vstage[k * TH + threadIdx.x], &e.V[k * vol + (long)x * N + y0]);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
     fft16_rows<N, 1>(qb, 1.0f, tw);
+    cp_async_wait<0>();
+    double2 vfirst[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) vfirst[k] = vstage[k * TH + threadIdx.x];
+    // the other ranks write into this CTA's output rows only after this barrier
     cluster.sync();
     const double se = e.sqrt_eps;
     const float* nf = e.nf32;
     int fl = 0;
-    constexpr int QUARTER = N / 4;
     // element y of pair row p (0..7) in its owner's shared memory
     auto orow = [&](int p, int y) -> float4* { return cluster.map_shared_rank(ob, p >> 1) + pad16((p & 1) * N + y); };
-    for (int y = (int)rank * QUARTER + threadIdx.x; y < ((int)rank + 1) * QUARTER; y += blockDim.x) {
+    // one site: the update from get_v's old V, then the next step's noise and rotation
+    auto site_step = [&](int y, auto get_v) {
         const long site = (long)x * N + y;
         float2 v32[9];
         {
             double2 v[9];
-            p3_site_g(e, [&](int j) { return *(cluster.map_shared_rank(qb, j) + pad16(y)); }, site, vol, se, v, fl);
+            p3_site_gv(e, [&](int j) { return *(cluster.map_shared_rank(qb, j) + pad16(y)); }, get_v, se, v, fl);
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
                 e.V[k * vol + site] = v[k];
@@ -1067,7 +1099,11 @@ __global__ void __cluster_dims__(1, 4, 1) __launch_bounds__(kQuadThreads, 2)
 #pragma unroll
         for (int j = 0; j < 4; ++j)  // (BX_j, BY_j)
             *orow(4 + j, y) = make_float4(hx[2 * j], hx[2 * j + 1], hy[2 * j], hy[2 * j + 1]);
-    }
+    };
+    site_step(y0, [&](int k) { return vfirst[k]; });
+#pragma unroll 1
+    for (int y = y0 + TH; y < ((int)rank + 1) * QUARTER; y += TH)
+        site_step(y, [&](int k) { return e.V[k * vol + (long)x * N + y]; });
     if (fl) atomicOr(flags, fl);
     cluster.sync();
     fft16_rows2_store<N>(ob, -1.0f, tw, P + ((long)b * 8 + 2 * rank) * vol + (long)x * N, vol);
