@@ -212,8 +212,13 @@ __device__ __forceinline__ double2 chirp_at(const double2* __restrict__ chirp, i
     return w;
 }
 
-// Rows: ROWS = 4096 / M rows of length N per CTA, each zero-padded to M in
-// shared memory (one resident sequence per row, M / 8 threads on it).
+// Rows: ROWS = 4096 / M rows of length N per CTA, each zero-padded to M
+// (M / 8 threads per row).  Thread t of a row holds elements t + m M/8 (m < 8)
+// in registers: they load from global memory times the chirp, the forward
+// transform starts from and ends in registers (the 16-byte-element core's
+// hand-off), the kernel spectrum multiplies in registers, and the inverse
+// transform ends in registers that are stored times the chirp.  Shared memory
+// carries only the passes in between.
 template <int M>
 __global__ void __launch_bounds__(512) k_chirp_rows(double2* __restrict__ data, long nrows, int N, double sign,
                                                     const double2* __restrict__ chirp,
@@ -222,60 +227,72 @@ __global__ void __launch_bounds__(512) k_chirp_rows(double2* __restrict__ data, 
     constexpr int ROWS = 4096 / M, TPS = M / 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* sm = reinterpret_cast<double2*>(smem_raw);
-    const int tid = threadIdx.x;
-    const long row0 = (long)blockIdx.x * ROWS;
-    const int nr = (int)min((long)ROWS, nrows - row0);
-    double2* g = data + row0 * N;
-    for (int i = tid; i < ROWS * M; i += blockDim.x) {
-        const int r = i / M, e = i % M;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < nr && e < N) v = cmul(g[(long)r * N + e], chirp_at(chirp, e, sign));
-        sm[pad(i)] = v;
+    const int tid = threadIdx.x, r = tid / TPS, t = tid % TPS;
+    const long row = (long)blockIdx.x * ROWS + r;
+    const bool active = row < nrows;
+    double2* g = data + row * N;
+    double2 reg[1][8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int e = t + m * TPS;
+        reg[0][m] = active && e < N ? cmul(g[e], chirp_at(chirp, e, sign)) : make_double2(0.0, 0.0);
     }
-    __syncthreads();
-    const int r = tid / TPS, t = tid % TPS;
-    const bool active = r < nr;
-    fft_smem<double, M>(sm, RowIdx{r * M}, t, active, -1.0, twM);
-    for (int i = tid; i < ROWS * M; i += blockDim.x) sm[pad(i)] = cmul(sm[pad(i)], __ldg(&bhat[i % M]));
-    __syncthreads();
-    fft_smem<double, M>(sm, RowIdx{r * M}, t, active, 1.0, twM);
-    for (int i = tid; i < ROWS * N; i += blockDim.x) {
-        const int rr = i / N, e = i % N;
-        if (rr < nr) g[(long)rr * N + e] = cmul(sm[pad(rr * M + e)], chirp_at(chirp, e, sign));
+    const RowIdx16 idx{r * M};
+    fft16x<double, M, true, true>(sm, idx, t, active, -1.0, twM, reg);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) reg[0][m] = cmul(reg[0][m], __ldg(&bhat[t + m * TPS]));
+    fft16x<double, M, true, true>(sm, idx, t, active, 1.0, twM, reg);
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int e = t + m * TPS;
+            if (e < N) g[e] = cmul(reg[0][m], chirp_at(chirp, e, sign));
+        }
     }
 }
 
 // Columns: a tile of C adjacent columns of one plane (blockIdx.y), each
-// zero-padded to M; the last tile of a row may be narrower.
+// zero-padded to M; the last tile of a row may be narrower.  Thread (c, t)
+// holds elements t + m M/8 of column c in registers, as in the row kernel.
+// Tiles narrower than 8 columns (rows under 128 bytes) are padded by one row
+// every 8 rows in shared memory.
 template <int M> constexpr int chirp_cols_per_cta() { return M >= 512 ? 4096 / M : 8; }
+template <int C>
+struct ChirpColIdx {
+    int c;
+    __device__ __forceinline__ int operator()(int e) const { return e * C + c + (C >= 8 ? 0 : (e >> 3) * C); }
+};
+template <int M, int C> constexpr int chirp_col_len() { return M * C + (C >= 8 ? 0 : (M / 8) * C); }
 
 template <int M, int C>
 __global__ void __launch_bounds__(C * (M / 8)) k_chirp_cols(double2* __restrict__ data, int N, double sign,
                                                             const double2* __restrict__ chirp,
                                                             const double2* __restrict__ bhat,
                                                             const double2* __restrict__ twM, double scale) {
+    constexpr int TPS = M / 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* sm = reinterpret_cast<double2*>(smem_raw);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, cc = tid % C, t = tid / C;
     const int x0 = blockIdx.x * C;
-    const int nc = min(C, N - x0);
-    double2* g = data + (size_t)blockIdx.y * N * N + x0;
-    for (int i = tid; i < M * C; i += blockDim.x) {
-        const int e = i / C, cc = i % C;
-        double2 v = make_double2(0.0, 0.0);
-        if (e < N && cc < nc) v = cmul(g[(size_t)e * N + cc], chirp_at(chirp, e, sign));
-        sm[pad(i)] = v;
+    const bool active = cc < N - x0;
+    double2* g = data + (size_t)blockIdx.y * N * N + x0 + cc;
+    double2 reg[1][8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int e = t + m * TPS;
+        reg[0][m] = active && e < N ? cmul(g[(size_t)e * N], chirp_at(chirp, e, sign)) : make_double2(0.0, 0.0);
     }
-    __syncthreads();
-    const int cc = tid % C, t = tid / C;
-    const bool active = cc < nc;
-    fft_smem<double, M>(sm, ColIdx<C>{cc}, t, active, -1.0, twM);
-    for (int i = tid; i < M * C; i += blockDim.x) sm[pad(i)] = cmul(sm[pad(i)], __ldg(&bhat[i / C]));
-    __syncthreads();
-    fft_smem<double, M>(sm, ColIdx<C>{cc}, t, active, 1.0, twM);
-    for (int i = tid; i < N * C; i += blockDim.x) {
-        const int e = i / C, c2 = i % C;
-        if (c2 < nc) g[(size_t)e * N + c2] = cscale(cmul(sm[pad(i)], chirp_at(chirp, e, sign)), scale);
+    const ChirpColIdx<C> idx{cc};
+    fft16x<double, M, true, true>(sm, idx, t, active, -1.0, twM, reg);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) reg[0][m] = cmul(reg[0][m], __ldg(&bhat[t + m * TPS]));
+    fft16x<double, M, true, true>(sm, idx, t, active, 1.0, twM, reg);
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int e = t + m * TPS;
+            if (e < N) g[(size_t)e * N] = cscale(cmul(reg[0][m], chirp_at(chirp, e, sign)), scale);
+        }
     }
 }
 
@@ -287,8 +304,8 @@ static cudaError_t chirp2d_m(double2* planes, int nplanes, int dir, double scale
     const double2* bhat = tw.bhat + (dir ? 0 : M);
     constexpr int ROWS = 4096 / M;
     constexpr int C = chirp_cols_per_cta<M>();
-    const size_t smr = sizeof(double2) * padded_len(ROWS * M);
-    const size_t smc = sizeof(double2) * padded_len(M * C);
+    const size_t smr = sizeof(double2) * padded_len16(ROWS * M);
+    const size_t smc = sizeof(double2) * chirp_col_len<M, C>();
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_chirp_rows<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr);
