@@ -38,12 +38,14 @@ using namespace jw;
 struct jw_cholesky {
     jw_context* ctx = nullptr;
     long n = 0;                  // N*N
-    double2* d_L = nullptr;      // n*n complex, row-major lower, zero above the diagonal
+    long np = 0;                 // the factor's order: n padded to the blocking (a multiple of 16 up to 128,
+                                 // of 128 above) with an identity block, whose factor is itself
+    double2* d_L = nullptr;      // np*np complex, row-major lower, zero above the diagonal
     int2* d_units = nullptr;     // apply work list: (row strip, column chunk)
     int n_units = 0;
     int n_chunks = 0;
-    double* d_X = nullptr;       // n x kMaxR real right-hand sides, site-major
-    double2* d_P = nullptr;      // n_chunks x n x kMaxR partial products
+    double* d_X = nullptr;       // np x kMaxR real right-hand sides, site-major (rows past n stay zero)
+    double2* d_P = nullptr;      // n_chunks x np x kMaxR partial products
     // d_P holds the correlated noise of step `cached_step` (seed `cached_seed`)
     // as the second half of the last two-step apply; any other use of d_P clears it
     mutable bool cached = false;
@@ -172,13 +174,15 @@ __device__ __forceinline__ double2 cdiv_smith(double2 a, double2 b) {
 }
 
 // S(i, j) = corr(|x_i - x_j|, |y_i - y_j|) on and below the diagonal, zero
-// above (matrix.h:190-196: non-periodic distances).
-__global__ void k_chol_fill(double2* __restrict__ M, const double2* __restrict__ corr, int N, long n) {
-    const long total = n * n;
+// above (matrix.h:190-196: non-periodic distances), for i, j < n; the rows
+// and columns from n to np are those of the identity, so the factor of the
+// padded matrix is the factor of S with an identity block after it.
+__global__ void k_chol_fill(double2* __restrict__ M, const double2* __restrict__ corr, int N, long n, long np) {
+    const long total = np * np;
     for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
-        const long i = idx / n, j = idx - i * n;
-        double2 v = make_double2(0.0, 0.0);
-        if (j <= i) {
+        const long i = idx / np, j = idx - i * np;
+        double2 v = make_double2(i == j ? 1.0 : 0.0, 0.0);
+        if (i < n && j <= i) {
             const int xi = (int)(i / N), yi = (int)(i % N), xj = (int)(j / N), yj = (int)(j % N);
             v = corr[(long)abs(xi - xj) * N + abs(yi - yj)];
         }
@@ -525,16 +529,16 @@ __global__ void k_chol_gather_field(const double2* __restrict__ xi, double* __re
 
 // xi_k = Y_k + i Y_{t+k}, Y = sum of the chunk partials in chunk order.
 template <int t, int RP>
-__global__ void k_chol_finish_field(const double2* __restrict__ P, double2* __restrict__ xi, long n) {
+__global__ void k_chol_finish_field(const double2* __restrict__ P, double2* __restrict__ xi, long n, long np) {
     constexpr int R = 2 * t;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 y[R];
 #pragma unroll
     for (int c = 0; c < R; ++c) y[c] = make_double2(0.0, 0.0);
-    const int nc = chunks_of_row(i, n);
+    const int nc = chunks_of_row(i, np);
     for (int ch = 0; ch < nc; ++ch) {
-        const double2* p = P + ((long)ch * n + i) * RP;
+        const double2* p = P + ((long)ch * np + i) * RP;
 #pragma unroll
         for (int c = 0; c < R; ++c) y[c] = cadd(y[c], p[c]);
     }
@@ -565,15 +569,15 @@ __global__ void k_chol_noise_X(double* __restrict__ X, long n, uint64_t seed, ui
 // with the (linear) embedding applied after L.
 // P holds rp right-hand sides per site; this step's 16 start at column off.
 __global__ void k_chol_finish_noise(const double2* __restrict__ P, double2* __restrict__ xx, double2* __restrict__ xy,
-                                    long n, int rp, int off) {
+                                    long n, long np, int rp, int off) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 y[16];
 #pragma unroll
     for (int c = 0; c < 16; ++c) y[c] = make_double2(0.0, 0.0);
-    const int nc = chunks_of_row(i, n);
+    const int nc = chunks_of_row(i, np);
     for (int ch = 0; ch < nc; ++ch) {
-        const double2* p = P + ((long)ch * n + i) * rp + off;
+        const double2* p = P + ((long)ch * np + i) * rp + off;
 #pragma unroll
         for (int c = 0; c < 16; ++c) y[c] = cadd(y[c], p[c]);
     }
@@ -654,7 +658,7 @@ jw_status launch_apply(const jw_cholesky* L, cudaStream_t s) {
     constexpr int smem = kStages * apply_stage_bytes<NT>();
     JW_CUDA(cudaFuncSetAttribute(k_chol_apply<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = apply_grid((const void*)k_chol_apply<NT>, smem, L->n_units);
-    k_chol_apply<NT><<<grid, kTR, smem, s>>>(L->d_L, L->d_X, L->d_P, L->d_units, L->n_units, L->n);
+    k_chol_apply<NT><<<grid, kTR, smem, s>>>(L->d_L, L->d_X, L->d_P, L->d_units, L->n_units, L->np);
     JW_CUDA(cudaGetLastError());
     return JW_OK;
 }
@@ -680,7 +684,7 @@ jw_status cholesky_noise_apply(jw_context* c, const jw_cholesky* L, uint64_t ste
 jw_status cholesky_noise_finish(jw_context* c, const jw_cholesky* L, jw_field* xx, jw_field* xy, int nsteps,
                                 int which) {
     const long n = L->n;
-    k_chol_finish_noise<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xx->d, xy->d, n, 16 * nsteps,
+    k_chol_finish_noise<<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xx->d, xy->d, n, L->np, 16 * nsteps,
                                                                    16 * which);
     JW_CUDA(cudaGetLastError());
     return JW_OK;
@@ -756,14 +760,17 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     *out = nullptr;
     const int N = c->N;
     const long n = (long)N * N;
-    const size_t bytesL = sizeof(double2) * (size_t)n * n;
-    int n_chunks = (int)((n + kTC - 1) / kTC);
-    const size_t bytesX = sizeof(double) * (size_t)n * kMaxR;
-    const size_t bytesP = sizeof(double2) * (size_t)n_chunks * n * kMaxR;
+    // the blocked factorisation and the apply tiles take orders that are
+    // multiples of the diagonal block (above one block) and of the apply's
+    // 16-column stage (up to one block); other orders are padded
+    const long np = n <= kDiagBlock ? (n + kKT - 1) / kKT * kKT : (n + kDiagBlock - 1) / kDiagBlock * kDiagBlock;
+    const size_t bytesL = sizeof(double2) * (size_t)np * np;
+    int n_chunks = (int)((np + kTC - 1) / kTC);
+    const size_t bytesX = sizeof(double) * (size_t)np * kMaxR;
+    const size_t bytesP = sizeof(double2) * (size_t)n_chunks * np * kMaxR;
     size_t free_b = 0, total_b = 0;
     JW_CUDA(cudaMemGetInfo(&free_b, &total_b));
     if (bytesL + bytesX + bytesP + ((size_t)1 << 30) > free_b) return JW_ENOMEM;
-    if (n > kDiagBlock && n % kDiagBlock != 0) return JW_EUNSUPPORTED;  // N^2 for power-of-two N >= 16 always divides
     static bool configured = false;
     if (!configured) {
         JW_CUDA(cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem_bytes()));
@@ -777,6 +784,7 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     jw_cholesky* L = new jw_cholesky();
     L->ctx = c;
     L->n = n;
+    L->np = np;
     L->n_chunks = n_chunks;
     if (cudaMalloc(&L->d_L, bytesL) != cudaSuccess || cudaMalloc(&L->d_X, bytesX) != cudaSuccess ||
         cudaMalloc(&L->d_P, bytesP) != cudaSuccess) {
@@ -785,12 +793,12 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     }
     // apply work list, longest units first
     std::vector<int2> units;
-    const long strips = (n + kTR - 1) / kTR;
+    const long strips = (np + kTR - 1) / kTR;
     for (long s = 0; s < strips; ++s) {
-        const long last = std::min(n, (s + 1) * kTR) - 1;
+        const long last = std::min(np, (s + 1) * kTR) - 1;
         for (long ch = 0; ch <= last / kTC; ++ch) units.push_back(make_int2((int)s, (int)ch));
     }
-    auto work = [&](int2 u) { return std::min((long)(u.y + 1) * kTC, std::min(n, (long)(u.x + 1) * kTR)) - (long)u.y * kTC; };
+    auto work = [&](int2 u) { return std::min((long)(u.y + 1) * kTC, std::min(np, (long)(u.x + 1) * kTR)) - (long)u.y * kTC; };
     std::stable_sort(units.begin(), units.end(), [&](int2 a, int2 b) { return work(a) > work(b); });
     L->n_units = (int)units.size();
     if (cudaMalloc(&L->d_units, sizeof(int2) * units.size()) != cudaSuccess) {
@@ -805,24 +813,26 @@ JW_EXPORT jw_status jw_cholesky_decompose(jw_context* c, const jw_field* corr, j
     if (cudaMemcpyAsync(L->d_units, units.data(), sizeof(int2) * units.size(), cudaMemcpyHostToDevice, c->stream) !=
         cudaSuccess)
         return fail(JW_ECUDA);
-    k_chol_fill<<<148 * 16, kThreads, 0, c->stream>>>(L->d_L, corr->d, N, n);
+    // the right-hand-side rows past n stay zero: the noise and field kernels write rows < n only
+    if (cudaMemsetAsync(L->d_X, 0, bytesX, c->stream) != cudaSuccess) return fail(JW_ECUDA);
+    k_chol_fill<<<148 * 16, kThreads, 0, c->stream>>>(L->d_L, corr->d, N, n, np);
     if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
     // right-looking blocked factorisation, b = 128: factor the diagonal block,
     // solve the panel below it, update the trailing lower triangle
-    for (long k0 = 0; k0 < n; k0 += kDiagBlock) {
-        const long b = std::min((long)kDiagBlock, n - k0);
-        double2* Akk = L->d_L + k0 * n + k0;
-        k_chol_diag<<<1, 1024, diag_smem_bytes(), c->stream>>>(Akk, n, (int)b);
+    for (long k0 = 0; k0 < np; k0 += kDiagBlock) {
+        const long b = std::min((long)kDiagBlock, np - k0);
+        double2* Akk = L->d_L + k0 * np + k0;
+        k_chol_diag<<<1, 1024, diag_smem_bytes(), c->stream>>>(Akk, np, (int)b);
         if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
-        const long rest = n - k0 - b;
+        const long rest = np - k0 - b;
         if (rest == 0) break;
         const long warps = kTrsmThreads / 32;
         k_chol_trsm<<<(unsigned)std::min((rest + warps - 1) / warps, (long)sms), kTrsmThreads, trsm_smem_bytes(),
-                      c->stream>>>(L->d_L, n, k0, rest);
+                      c->stream>>>(L->d_L, np, k0, rest);
         const int nt = (int)(rest / kSyT);
         const long ntiles = (long)nt * (nt + 1) / 2;
         k_chol_syrk<<<(unsigned)std::min(ntiles, 2L * sms), kSyThreads, syrk_smem_bytes(), c->stream>>>(
-            L->d_L, n, k0, k0 + b, nt);
+            L->d_L, np, k0, k0 + b, nt);
         if (cudaGetLastError() != cudaSuccess) return fail(JW_ECUDA);
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(JW_ECUDA);
@@ -843,7 +853,9 @@ JW_EXPORT jw_status jw_cholesky_destroy(jw_cholesky* L) {
 JW_EXPORT jw_status jw_cholesky_get(const jw_cholesky* L, double* host) {
     JW_CHECK(L && host);
     JW_CUDA(cudaStreamSynchronize(L->ctx->stream));
-    JW_CUDA(cudaMemcpy(host, L->d_L, sizeof(double2) * (size_t)L->n * L->n, cudaMemcpyDeviceToHost));
+    // the n x n factor of S: the top-left block of the padded factor
+    JW_CUDA(cudaMemcpy2D(host, sizeof(double2) * (size_t)L->n, L->d_L, sizeof(double2) * (size_t)L->np,
+                         sizeof(double2) * (size_t)L->n, (size_t)L->n, cudaMemcpyDeviceToHost));
     return JW_OK;
 }
 
@@ -858,11 +870,11 @@ JW_EXPORT jw_status jw_multiply_by_cholesky(jw_context* c, jw_field* xi, const j
     if (xi->t == 9) {
         s = launch_apply<3>(L, c->stream);
         if (s) return s;
-        k_chol_finish_field<9, 24><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
+        k_chol_finish_field<9, 24><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n, L->np);
     } else {
         s = launch_apply<1>(L, c->stream);
         if (s) return s;
-        k_chol_finish_field<1, 8><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n);
+        k_chol_finish_field<1, 8><<<blocks_for(n), kThreads, 0, c->stream>>>(L->d_P, xi->d, n, L->np);
     }
     JW_CUDA(cudaGetLastError());
     return JW_OK;

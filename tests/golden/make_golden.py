@@ -238,6 +238,11 @@ def main(only: list[str]) -> None:
                                       steps=3, slices=6),
         "position_sqrt_sin_N15": dict(N=15, seed=25, coupling="SQRT_COUPLING_CONSTANT", kernel="SIN_KERNEL", steps=3,
                                       slices=6),
+        # Cholesky-correlated noise where N^2 is not a multiple of the factor's blocking
+        "position_cholesky_N10": dict(N=10, seed=26, coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL", steps=3,
+                                      slices=6),
+        "position_cholesky_N12": dict(N=12, seed=27, coupling="NOISE_COUPLING_CONSTANT", kernel="SIN_KERNEL", steps=3,
+                                      slices=6),
     }
     for name, kw in pos.items():
         if not wanted(name):

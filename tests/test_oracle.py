@@ -52,7 +52,8 @@ def test_oracle_matches_golden_functions(oracle, gold, name):
 
 
 @pytest.mark.parametrize("name", ["position_sqrt_sin_N16", "position_sqrt_linear_N8", "position_cholesky_N8",
-                                  "position_cholesky_N16", "position_sqrt_sin_N15"])
+                                  "position_cholesky_N16", "position_sqrt_sin_N15", "position_cholesky_N10",
+                                  "position_cholesky_N12"])
 def test_oracle_matches_golden_position(oracle, gold, name):
     """Position-space evolution (main_optimized.cpp:271-304) with Cholesky-
     correlated noise for NOISE coupling (main_optimized.cpp:145-157)."""

@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 COUPLING = {"SQRT_COUPLING_CONSTANT": 0, "NOISE_COUPLING_CONSTANT": 1}
 HATTA = 2
 POSITION_FIXTURES = ["position_sqrt_sin_N16", "position_sqrt_linear_N8", "position_cholesky_N8",
-                     "position_cholesky_N16", "position_sqrt_sin_N15"]
+                     "position_cholesky_N16", "position_sqrt_sin_N15", "position_cholesky_N10",
+                     "position_cholesky_N12"]
 
 
 @pytest.fixture(scope="module")
@@ -124,10 +125,11 @@ def test_hatta_matches_oracle(jw, oracle, N, kernel, rr):
     assert np.abs(V.get() - V1).max() <= 1e-12
 
 
-@pytest.mark.parametrize("N", [32, 64])
+@pytest.mark.parametrize("N", [32, 64, 10, 12, 24])
 def test_cholesky_factor_reproduces_correlation(jw, N):
     """L L^T = S over several 128-row diagonal blocks, and L xi against numpy
-    for a 9-component and a 1-component field."""
+    for a 9-component and a 1-component field.  At 10^2, 12^2 and 24^2 the
+    order N^2 is padded to the blocking (112, 256, 640) with an identity block."""
     ctx = ctx_for(jw, N, 3, 0.0004, 1, 1)
     corr = ctx.field(1)
     ctx.set_correlations_for_coupling_constant(corr)
@@ -149,7 +151,7 @@ def test_cholesky_factor_reproduces_correlation(jw, N):
     assert ctx.sync() == jw.OK
 
 
-@pytest.mark.parametrize("N", [16, 32])
+@pytest.mark.parametrize("N", [16, 32, 12, 24])
 def test_cholesky_matches_oracle(jw, oracle, N):
     """The blocked factorisation (diagonal blocks, panel solves, tensor-core
     trailing updates: one panel at 16^2, eight at 32^2) against the oracle's
