@@ -684,12 +684,10 @@ __device__ __forceinline__ void p3_site_gv(const EventDev& e, GetU get_u, GetV g
     double2 v0[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) v0[k] = get_v(k);
-    double a[8], bq[8];
+    double bq[8];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const float4 u = get_u(j);
-        a[2 * j] = __dmul_rn((double)u.x, se);
-        a[2 * j + 1] = __dmul_rn((double)u.y, se);
         bq[2 * j] = __dmul_rn((double)u.z, -se);
         bq[2 * j + 1] = __dmul_rn((double)u.w, -se);
     }
@@ -698,6 +696,15 @@ __device__ __forceinline__ void p3_site_gv(const EventDev& e, GetU get_u, GetV g
     embed_lambda_x(bq, m);
     xr::expi_ch(m, -1.0);  // exp(+i sqrt(eps) B)
     xr::mul3(m, v0, tmp);
+    // A's coefficients are read again here rather than held through the first
+    // exponential (fewer live registers there)
+    double a[8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float4 u = get_u(j);
+        a[2 * j] = __dmul_rn((double)u.x, se);
+        a[2 * j + 1] = __dmul_rn((double)u.y, se);
+    }
     embed_lambda_x(a, m);
     xr::expi_ch(m, -1.0);  // exp(-i sqrt(eps) A)
     xr::mul3(tmp, m, v);
