@@ -153,9 +153,12 @@ def test_driver_matches_reference_main(gold, tmp_path, name, mode):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["batched", "batched-mixed", "call-for-call"])
-def test_driver_hatta_matches_oracle(oracle, tmp_path, mode):
-    N, seed = 8, 5
+@pytest.mark.parametrize("mode,N", [("batched", 8), ("batched-mixed", 8), ("call-for-call", 8), ("batched", 6)])
+def test_driver_hatta_matches_oracle(oracle, tmp_path, mode, N):
+    """The Hatta branches as engine events (batched), or one after another:
+    with --call-for-call, and at a size that is not a power of two (6), which
+    the engine does not take, whatever the mode."""
+    seed = 5
     cfg = tmp_path / "config"
     cfg.write_text(HATTA_CONFIG)
     args = [DRIVER, "1", "1", str(cfg), "--N", str(N), "--seed", str(seed)]
