@@ -31,7 +31,9 @@
  *    (JW_ENOCONV when the QL eigensolver did not converge at some site,
  *    JW_ENAN for a non-finite result).
  *  - A context or engine may be used from one host thread at a time.
- *  - Lattice sides are powers of two from 8 to 2048 (Nx == Ny).
+ *  - Lattices are square (Nx == Ny).  A context (the call-for-call and
+ *    position layers) takes any side from 2 to 2048; the batched engine and
+ *    the server take powers of two from 8 to 2048.
  */
 #ifndef JIMWLK_H
 #define JIMWLK_H
